@@ -1,0 +1,87 @@
+"""ctypes binding of libobvh_b200.so (the C ABI declared in include/*.h).
+
+The library is the only compute path: if it cannot be found or built, every
+entry point raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import threading
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "libobvh_b200.so")
+INCLUDE = os.path.join(ROOT, "include")
+
+_lock = threading.Lock()
+_lib = None
+
+
+class ObvhError(RuntimeError):
+    """A non-NULL kr_error returned by the native library."""
+
+
+class Obb3(ctypes.Structure):
+    _fields_ = [("v", ctypes.c_float * 15)]
+
+
+def _declare(lib: ctypes.CDLL) -> None:
+    c = ctypes
+    vp = c.c_void_p
+    err = c.c_void_p  # kr_error: NULL or a static C string
+    sig = {
+        "obvh_version": (c.c_char_p, []),
+        "obvh_last_error": (err, []),
+        "kr_cuda_points_obb": (Obb3, [vp, c.c_uint64, c.POINTER(c.c_float)]),
+        "obvh_points_obb": (err, [vp, c.c_uint64, c.c_uint32, vp, c.POINTER(c.c_float)]),
+        "obvh_dito_workspace_bytes": (c.c_uint64, []),
+        "obvh_dito_workspace_init": (err, [vp, vp]),
+        "obvh_dito_fit_async": (err, [vp, c.c_uint64, c.c_uint32, vp, vp, vp]),
+        "obvh_dito_fit_pass_async": (err, [vp, c.c_uint64, c.c_uint32, vp, vp, vp, c.c_int]),
+        "obvh_dito_workspace_report": (err, [vp, vp, c.POINTER(c.c_uint32), c.POINTER(c.c_float),
+                                             c.POINTER(c.c_uint32)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+
+
+def declared_symbols() -> list[str]:
+    """Every OBVH_EXPORT function named in include/*.h."""
+    names = []
+    pat = re.compile(r"OBVH_EXPORT\s+[\w\s\*]+?\b(\w+)\s*\(")
+    for f in sorted(os.listdir(INCLUDE)):
+        if f.endswith(".h"):
+            with open(os.path.join(INCLUDE, f)) as fh:
+                names += pat.findall(fh.read())
+    return names
+
+
+def lib(build_if_missing: bool = True) -> ctypes.CDLL:
+    """Loads the native library (building it from csrc/ if it is out of date)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if build_if_missing:
+            from . import build as _build
+            try:
+                _build.build_core()
+            except Exception as e:  # pragma: no cover - no toolchain and no prebuilt library
+                if not os.path.exists(LIB_PATH):
+                    raise ObvhError(f"libobvh_b200.so is missing and could not be built: {e}") from e
+        if not os.path.exists(LIB_PATH):
+            raise ObvhError(f"native library not found: {LIB_PATH}")
+        l = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+        _declare(l)
+        _lib = l
+        return l
+
+
+def check(e) -> None:
+    """Raises ObvhError for a non-NULL kr_error."""
+    if e:
+        raise ObvhError(ctypes.string_at(e).decode(errors="replace"))

@@ -1,0 +1,580 @@
+// dito.cu - DiTO-14 OBB fit of one point set: two streaming passes over HBM.
+//
+// Pass 1 (dito_extremal_pass): every point is projected on the 7 fixed slab
+//   directions x, y, z, x+y+z, x+y-z, x-y+z, x-y-z and the first point
+//   reaching each min/max is kept -- the reference's
+//   findExtremalPoints_7FixedDirs (src/common/algorithm/dito/dito.cpp:105-191).
+//   The reference GPU needs two full passes and one float CAS per block and
+//   value for this (dito.cu:76-231); here the index rides along with the value
+//   and a CTA writes one (value, index) record per direction.  The last CTA to
+//   finish reduces the records and runs the candidate-axis search
+//   (dito.cpp:280-418) with one warp: the up to 21 candidate frames are scored
+//   by 21 lanes at once.
+// Pass 2 (dito_extent_pass): projections on the chosen axes b0, b1, b2
+//   (computeObbDimensions, dito.cpp:420-426); the last CTA applies the final
+//   OBB-vs-AABB test and the kr_points_obb clamp (geometry.cpp:232-252).
+//
+// Data movement: the point stream is cut into 24 KB tiles that the TMA engine
+// copies into a 4-stage shared-memory ring (cp.async.bulk, no tensor map,
+// no multicast), so every byte crosses HBM once per pass with coalesced 16-byte
+// transactions; threads then read whole 4-point groups (3 x 16 B) from shared
+// memory without bank conflicts.  Pass 2 walks each CTA's slice backwards so
+// that the tail of pass 1, still in the 126 MB L2, is consumed first.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+
+#include "device_common.cuh"
+#include "dito_device.cuh"
+#include "obvh_api.h"
+#include "obvh_dito.h"
+#include "runtime.h"
+
+namespace obvh {
+namespace dito {
+
+// ---------------------------------------------------------------------------
+// Workspace layout (device): Ctl (dito_device.cuh), an output slot used by the
+// host-pointer entry points, then the per-CTA records of both passes.
+
+constexpr int kMaxGrid = 1024;
+constexpr size_t kOffObb = 256;                                   // host-API output slot
+constexpr size_t kOffRec1Val = 512;                               // [kMaxGrid][14] float
+constexpr size_t kOffRec1Idx = kOffRec1Val + kMaxGrid * 14 * 4;   // [kMaxGrid][14] u64
+constexpr size_t kOffRec2 = kOffRec1Idx + kMaxGrid * 14 * 8;      // [kMaxGrid][6] float
+constexpr size_t kWorkspaceBytes = kOffRec2 + kMaxGrid * 6 * 4;
+
+// ---------------------------------------------------------------------------
+// Launch geometry.
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kTileGroups = 512;              // 4-point groups per tile
+constexpr int kTileBytes = kTileGroups * 48;  // 24 KB
+constexpr int kStages = 4;
+constexpr int kSmemBytes = kStages * kTileBytes;
+
+// The point array is split into an unaligned head (< 4 points), a body of
+// 16-byte-aligned 4-point groups, and a tail (< 4 points).  Head and tail are
+// read directly by CTA 0.
+struct Split {
+    const float* xyz;     // all points, packed
+    uint64_t n;
+    uint64_t head;        // points before the aligned body
+    uint64_t groups;      // 4-point groups in the body
+    uint64_t ntiles;
+};
+
+__host__ __device__ inline Split make_split(const float* xyz, uint64_t n) {
+    Split s;
+    s.xyz = xyz;
+    s.n = n;
+    uint64_t mis = (reinterpret_cast<uintptr_t>(xyz) & 15u) / 4u;  // misalignment in floats: 0..3
+    // head h with (mis + 3h) % 4 == 0
+    uint64_t h = 0;
+    while ((mis + 3 * h) % 4 != 0) ++h;
+    if (h > n) h = n;
+    s.head = h;
+    s.groups = (n - h) / 4;
+    s.ntiles = (s.groups + kTileGroups - 1) / kTileGroups;
+    return s;
+}
+
+__device__ __forceinline__ void slab7(float x, float y, float z, float s[7]) {
+    s[0] = x;
+    s[1] = y;
+    s[2] = z;
+    float a = x + y, b = x - y;
+    s[3] = a + z;
+    s[4] = a - z;
+    s[5] = b + z;
+    s[6] = b - z;
+}
+
+// Per-thread running extremes with the index of the first point reaching them.
+struct Extremes {
+    float mn[7], mx[7];
+    uint64_t imn[7], imx[7];
+    __device__ void init() {
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            mn[k] = kInf;  // +inf
+            mx[k] = -kInf;
+            imn[k] = ~0ull;
+            imx[k] = ~0ull;
+        }
+    }
+    __device__ __forceinline__ void point(float x, float y, float z, uint64_t i) {
+        float s[7];
+        slab7(x, y, z, s);
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            if (better_min(s[k], i, mn[k], imn[k])) { mn[k] = s[k]; imn[k] = i; }
+            if (better_max(s[k], i, mx[k], imx[k])) { mx[k] = s[k]; imx[k] = i; }
+        }
+    }
+    // 4 consecutive points with indices base..base+3, all larger than any seen so far.
+    __device__ __forceinline__ void group(const float4& a, const float4& b, const float4& c, uint64_t base) {
+        float s0[7], s1[7], s2[7], s3[7];
+        slab7(a.x, a.y, a.z, s0);
+        slab7(a.w, b.x, b.y, s1);
+        slab7(b.z, b.w, c.x, s2);
+        slab7(c.y, c.z, c.w, s3);
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            float gm = fminf(fminf(s0[k], s1[k]), fminf(s2[k], s3[k]));
+            if (gm < mn[k]) {  // rare after the first few groups
+                mn[k] = gm;
+                imn[k] = base + (s0[k] == gm ? 0 : s1[k] == gm ? 1 : s2[k] == gm ? 2 : 3);
+            }
+            float gx = fmaxf(fmaxf(s0[k], s1[k]), fmaxf(s2[k], s3[k]));
+            if (gx > mx[k]) {
+                mx[k] = gx;
+                imx[k] = base + (s0[k] == gx ? 0 : s1[k] == gx ? 1 : s2[k] == gx ? 2 : 3);
+            }
+        }
+    }
+};
+
+// Extents along three axes (no index needed: only the values are used).
+struct Extents {
+    f3 b0, b1, b2;
+    float lo[3], hi[3];
+    __device__ void init(const float* axes) {
+        b0 = mk3(axes[0], axes[1], axes[2]);
+        b1 = mk3(axes[3], axes[4], axes[5]);
+        b2 = mk3(axes[6], axes[7], axes[8]);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { lo[k] = kInf; hi[k] = -kInf; }
+    }
+    __device__ __forceinline__ void point(float x, float y, float z) {
+        f3 p = mk3(x, y, z);
+        float q0 = dot3(p, b0), q1 = dot3(p, b1), q2 = dot3(p, b2);
+        lo[0] = fminf(lo[0], q0); hi[0] = fmaxf(hi[0], q0);
+        lo[1] = fminf(lo[1], q1); hi[1] = fmaxf(hi[1], q1);
+        lo[2] = fminf(lo[2], q2); hi[2] = fmaxf(hi[2], q2);
+    }
+    __device__ __forceinline__ void group(const float4& a, const float4& b, const float4& c) {
+        point(a.x, a.y, a.z);
+        point(a.w, b.x, b.y);
+        point(b.z, b.w, c.x);
+        point(c.y, c.z, c.w);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Tile pipeline: the CTA consumes tiles [t_begin, t_end) of the body (in
+// reverse when `reverse`), calling fn(groups, group_base, smem_tile) per tile.
+// Returns false if a wait timed out (the whole CTA agrees).
+template <class Fn>
+__device__ bool tile_pipeline(const Split& sp, uint64_t t_begin, uint64_t t_end, bool reverse,
+                              float4* ring, uint64_t* full, uint32_t* err, Fn&& fn) {
+    const int tid = threadIdx.x;
+    const uint64_t count = t_end - t_begin;
+    const char* body = reinterpret_cast<const char*>(sp.xyz + 3 * sp.head);
+    auto tile_of = [&](uint64_t it) { return reverse ? (t_end - 1 - it) : (t_begin + it); };
+    auto groups_of = [&](uint64_t t) -> uint32_t {
+        uint64_t g0 = t * kTileGroups;
+        uint64_t g = sp.groups - g0;
+        return static_cast<uint32_t>(g < kTileGroups ? g : kTileGroups);
+    };
+    auto issue = [&](uint64_t it, int s) {
+        uint64_t t = tile_of(it);
+        uint32_t bytes = groups_of(t) * 48u;
+        mbar_expect_tx(&full[s], bytes);
+        bulk_g2s(ring + s * (kTileBytes / 16), body + t * static_cast<uint64_t>(kTileBytes), bytes, &full[s]);
+    };
+    if (tid == 0) {
+        for (int s = 0; s < kStages && s < static_cast<int>(count); ++s) issue(s, s);
+    }
+    bool ok = true;
+    uint64_t it = 0;
+    for (; it < count; ++it) {
+        const int s = static_cast<int>(it % kStages);
+        const uint32_t parity = static_cast<uint32_t>((it / kStages) & 1u);
+        bool mine = mbar_wait_bounded(&full[s], parity, err);
+        if (mine) {
+            uint64_t t = tile_of(it);
+            fn(groups_of(t), t * kTileGroups, ring + s * (kTileBytes / 16));
+        }
+        if (__syncthreads_or(!mine)) { ok = false; break; }
+        if (tid == 0 && it + kStages < count) {
+            fence_proxy_async_smem();
+            issue(it + kStages, s);
+        }
+    }
+    if (!ok && tid == 0) {
+        // Let the copies still in flight land before the CTA's shared memory is released.
+        for (uint64_t j = it + 1; j < count && j < it + kStages; ++j)
+            mbar_wait_bounded(&full[j % kStages], static_cast<uint32_t>((j / kStages) & 1u), err);
+    }
+    return ok;
+}
+
+__device__ __forceinline__ void cta_tiles(uint64_t ntiles, uint64_t& b, uint64_t& e) {
+    b = ntiles * blockIdx.x / gridDim.x;
+    e = ntiles * (blockIdx.x + 1) / gridDim.x;
+}
+
+// Points outside the aligned body, given to the first threads of CTA 0: the
+// head (indices below the body, handled before the tiles) and the tail
+// (indices above it, handled after), which keeps each thread's points in
+// increasing index order as the first-index tie rule needs.
+__device__ __forceinline__ bool head_point(const Split& sp, uint64_t& idx) {
+    if (blockIdx.x != 0 || threadIdx.x >= sp.head) return false;
+    idx = threadIdx.x;
+    return true;
+}
+__device__ __forceinline__ bool tail_point(const Split& sp, uint64_t& idx) {
+    const uint64_t tail0 = sp.head + 4 * sp.groups;
+    if (blockIdx.x != 0 || threadIdx.x >= sp.n - tail0) return false;
+    idx = tail0 + threadIdx.x;
+    return true;
+}
+
+// Signals this CTA's completion; true in exactly one CTA, the last one.
+__device__ bool last_cta(uint32_t* ticket) {
+    __shared__ uint32_t s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1) ? 1u : 0u;
+    __syncthreads();
+    if (s_last) __threadfence();
+    return s_last != 0;
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 2)
+    dito_extremal_pass(Split sp, char* ws, kr_obb3* out, uint32_t flags) {
+    extern __shared__ __align__(128) float4 ring[];
+    __shared__ uint64_t full[kStages];
+    __shared__ float s_val[kWarps][14];
+    __shared__ uint64_t s_idx[kWarps][14];
+
+    Ctl* ctl = reinterpret_cast<Ctl*>(ws);
+    float* rec_val = reinterpret_cast<float*>(ws + kOffRec1Val);
+    uint64_t* rec_idx = reinterpret_cast<uint64_t*>(ws + kOffRec1Idx);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    Extremes ex;
+    ex.init();
+    uint64_t xi;
+    if (head_point(sp, xi)) ex.point(sp.xyz[3 * xi], sp.xyz[3 * xi + 1], sp.xyz[3 * xi + 2], xi);
+
+    uint64_t tb, te;
+    cta_tiles(sp.ntiles, tb, te);
+    tile_pipeline(sp, tb, te, false, ring, full, &ctl->error,
+                  [&](uint32_t groups, uint64_t g0, const float4* tile) {
+                      for (uint32_t g = tid; g < groups; g += kThreads) {
+                          float4 a = tile[3 * g], b = tile[3 * g + 1], c = tile[3 * g + 2];
+                          ex.group(a, b, c, sp.head + 4 * (g0 + g));
+                      }
+                  });
+    if (tail_point(sp, xi)) ex.point(sp.xyz[3 * xi], sp.xyz[3 * xi + 1], sp.xyz[3 * xi + 2], xi);
+
+    // CTA reduction -> one record of 7 (min, argmin) + 7 (max, argmax).
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        warp_argmin(ex.mn[k], ex.imn[k]);
+        warp_argmax(ex.mx[k], ex.imx[k]);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            s_val[warp][k] = ex.mn[k];
+            s_idx[warp][k] = ex.imn[k];
+            s_val[warp][7 + k] = ex.mx[k];
+            s_idx[warp][7 + k] = ex.imx[k];
+        }
+    }
+    __syncthreads();
+    if (tid < 14) {
+        float v = s_val[0][tid];
+        uint64_t i = s_idx[0][tid];
+        for (int w = 1; w < kWarps; ++w) {
+            float ov = s_val[w][tid];
+            uint64_t oi = s_idx[w][tid];
+            bool b = tid < 7 ? better_min(ov, oi, v, i) : better_max(ov, oi, v, i);
+            if (b) { v = ov; i = oi; }
+        }
+        rec_val[blockIdx.x * 14 + tid] = v;
+        rec_idx[blockIdx.x * 14 + tid] = i;
+    }
+    if (!last_cta(&ctl->ticket[0])) return;
+
+    // ---- last CTA: global extremes, then the candidate search -------------
+    __shared__ float g_val[14];
+    __shared__ uint64_t g_idx[14];
+    for (int e = warp; e < 14; e += kWarps) {
+        float v = e < 7 ? kInf : -kInf;
+        uint64_t i = ~0ull;
+        for (int r = lane; r < static_cast<int>(gridDim.x); r += 32) {
+            float ov = __ldcg(rec_val + r * 14 + e);
+            uint64_t oi = __ldcg(reinterpret_cast<const unsigned long long*>(rec_idx) + r * 14 + e);
+            bool b = e < 7 ? better_min(ov, oi, v, i) : better_max(ov, oi, v, i);
+            if (b) { v = ov; i = oi; }
+        }
+        if (e < 7) warp_argmin(v, i); else warp_argmax(v, i);
+        if (lane == 0) { g_val[e] = v; g_idx[e] = i; }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        CandidateInput in;
+        in.n = sp.n;
+        for (int k = 0; k < 14; ++k) in.val[k] = g_val[k];
+        if (sp.n > 0) {
+            for (int k = 0; k < 14; ++k) {
+                uint64_t i = g_idx[k];
+                if (i >= sp.n) {  // only when no finite projection exists (non-finite input)
+                    if (lane == 0) atomicOr(&ctl->error, kErrBadInput);
+                    i = 0;
+                }
+                const float* p = sp.xyz + 3 * i;
+                in.sel[k] = mk3(p[0], p[1], p[2]);
+            }
+        }
+        candidate_warp(in, sp.xyz, flags, ctl, out);
+    }
+    if (tid == 0) ctl->ticket[0] = 0;
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+    dito_extent_pass(Split sp, char* ws, kr_obb3* out, uint32_t flags) {
+    extern __shared__ __align__(128) float4 ring[];
+    __shared__ uint64_t full[kStages];
+    __shared__ float s_lohi[kWarps][6];
+
+    Ctl* ctl = reinterpret_cast<Ctl*>(ws);
+    if (ctl->plan == 0) return;  // box already final (uniform across the grid)
+    float* rec = reinterpret_cast<float*>(ws + kOffRec2);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    Extents ex;
+    ex.init(ctl->axes);
+    uint64_t xi;
+    if (head_point(sp, xi) || tail_point(sp, xi)) ex.point(sp.xyz[3 * xi], sp.xyz[3 * xi + 1], sp.xyz[3 * xi + 2]);
+
+    uint64_t tb, te;
+    cta_tiles(sp.ntiles, tb, te);
+    tile_pipeline(sp, tb, te, true, ring, full, &ctl->error,
+                  [&](uint32_t groups, uint64_t, const float4* tile) {
+                      for (uint32_t g = tid; g < groups; g += kThreads)
+                          ex.group(tile[3 * g], tile[3 * g + 1], tile[3 * g + 2]);
+                  });
+
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        ex.lo[k] = warp_min(ex.lo[k]);
+        ex.hi[k] = warp_max(ex.hi[k]);
+    }
+    if (lane == 0) {
+        for (int k = 0; k < 3; ++k) { s_lohi[warp][k] = ex.lo[k]; s_lohi[warp][3 + k] = ex.hi[k]; }
+    }
+    __syncthreads();
+    if (tid < 6) {
+        float v = s_lohi[0][tid];
+        for (int w = 1; w < kWarps; ++w) v = tid < 3 ? fminf(v, s_lohi[w][tid]) : fmaxf(v, s_lohi[w][tid]);
+        rec[blockIdx.x * 6 + tid] = v;
+    }
+    if (!last_cta(&ctl->ticket[1])) return;
+
+    __shared__ float g_lohi[6];
+    if (warp == 0) {
+        for (int e = 0; e < 6; ++e) {
+            float v = e < 3 ? kInf : -kInf;
+            for (int r = lane; r < static_cast<int>(gridDim.x); r += 32) {
+                float o = __ldcg(rec + r * 6 + e);
+                v = e < 3 ? fminf(v, o) : fmaxf(v, o);
+            }
+            v = e < 3 ? warp_min(v) : warp_max(v);
+            if (lane == 0) g_lohi[e] = v;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        finalize_extents(ctl, g_lohi, flags, out);
+        ctl->ticket[1] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+int grid_for(const Split& sp) {
+    const DeviceInfo& info = device_info();
+    uint64_t g = 2ull * info.sm_count;
+    if (g > kMaxGrid) g = kMaxGrid;
+    if (sp.ntiles < g) g = sp.ntiles;
+    if (g < 1) g = 1;
+    return static_cast<int>(g);
+}
+
+kr_error configure_once() {
+    static std::once_flag once;
+    static cudaError_t status = cudaSuccess;
+    std::call_once(once, []() {
+        status = cudaFuncSetAttribute(dito_extremal_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        if (status == cudaSuccess)
+            status = cudaFuncSetAttribute(dito_extent_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    });
+    return status == cudaSuccess ? kr_success : cuda_error(status);
+}
+
+kr_error enqueue(const kr_vec3* d_points, uint64_t count, uint32_t flags, kr_obb3* d_obb, void* ws,
+                 cudaStream_t stream, int passes = 3) {
+    if (!ws || !d_obb || (count > 0 && !d_points)) return "obvh_dito: null pointer argument";
+    if (reinterpret_cast<uintptr_t>(d_points) & 3u) return "obvh_dito: points must be 4-byte aligned";
+    if (reinterpret_cast<uintptr_t>(ws) & 255u) return "obvh_dito: workspace must be 256-byte aligned";
+    OBVH_TRY(configure_once());
+    Split sp = make_split(reinterpret_cast<const float*>(d_points), count);
+    int grid = grid_for(sp);
+    if (passes & 1) {
+        dito_extremal_pass<<<grid, kThreads, kSmemBytes, stream>>>(sp, static_cast<char*>(ws), d_obb, flags);
+        OBVH_TRY_CUDA(cudaGetLastError());
+    }
+    if (passes & 2) {
+        dito_extent_pass<<<grid, kThreads, kSmemBytes, stream>>>(sp, static_cast<char*>(ws), d_obb, flags);
+        OBVH_TRY_CUDA(cudaGetLastError());
+    }
+    return kr_success;
+}
+
+// Per-device state of the host-pointer entry points.
+struct HostContext {
+    std::mutex mutex;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DeviceBuffer points;
+    DeviceBuffer ws;
+    PinnedBuffer result;  // Ctl + obb read back together
+    bool ready = false;
+
+    kr_error init() {
+        if (ready) return kr_success;
+        OBVH_TRY_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        OBVH_TRY_CUDA(cudaEventCreate(&ev0));
+        OBVH_TRY_CUDA(cudaEventCreate(&ev1));
+        OBVH_TRY(ws.reserve(kWorkspaceBytes));
+        OBVH_TRY_CUDA(cudaMemsetAsync(ws.ptr, 0, kWorkspaceBytes, stream));
+        OBVH_TRY(result.reserve(kOffObb + sizeof(kr_obb3)));
+        ready = true;
+        return kr_success;
+    }
+};
+
+HostContext& host_context() {
+    static std::mutex m;
+    static std::unordered_map<int, HostContext*> ctxs;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(m);
+    HostContext*& c = ctxs[dev];
+    if (!c) c = new HostContext();  // lives until process exit
+    return *c;
+}
+
+kr_error fit_host(const kr_vec3* points, uint64_t count, uint32_t flags, kr_obb3* obb, float* elapsed) {
+    if (!obb || (count > 0 && !points)) return "obvh_points_obb: null pointer argument";
+    HostContext& hc = host_context();
+    std::lock_guard<std::mutex> lock(hc.mutex);
+    OBVH_TRY(hc.init());
+    const size_t bytes = count * sizeof(kr_vec3);
+    OBVH_TRY(hc.points.reserve(bytes > 0 ? bytes : 16));
+    if (bytes) OBVH_TRY_CUDA(cudaMemcpyAsync(hc.points.ptr, points, bytes, cudaMemcpyHostToDevice, hc.stream));
+    char* ws = static_cast<char*>(hc.ws.ptr);
+    kr_obb3* d_obb = reinterpret_cast<kr_obb3*>(ws + kOffObb);
+    OBVH_TRY_CUDA(cudaEventRecord(hc.ev0, hc.stream));
+    OBVH_TRY(enqueue(static_cast<const kr_vec3*>(hc.points.ptr), count, flags, d_obb, ws, hc.stream));
+    OBVH_TRY_CUDA(cudaEventRecord(hc.ev1, hc.stream));
+    OBVH_TRY_CUDA(cudaMemcpyAsync(hc.result.ptr, ws, kOffObb + sizeof(kr_obb3), cudaMemcpyDeviceToHost, hc.stream));
+    OBVH_TRY_CUDA(cudaStreamSynchronize(hc.stream));
+    const Ctl* ctl = static_cast<const Ctl*>(hc.result.ptr);
+    if (ctl->error) {
+        cudaMemsetAsync(ws, 0, sizeof(Ctl), hc.stream);
+        cudaStreamSynchronize(hc.stream);
+        return "obvh_points_obb: device wait timed out";
+    }
+    std::memcpy(obb, static_cast<const char*>(hc.result.ptr) + kOffObb, sizeof(kr_obb3));
+    if (elapsed) {
+        float ms = 0.f;
+        OBVH_TRY_CUDA(cudaEventElapsedTime(&ms, hc.ev0, hc.ev1));
+        *elapsed = ms;
+    }
+    return kr_success;
+}
+
+}  // namespace dito
+}  // namespace obvh
+
+using namespace obvh;
+
+extern "C" kr_size obvh_dito_workspace_bytes(void) { return dito::kWorkspaceBytes; }
+
+extern "C" kr_error obvh_dito_workspace_init(void* d_workspace, void* stream) {
+    if (!d_workspace) return "obvh_dito_workspace_init: null workspace";
+    cudaError_t e = cudaMemsetAsync(d_workspace, 0, dito::kWorkspaceBytes, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? kr_success : cuda_error(e);
+}
+
+extern "C" kr_error obvh_dito_fit_async(const kr_vec3* d_points, kr_size count, kr_u32 flags, kr_obb3* d_obb,
+                                        void* d_workspace, void* stream) {
+    kr_error e = dito::enqueue(d_points, count, flags, d_obb, d_workspace, static_cast<cudaStream_t>(stream));
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error obvh_dito_fit_pass_async(const kr_vec3* d_points, kr_size count, kr_u32 flags, kr_obb3* d_obb,
+                                             void* d_workspace, void* stream, int pass) {
+    if (pass != 1 && pass != 2) return "obvh_dito_fit_pass_async: pass must be 1 or 2";
+    kr_error e = dito::enqueue(d_points, count, flags, d_obb, d_workspace, static_cast<cudaStream_t>(stream), pass);
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error obvh_dito_workspace_report(const void* d_workspace, void* stream, kr_u32* path,
+                                               kr_scalar axes[9], kr_u32* device_error) {
+    if (!d_workspace) return "obvh_dito_workspace_report: null workspace";
+    dito::Ctl ctl;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(&ctl, d_workspace, sizeof ctl, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_error(e);
+    if (path) *path = ctl.path;
+    if (axes) std::memcpy(axes, ctl.axes, sizeof ctl.axes);
+    if (device_error) *device_error = ctl.error;
+    return kr_success;
+}
+
+extern "C" kr_error obvh_points_obb(const kr_vec3* points, kr_size count, kr_u32 flags, kr_obb3* obb,
+                                    kr_scalar* elapsed_time) {
+    kr_error e = dito::fit_host(points, count, flags, obb, elapsed_time);
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_obb3 kr_cuda_points_obb(const kr_vec3* points, kr_size count, kr_scalar* elapsed_time) {
+    kr_obb3 obb;
+    std::memset(&obb, 0, sizeof obb);
+    if (elapsed_time) *elapsed_time = 0.f;
+    kr_error e = dito::fit_host(points, count, 0u, &obb, elapsed_time);
+    if (e) {
+        set_last_error(e);
+        std::memset(&obb, 0, sizeof obb);
+    }
+    return obb;
+}

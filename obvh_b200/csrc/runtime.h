@@ -1,0 +1,56 @@
+// runtime.h - host-side runtime shared by every entry point: error strings,
+// device properties, and growable cached device/pinned buffers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+
+#include "obvh_types.h"
+
+namespace obvh {
+
+// kr_error values are static strings; NULL is success.
+kr_error cuda_error(cudaError_t e);  // maps a CUDA error to a static string
+void set_last_error(kr_error e);     // thread-local, read by obvh_last_error()
+
+#define OBVH_TRY_CUDA(expr)                                      \
+    do {                                                         \
+        cudaError_t _e = (expr);                                 \
+        if (_e != cudaSuccess) return ::obvh::cuda_error(_e);    \
+    } while (0)
+
+#define OBVH_TRY(expr)                                           \
+    do {                                                         \
+        kr_error _k = (expr);                                    \
+        if (_k) return _k;                                       \
+    } while (0)
+
+struct DeviceInfo {
+    int device = 0;
+    int sm_count = 0;
+    size_t smem_optin = 0;
+};
+
+// Properties of the current device (cached per device id).
+const DeviceInfo& device_info();
+
+// A device buffer that only grows; not thread-safe on its own.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    kr_error reserve(size_t need);
+    void release();
+};
+
+// Pinned host buffer that only grows.
+struct PinnedBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    kr_error reserve(size_t need);
+    void release();
+};
+
+}  // namespace obvh

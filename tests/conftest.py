@@ -1,0 +1,41 @@
+"""Shared pytest configuration: the `gpu` marker and small helpers."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def golden_dito():
+    d = np.load(os.path.join(GOLDEN, "dito_golden.npz"))
+    for i, name in enumerate(d["names"]):
+        yield str(name), d["points"][d["offsets"][i]:d["offsets"][i + 1]], d["boxes"][i]
+
+
+def obb_contains(points: np.ndarray, obb: np.ndarray, rel: float = 1e-5) -> int:
+    """Number of points outside the box (FP64, tolerance rel * box scale)."""
+    p = points.astype(np.float64)
+    mid = obb[0:3].astype(np.float64)
+    axes = obb[3:12].astype(np.float64).reshape(3, 3)
+    ext = obb[12:15].astype(np.float64)
+    local = (p - mid) @ axes.T
+    scale = max(1.0, float(np.abs(p).max()) if len(p) else 1.0)
+    return int(np.count_nonzero(np.abs(local) > ext + rel * scale))
+
+
+def same_bits(a, b) -> bool:
+    """Bitwise equality of float arrays, treating -0.0 == +0.0."""
+    a = np.asarray(a, np.float32) + np.float32(0.0)
+    b = np.asarray(b, np.float32) + np.float32(0.0)
+    return bool(np.array_equal(a.view(np.uint32), b.view(np.uint32)))
