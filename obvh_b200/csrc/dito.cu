@@ -367,7 +367,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     Extents ex;
     ex.init(ctl->axes);
     uint64_t xi;
-    if (head_point(sp, xi) || tail_point(sp, xi)) ex.point(sp.xyz[3 * xi], sp.xyz[3 * xi + 1], sp.xyz[3 * xi + 2]);
+    if (head_point(sp, xi)) ex.point(sp.xyz[3 * xi], sp.xyz[3 * xi + 1], sp.xyz[3 * xi + 2]);
+    if (tail_point(sp, xi)) ex.point(sp.xyz[3 * xi], sp.xyz[3 * xi + 1], sp.xyz[3 * xi + 2]);
 
     uint64_t tb, te;
     cta_tiles(sp.ntiles, tb, te);
