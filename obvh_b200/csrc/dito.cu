@@ -33,6 +33,7 @@
 #include "obvh_api.h"
 #include "obvh_dito.h"
 #include "runtime.h"
+#include "stream_pipeline.cuh"
 
 namespace obvh {
 namespace dito {
@@ -49,17 +50,19 @@ constexpr size_t kOffRec2 = kOffRec1Idx + kMaxGrid * 14 * 8;      // [kMaxGrid][
 constexpr size_t kWorkspaceBytes = kOffRec2 + kMaxGrid * 6 * 4;
 
 // ---------------------------------------------------------------------------
-// Launch geometry.
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
-constexpr int kTileGroups = 512;              // 4-point groups per tile
+// Launch geometry: 8 consumer warps + 1 producer warp, 2 CTAs per SM.
+constexpr int kConsumerWarps = 8;
+constexpr int kConsumers = kConsumerWarps * 32;
+constexpr int kThreads = kConsumers + 32;
+constexpr int kCtasPerSm = 2;
+constexpr int kTileGroups = 2 * kConsumers;   // 4-point groups per tile: two per consumer thread
 constexpr int kTileBytes = kTileGroups * 48;  // 24 KB
 constexpr int kStages = 4;
 constexpr int kSmemBytes = kStages * kTileBytes;
 
 // The point array is split into an unaligned head (< 4 points), a body of
-// 16-byte-aligned 4-point groups, and a tail (< 4 points).  Head and tail are
-// read directly by CTA 0.
+// 16-byte-aligned 4-point groups, and a tail (< 4 points).  CTA 0 reads the
+// head and the last CTA the tail directly.
 struct Split {
     const float* xyz;     // all points, packed
     uint64_t n;
@@ -73,8 +76,7 @@ __host__ __device__ inline Split make_split(const float* xyz, uint64_t n) {
     s.xyz = xyz;
     s.n = n;
     uint64_t mis = (reinterpret_cast<uintptr_t>(xyz) & 15u) / 4u;  // misalignment in floats: 0..3
-    // head h with (mis + 3h) % 4 == 0
-    uint64_t h = 0;
+    uint64_t h = 0;  // smallest h with (mis + 3h) % 4 == 0
     while ((mis + 3 * h) % 4 != 0) ++h;
     if (h > n) h = n;
     s.head = h;
@@ -83,63 +85,77 @@ __host__ __device__ inline Split make_split(const float* xyz, uint64_t n) {
     return s;
 }
 
-__device__ __forceinline__ void slab7(float x, float y, float z, float s[7]) {
-    s[0] = x;
-    s[1] = y;
-    s[2] = z;
-    float a = x + y, b = x - y;
-    s[3] = a + z;
-    s[4] = a - z;
-    s[5] = b + z;
-    s[6] = b - z;
+// Slab projection k of the 7 fixed DiTO directions, in the reference's
+// evaluation order (dito.cpp:115-172); k is a compile-time constant after unrolling.
+__device__ __forceinline__ float slab(int k, float x, float y, float z) {
+    switch (k) {
+        case 0: return x;
+        case 1: return y;
+        case 2: return z;
+        case 3: return x + y + z;
+        case 4: return x + y - z;
+        case 5: return x - y + z;
+        default: return x - y - z;
+    }
 }
 
-// Per-thread running extremes with the index of the first point reaching them.
+// Per-thread running extremes with the CTA-local index of the first point
+// reaching them.  A thread sees its points in increasing index order.
 struct Extremes {
     float mn[7], mx[7];
-    uint64_t imn[7], imx[7];
+    uint32_t imn[7], imx[7];
     __device__ void init() {
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-            mn[k] = kInf;  // +inf
+            mn[k] = kInf;
             mx[k] = -kInf;
-            imn[k] = ~0ull;
-            imx[k] = ~0ull;
+            imn[k] = 0xffffffffu;
+            imx[k] = 0xffffffffu;
         }
     }
-    __device__ __forceinline__ void point(float x, float y, float z, uint64_t i) {
-        float s[7];
-        slab7(x, y, z, s);
+    // One point, index-aware (used for head/tail points).
+    __device__ __forceinline__ void point(float x, float y, float z, uint32_t i) {
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-            if (better_min(s[k], i, mn[k], imn[k])) { mn[k] = s[k]; imn[k] = i; }
-            if (better_max(s[k], i, mx[k], imx[k])) { mx[k] = s[k]; imx[k] = i; }
+            float v = slab(k, x, y, z);
+            if (v < mn[k] || (v == mn[k] && i < imn[k])) { mn[k] = v; imn[k] = i; }
+            if (v > mx[k] || (v == mx[k] && i < imx[k])) { mx[k] = v; imx[k] = i; }
         }
     }
-    // 4 consecutive points with indices base..base+3, all larger than any seen so far.
-    __device__ __forceinline__ void group(const float4& a, const float4& b, const float4& c, uint64_t base) {
-        float s0[7], s1[7], s2[7], s3[7];
-        slab7(a.x, a.y, a.z, s0);
-        slab7(a.w, b.x, b.y, s1);
-        slab7(b.z, b.w, c.x, s2);
-        slab7(c.y, c.z, c.w, s3);
+    // NP points p[0..NP) with consecutive indices from base (NP = 4 or 8; the
+    // second half of 8 starts at base2).  Fast path: group extremes only and a
+    // single branch; the rare improving group is re-scanned for the first index.
+    template <int NP>
+    __device__ __forceinline__ void points(const float* px, const float* py, const float* pz, uint32_t base,
+                                           uint32_t base2) {
+        bool any = false;
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-            float gm = fminf(fminf(s0[k], s1[k]), fminf(s2[k], s3[k]));
-            if (gm < mn[k]) {  // rare after the first few groups
-                mn[k] = gm;
-                imn[k] = base + (s0[k] == gm ? 0 : s1[k] == gm ? 1 : s2[k] == gm ? 2 : 3);
+            float lo = slab(k, px[0], py[0], pz[0]), hi = lo;
+#pragma unroll
+            for (int j = 1; j < NP; ++j) {
+                float v = slab(k, px[j], py[j], pz[j]);
+                lo = fminf(lo, v);
+                hi = fmaxf(hi, v);
             }
-            float gx = fmaxf(fmaxf(s0[k], s1[k]), fmaxf(s2[k], s3[k]));
-            if (gx > mx[k]) {
-                mx[k] = gx;
-                imx[k] = base + (s0[k] == gx ? 0 : s1[k] == gx ? 1 : s2[k] == gx ? 2 : 3);
+            any |= (lo < mn[k]) | (hi > mx[k]);
+        }
+        if (__builtin_expect(any, 0)) {
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+#pragma unroll
+                for (int j = 0; j < NP; ++j) {
+                    float v = slab(k, px[j], py[j], pz[j]);
+                    uint32_t i = (j < 4) ? base + j : base2 + (j - 4);
+                    if (v < mn[k]) { mn[k] = v; imn[k] = i; }
+                    if (v > mx[k]) { mx[k] = v; imx[k] = i; }
+                }
             }
         }
     }
 };
 
-// Extents along three axes (no index needed: only the values are used).
+// Extents along three axes (values only).
 struct Extents {
     f3 b0, b1, b2;
     float lo[3], hi[3];
@@ -157,61 +173,15 @@ struct Extents {
         lo[1] = fminf(lo[1], q1); hi[1] = fmaxf(hi[1], q1);
         lo[2] = fminf(lo[2], q2); hi[2] = fmaxf(hi[2], q2);
     }
-    __device__ __forceinline__ void group(const float4& a, const float4& b, const float4& c) {
-        point(a.x, a.y, a.z);
-        point(a.w, b.x, b.y);
-        point(b.z, b.w, c.x);
-        point(c.y, c.z, c.w);
-    }
 };
 
-// ---------------------------------------------------------------------------
-// Tile pipeline: the CTA consumes tiles [t_begin, t_end) of the body (in
-// reverse when `reverse`), calling fn(groups, group_base, smem_tile) per tile.
-// Returns false if a wait timed out (the whole CTA agrees).
-template <class Fn>
-__device__ bool tile_pipeline(const Split& sp, uint64_t t_begin, uint64_t t_end, bool reverse,
-                              float4* ring, uint64_t* full, uint32_t* err, Fn&& fn) {
-    const int tid = threadIdx.x;
-    const uint64_t count = t_end - t_begin;
-    const char* body = reinterpret_cast<const char*>(sp.xyz + 3 * sp.head);
-    auto tile_of = [&](uint64_t it) { return reverse ? (t_end - 1 - it) : (t_begin + it); };
-    auto groups_of = [&](uint64_t t) -> uint32_t {
-        uint64_t g0 = t * kTileGroups;
-        uint64_t g = sp.groups - g0;
-        return static_cast<uint32_t>(g < kTileGroups ? g : kTileGroups);
-    };
-    auto issue = [&](uint64_t it, int s) {
-        uint64_t t = tile_of(it);
-        uint32_t bytes = groups_of(t) * 48u;
-        mbar_expect_tx(&full[s], bytes);
-        bulk_g2s(ring + s * (kTileBytes / 16), body + t * static_cast<uint64_t>(kTileBytes), bytes, &full[s]);
-    };
-    if (tid == 0) {
-        for (int s = 0; s < kStages && s < static_cast<int>(count); ++s) issue(s, s);
-    }
-    bool ok = true;
-    uint64_t it = 0;
-    for (; it < count; ++it) {
-        const int s = static_cast<int>(it % kStages);
-        const uint32_t parity = static_cast<uint32_t>((it / kStages) & 1u);
-        bool mine = mbar_wait_bounded(&full[s], parity, err);
-        if (mine) {
-            uint64_t t = tile_of(it);
-            fn(groups_of(t), t * kTileGroups, ring + s * (kTileBytes / 16));
-        }
-        if (__syncthreads_or(!mine)) { ok = false; break; }
-        if (tid == 0 && it + kStages < count) {
-            fence_proxy_async_smem();
-            issue(it + kStages, s);
-        }
-    }
-    if (!ok && tid == 0) {
-        // Let the copies still in flight land before the CTA's shared memory is released.
-        for (uint64_t j = it + 1; j < count && j < it + kStages; ++j)
-            mbar_wait_bounded(&full[j % kStages], static_cast<uint32_t>((j / kStages) & 1u), err);
-    }
-    return ok;
+// Unpacks 4-point groups (3 float4 each) into coordinate arrays.
+__device__ __forceinline__ void unpack4(const float4& a, const float4& b, const float4& c, float* x, float* y,
+                                        float* z) {
+    x[0] = a.x; y[0] = a.y; z[0] = a.z;
+    x[1] = a.w; y[1] = b.x; z[1] = b.y;
+    x[2] = b.z; y[2] = b.w; z[2] = c.x;
+    x[3] = c.y; y[3] = c.z; z[3] = c.w;
 }
 
 __device__ __forceinline__ void cta_tiles(uint64_t ntiles, uint64_t& b, uint64_t& e) {
@@ -219,73 +189,96 @@ __device__ __forceinline__ void cta_tiles(uint64_t ntiles, uint64_t& b, uint64_t
     e = ntiles * (blockIdx.x + 1) / gridDim.x;
 }
 
-// Points outside the aligned body, given to the first threads of CTA 0: the
-// head (indices below the body, handled before the tiles) and the tail
-// (indices above it, handled after), which keeps each thread's points in
-// increasing index order as the first-index tie rule needs.
-__device__ __forceinline__ bool head_point(const Split& sp, uint64_t& idx) {
-    if (blockIdx.x != 0 || threadIdx.x >= sp.head) return false;
-    idx = threadIdx.x;
-    return true;
-}
-__device__ __forceinline__ bool tail_point(const Split& sp, uint64_t& idx) {
-    const uint64_t tail0 = sp.head + 4 * sp.groups;
-    if (blockIdx.x != 0 || threadIdx.x >= sp.n - tail0) return false;
-    idx = tail0 + threadIdx.x;
-    return true;
+// Producer: the tiles of this CTA's slice, forwards or backwards.
+__device__ __forceinline__ void produce_slice(const Split& sp, uint64_t tb, uint64_t te, bool reverse, char* ring,
+                                              RingBarriers<kStages>& rb, uint32_t* err) {
+    const char* body = reinterpret_cast<const char*>(sp.xyz + 3 * sp.head);
+    produce_tiles<kStages>(te - tb, ring, kTileBytes, rb, err, [&](uint64_t it, uint32_t& bytes) {
+        uint64_t t = reverse ? (te - 1 - it) : (tb + it);
+        uint64_t g = sp.groups - t * kTileGroups;
+        bytes = static_cast<uint32_t>(g < kTileGroups ? g : kTileGroups) * 48u;
+        return static_cast<const void*>(body + t * static_cast<uint64_t>(kTileBytes));
+    });
 }
 
-// Signals this CTA's completion; true in exactly one CTA, the last one.
+// Signals the completion of this CTA's consumers; true in exactly one CTA,
+// the last one.  Consumer threads only.
 __device__ bool last_cta(uint32_t* ticket) {
     __shared__ uint32_t s_last;
     __threadfence();
-    __syncthreads();
+    named_sync(1, kConsumers);
     if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1u) == gridDim.x - 1) ? 1u : 0u;
-    __syncthreads();
+    named_sync(1, kConsumers);
     if (s_last) __threadfence();
     return s_last != 0;
 }
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, kCtasPerSm)
     dito_extremal_pass(Split sp, char* ws, kr_obb3* out, uint32_t flags) {
-    extern __shared__ __align__(128) float4 ring[];
-    __shared__ uint64_t full[kStages];
-    __shared__ float s_val[kWarps][14];
-    __shared__ uint64_t s_idx[kWarps][14];
+    extern __shared__ __align__(128) char ring[];
+    __shared__ RingBarriers<kStages> rb;
+    __shared__ float s_val[kConsumerWarps][14];
+    __shared__ uint32_t s_idx[kConsumerWarps][14];
 
     Ctl* ctl = reinterpret_cast<Ctl*>(ws);
     float* rec_val = reinterpret_cast<float*>(ws + kOffRec1Val);
     uint64_t* rec_idx = reinterpret_cast<uint64_t*>(ws + kOffRec1Idx);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
-        mbar_fence_init();
-    }
+    if (tid == 0) rb.init(kConsumerWarps);
     __syncthreads();
-
-    Extremes ex;
-    ex.init();
-    uint64_t xi;
-    if (head_point(sp, xi)) ex.point(sp.xyz[3 * xi], sp.xyz[3 * xi + 1], sp.xyz[3 * xi + 2], xi);
 
     uint64_t tb, te;
     cta_tiles(sp.ntiles, tb, te);
-    tile_pipeline(sp, tb, te, false, ring, full, &ctl->error,
-                  [&](uint32_t groups, uint64_t g0, const float4* tile) {
-                      for (uint32_t g = tid; g < groups; g += kThreads) {
-                          float4 a = tile[3 * g], b = tile[3 * g + 1], c = tile[3 * g + 2];
-                          ex.group(a, b, c, sp.head + 4 * (g0 + g));
-                      }
-                  });
-    if (tail_point(sp, xi)) ex.point(sp.xyz[3 * xi], sp.xyz[3 * xi + 1], sp.xyz[3 * xi + 2], xi);
+    if (warp == kConsumerWarps) {
+        produce_slice(sp, tb, te, false, ring, rb, &ctl->error);
+        return;
+    }
+
+    // Indices are kept relative to the CTA's first point (CTA 0 starts at the head).
+    const uint64_t cta_base = blockIdx.x == 0 ? 0 : sp.head + 4 * tb * kTileGroups;
+    Extremes ex;
+    ex.init();
+    if (blockIdx.x == 0 && static_cast<uint64_t>(tid) < sp.head) {
+        const float* p = sp.xyz + 3 * tid;
+        ex.point(p[0], p[1], p[2], static_cast<uint32_t>(tid));
+    }
+    consume_tiles<kStages>(te - tb, ring, kTileBytes, rb, &ctl->error, [&](uint64_t it, const char* slot) {
+        const uint64_t t = tb + it;
+        const uint64_t g0 = t * kTileGroups;
+        const uint64_t left = sp.groups - g0;
+        const uint32_t groups = static_cast<uint32_t>(left < kTileGroups ? left : kTileGroups);
+        const float4* tile = reinterpret_cast<const float4*>(slot);
+        const uint32_t ga = tid, gb = tid + kConsumers;
+        const uint32_t ia = static_cast<uint32_t>(sp.head + 4 * (g0 + ga) - cta_base);
+        const uint32_t ib = ia + 4 * kConsumers;
+        float x[8], y[8], z[8];
+        if (gb < groups) {
+            unpack4(tile[3 * ga], tile[3 * ga + 1], tile[3 * ga + 2], x, y, z);
+            unpack4(tile[3 * gb], tile[3 * gb + 1], tile[3 * gb + 2], x + 4, y + 4, z + 4);
+            ex.points<8>(x, y, z, ia, ib);
+        } else if (ga < groups) {
+            unpack4(tile[3 * ga], tile[3 * ga + 1], tile[3 * ga + 2], x, y, z);
+            ex.points<4>(x, y, z, ia, ia + 4);
+        }
+    });
+    if (blockIdx.x == gridDim.x - 1) {
+        const uint64_t tail0 = sp.head + 4 * sp.groups;
+        if (static_cast<uint64_t>(tid) < sp.n - tail0) {
+            const float* p = sp.xyz + 3 * (tail0 + tid);
+            ex.point(p[0], p[1], p[2], static_cast<uint32_t>(tail0 + tid - cta_base));
+        }
+    }
 
     // CTA reduction -> one record of 7 (min, argmin) + 7 (max, argmax).
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
-        warp_argmin(ex.mn[k], ex.imn[k]);
-        warp_argmax(ex.mx[k], ex.imx[k]);
+        uint64_t a = ex.imn[k], b = ex.imx[k];
+        warp_argmin(ex.mn[k], a);
+        warp_argmax(ex.mx[k], b);
+        ex.imn[k] = static_cast<uint32_t>(a);
+        ex.imx[k] = static_cast<uint32_t>(b);
     }
     if (lane == 0) {
 #pragma unroll
@@ -296,25 +289,25 @@ __global__ void __launch_bounds__(kThreads, 2)
             s_idx[warp][7 + k] = ex.imx[k];
         }
     }
-    __syncthreads();
+    named_sync(1, kConsumers);
     if (tid < 14) {
         float v = s_val[0][tid];
-        uint64_t i = s_idx[0][tid];
-        for (int w = 1; w < kWarps; ++w) {
+        uint32_t i = s_idx[0][tid];
+        for (int w = 1; w < kConsumerWarps; ++w) {
             float ov = s_val[w][tid];
-            uint64_t oi = s_idx[w][tid];
+            uint32_t oi = s_idx[w][tid];
             bool b = tid < 7 ? better_min(ov, oi, v, i) : better_max(ov, oi, v, i);
             if (b) { v = ov; i = oi; }
         }
         rec_val[blockIdx.x * 14 + tid] = v;
-        rec_idx[blockIdx.x * 14 + tid] = i;
+        rec_idx[blockIdx.x * 14 + tid] = (i == 0xffffffffu) ? ~0ull : cta_base + i;
     }
     if (!last_cta(&ctl->ticket[0])) return;
 
     // ---- last CTA: global extremes, then the candidate search -------------
     __shared__ float g_val[14];
     __shared__ uint64_t g_idx[14];
-    for (int e = warp; e < 14; e += kWarps) {
+    for (int e = warp; e < 14; e += kConsumerWarps) {
         float v = e < 7 ? kInf : -kInf;
         uint64_t i = ~0ull;
         for (int r = lane; r < static_cast<int>(gridDim.x); r += 32) {
@@ -326,7 +319,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (e < 7) warp_argmin(v, i); else warp_argmax(v, i);
         if (lane == 0) { g_val[e] = v; g_idx[e] = i; }
     }
-    __syncthreads();
+    named_sync(1, kConsumers);
     if (warp == 0) {
         CandidateInput in;
         in.n = sp.n;
@@ -347,36 +340,59 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (tid == 0) ctl->ticket[0] = 0;
 }
 
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, kCtasPerSm)
     dito_extent_pass(Split sp, char* ws, kr_obb3* out, uint32_t flags) {
-    extern __shared__ __align__(128) float4 ring[];
-    __shared__ uint64_t full[kStages];
-    __shared__ float s_lohi[kWarps][6];
+    extern __shared__ __align__(128) char ring[];
+    __shared__ RingBarriers<kStages> rb;
+    __shared__ float s_lohi[kConsumerWarps][6];
 
     Ctl* ctl = reinterpret_cast<Ctl*>(ws);
     if (ctl->plan == 0) return;  // box already final (uniform across the grid)
     float* rec = reinterpret_cast<float*>(ws + kOffRec2);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
-        mbar_fence_init();
-    }
+    if (tid == 0) rb.init(kConsumerWarps);
     __syncthreads();
-
-    Extents ex;
-    ex.init(ctl->axes);
-    uint64_t xi;
-    if (head_point(sp, xi)) ex.point(sp.xyz[3 * xi], sp.xyz[3 * xi + 1], sp.xyz[3 * xi + 2]);
-    if (tail_point(sp, xi)) ex.point(sp.xyz[3 * xi], sp.xyz[3 * xi + 1], sp.xyz[3 * xi + 2]);
 
     uint64_t tb, te;
     cta_tiles(sp.ntiles, tb, te);
-    tile_pipeline(sp, tb, te, true, ring, full, &ctl->error,
-                  [&](uint32_t groups, uint64_t, const float4* tile) {
-                      for (uint32_t g = tid; g < groups; g += kThreads)
-                          ex.group(tile[3 * g], tile[3 * g + 1], tile[3 * g + 2]);
-                  });
+    if (warp == kConsumerWarps) {
+        // Backwards: the end of each slice, read last by pass 1, is still in L2.
+        produce_slice(sp, tb, te, true, ring, rb, &ctl->error);
+        return;
+    }
+
+    Extents ex;
+    ex.init(ctl->axes);
+    if (blockIdx.x == 0 && static_cast<uint64_t>(tid) < sp.head) {
+        const float* p = sp.xyz + 3 * tid;
+        ex.point(p[0], p[1], p[2]);
+    }
+    if (blockIdx.x == gridDim.x - 1) {
+        const uint64_t tail0 = sp.head + 4 * sp.groups;
+        if (static_cast<uint64_t>(tid) < sp.n - tail0) {
+            const float* p = sp.xyz + 3 * (tail0 + tid);
+            ex.point(p[0], p[1], p[2]);
+        }
+    }
+    consume_tiles<kStages>(te - tb, ring, kTileBytes, rb, &ctl->error, [&](uint64_t it, const char* slot) {
+        const uint64_t t = te - 1 - it;
+        const uint64_t left = sp.groups - t * kTileGroups;
+        const uint32_t groups = static_cast<uint32_t>(left < kTileGroups ? left : kTileGroups);
+        const float4* tile = reinterpret_cast<const float4*>(slot);
+        const uint32_t ga = tid, gb = tid + kConsumers;
+        float x[8], y[8], z[8];
+        if (gb < groups) {
+            unpack4(tile[3 * ga], tile[3 * ga + 1], tile[3 * ga + 2], x, y, z);
+            unpack4(tile[3 * gb], tile[3 * gb + 1], tile[3 * gb + 2], x + 4, y + 4, z + 4);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) ex.point(x[j], y[j], z[j]);
+        } else if (ga < groups) {
+            unpack4(tile[3 * ga], tile[3 * ga + 1], tile[3 * ga + 2], x, y, z);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) ex.point(x[j], y[j], z[j]);
+        }
+    });
 
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -386,10 +402,10 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (lane == 0) {
         for (int k = 0; k < 3; ++k) { s_lohi[warp][k] = ex.lo[k]; s_lohi[warp][3 + k] = ex.hi[k]; }
     }
-    __syncthreads();
+    named_sync(1, kConsumers);
     if (tid < 6) {
         float v = s_lohi[0][tid];
-        for (int w = 1; w < kWarps; ++w) v = tid < 3 ? fminf(v, s_lohi[w][tid]) : fmaxf(v, s_lohi[w][tid]);
+        for (int w = 1; w < kConsumerWarps; ++w) v = tid < 3 ? fminf(v, s_lohi[w][tid]) : fmaxf(v, s_lohi[w][tid]);
         rec[blockIdx.x * 6 + tid] = v;
     }
     if (!last_cta(&ctl->ticket[1])) return;
@@ -406,7 +422,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (lane == 0) g_lohi[e] = v;
         }
     }
-    __syncthreads();
+    named_sync(1, kConsumers);
     if (tid == 0) {
         finalize_extents(ctl, g_lohi, flags, out);
         ctl->ticket[1] = 0;
@@ -418,7 +434,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
 int grid_for(const Split& sp) {
     const DeviceInfo& info = device_info();
-    uint64_t g = 2ull * info.sm_count;
+    uint64_t g = static_cast<uint64_t>(kCtasPerSm) * info.sm_count;
     if (g > kMaxGrid) g = kMaxGrid;
     if (sp.ntiles < g) g = sp.ntiles;
     if (g < 1) g = 1;
@@ -429,9 +445,13 @@ kr_error configure_once() {
     static std::once_flag once;
     static cudaError_t status = cudaSuccess;
     std::call_once(once, []() {
-        status = cudaFuncSetAttribute(dito_extremal_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-        if (status == cudaSuccess)
-            status = cudaFuncSetAttribute(dito_extent_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        for (const void* f : {reinterpret_cast<const void*>(dito_extremal_pass),
+                              reinterpret_cast<const void*>(dito_extent_pass)}) {
+            if (status == cudaSuccess)
+                status = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+            if (status == cudaSuccess)
+                status = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        }
     });
     return status == cudaSuccess ? kr_success : cuda_error(status);
 }
