@@ -99,58 +99,37 @@ __device__ __forceinline__ float slab(int k, float x, float y, float z) {
     }
 }
 
-// Per-thread running extremes with the CTA-local index of the first point
-// reaching them.  A thread sees its points in increasing index order.
+// Per-thread running extremes.  For each direction the thread keeps the
+// extreme value and the CTA-local index of the first point of the first
+// 4-point group reaching it (groups are visited in increasing index order and
+// replaced only on strict improvement).  The hot loop is branch-free; the
+// exact point inside a winning group is resolved once per CTA.
 struct Extremes {
     float mn[7], mx[7];
-    uint32_t imn[7], imx[7];
+    uint32_t gmn[7], gmx[7];
     __device__ void init() {
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
             mn[k] = kInf;
             mx[k] = -kInf;
-            imn[k] = 0xffffffffu;
-            imx[k] = 0xffffffffu;
+            gmn[k] = 0xffffffffu;
+            gmx[k] = 0xffffffffu;
         }
     }
-    // One point, index-aware (used for head/tail points).
-    __device__ __forceinline__ void point(float x, float y, float z, uint32_t i) {
+    // the 4 points x/y/z[0..4) with indices g, g+1, g+2, g+3
+    __device__ __forceinline__ void group(const float* x, const float* y, const float* z, uint32_t g) {
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-            float v = slab(k, x, y, z);
-            if (v < mn[k] || (v == mn[k] && i < imn[k])) { mn[k] = v; imn[k] = i; }
-            if (v > mx[k] || (v == mx[k] && i < imx[k])) { mx[k] = v; imx[k] = i; }
-        }
-    }
-    // NP points p[0..NP) with consecutive indices from base (NP = 4 or 8; the
-    // second half of 8 starts at base2).  Fast path: group extremes only and a
-    // single branch; the rare improving group is re-scanned for the first index.
-    template <int NP>
-    __device__ __forceinline__ void points(const float* px, const float* py, const float* pz, uint32_t base,
-                                           uint32_t base2) {
-        bool any = false;
-#pragma unroll
-        for (int k = 0; k < 7; ++k) {
-            float lo = slab(k, px[0], py[0], pz[0]), hi = lo;
-#pragma unroll
-            for (int j = 1; j < NP; ++j) {
-                float v = slab(k, px[j], py[j], pz[j]);
-                lo = fminf(lo, v);
-                hi = fmaxf(hi, v);
-            }
-            any |= (lo < mn[k]) | (hi > mx[k]);
-        }
-        if (__builtin_expect(any, 0)) {
-#pragma unroll
-            for (int k = 0; k < 7; ++k) {
-#pragma unroll
-                for (int j = 0; j < NP; ++j) {
-                    float v = slab(k, px[j], py[j], pz[j]);
-                    uint32_t i = (j < 4) ? base + j : base2 + (j - 4);
-                    if (v < mn[k]) { mn[k] = v; imn[k] = i; }
-                    if (v > mx[k]) { mx[k] = v; imx[k] = i; }
-                }
-            }
+            float v0 = slab(k, x[0], y[0], z[0]), v1 = slab(k, x[1], y[1], z[1]);
+            float v2 = slab(k, x[2], y[2], z[2]), v3 = slab(k, x[3], y[3], z[3]);
+            float lo = fminf(fminf(v0, v1), fminf(v2, v3));
+            float hi = fmaxf(fmaxf(v0, v1), fmaxf(v2, v3));
+            bool a = lo < mn[k];
+            mn[k] = a ? lo : mn[k];
+            gmn[k] = a ? g : gmn[k];
+            bool b = hi > mx[k];
+            mx[k] = b ? hi : mx[k];
+            gmx[k] = b ? g : gmx[k];
         }
     }
 };
@@ -219,7 +198,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm)
     extern __shared__ __align__(128) char ring[];
     __shared__ RingBarriers<kStages> rb;
     __shared__ float s_val[kConsumerWarps][14];
-    __shared__ uint32_t s_idx[kConsumerWarps][14];
+    __shared__ uint32_t s_idx[kConsumerWarps][14];  // CTA-local first index of a 4-point group
 
     Ctl* ctl = reinterpret_cast<Ctl*>(ws);
     float* rec_val = reinterpret_cast<float*>(ws + kOffRec1Val);
@@ -236,71 +215,81 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm)
         return;
     }
 
-    // Indices are kept relative to the CTA's first point (CTA 0 starts at the head).
-    const uint64_t cta_base = blockIdx.x == 0 ? 0 : sp.head + 4 * tb * kTileGroups;
+    // Indices are kept relative to the CTA's first body point.
+    const uint64_t cta_base = sp.head + 4 * tb * kTileGroups;
     Extremes ex;
     ex.init();
-    if (blockIdx.x == 0 && static_cast<uint64_t>(tid) < sp.head) {
-        const float* p = sp.xyz + 3 * tid;
-        ex.point(p[0], p[1], p[2], static_cast<uint32_t>(tid));
-    }
     consume_tiles<kStages>(te - tb, ring, kTileBytes, rb, &ctl->error, [&](uint64_t it, const char* slot) {
         const uint64_t t = tb + it;
-        const uint64_t g0 = t * kTileGroups;
-        const uint64_t left = sp.groups - g0;
+        const uint64_t left = sp.groups - t * kTileGroups;
         const uint32_t groups = static_cast<uint32_t>(left < kTileGroups ? left : kTileGroups);
         const float4* tile = reinterpret_cast<const float4*>(slot);
         const uint32_t ga = tid, gb = tid + kConsumers;
-        const uint32_t ia = static_cast<uint32_t>(sp.head + 4 * (g0 + ga) - cta_base);
-        const uint32_t ib = ia + 4 * kConsumers;
+        const uint32_t ia = static_cast<uint32_t>(4 * (it * kTileGroups + ga));
         float x[8], y[8], z[8];
         if (gb < groups) {
             unpack4(tile[3 * ga], tile[3 * ga + 1], tile[3 * ga + 2], x, y, z);
             unpack4(tile[3 * gb], tile[3 * gb + 1], tile[3 * gb + 2], x + 4, y + 4, z + 4);
-            ex.points<8>(x, y, z, ia, ib);
+            ex.group(x, y, z, ia);
+            ex.group(x + 4, y + 4, z + 4, ia + 4 * kConsumers);
         } else if (ga < groups) {
             unpack4(tile[3 * ga], tile[3 * ga + 1], tile[3 * ga + 2], x, y, z);
-            ex.points<4>(x, y, z, ia, ia + 4);
+            ex.group(x, y, z, ia);
         }
     });
-    if (blockIdx.x == gridDim.x - 1) {
-        const uint64_t tail0 = sp.head + 4 * sp.groups;
-        if (static_cast<uint64_t>(tid) < sp.n - tail0) {
-            const float* p = sp.xyz + 3 * (tail0 + tid);
-            ex.point(p[0], p[1], p[2], static_cast<uint32_t>(tail0 + tid - cta_base));
-        }
-    }
 
-    // CTA reduction -> one record of 7 (min, argmin) + 7 (max, argmax).
+    // CTA reduction of (value, group) pairs: the first group reaching each extreme.
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
-        uint64_t a = ex.imn[k], b = ex.imx[k];
+        uint64_t a = ex.gmn[k], b = ex.gmx[k];
         warp_argmin(ex.mn[k], a);
         warp_argmax(ex.mx[k], b);
-        ex.imn[k] = static_cast<uint32_t>(a);
-        ex.imx[k] = static_cast<uint32_t>(b);
+        ex.gmn[k] = static_cast<uint32_t>(a);
+        ex.gmx[k] = static_cast<uint32_t>(b);
     }
     if (lane == 0) {
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
             s_val[warp][k] = ex.mn[k];
-            s_idx[warp][k] = ex.imn[k];
+            s_idx[warp][k] = ex.gmn[k];
             s_val[warp][7 + k] = ex.mx[k];
-            s_idx[warp][7 + k] = ex.imx[k];
+            s_idx[warp][7 + k] = ex.gmx[k];
         }
     }
     named_sync(1, kConsumers);
     if (tid < 14) {
+        const int k = tid < 7 ? tid : tid - 7;
+        const bool is_min = tid < 7;
         float v = s_val[0][tid];
-        uint32_t i = s_idx[0][tid];
+        uint32_t g = s_idx[0][tid];
         for (int w = 1; w < kConsumerWarps; ++w) {
             float ov = s_val[w][tid];
-            uint32_t oi = s_idx[w][tid];
-            bool b = tid < 7 ? better_min(ov, oi, v, i) : better_max(ov, oi, v, i);
-            if (b) { v = ov; i = oi; }
+            uint32_t og = s_idx[w][tid];
+            bool b = is_min ? better_min(ov, og, v, g) : better_max(ov, og, v, g);
+            if (b) { v = ov; g = og; }
         }
+        // The first point of the winning group that reaches the value.
+        uint64_t best_i = ~0ull;
+        if (g != 0xffffffffu) {
+            for (int j = 3; j >= 0; --j) {
+                const float* p = sp.xyz + 3 * (cta_base + g + j);
+                if (slab(k, p[0], p[1], p[2]) == v) best_i = cta_base + g + j;
+            }
+        }
+        // Points outside the aligned body: the head precedes every body point
+        // (CTA 0), the tail follows them (last CTA).
+        auto merge = [&](uint64_t i) {
+            const float* p = sp.xyz + 3 * i;
+            float q = slab(k, p[0], p[1], p[2]);
+            bool b = is_min ? better_min(q, i, v, best_i) : better_max(q, i, v, best_i);
+            if (b) { v = q; best_i = i; }
+        };
+        if (blockIdx.x == 0)
+            for (uint64_t i = 0; i < sp.head; ++i) merge(i);
+        if (blockIdx.x == gridDim.x - 1)
+            for (uint64_t i = sp.head + 4 * sp.groups; i < sp.n; ++i) merge(i);
         rec_val[blockIdx.x * 14 + tid] = v;
-        rec_idx[blockIdx.x * 14 + tid] = (i == 0xffffffffu) ? ~0ull : cta_base + i;
+        rec_idx[blockIdx.x * 14 + tid] = best_i;
     }
     if (!last_cta(&ctl->ticket[0])) return;
 
