@@ -30,6 +30,7 @@
 
 #include "device_common.cuh"
 #include "dito_device.cuh"
+#include "dito_host.h"
 #include "obvh_api.h"
 #include "obvh_dito.h"
 #include "runtime.h"
@@ -37,17 +38,6 @@
 
 namespace obvh {
 namespace dito {
-
-// ---------------------------------------------------------------------------
-// Workspace layout (device): Ctl (dito_device.cuh), an output slot used by the
-// host-pointer entry points, then the per-CTA records of both passes.
-
-constexpr int kMaxGrid = 1024;
-constexpr size_t kOffObb = 256;                                   // host-API output slot
-constexpr size_t kOffRec1Val = 512;                               // [kMaxGrid][14] float
-constexpr size_t kOffRec1Idx = kOffRec1Val + kMaxGrid * 14 * 4;   // [kMaxGrid][14] u64
-constexpr size_t kOffRec2 = kOffRec1Idx + kMaxGrid * 14 * 8;      // [kMaxGrid][6] float
-constexpr size_t kWorkspaceBytes = kOffRec2 + kMaxGrid * 6 * 4;
 
 // ---------------------------------------------------------------------------
 // Launch geometry: 8 consumer warps + 1 producer warp, 2 CTAs per SM.
@@ -446,7 +436,7 @@ kr_error configure_once() {
 }
 
 kr_error enqueue(const kr_vec3* d_points, uint64_t count, uint32_t flags, kr_obb3* d_obb, void* ws,
-                 cudaStream_t stream, int passes = 3) {
+                 cudaStream_t stream, int passes) {
     if (!ws || !d_obb || (count > 0 && !d_points)) return "obvh_dito: null pointer argument";
     if (reinterpret_cast<uintptr_t>(d_points) & 3u) return "obvh_dito: points must be 4-byte aligned";
     if (reinterpret_cast<uintptr_t>(ws) & 255u) return "obvh_dito: workspace must be 256-byte aligned";

@@ -29,6 +29,15 @@ struct Ctl {
 };
 static_assert(sizeof(Ctl) == 256, "control block is 256 bytes");
 
+// Workspace layout (device): the control block, an output slot used by the
+// host-pointer entry points, then the per-CTA records of both passes.
+constexpr int kMaxGrid = 1024;
+constexpr size_t kOffObb = 256;                                   // host-API output slot
+constexpr size_t kOffRec1Val = 512;                               // [kMaxGrid][14] float
+constexpr size_t kOffRec1Idx = kOffRec1Val + kMaxGrid * 14 * 4;   // [kMaxGrid][14] u64
+constexpr size_t kOffRec2 = kOffRec1Idx + kMaxGrid * 14 * 8;      // [kMaxGrid][6] float
+constexpr size_t kWorkspaceBytes = kOffRec2 + kMaxGrid * 6 * 4;
+
 struct CandidateInput {
     uint64_t n;
     float val[14];  // min of slab 0..6, then max of slab 0..6
