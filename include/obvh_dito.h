@@ -66,6 +66,27 @@ OBVH_EXPORT kr_error obvh_dito_fit_pass_async(const kr_vec3* d_points, kr_size c
                                               kr_obb3* d_obb, void* d_workspace, void* stream, int pass);
 
 /*
+ * A DiTO-14 fit that allocates nothing, for callers that may not allocate
+ * device memory when they fit a box (a plugin whose host application owns the
+ * GPU memory, a service that reserves its whole budget at start-up).  No
+ * counterpart in the reference, whose kr_cuda_points_obb allocates (and leaks)
+ * on every call.
+ *
+ * `points` is a HOST array of at most 1,048,576 points (larger counts return
+ * an error), `obb` a host output; the fit runs on `stream` (NULL = legacy
+ * default stream) and the call returns after synchronising it.  The points
+ * are staged in a 12 MB array and the fit uses a 197 KB workspace, both
+ * file-scope device arrays of the library that every GPU loading it keeps
+ * until the process exits.  The first call on a device looks up their device
+ * addresses (once per device); make that first call before any stream
+ * capture.  All calls on a device share the arrays: calls whose GPU work
+ * overlapped would race, so the library serialises calls with a lock and
+ * never returns with work in flight.
+ */
+OBVH_EXPORT kr_error obvh_points_obb_noalloc(const kr_vec3* points, kr_size count, kr_u32 flags,
+                                             kr_obb3* obb, void* stream);
+
+/*
  * Reads back the diagnostics of the last fit made with a workspace
  * (synchronises `stream`): the path taken (0 empty, 1 degenerate pair,
  * 2 degenerate line, 3 OBB, 4 AABB kept by the final test), the candidate

@@ -40,6 +40,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "obvh_dito_workspace_init": (err, [vp, vp]),
         "obvh_dito_fit_async": (err, [vp, c.c_uint64, c.c_uint32, vp, vp, vp]),
         "obvh_dito_fit_pass_async": (err, [vp, c.c_uint64, c.c_uint32, vp, vp, vp, c.c_int]),
+        "obvh_points_obb_noalloc": (err, [vp, c.c_uint64, c.c_uint32, vp, vp]),
         "obvh_dito_workspace_report": (err, [vp, vp, c.POINTER(c.c_uint32), c.POINTER(c.c_float),
                                              c.POINTER(c.c_uint32)]),
     }

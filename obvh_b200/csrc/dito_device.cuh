@@ -111,7 +111,7 @@ __device__ __forceinline__ void extent_1d(const f3* P, int np, f3 dir, float& lo
 // order, and the reference's "strictly better than the best so far" scan is
 // reproduced as an argmin with the lowest frame index winning ties.
 // Writes the plan for the extent pass into ctl, or the final box into out.
-__device__ void candidate_warp(const CandidateInput& in, const float* xyz, uint32_t flags, Ctl* ctl,
+inline __device__ void candidate_warp(const CandidateInput& in, const float* xyz, uint32_t flags, Ctl* ctl,
                                kr_obb3* out) {
     const int lane = threadIdx.x & 31;
     const Mode md{(flags & OBVH_DITO_REFERENCE_GPU) != 0};
