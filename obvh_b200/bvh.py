@@ -1,0 +1,106 @@
+"""BVH builds and transforms through the C ABI (include/obvh_lbvh.h,
+include/obvh_transforms.h).  Device buffers are torch tensors (raw bytes for
+the 36-byte kr_bvh_node records); numpy views use the NODE dtype.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native
+
+NODE = np.dtype([("b", "<f4", (6,)), ("left", "<u4"), ("right", "<u4"), ("n_prims", "<u2"),
+                 ("axis", "u1"), ("pad", "u1")])
+NODE_BYTES = 36
+assert NODE.itemsize == NODE_BYTES
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(torch, stream):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def nodes_numpy(t) -> np.ndarray:
+    """A device node buffer (uint8 [k*36]) as a numpy NODE array."""
+    return t.cpu().numpy().view(NODE).reshape(-1)
+
+
+def as_faces4(faces) -> np.ndarray:
+    f = np.ascontiguousarray(faces, dtype=np.uint32)
+    if f.shape[1] == 3:
+        f = np.concatenate([f, np.zeros((f.shape[0], 1), np.uint32)], axis=1)
+    return np.ascontiguousarray(f)
+
+
+class Mesh:
+    """A triangle mesh resident on the device (vertices float32 [V,3], faces
+    uint32 [F,4] stored in an int32 tensor)."""
+
+    def __init__(self, verts, faces, device="cuda"):
+        import torch
+        v = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 3)
+        f = as_faces4(faces)
+        self.n_vertices = v.shape[0]
+        self.n_faces = f.shape[0]
+        self.verts = torch.from_numpy(v).to(device)
+        self.faces = torch.from_numpy(f.view(np.int32)).to(device)
+
+
+class LbvhBuilder:
+    """obvh_lbvh_build_async with a workspace kept between builds."""
+
+    def __init__(self, device="cuda"):
+        import torch
+        self.torch = torch
+        self.device = torch.device(device)
+        self.lib = _native.lib()
+        self.ws = None
+        self.ws_prims = -1
+
+    def _workspace(self, n, stream):
+        if self.ws is None or n > self.ws_prims:
+            nbytes = int(self.lib.obvh_lbvh_workspace_bytes(n))
+            self.ws = self.torch.empty(nbytes, dtype=self.torch.uint8, device=self.device)
+            self.ws_prims = n
+            _native.check(self.lib.obvh_lbvh_workspace_init(_ptr(self.ws), n, stream))
+        return self.ws
+
+    def build(self, mesh: Mesh, stream=None, out=None):
+        """Enqueues the build; returns dict(nodes, parents, counts, costs, bounds) of device tensors."""
+        t = self.torch
+        n = mesh.n_faces
+        nn = 2 * n - 1
+        s = _stream(t, stream)
+        ws = self._workspace(n, s)
+        if out is None:
+            out = {
+                "nodes": t.empty(nn * NODE_BYTES, dtype=t.uint8, device=self.device),
+                "parents": t.empty(nn, dtype=t.int32, device=self.device),
+                "counts": t.empty(nn, dtype=t.int32, device=self.device),
+                "costs": t.empty(nn, dtype=t.float32, device=self.device),
+                "bounds": t.empty(12, dtype=t.float32, device=self.device),
+            }
+        e = self.lib.obvh_lbvh_build_async(_ptr(mesh.verts), _ptr(mesh.faces), n, _ptr(out["nodes"]),
+                                           _ptr(out["parents"]), _ptr(out["counts"]), _ptr(out["costs"]),
+                                           _ptr(out["bounds"]), _ptr(ws), s)
+        _native.check(e)
+        return out
+
+
+def bbox_calculate(mesh: Mesh, centroid: bool = False, prefill=None):
+    """kr_cuda_bbox_calculate / kr_cuda_centroid_bbox_calculate on a device mesh;
+    returns the 6 floats of the (pre-filled, default empty) box after the call."""
+    import torch
+    lib = _native.lib()
+    big = np.float32(3.402823466e+38)
+    init = np.array([big, big, big, -big, -big, -big], np.float32) if prefill is None else np.asarray(prefill,
+                                                                                                       np.float32)
+    box = torch.from_numpy(init.copy()).cuda()
+    f = lib.kr_cuda_centroid_bbox_calculate if centroid else lib.kr_cuda_bbox_calculate
+    _native.check(f(_ptr(mesh.faces), _ptr(mesh.verts), mesh.n_faces, _ptr(box)))
+    return box.cpu().numpy()

@@ -1,0 +1,428 @@
+// lbvh.cu - linear BVH over triangles: the reference's lbvh_gpu build
+// (src/ads/lbvh_gpu/lbvh.cu:1646-1690) as a chain of kernels on one stream.
+//
+//   tri_bounds   one pass over faces + vertices: every triangle's AABB (kept
+//                for the leaves) and the scene and centroid AABBs (per-CTA
+//                records, the last CTA reduces; kr_cuda_bbox_calculate and
+//                kr_cuda_centroid_bbox_calculate, transforms.cu:1127-1250)
+//   morton       30-bit codes of the centroids normalised by the centroid
+//                AABB (mortons_kernel, lbvh.cu:252-282)
+//   radix sort   stable (key, index) sort (sort.cu; thrust::stable_sort_by_key
+//                over the 36-byte leaves in the reference, lbvh.cu:1670)
+//   leaves       sorted leaves gathered once: bounds, primitive index
+//   karras       radix tree (radix_tree_build_kernel, lbvh.cu:284-396)
+//   aabb_up      bottom-up bounds, primitive counts and SAH costs with an
+//                arrival counter per node (calculate_aabbs_kernel, :399-457)
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+
+#include "device_common.cuh"
+#include "lbvh_host.h"
+#include "obvh_lbvh.h"
+#include "obvh_transforms.h"
+#include "runtime.h"
+#include "sort.h"
+#include "tree_device.cuh"
+
+namespace obvh {
+namespace lbvh {
+
+using tree::kmax;
+using tree::kmin;
+
+constexpr int kThreads = 256;
+constexpr int kMaxGrid = 1024;
+
+struct BoundsRec {
+    float v[12];  // scene lo, scene hi, centroid lo, centroid hi
+};
+
+struct Ctl {
+    uint32_t ticket;
+    uint32_t error;
+    uint32_t pad[62];
+};
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void tri_box(const kr_vec3* verts, uint4 f, f3& lo, f3& hi) {
+    const f3 a = tree::load_vertex(verts, f.x), b = tree::load_vertex(verts, f.y), c = tree::load_vertex(verts, f.z);
+    lo = a;  // kr_aabb_create3(va, va), then expand by vb, vc
+    hi = a;
+    lo = tree::vmin3(lo, b);
+    hi = tree::vmax3(hi, b);
+    lo = tree::vmin3(lo, c);
+    hi = tree::vmax3(hi, c);
+}
+
+__device__ __forceinline__ float warp_red(float v, bool is_min) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        float t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = is_min ? fminf(v, t) : fmaxf(v, t);
+    }
+    return v;
+}
+
+// One pass over the triangles: per-triangle AABB (optional) and the scene and
+// centroid AABBs (each output nullable).  With `overwrite` the outputs are
+// replaced, otherwise expanded, as the reference's atomics expand the box the
+// caller pre-filled.
+__global__ void __launch_bounds__(kThreads) tri_bounds_kernel(const kr_vec3* verts, const uint4* faces, uint32_t n,
+                                                              float* tri_boxes, BoundsRec* recs, Ctl* ctl,
+                                                              kr_aabb3* scene_out, kr_aabb3* centroid_out,
+                                                              bool overwrite) {
+    float acc[12];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        acc[k] = kInf; acc[3 + k] = -kInf; acc[6 + k] = kInf; acc[9 + k] = -kInf;
+    }
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        f3 lo, hi;
+        tri_box(verts, __ldg(faces + i), lo, hi);
+        if (tri_boxes) {
+            float* b = tri_boxes + 6 * static_cast<size_t>(i);
+            b[0] = lo.x; b[1] = lo.y; b[2] = lo.z; b[3] = hi.x; b[4] = hi.y; b[5] = hi.z;
+        }
+        const f3 c = tree::mulv(add3(lo, hi), 0.5f);  // kr_aabb_center3
+        acc[0] = fminf(acc[0], lo.x); acc[1] = fminf(acc[1], lo.y); acc[2] = fminf(acc[2], lo.z);
+        acc[3] = fmaxf(acc[3], hi.x); acc[4] = fmaxf(acc[4], hi.y); acc[5] = fmaxf(acc[5], hi.z);
+        acc[6] = fminf(acc[6], c.x); acc[7] = fminf(acc[7], c.y); acc[8] = fminf(acc[8], c.z);
+        acc[9] = fmaxf(acc[9], c.x); acc[10] = fmaxf(acc[10], c.y); acc[11] = fmaxf(acc[11], c.z);
+    }
+    __shared__ float s[kThreads / 32][12];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = warp_red(acc[k], (k % 6) < 3);
+    if (lane == 0)
+        for (int k = 0; k < 12; ++k) s[warp][k] = acc[k];
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        const int k = threadIdx.x;
+        float v = s[0][k];
+        for (int w = 1; w < kThreads / 32; ++w) v = ((k % 6) < 3) ? fminf(v, s[w][k]) : fmaxf(v, s[w][k]);
+        recs[blockIdx.x].v[k] = v;
+    }
+    __shared__ uint32_t last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&ctl->ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x < 12) {
+        const int k = threadIdx.x;
+        const bool mn = (k % 6) < 3;
+        float v = mn ? kInf : -kInf;
+        for (uint32_t r = 0; r < gridDim.x; ++r) {
+            float o = __ldcg(&recs[r].v[k]);
+            v = mn ? fminf(v, o) : fmaxf(v, o);
+        }
+        kr_aabb3* box = k < 6 ? scene_out : centroid_out;
+        if (box) {
+            float* dst = reinterpret_cast<float*>(box) + (k % 6);
+            if (!overwrite) v = mn ? kmin(*dst, v) : kmax(*dst, v);
+            *dst = v;
+        }
+    }
+    if (threadIdx.x == 0) ctl->ticket = 0;
+}
+
+// 30-bit Morton code of the triangle centroid (mortons_kernel); value = index.
+__device__ __forceinline__ uint32_t stretch3(uint32_t x) {
+    x &= 0x3ffu;
+    x = (x | (x << 16)) & 0x30000ffu;
+    x = (x | (x << 8)) & 0x300f00fu;
+    x = (x | (x << 4)) & 0x30c30c3u;
+    x = (x | (x << 2)) & 0x9249249u;
+    return x;
+}
+
+__device__ __forceinline__ uint32_t morton30(f3 c) {  // kr_v32morton3
+    const float q[3] = {c.x, c.y, c.z};
+    uint32_t code = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) code |= stretch3(static_cast<uint32_t>(kmin(kmax(q[k] * 1024.0f, 0.0f), 1023.0f)))
+                                       << (2 - k);
+    return code;
+}
+
+__global__ void __launch_bounds__(kThreads) morton_kernel(const float* tri_boxes, uint32_t n, const kr_aabb3* boxes,
+                                                          uint32_t* keys, uint32_t* vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* cb = reinterpret_cast<const float*>(boxes + 1);  // centroid box
+    const f3 cmin = mk3(cb[0], cb[1], cb[2]);
+    const f3 ext = sub3(mk3(cb[3], cb[4], cb[5]), cmin);
+    const f3 neg = mk3(-cmin.x, -cmin.y, -cmin.z);
+    const float* b = tri_boxes + 6 * static_cast<size_t>(i);
+    const f3 lo = add3(mk3(b[0], b[1], b[2]), neg), hi = add3(mk3(b[3], b[4], b[5]), neg);  // kr_aabb_offset3
+    f3 c = tree::mulv(add3(lo, hi), 0.5f);
+    c = mk3(ext.x != 0 ? c.x / ext.x : 0.f, ext.y != 0 ? c.y / ext.y : 0.f, ext.z != 0 ? c.z / ext.z : 0.f);  // kr_vdiv3s
+    keys[i] = morton30(c);
+    vals[i] = i;
+}
+
+// Sorted leaf j -> node internal + j.
+__global__ void __launch_bounds__(kThreads) leaves_kernel(const float* tri_boxes, const uint32_t* order, uint32_t n,
+                                                          kr_bvh_node* nodes) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t i = order[j];
+    const float* b = tri_boxes + 6 * static_cast<size_t>(i);
+    uint32_t* w = reinterpret_cast<uint32_t*>(nodes + (n - 1) + j);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) w[k] = __float_as_uint(b[k]);
+    w[6] = i;  // primitivesOffset
+    w[7] = 0;
+    w[8] = 1;  // nPrimitives = 1, axis = 0
+}
+
+__device__ __forceinline__ int delta(const uint32_t* codes, int i, int j, uint32_t n) {
+    if (j > static_cast<int>(n) - 1 || j < 0) return -1;
+    const uint32_t a = codes[i], b = codes[j];
+    if (a == b) return 32 + __clz(static_cast<uint32_t>(i) ^ static_cast<uint32_t>(j));
+    return __clz(a ^ b);
+}
+
+__device__ __forceinline__ int halve_up(int x) { return x == 1 ? 0 : ((x % 2) == 1 ? x / 2 + 1 : x / 2); }
+
+__global__ void __launch_bounds__(kThreads) karras_kernel(const uint32_t* codes, uint32_t n, kr_bvh_node* nodes,
+                                                          uint32_t* parents) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t internal = n - 1;
+    if (i >= static_cast<int>(internal)) return;
+    const int da = delta(codes, i, i + 1, n), db = delta(codes, i, i - 1, n);
+    const int d = (da - db > 0) - (da - db < 0);
+    const int dmin = delta(codes, i, i - d, n);
+    int lmax = 2;
+    while (delta(codes, i, i + lmax * d, n) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (delta(codes, i, i + (l + t) * d, n) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = delta(codes, i, j, n);
+    int s = 0;
+    for (int t = halve_up(l); t >= 1; t = halve_up(t))
+        if (delta(codes, i, i + (s + t) * d, n) > dnode) s += t;
+    const int split = i + s * d + (d < 0 ? d : 0);
+    const int lo = i < j ? i : j, hi = i < j ? j : i;
+    const uint32_t left = static_cast<uint32_t>(split) + (lo == split ? internal : 0u);
+    const uint32_t right = static_cast<uint32_t>(split) + 1u + (hi == split + 1 ? internal : 0u);
+    parents[left] = static_cast<uint32_t>(i);
+    parents[right] = static_cast<uint32_t>(i);
+    uint32_t* w = reinterpret_cast<uint32_t*>(nodes + i);
+    const uint32_t big = __float_as_uint(3.402823466e+38f), nbig = __float_as_uint(-3.402823466e+38f);
+    w[0] = w[1] = w[2] = big;  // kr_aabb_empty3
+    w[3] = w[4] = w[5] = nbig;
+    w[6] = left;
+    w[7] = right;
+    w[8] = 0;  // nPrimitives 0, axis 0
+    if (i == 0) parents[0] = tree::kNoParent;
+}
+
+// Bottom-up bounds, counts and costs; the second thread to reach a node
+// continues (ct = 1, ci = 1.2 as hard-coded at lbvh.cu:421-422).
+__global__ void __launch_bounds__(kThreads) aabb_up_kernel(kr_bvh_node* nodes, const uint32_t* parents,
+                                                           uint32_t* counts, float* costs, uint32_t* visits,
+                                                           uint32_t n, uint32_t* err) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t internal = n - 1;
+    const uint32_t leaf = internal + j;
+    {
+        const tree::NodeView lf = tree::load_node(nodes, leaf);
+        __stcg(costs + leaf, 1.0f * tree::box_area(lf.lo, lf.hi));
+        __stcg(counts + leaf, 1u);
+    }
+    uint32_t p = parents[leaf];
+    for (uint32_t steps = 0; p != tree::kNoParent; ++steps) {
+        if (steps > internal || p >= internal) {
+            atomicOr(err, kErrCycle);
+            return;
+        }
+        __threadfence();
+        if (atomicAdd(visits + p, 1u) == 0) return;
+        __threadfence();
+        const tree::NodeView pn = tree::load_node(nodes, p);
+        const tree::NodeView L = tree::load_node(nodes, pn.left), R = tree::load_node(nodes, pn.right);
+        float lo[3], hi[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {  // kr_aabb_expand(left, right)
+            lo[k] = kmin(kmin(L.lo[k], R.lo[k]), R.hi[k]);
+            hi[k] = kmax(kmax(L.hi[k], R.lo[k]), R.hi[k]);
+        }
+        uint32_t* w = reinterpret_cast<uint32_t*>(nodes + p);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            __stcg(w + k, __float_as_uint(lo[k]));
+            __stcg(w + 3 + k, __float_as_uint(hi[k]));
+        }
+        __stcg(counts + p, __ldcg(counts + pn.left) + __ldcg(counts + pn.right));
+        __stcg(costs + p, 1.2f * tree::box_area(lo, hi) + __ldcg(costs + pn.right) + __ldcg(costs + pn.left));
+        p = parents[p];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+Layout layout(uint32_t n) {
+    Layout L;
+    size_t o = 0;
+    L.ctl = o;        o += align256(sizeof(Ctl));
+    L.recs = o;       o += align256(sizeof(BoundsRec) * kMaxGrid);
+    L.boxes = o;      o += align256(sizeof(kr_aabb3) * 2);
+    L.tri = o;        o += align256(24ull * n);
+    L.keys0 = o;      o += align256(4ull * n);
+    L.keys1 = o;      o += align256(4ull * n);
+    L.vals0 = o;      o += align256(4ull * n);
+    L.vals1 = o;      o += align256(4ull * n);
+    L.visits = o;     o += align256(4ull * (n > 0 ? n : 1));
+    L.sort = o;       o += align256(radix_sort_temp_bytes(n));
+    L.total = o;
+    return L;
+}
+
+int bounds_grid(uint32_t n) {
+    int g = 2 * device_info().sm_count;
+    const int need = static_cast<int>((n + kThreads - 1) / kThreads);
+    if (need < g) g = need;
+    if (g < 1) g = 1;
+    if (g > kMaxGrid) g = kMaxGrid;
+    return g;
+}
+
+kr_error enqueue_bounds(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, float* tri_boxes, char* ws,
+                        kr_aabb3* scene_out, kr_aabb3* centroid_out, bool overwrite, cudaStream_t s) {
+    const Layout L = layout(0);
+    tri_bounds_kernel<<<bounds_grid(n), kThreads, 0, s>>>(verts, reinterpret_cast<const uint4*>(faces), n, tri_boxes,
+                                                          reinterpret_cast<BoundsRec*>(ws + L.recs),
+                                                          reinterpret_cast<Ctl*>(ws + L.ctl), scene_out, centroid_out,
+                                                          overwrite);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    return kr_success;
+}
+
+kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, kr_bvh_node* nodes,
+                       uint32_t* parents, uint32_t* counts, float* costs, kr_aabb3* bounds_out, void* workspace,
+                       cudaStream_t s) {
+    if (n < 1) return "obvh_lbvh_build: at least one primitive is needed";
+    if (!verts || !faces || !nodes || !parents || !counts || !costs || !workspace)
+        return "obvh_lbvh_build: null pointer argument";
+    if (reinterpret_cast<uintptr_t>(workspace) & 255) return "obvh_lbvh_build: workspace must be 256-byte aligned";
+    char* ws = static_cast<char*>(workspace);
+    const Layout L = layout(n);
+    float* tri = reinterpret_cast<float*>(ws + L.tri);
+    kr_aabb3* boxes = reinterpret_cast<kr_aabb3*>(ws + L.boxes);
+    uint32_t* err = &reinterpret_cast<Ctl*>(ws + L.ctl)->error;
+    const unsigned grid_n = (n + kThreads - 1) / kThreads;
+
+    OBVH_TRY(enqueue_bounds(verts, faces, n, tri, ws, boxes, boxes + 1, true, s));
+    morton_kernel<<<grid_n, kThreads, 0, s>>>(tri, n, boxes, reinterpret_cast<uint32_t*>(ws + L.keys0),
+                                              reinterpret_cast<uint32_t*>(ws + L.vals0));
+    OBVH_TRY_CUDA(cudaGetLastError());
+    bool alt = false;
+    OBVH_TRY(radix_sort_pairs(ws + L.keys0, ws + L.keys1, reinterpret_cast<uint32_t*>(ws + L.vals0),
+                              reinterpret_cast<uint32_t*>(ws + L.vals1), n, 4, 0, 30, ws + L.sort, s, &alt));
+    const uint32_t* codes = reinterpret_cast<const uint32_t*>(ws + (alt ? L.keys1 : L.keys0));
+    const uint32_t* order = reinterpret_cast<const uint32_t*>(ws + (alt ? L.vals1 : L.vals0));
+    leaves_kernel<<<grid_n, kThreads, 0, s>>>(tri, order, n, nodes);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    if (n >= 2) {
+        karras_kernel<<<(n - 1 + kThreads - 1) / kThreads, kThreads, 0, s>>>(codes, n, nodes, parents);
+        OBVH_TRY_CUDA(cudaGetLastError());
+        OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.visits, 0, 4ull * (n - 1), s));
+    } else {
+        OBVH_TRY_CUDA(cudaMemsetAsync(parents, 0xff, sizeof(uint32_t), s));
+    }
+    aabb_up_kernel<<<grid_n, kThreads, 0, s>>>(nodes, parents, counts, costs, reinterpret_cast<uint32_t*>(ws + L.visits),
+                                               n, err);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    if (bounds_out)
+        OBVH_TRY_CUDA(cudaMemcpyAsync(bounds_out, boxes, 2 * sizeof(kr_aabb3), cudaMemcpyDeviceToDevice, s));
+    return kr_success;
+}
+
+const uint32_t* sorted_codes(const void* workspace, uint32_t n) {
+    // the radix sort of 30-bit keys makes 4 passes: the result is in keys0/vals0
+    return reinterpret_cast<const uint32_t*>(static_cast<const char*>(workspace) + layout(n).keys0);
+}
+
+uint32_t* error_word(void* workspace) { return &reinterpret_cast<Ctl*>(static_cast<char*>(workspace))->error; }
+
+// Per-device cached workspace for the synchronous reference entry points.
+struct SyncContext {
+    std::mutex mutex;
+    DeviceBuffer ws;
+    bool zeroed = false;
+};
+
+SyncContext& sync_context() {
+    static std::mutex m;
+    static std::unordered_map<int, SyncContext*> ctxs;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(m);
+    SyncContext*& c = ctxs[dev];
+    if (!c) c = new SyncContext();
+    return *c;
+}
+
+kr_error bbox_sync(const kr_uvec4* faces, const kr_vec3* verts, uint32_t n, kr_aabb3* d_aabb, bool centroid) {
+    if (!d_aabb || (n > 0 && (!faces || !verts))) return "kr_cuda_bbox_calculate: null pointer argument";
+    if (n == 0) return kr_success;
+    SyncContext& c = sync_context();
+    std::lock_guard<std::mutex> lock(c.mutex);
+    OBVH_TRY(c.ws.reserve(layout(0).total));
+    if (!c.zeroed) {
+        OBVH_TRY_CUDA(cudaMemset(c.ws.ptr, 0, layout(0).total));
+        c.zeroed = true;
+    }
+    OBVH_TRY(enqueue_bounds(verts, faces, n, nullptr, static_cast<char*>(c.ws.ptr), centroid ? nullptr : d_aabb,
+                            centroid ? d_aabb : nullptr, false, nullptr));
+    OBVH_TRY_CUDA(cudaStreamSynchronize(nullptr));
+    return kr_success;
+}
+
+}  // namespace lbvh
+}  // namespace obvh
+
+using namespace obvh;
+
+extern "C" kr_error kr_cuda_bbox_calculate(const kr_uvec4* faces, const kr_vec3* vertices, kr_u32 face_count,
+                                           kr_aabb3* aabb) {
+    kr_error e = lbvh::bbox_sync(faces, vertices, face_count, aabb, false);
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error kr_cuda_centroid_bbox_calculate(const kr_uvec4* faces, const kr_vec3* vertices, kr_u32 face_count,
+                                                    kr_aabb3* aabb) {
+    kr_error e = lbvh::bbox_sync(faces, vertices, face_count, aabb, true);
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_size obvh_lbvh_workspace_bytes(kr_u32 primitive_count) { return lbvh::layout(primitive_count).total; }
+
+extern "C" kr_error obvh_lbvh_build_async(const kr_vec3* d_vertices, const kr_uvec4* d_faces, kr_u32 face_count,
+                                          kr_bvh_node* d_nodes, kr_u32* d_parents, kr_u32* d_primitive_counts,
+                                          kr_scalar* d_costs, kr_aabb3* d_bounds, void* d_workspace, void* stream) {
+    kr_error e = lbvh::enqueue_build(d_vertices, d_faces, face_count, d_nodes, d_parents, d_primitive_counts, d_costs,
+                                     d_bounds, d_workspace, static_cast<cudaStream_t>(stream));
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error obvh_lbvh_workspace_init(void* d_workspace, kr_u32 primitive_count, void* stream) {
+    if (!d_workspace) return "obvh_lbvh_workspace_init: null workspace";
+    cudaError_t e = cudaMemsetAsync(d_workspace, 0, lbvh::layout(primitive_count).ctl + 256,
+                                    static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? kr_success : cuda_error(e);
+}

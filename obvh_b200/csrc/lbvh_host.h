@@ -1,0 +1,36 @@
+// lbvh_host.h - host-side interface of the LBVH builder (lbvh.cu) for the
+// other builders and the plugins.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "obvh_types.h"
+
+namespace obvh {
+namespace lbvh {
+
+// Byte offsets inside an LBVH workspace of n primitives.
+struct Layout {
+    size_t ctl, recs, boxes, tri, keys0, keys1, vals0, vals1, visits, sort, total;
+};
+Layout layout(uint32_t n);
+
+// Scene/centroid bounds of the triangles (either output nullable); with
+// `overwrite` false the outputs are expanded like the reference's atomics.
+kr_error enqueue_bounds(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, float* tri_boxes, char* ws,
+                        kr_aabb3* scene_out, kr_aabb3* centroid_out, bool overwrite, cudaStream_t s);
+
+// Full build into caller buffers (nodes/parents/counts/costs of 2n-1 entries).
+kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, kr_bvh_node* nodes,
+                       uint32_t* parents, uint32_t* counts, float* costs, kr_aabb3* bounds_out, void* workspace,
+                       cudaStream_t s);
+
+// The sorted Morton codes left in the workspace by the last build of n primitives.
+const uint32_t* sorted_codes(const void* workspace, uint32_t n);
+uint32_t* error_word(void* workspace);
+
+}  // namespace lbvh
+}  // namespace obvh

@@ -1,0 +1,30 @@
+// sort.h - device-wide primitives used by the BVH builders: exclusive scan of
+// u32 and a stable LSD radix sort of (key, u32 value) pairs with u32 or u64
+// keys.  Both only enqueue work on the given stream and use caller-provided
+// temporary storage (query its size with the *_temp_bytes functions).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "obvh_types.h"
+
+namespace obvh {
+
+size_t scan_temp_bytes(uint64_t n);
+// out[i] = sum of in[0..i); in == out allowed.  If total != nullptr the sum of
+// all inputs is written there (device pointer).
+kr_error exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* total, void* temp,
+                            cudaStream_t stream);
+
+size_t radix_sort_temp_bytes(uint64_t n);
+// Stable sort of keys[0..n) (key_bytes 4 or 8) with their values by bits
+// [begin_bit, end_bit).  keys/vals hold the input; keys_alt/vals_alt are
+// scratch of the same size.  On return *in_alt says whether the sorted data
+// ended in the *_alt buffers.
+kr_error radix_sort_pairs(void* keys, void* keys_alt, uint32_t* vals, uint32_t* vals_alt, uint64_t n, int key_bytes,
+                          int begin_bit, int end_bit, void* temp, cudaStream_t stream, bool* in_alt);
+
+}  // namespace obvh

@@ -1,0 +1,366 @@
+// tree_device.cuh - device pieces shared by the BVH kernels: node layout,
+// the reference's GPU-side vector semantics, 4x4 matrices, and the per-node
+// DiTO-14 candidate search of the OBB-tree transform.
+//
+// The reference evaluates these on the GPU (src/ads/common/cuda/transforms.cu
+// with src/common/vecmath.h): normalisation divides by the length
+// (kr_vnormalize3), kr_min/kr_max are "(a < b) ? a : b" / "(a < b) ? b : a",
+// cross products form y as az*bx - ax*bz.  Everything here is compiled
+// uncontracted (--fmad=false), i.e. the reference built with --fmad=false.
+#pragma once
+
+#include <cstdint>
+
+#include "device_common.cuh"
+#include "obvh_types.h"
+
+namespace obvh {
+namespace tree {
+
+constexpr uint32_t kNoParent = 0xffffffffu;
+
+// kr_bvh_node field access through 4-byte words (the struct is 36 bytes,
+// 4-byte aligned): words 0..5 bounds, 6 left|primitivesOffset, 7 right,
+// 8 nPrimitives | axis << 16.
+struct NodeView {
+    float lo[3], hi[3];
+    uint32_t left, right;
+    uint32_t nprims;  // low 16 bits of word 8
+};
+
+__device__ __forceinline__ NodeView load_node(const kr_bvh_node* nodes, uint32_t i) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(nodes + i);
+    NodeView n;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        n.lo[k] = __uint_as_float(__ldcg(w + k));
+        n.hi[k] = __uint_as_float(__ldcg(w + 3 + k));
+    }
+    n.left = __ldcg(w + 6);
+    n.right = __ldcg(w + 7);
+    n.nprims = __ldcg(w + 8) & 0xffffu;
+    return n;
+}
+
+__device__ __forceinline__ float kmin(float a, float b) { return (a < b) ? a : b; }
+__device__ __forceinline__ float kmax(float a, float b) { return (a < b) ? b : a; }
+__device__ __forceinline__ f3 vmin3(f3 a, f3 b) { return mk3(kmin(a.x, b.x), kmin(a.y, b.y), kmin(a.z, b.z)); }
+__device__ __forceinline__ f3 vmax3(f3 a, f3 b) { return mk3(kmax(a.x, b.x), kmax(a.y, b.y), kmax(a.z, b.z)); }
+__device__ __forceinline__ f3 cross3(f3 a, f3 b) {
+    return mk3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ f3 unit3(f3 a) {
+    float l = sqrtf(len2_3(a));
+    return mk3(a.x / l, a.y / l, a.z / l);
+}
+__device__ __forceinline__ f3 mulv(f3 a, float s) { return mk3(a.x * s, a.y * s, a.z * s); }
+
+// kr_aabb_surface_area3
+__device__ __forceinline__ float box_area(const float* lo, const float* hi) {
+    float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return 2.0f * (dx * dy + dx * dz + dy * dz);
+}
+
+__device__ __forceinline__ f3 load_vertex(const kr_vec3* verts, uint32_t i) {
+    const float* p = reinterpret_cast<const float*>(verts) + 3 * static_cast<size_t>(i);
+    return mk3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
+}
+
+// ---------------------------------------------------------------------------
+// 4x4 matrices (column-major, kr_mat4).
+struct M4 {
+    float v[16];
+};
+
+// kr_minverse4 (vecmath.h:946-1076): each adjugate entry is a signed sum of
+// six triple products in the reference's order; then det and 1/det scaling.
+__device__ __forceinline__ float adj_term(const M4& m, int s, int a, int b, int c, float acc, bool first) {
+    float p = m.v[a] * m.v[b] * m.v[c];
+    if (first) return s < 0 ? -p : p;
+    return s < 0 ? acc - p : acc + p;
+}
+
+__device__ inline M4 minverse4(const M4& m) {
+    // sign, factor, factor, factor for the 6 terms of each of the 16 entries
+    constexpr signed char T[16][6][4] = {
+        {{1, 5, 10, 15}, {-1, 5, 11, 14}, {-1, 9, 6, 15}, {1, 9, 7, 14}, {1, 13, 6, 11}, {-1, 13, 7, 10}},
+        {{-1, 1, 10, 15}, {1, 1, 11, 14}, {1, 9, 2, 15}, {-1, 9, 3, 14}, {-1, 13, 2, 11}, {1, 13, 3, 10}},
+        {{1, 1, 6, 15}, {-1, 1, 7, 14}, {-1, 5, 2, 15}, {1, 5, 3, 14}, {1, 13, 2, 7}, {-1, 13, 3, 6}},
+        {{-1, 1, 6, 11}, {1, 1, 7, 10}, {1, 5, 2, 11}, {-1, 5, 3, 10}, {-1, 9, 2, 7}, {1, 9, 3, 6}},
+        {{-1, 4, 10, 15}, {1, 4, 11, 14}, {1, 8, 6, 15}, {-1, 8, 7, 14}, {-1, 12, 6, 11}, {1, 12, 7, 10}},
+        {{1, 0, 10, 15}, {-1, 0, 11, 14}, {-1, 8, 2, 15}, {1, 8, 3, 14}, {1, 12, 2, 11}, {-1, 12, 3, 10}},
+        {{-1, 0, 6, 15}, {1, 0, 7, 14}, {1, 4, 2, 15}, {-1, 4, 3, 14}, {-1, 12, 2, 7}, {1, 12, 3, 6}},
+        {{1, 0, 6, 11}, {-1, 0, 7, 10}, {-1, 4, 2, 11}, {1, 4, 3, 10}, {1, 8, 2, 7}, {-1, 8, 3, 6}},
+        {{1, 4, 9, 15}, {-1, 4, 11, 13}, {-1, 8, 5, 15}, {1, 8, 7, 13}, {1, 12, 5, 11}, {-1, 12, 7, 9}},
+        {{-1, 0, 9, 15}, {1, 0, 11, 13}, {1, 8, 1, 15}, {-1, 8, 3, 13}, {-1, 12, 1, 11}, {1, 12, 3, 9}},
+        {{1, 0, 5, 15}, {-1, 0, 7, 13}, {-1, 4, 1, 15}, {1, 4, 3, 13}, {1, 12, 1, 7}, {-1, 12, 3, 5}},
+        {{-1, 0, 5, 11}, {1, 0, 7, 9}, {1, 4, 1, 11}, {-1, 4, 3, 9}, {-1, 8, 1, 7}, {1, 8, 3, 5}},
+        {{-1, 4, 9, 14}, {1, 4, 10, 13}, {1, 8, 5, 14}, {-1, 8, 6, 13}, {-1, 12, 5, 10}, {1, 12, 6, 9}},
+        {{1, 0, 9, 14}, {-1, 0, 10, 13}, {-1, 8, 1, 14}, {1, 8, 2, 13}, {1, 12, 1, 10}, {-1, 12, 2, 9}},
+        {{-1, 0, 5, 14}, {1, 0, 6, 13}, {1, 4, 1, 14}, {-1, 4, 2, 13}, {-1, 12, 1, 6}, {1, 12, 2, 5}},
+        {{1, 0, 5, 10}, {-1, 0, 6, 9}, {-1, 4, 1, 10}, {1, 4, 2, 9}, {1, 8, 1, 6}, {-1, 8, 2, 5}},
+    };
+    M4 ret;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        float acc = 0.f;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) acc = adj_term(m, T[e][t][0], T[e][t][1], T[e][t][2], T[e][t][3], acc, t == 0);
+        ret.v[e] = acc;
+    }
+    float det = m.v[0] * ret.v[0] + m.v[1] * ret.v[4] + m.v[2] * ret.v[8] + m.v[3] * ret.v[12];
+    M4 inv;
+    if (det == 0) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) inv.v[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+        return inv;
+    }
+    det = 1.0f / det;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) inv.v[i] = ret.v[i] * det;
+    return inv;
+}
+
+// kr_mmul4 (vecmath.h:1214-1236)
+__device__ __forceinline__ M4 mmul4(const M4& l, const M4& r) {
+    M4 o;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int row = 0; row < 4; ++row)
+            o.v[4 * c + row] = l.v[row] * r.v[4 * c] + l.v[4 + row] * r.v[4 * c + 1] + l.v[8 + row] * r.v[4 * c + 2] +
+                               l.v[12 + row] * r.v[4 * c + 3];
+    return o;
+}
+
+// kr_mobb3: the axes as the first three columns
+__device__ __forceinline__ M4 mframe(f3 a, f3 b, f3 c) {
+    return M4{{a.x, a.y, a.z, 0, b.x, b.y, b.z, 0, c.x, c.y, c.z, 0, 0, 0, 0, 1}};
+}
+
+// kr_mvmul43
+__device__ __forceinline__ f3 mtransform(const M4& l, f3 r) {
+    return mk3(l.v[0] * r.x + l.v[4] * r.y + l.v[8] * r.z + l.v[12],
+               l.v[1] * r.x + l.v[5] * r.y + l.v[9] * r.z + l.v[13],
+               l.v[2] * r.x + l.v[6] * r.y + l.v[10] * r.z + l.v[14]);
+}
+
+// Writes obb (mid, axes, ext clamped to 0.001) and transform = inverse of
+// T(mid) R(axes) S(2 ext) for the box [lo, hi] in the frame's coordinates
+// (transforms.cu:826-834 and :928-963).
+__device__ inline void write_box(kr_obb3* obb, kr_mat4* xf, f3 a0, f3 a1, f3 a2, f3 lo, f3 hi) {
+    f3 m = mulv(add3(lo, hi), 0.5f);
+    f3 ext = vmax3(mulv(sub3(hi, lo), 0.5f), mk3(0.001f, 0.001f, 0.001f));
+    f3 mid = mulv(a0, m.x);
+    mid = add3(mid, mulv(a1, m.y));
+    mid = add3(mid, mulv(a2, m.z));
+    float* o = reinterpret_cast<float*>(obb);
+    o[0] = mid.x; o[1] = mid.y; o[2] = mid.z;
+    o[3] = a0.x; o[4] = a0.y; o[5] = a0.z;
+    o[6] = a1.x; o[7] = a1.y; o[8] = a1.z;
+    o[9] = a2.x; o[10] = a2.y; o[11] = a2.z;
+    o[12] = ext.x; o[13] = ext.y; o[14] = ext.z;
+    const M4 r = mframe(a0, a1, a2);
+    const M4 s{{ext.x * 2.0f, 0, 0, 0, 0, ext.y * 2.0f, 0, 0, 0, 0, ext.z * 2.0f, 0, 0, 0, 0, 1}};
+    const M4 t{{1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, mid.x, mid.y, mid.z, 1}};
+    const M4 inv = minverse4(mmul4(t, mmul4(r, s)));
+    float4* x = reinterpret_cast<float4*>(xf);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) x[c] = make_float4(inv.v[4 * c], inv.v[4 * c + 1], inv.v[4 * c + 2], inv.v[4 * c + 3]);
+}
+
+// Leaf OBB from the triangle frame (refit_obbs_kernel_new, transforms.cu:794-834):
+// a0 = e0/|e0|, a2 = e0 x e1 (not normalised), a1 = unit(a0 x a2).
+__device__ inline void leaf_box(f3 v0, f3 v1, f3 v2, kr_obb3* obb, kr_mat4* xf) {
+    const f3 e0 = sub3(v1, v0), e1 = sub3(v2, v0);
+    const f3 a2 = cross3(e0, e1);
+    const f3 a0 = unit3(e0);
+    const f3 a1 = unit3(cross3(a0, a2));
+    const M4 inv = minverse4(mframe(a0, a1, a2));
+    const f3 l0 = mtransform(inv, v0), l1 = mtransform(inv, v1), l2 = mtransform(inv, v2);
+    const f3 hi = vmax3(l0, vmax3(l1, l2));
+    const f3 lo = vmin3(l0, vmin3(l1, l2));
+    write_box(obb, xf, a0, a1, a2, lo, hi);
+}
+
+// ---------------------------------------------------------------------------
+// 7-direction summary of a subtree: per slab the extreme projections and the
+// vertex reaching them.  Stored per internal node as 7 x uint4
+// {min value bits, max value bits, min vertex, max vertex} = 112 bytes.
+struct Summary {
+    float lo[7], hi[7];
+    uint32_t ilo[7], ihi[7];
+};
+
+__device__ __forceinline__ void slab7(f3 p, float s[7]) {
+    s[0] = p.x; s[1] = p.y; s[2] = p.z;
+    s[3] = p.x + p.y + p.z;
+    s[4] = p.x + p.y - p.z;
+    s[5] = p.x - p.y + p.z;
+    s[6] = p.x - p.y - p.z;
+}
+
+// lbvh_dito14_fixed_projections over a triangle (transforms.cu:216-285)
+__device__ inline void leaf_summary(const kr_vec3* verts, uint4 face, Summary& s) {
+    const uint32_t id[3] = {face.x, face.y, face.z};
+    float q[7];
+    slab7(load_vertex(verts, id[0]), q);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) { s.lo[k] = s.hi[k] = q[k]; s.ilo[k] = s.ihi[k] = id[0]; }
+#pragma unroll
+    for (int i = 1; i < 3; ++i) {
+        slab7(load_vertex(verts, id[i]), q);
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            if (q[k] < s.lo[k]) { s.lo[k] = q[k]; s.ilo[k] = id[i]; }
+            if (q[k] > s.hi[k]) { s.hi[k] = q[k]; s.ihi[k] = id[i]; }
+        }
+    }
+}
+
+__device__ __forceinline__ void store_summary(uint4* dst, const Summary& s) {
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+        __stcg(dst + k, make_uint4(__float_as_uint(s.lo[k]), __float_as_uint(s.hi[k]), s.ilo[k], s.ihi[k]));
+}
+
+__device__ __forceinline__ void load_summary(const uint4* src, Summary& s) {
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        uint4 w = __ldcg(src + k);
+        s.lo[k] = __uint_as_float(w.x);
+        s.hi[k] = __uint_as_float(w.y);
+        s.ilo[k] = w.z;
+        s.ihi[k] = w.w;
+    }
+}
+
+// Left child's summary, then the right child's value where strictly better.
+__device__ __forceinline__ void merge_right(Summary& a, const Summary& b) {
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        if (a.lo[k] > b.lo[k]) { a.lo[k] = b.lo[k]; a.ilo[k] = b.ilo[k]; }
+        if (a.hi[k] < b.hi[k]) { a.hi[k] = b.hi[k]; a.ihi[k] = b.ihi[k]; }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// DiTO-14 candidate of one internal node (calculate_candidate_obb_kernel,
+// transforms.cu:676-756, with the helpers at :413-674).  P holds the 14
+// extremal vertices interleaved (min, max) per slab as the reference reads its
+// kr_minmax_pair array.  Outputs the axes and the initial extents along them:
+// on a degenerate base triangle or a flat set the axes are the identity and
+// the extents keep the slab 3..5 values (lo/hi inputs), as in the reference.
+struct Candidate {
+    f3 b0, b1, b2;
+    f3 lo, hi;  // slots 3..5
+};
+
+__device__ __forceinline__ void extent_proj(const f3* P, f3 d, float& lo, float& hi) {
+    lo = hi = dot3(P[0], d);
+#pragma unroll
+    for (int i = 1; i < 14; ++i) {
+        float q = dot3(P[i], d);
+        lo = kmin(lo, q);
+        hi = kmax(hi, q);
+    }
+}
+
+__device__ __forceinline__ void score_frames(const f3* P, f3 n, f3 e0, f3 e1, f3 e2, f3* b, f3& blen, f3& bmid,
+                                             float& best) {
+    const f3 e[3] = {e0, e1, e2};
+    float nlo, nhi;
+    extent_proj(P, n, nlo, nhi);
+    const float dy = nhi - nlo;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const f3 m = cross3(e[k], n);
+        float elo, ehi, mlo, mhi;
+        extent_proj(P, e[k], elo, ehi);
+        extent_proj(P, m, mlo, mhi);
+        const f3 dlen = mk3(ehi - elo, dy, mhi - mlo);
+        const float q = half_area3(dlen);
+        if (q < best) {
+            best = q;
+            bmid = mk3(ehi, nhi, mhi);
+            blen = mk3(elo, nlo, mlo);
+            b[0] = e[k]; b[1] = n; b[2] = m;
+        }
+    }
+}
+
+__device__ inline Candidate node_candidate(const f3* P, const Summary& s) {
+    const float eps = 0.000001f;
+    Candidate c;
+    c.b0 = mk3(1, 0, 0); c.b1 = mk3(0, 1, 0); c.b2 = mk3(0, 0, 1);
+    c.lo = mk3(s.lo[3], s.lo[4], s.lo[5]);
+    c.hi = mk3(s.hi[3], s.hi[4], s.hi[5]);
+    const Candidate stale = c;
+
+    float best = half_area3(mk3(s.hi[0] - s.lo[0], s.hi[1] - s.lo[1], s.hi[2] - s.lo[2]));
+    f3 b[3] = {c.b0, c.b1, c.b2};
+    f3 blen = mk3(s.lo[0], s.lo[1], s.lo[2]), bmid = mk3(s.hi[0], s.hi[1], s.hi[2]);
+
+    int at = 0;
+    float far = len2_3(sub3(P[1], P[0]));
+#pragma unroll
+    for (int k = 1; k < 7; ++k) {
+        float d = len2_3(sub3(P[2 * k + 1], P[2 * k]));
+        if (d > far) { far = d; at = k; }
+    }
+    const f3 p0 = P[2 * at], p1 = P[2 * at + 1];
+    if (len2_3(sub3(p1, p0)) < eps) return stale;
+    const f3 e0 = unit3(sub3(p0, p1));
+    const float l2 = len2_3(e0);
+    int fi = 0;
+    float fd;
+    {
+        f3 u = sub3(P[0], p0);
+        float t = dot3(e0, u);
+        fd = len2_3(u) - t * t / l2;
+#pragma unroll
+        for (int i = 1; i < 14; ++i) {
+            u = sub3(P[i], p0);
+            t = dot3(e0, u);
+            float d = len2_3(u) - t * t / l2;
+            if (d > fd) { fd = d; fi = i; }
+        }
+    }
+    const f3 p2 = P[fi];
+    if (fd < eps) return stale;
+    const f3 e1 = unit3(sub3(p1, p2));
+    const f3 e2 = unit3(sub3(p2, p0));
+    const f3 n = unit3(cross3(e1, e0));
+    score_frames(P, n, e0, e1, e2, b, blen, bmid, best);
+
+    float qlo = dot3(P[0], n), qhi = qlo;
+    f3 q1 = P[0], q0 = P[0];
+#pragma unroll
+    for (int i = 1; i < 14; ++i) {
+        float q = dot3(P[i], n);
+        if (q < qlo) { qlo = q; q1 = P[i]; }
+        if (q > qhi) { qhi = q; q0 = P[i]; }
+    }
+    const float tri = dot3(p0, n);
+    const bool up = qhi - eps > tri, down = qlo + eps < tri;
+    if (!up && !down) return stale;
+    if (up) {
+        const f3 f0 = unit3(sub3(q0, p0)), f1 = unit3(sub3(q0, p1)), f2 = unit3(sub3(q0, p2));
+        score_frames(P, unit3(cross3(f1, e0)), e0, f1, f0, b, blen, bmid, best);
+        score_frames(P, unit3(cross3(f2, e1)), e1, f2, f1, b, blen, bmid, best);
+        score_frames(P, unit3(cross3(f0, e2)), e2, f0, f2, b, blen, bmid, best);
+    }
+    if (down) {
+        const f3 g0 = unit3(sub3(q1, p0)), g1 = unit3(sub3(q1, p1)), g2 = unit3(sub3(q1, p2));
+        score_frames(P, unit3(cross3(g1, e0)), e0, g1, g0, b, blen, bmid, best);
+        score_frames(P, unit3(cross3(g2, e1)), e1, g2, g1, b, blen, bmid, best);
+        score_frames(P, unit3(cross3(g0, e2)), e2, g0, g2, b, blen, bmid, best);
+    }
+    c.b0 = b[0]; c.b1 = b[1]; c.b2 = b[2];
+    c.lo = blen;
+    c.hi = bmid;
+    return c;
+}
+
+}  // namespace tree
+}  // namespace obvh

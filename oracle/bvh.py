@@ -1,0 +1,166 @@
+"""TEST INFRASTRUCTURE ONLY: numpy access to the tree restatement (bvh_oracle.c)
+and to the reference's host-callable vecmath helpers (oracle/_ref)."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import HERE, lib
+
+NODE = np.dtype([("b", "<f4", (6,)), ("left", "<u4"), ("right", "<u4"), ("n_prims", "<u2"),
+                 ("axis", "u1"), ("pad", "u1")])
+assert NODE.itemsize == 36
+
+_f32 = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_u32 = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_node = np.ctypeslib.ndpointer(dtype=NODE, flags="C_CONTIGUOUS")
+_bound = False
+
+
+def _bind():
+    global _bound
+    if _bound:
+        return lib()
+    l = lib()
+    c = ctypes
+    sig = {
+        "oracle_morton30": (c.c_uint32, [c.c_float, c.c_float, c.c_float]),
+        "oracle_minverse4": (None, [_f32, _f32]),
+        "oracle_mmul4": (None, [_f32, _f32, _f32]),
+        "oracle_aabb_area": (c.c_float, [_f32]),
+        "oracle_scene_bounds": (None, [_f32, _u32, c.c_uint32, _f32, _f32]),
+        "oracle_lbvh_codes": (None, [_f32, _u32, c.c_uint32, _f32, _u32]),
+        "oracle_stable_order": (None, [_u32, c.c_uint32, _u32]),
+        "oracle_karras": (None, [_u32, c.c_uint32, _node, _u32]),
+        "oracle_lbvh_build": (None, [_f32, _u32, c.c_uint32, _node, _u32, _u32, _u32, _f32, _f32, _f32]),
+        "oracle_leaf_obb": (None, [_f32, _f32, _f32]),
+        "oracle_obb_tree": (c.c_int, [_node, _u32, _f32, _u32, c.c_uint32, c.c_uint32, _f32, _f32, _f32]),
+        "oracle_collapse": (c.c_int, [_node, _u32, _node, _u32, _u32, _f32, c.c_float, c.c_float, c.c_uint32,
+                                      c.c_uint32]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(l, name)
+        f.restype = res
+        f.argtypes = args
+    _bound = True
+    return l
+
+
+def _mesh(verts, faces):
+    v = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1)
+    f = np.ascontiguousarray(faces, dtype=np.uint32)
+    if f.ndim == 2 and f.shape[1] == 3:
+        f = np.concatenate([f, np.zeros((f.shape[0], 1), np.uint32)], axis=1)
+    return v, np.ascontiguousarray(f.reshape(-1), dtype=np.uint32), f.reshape(-1, 4).shape[0]
+
+
+def scene_bounds(verts, faces):
+    l = _bind()
+    v, f, n = _mesh(verts, faces)
+    s = np.zeros(6, np.float32)
+    c = np.zeros(6, np.float32)
+    l.oracle_scene_bounds(v, f, n, s, c)
+    return s, c
+
+
+def lbvh_codes(verts, faces, centroid_box):
+    l = _bind()
+    v, f, n = _mesh(verts, faces)
+    codes = np.zeros(n, np.uint32)
+    l.oracle_lbvh_codes(v, f, n, np.ascontiguousarray(centroid_box, np.float32), codes)
+    return codes
+
+
+def lbvh_build(verts, faces):
+    """The full LBVH build: dict of nodes, parents, sorted codes, counts, costs, scene, centroid."""
+    l = _bind()
+    v, f, n = _mesh(verts, faces)
+    nn = 2 * n - 1
+    nodes = np.zeros(nn, NODE)
+    parents = np.zeros(nn, np.uint32)
+    codes = np.zeros(n, np.uint32)
+    counts = np.zeros(nn, np.uint32)
+    costs = np.zeros(nn, np.float32)
+    s = np.zeros(6, np.float32)
+    c = np.zeros(6, np.float32)
+    l.oracle_lbvh_build(v, f, n, nodes, parents, codes, counts, costs, s, c)
+    return {"nodes": nodes, "parents": parents, "codes": codes, "counts": counts, "costs": costs,
+            "scene": s, "centroid": c}
+
+
+def karras(codes_sorted):
+    l = _bind()
+    codes = np.ascontiguousarray(codes_sorted, np.uint32)
+    n = codes.shape[0]
+    nodes = np.zeros(2 * n - 1, NODE)
+    parents = np.zeros(2 * n - 1, np.uint32)
+    l.oracle_karras(codes, n, nodes, parents)
+    return nodes, parents
+
+
+def obb_tree(nodes, parents, verts, faces):
+    """(obbs [nodes x 15], transforms [nodes x 16], internal axes [internal x 9])."""
+    l = _bind()
+    v, f, _ = _mesh(verts, faces)
+    nn = nodes.shape[0]
+    n = (nn + 1) // 2
+    ni = n - 1
+    obbs = np.zeros((nn, 15), np.float32)
+    xfs = np.zeros((nn, 16), np.float32)
+    axes = np.zeros((max(ni, 1), 9), np.float32)
+    rc = l.oracle_obb_tree(np.ascontiguousarray(nodes), np.ascontiguousarray(parents, np.uint32), v, f, n, ni,
+                           obbs.reshape(-1), xfs.reshape(-1), axes.reshape(-1))
+    if rc != 0:
+        raise ValueError("malformed tree")
+    return obbs, xfs, axes[:ni]
+
+
+def collapse(nodes, parents, counts, costs, ci=1.2, ct=1.0):
+    """(collapsed nodes, counts, primitives, costs, used primitive slots)."""
+    l = _bind()
+    nn = nodes.shape[0]
+    n = (nn + 1) // 2
+    out = np.zeros(nn, NODE)
+    cnt = np.ascontiguousarray(counts, np.uint32).copy()
+    cst = np.ascontiguousarray(costs, np.float32).copy()
+    prims = np.zeros(n, np.uint32)
+    used = l.oracle_collapse(np.ascontiguousarray(nodes), np.ascontiguousarray(parents, np.uint32), out, cnt, prims,
+                             cst, ci, ct, n, n - 1)
+    if used < 0:
+        raise ValueError("malformed tree")
+    return out, cnt, prims, cst, used
+
+
+def leaf_obb(tri9):
+    l = _bind()
+    o = np.zeros(15, np.float32)
+    x = np.zeros(16, np.float32)
+    l.oracle_leaf_obb(np.ascontiguousarray(tri9, np.float32).reshape(-1), o, x)
+    return o, x
+
+
+# ---- the reference's own helpers (oracle/_ref/libref_vecmath.so) ----------
+_vm = None
+
+
+def ref_vecmath():
+    global _vm
+    if _vm is None:
+        p = os.path.join(HERE, "_ref", "libref_vecmath.so")
+        if not os.path.exists(p):
+            raise FileNotFoundError(p)
+        l = ctypes.CDLL(p)
+        l.ref_v32morton3.restype = ctypes.c_uint32
+        l.ref_v32morton3.argtypes = [ctypes.c_float] * 3
+        l.ref_minverse4.argtypes = [_f32, _f32]
+        l.ref_mmul4.argtypes = [_f32, _f32, _f32]
+        l.ref_aabb_area.restype = ctypes.c_float
+        l.ref_aabb_area.argtypes = [_f32]
+        _vm = l
+    return _vm
+
+
+def ref_vecmath_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_vecmath.so"))

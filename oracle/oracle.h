@@ -10,6 +10,19 @@
 #define OBVH_ORACLE_DITO_CPU 0
 #define OBVH_ORACLE_DITO_GPU 1
 
+#define FLT_MAX_ORACLE 3.402823466e+38F
+
+/* kr_bvh_node (src/common/ads.h:131-142): bounds, left|primitivesOffset, right,
+ * nPrimitives, axis; 36 bytes */
+typedef struct {
+    float b[6];
+    uint32_t left;
+    uint32_t right;
+    uint16_t n_prims;
+    uint8_t axis;
+    uint8_t pad;
+} obvh_oracle_node;
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -23,7 +36,28 @@ void oracle_dito_extremal7(const float* xyz, int64_t n, float minp[7], float max
  * 2 degenerate line, 3 OBB, 4 AABB kept by the final test. */
 int oracle_dito14(const float* xyz, int64_t n, int mode, float out[15], float axes_out[9]);
 
+/* tree path (bvh_oracle.c) */
+uint32_t oracle_morton30(float x, float y, float z);
+void oracle_minverse4(const float* in, float* out);
+void oracle_mmul4(const float* l, const float* r, float* out);
+float oracle_aabb_area(const float* box);
+void oracle_scene_bounds(const float* verts, const uint32_t* faces4, uint32_t n, float scene[6], float centroid[6]);
+void oracle_lbvh_codes(const float* verts, const uint32_t* faces4, uint32_t n, const float cbox[6], uint32_t* codes);
+void oracle_stable_order(const uint32_t* keys, uint32_t n, uint32_t* order);
+void oracle_karras(const uint32_t* codes, uint32_t n, obvh_oracle_node* nodes, uint32_t* parents);
+void oracle_lbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, obvh_oracle_node* nodes,
+                       uint32_t* parents, uint32_t* codes_sorted, uint32_t* counts, float* costs,
+                       float scene[6], float centroid[6]);
+void oracle_leaf_obb(const float* tri9, float obb[15], float xf[16]);
+int oracle_obb_tree(const obvh_oracle_node* nodes, const uint32_t* parents, const float* verts,
+                    const uint32_t* faces4, uint32_t n_leaves, uint32_t n_internal, float* obbs, float* xfs,
+                    float* axes_out);
+int oracle_collapse(const obvh_oracle_node* nodes, const uint32_t* parents, obvh_oracle_node* collapsed,
+                    uint32_t* counts, uint32_t* prims, float* costs, float ci, float ct, uint32_t n_leaves,
+                    uint32_t n_internal);
+
 #ifdef __cplusplus
 }
 #endif
+_Static_assert(sizeof(obvh_oracle_node) == 36, "kr_bvh_node layout");
 #endif

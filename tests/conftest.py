@@ -39,3 +39,28 @@ def same_bits(a, b) -> bool:
     a = np.asarray(a, np.float32) + np.float32(0.0)
     b = np.asarray(b, np.float32) + np.float32(0.0)
     return bool(np.array_equal(a.view(np.uint32), b.view(np.uint32)))
+
+
+def obb_overshoot(points: np.ndarray, obb: np.ndarray) -> np.ndarray:
+    """World-space distance by which each point lies outside the box (FP64).
+
+    The box is mid + sum_k c_k a_k with |c_k| <= ext_k; the axes a_k need not be
+    unit length (the reference's leaf boxes keep an unnormalised third axis), so
+    c_k = (p - mid).a_k / |a_k|^2 and the overshoot along a_k is
+    (|c_k| - ext_k) |a_k|."""
+    p = np.asarray(points, np.float64).reshape(-1, 3)
+    mid = obb[0:3].astype(np.float64)
+    axes = obb[3:12].astype(np.float64).reshape(3, 3)
+    ext = obb[12:15].astype(np.float64)
+    la = np.linalg.norm(axes, axis=1)
+    c = (p - mid) @ axes.T / (la * la)
+    over = (np.abs(c) - ext) * la
+    return np.max(over, axis=1)
+
+
+def contained(points, obb, rel: float = 1e-6) -> bool:
+    """True if every point is inside the box up to rel * (1 + |p|) world units,
+    i.e. a few float32 ulps of the coordinates."""
+    p = np.asarray(points, np.float64).reshape(-1, 3)
+    tol = rel * (1.0 + np.abs(p).max(axis=1))
+    return bool(np.all(obb_overshoot(p, obb) <= tol))
