@@ -29,6 +29,67 @@ OBVH_EXPORT kr_error kr_cuda_bbox_calculate(const kr_uvec4* faces, const kr_vec3
 OBVH_EXPORT kr_error kr_cuda_centroid_bbox_calculate(const kr_uvec4* faces, const kr_vec3* vertices,
                                                      kr_u32 face_count, kr_aabb3* aabb);
 
+/*
+ * AABB-BVH -> OBB tree (kr_cuda_bvh_obb_tree, transforms.cuh:52-65,
+ * transforms.cu:966-1059).  Device pointers: nodes/parents of a binary BVH
+ * (internal nodes [0, internal_count), leaves after them, root 0,
+ * parents[0] = 0xFFFFFFFF, leaf primitivesOffset = face index), the mesh,
+ * and outputs obbs/transforms for every node.  Internal nodes get the DiTO-14
+ * box of their subtree's vertices (or their AABB when that is smaller); leaves
+ * get the triangle-frame box; transforms map each box to the unit cube.
+ * primitive_counts, costs, primitives, ci, ct, obb_cost, primitive_threshold
+ * are unused, as in the reference.  Synchronous.
+ */
+OBVH_EXPORT kr_error kr_cuda_bvh_obb_tree(kr_bvh_node* nodes, const kr_u32* parents, const kr_u32* primitive_counts,
+                                          const kr_scalar* costs, const kr_vec3* vertices, const kr_uvec4* faces,
+                                          const kr_u32* primitives, kr_obb3* obbs, kr_mat4* transforms, kr_scalar ci,
+                                          kr_scalar ct, kr_scalar obb_cost, kr_u32 primitive_count,
+                                          kr_u32 internal_count, kr_u32 primitive_threshold);
+
+/* Workspace bytes of obvh_bvh_obb_tree_async for `primitive_count` leaves. */
+OBVH_EXPORT kr_size obvh_obb_tree_workspace_bytes(kr_u32 primitive_count);
+
+/* kr_cuda_bvh_obb_tree on a caller workspace and stream, without
+ * synchronising.  No counterpart in the reference. */
+OBVH_EXPORT kr_error obvh_bvh_obb_tree_async(const kr_bvh_node* d_nodes, const kr_u32* d_parents,
+                                             const kr_vec3* d_vertices, const kr_uvec4* d_faces, kr_obb3* d_obbs,
+                                             kr_mat4* d_transforms, kr_u32 primitive_count, kr_u32 internal_count,
+                                             void* d_workspace, void* stream);
+
+/*
+ * Collapse of small subtrees into multi-primitive leaves (kr_cuda_bvh_collapse,
+ * transforms.cuh:40-50, transforms.cu:1061-1125).  Device pointers.  Copies
+ * `nodes` to `collapsed_nodes`, then bottom-up: primitive_counts (in/out; the
+ * leaves' entries are read) and costs (out: ct*area for leaves, the SAH cost or
+ * the collapsed cost for internal nodes) are rewritten; a node collapses when
+ * ct*A*n < ci*A + C_left + C_right and n <= 8, and its children get
+ * nPrimitives = 0xFFFF.  Every collapsed node with more than one primitive
+ * under an uncollapsed parent becomes a leaf listing its subtree's primitives
+ * in `primitives` (depth-first, right child first); its offset comes from an
+ * exclusive scan in node order (the reference uses atomicAdd: same lists,
+ * different placement).  metrics (nullable) accumulates the two phases' times
+ * in ms.  Synchronous.
+ */
+OBVH_EXPORT kr_error kr_cuda_bvh_collapse(const kr_bvh_node* nodes, const kr_u32* parents,
+                                          kr_bvh_node* collapsed_nodes, kr_u32* primitive_counts,
+                                          kr_u32* primitives, kr_scalar* costs, kr_scalar ci, kr_scalar ct,
+                                          kr_u32 leaf_count, kr_u32 internal_count, kr_ads_collapse_metrics* metrics);
+
+/* Workspace bytes of obvh_bvh_collapse_async for `leaf_count` leaves. */
+OBVH_EXPORT kr_size obvh_collapse_workspace_bytes(kr_u32 leaf_count);
+
+/* kr_cuda_bvh_collapse on a caller workspace and stream, without
+ * synchronising.  No counterpart in the reference. */
+OBVH_EXPORT kr_error obvh_bvh_collapse_async(const kr_bvh_node* d_nodes, const kr_u32* d_parents,
+                                             kr_bvh_node* d_collapsed, kr_u32* d_primitive_counts,
+                                             kr_u32* d_primitives, kr_scalar* d_costs, kr_scalar ci, kr_scalar ct,
+                                             kr_u32 leaf_count, kr_u32 internal_count, void* d_workspace,
+                                             void* stream);
+
+/* Reads the device error word of the last transform made with a workspace
+ * (synchronises `stream`): 0 ok, 4 parent walk longer than the tree. */
+OBVH_EXPORT kr_error obvh_obb_tree_error(const void* d_workspace, void* stream, kr_u32* device_error);
+
 #ifdef __cplusplus
 }
 #endif

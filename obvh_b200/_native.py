@@ -46,6 +46,15 @@ def _declare(lib: ctypes.CDLL) -> None:
         "obvh_lbvh_workspace_bytes": (c.c_uint64, [c.c_uint32]),
         "obvh_lbvh_workspace_init": (err, [vp, c.c_uint32, vp]),
         "obvh_lbvh_build_async": (err, [vp, vp, c.c_uint32, vp, vp, vp, vp, vp, vp, vp]),
+        "kr_cuda_bvh_obb_tree": (err, [vp, vp, vp, vp, vp, vp, vp, vp, vp, c.c_float, c.c_float, c.c_float,
+                                       c.c_uint32, c.c_uint32, c.c_uint32]),
+        "obvh_obb_tree_workspace_bytes": (c.c_uint64, [c.c_uint32]),
+        "obvh_bvh_obb_tree_async": (err, [vp, vp, vp, vp, vp, vp, c.c_uint32, c.c_uint32, vp, vp]),
+        "obvh_obb_tree_error": (err, [vp, vp, c.POINTER(c.c_uint32)]),
+        "kr_cuda_bvh_collapse": (err, [vp, vp, vp, vp, vp, vp, c.c_float, c.c_float, c.c_uint32, c.c_uint32, vp]),
+        "obvh_collapse_workspace_bytes": (c.c_uint64, [c.c_uint32]),
+        "obvh_bvh_collapse_async": (err, [vp, vp, vp, vp, vp, vp, c.c_float, c.c_float, c.c_uint32, c.c_uint32,
+                                          vp, vp]),
         "obvh_dito_workspace_report": (err, [vp, vp, c.POINTER(c.c_uint32), c.POINTER(c.c_float),
                                              c.POINTER(c.c_uint32)]),
     }

@@ -104,3 +104,69 @@ def bbox_calculate(mesh: Mesh, centroid: bool = False, prefill=None):
     f = lib.kr_cuda_centroid_bbox_calculate if centroid else lib.kr_cuda_bbox_calculate
     _native.check(f(_ptr(mesh.faces), _ptr(mesh.verts), mesh.n_faces, _ptr(box)))
     return box.cpu().numpy()
+
+
+def obb_tree(mesh: Mesh, tree: dict, obbs=None, transforms=None):
+    """kr_cuda_bvh_obb_tree (synchronous) on a device tree; returns (obbs [nn,15], transforms [nn,16])."""
+    import torch
+    lib = _native.lib()
+    nn = tree["parents"].numel()
+    n = (nn + 1) // 2
+    if obbs is None:
+        obbs = torch.empty((nn, 15), dtype=torch.float32, device=tree["parents"].device)
+    if transforms is None:
+        transforms = torch.empty((nn, 16), dtype=torch.float32, device=tree["parents"].device)
+    e = lib.kr_cuda_bvh_obb_tree(_ptr(tree["nodes"]), _ptr(tree["parents"]), _ptr(tree.get("counts")),
+                                 _ptr(tree.get("costs")), _ptr(mesh.verts), _ptr(mesh.faces), None, _ptr(obbs),
+                                 _ptr(transforms), 1.2, 1.0, 1.0, n, n - 1, 0xFFFFFFFF)
+    _native.check(e)
+    return obbs, transforms
+
+
+class ObbTreeTransformer:
+    """obvh_bvh_obb_tree_async with a workspace kept between calls."""
+
+    def __init__(self, device="cuda"):
+        import torch
+        self.torch = torch
+        self.device = torch.device(device)
+        self.lib = _native.lib()
+        self.ws = None
+        self.ws_prims = -1
+
+    def __call__(self, mesh: Mesh, tree: dict, obbs, transforms, stream=None):
+        t = self.torch
+        nn = tree["parents"].numel()
+        n = (nn + 1) // 2
+        if self.ws is None or n > self.ws_prims:
+            self.ws = t.empty(int(self.lib.obvh_obb_tree_workspace_bytes(n)), dtype=t.uint8, device=self.device)
+            self.ws_prims = n
+        e = self.lib.obvh_bvh_obb_tree_async(_ptr(tree["nodes"]), _ptr(tree["parents"]), _ptr(mesh.verts),
+                                             _ptr(mesh.faces), _ptr(obbs), _ptr(transforms), n, n - 1, _ptr(self.ws),
+                                             _stream(t, stream))
+        _native.check(e)
+
+    def device_error(self, stream=None):
+        v = ctypes.c_uint32(0)
+        _native.check(self.lib.obvh_obb_tree_error(_ptr(self.ws), _stream(self.torch, stream), ctypes.byref(v)))
+        return v.value
+
+
+def collapse(tree: dict, ci: float = 1.2, ct: float = 1.0, metrics: bool = False):
+    """kr_cuda_bvh_collapse (synchronous).  Rewrites tree['counts'] and tree['costs'] in
+    place like the reference; returns dict(collapsed, primitives[, metrics])."""
+    import torch
+    lib = _native.lib()
+    nn = tree["parents"].numel()
+    n = (nn + 1) // 2
+    dev = tree["parents"].device
+    out = {"collapsed": torch.empty(nn * NODE_BYTES, dtype=torch.uint8, device=dev),
+           "primitives": torch.zeros(n, dtype=torch.int32, device=dev)}
+    m = (ctypes.c_float * 2)(0.0, 0.0)
+    e = lib.kr_cuda_bvh_collapse(_ptr(tree["nodes"]), _ptr(tree["parents"]), _ptr(out["collapsed"]),
+                                 _ptr(tree["counts"]), _ptr(out["primitives"]), _ptr(tree["costs"]), ci, ct, n,
+                                 n - 1, ctypes.cast(m, ctypes.c_void_p) if metrics else None)
+    _native.check(e)
+    if metrics:
+        out["metrics"] = (m[0], m[1])
+    return out

@@ -1,0 +1,459 @@
+// obb_tree.cu - AABB-BVH -> OBB-tree transform (kr_cuda_bvh_obb_tree,
+// src/ads/common/cuda/transforms.cu:966-1059), re-planned for the B200.
+//
+// The reference needs four synchronising kernels and, for the extents, lets
+// every leaf walk to the root doing float CAS atomics on each ancestor
+// (refit_obbs_kernel_new, :759-901): O(N * depth) contended atomics.  Here:
+//
+//   summary_up   bottom-up (arrival counter per node): the leaf OBB and
+//                transform of every triangle (:794-834), the 7-direction
+//                extremal-vertex summary of every subtree (merge left, then
+//                right where strictly better; 112 B per node) and the subtree
+//                leaf counts.
+//   dfs_rank     each leaf's rank in depth-first order; its triangle is
+//                written to that slot, so every subtree's vertices are one
+//                contiguous run; each node learns its first rank.
+//   candidate    node-parallel DiTO-14 candidate axes from the 14 summary
+//                vertices (:676-756) and the initial extents along them.
+//   extents      min/max of every subtree vertex on the node's axes, read
+//                from the contiguous run: one thread per node up to 8 leaves,
+//                one warp per 1024-leaf unit above that (a persistent grid
+//                takes units from a counter); only nodes of more than one unit
+//                combine partial results, with 6 integer atomics per unit.
+//                Nodes finished here are finalised in place (:903-964).
+//   finalize     the multi-unit nodes.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <unordered_map>
+
+#include "device_common.cuh"
+#include "obb_tree_host.h"
+#include "obvh_transforms.h"
+#include "runtime.h"
+#include "sort.h"
+#include "tree_device.cuh"
+
+namespace obvh {
+namespace obbtree {
+
+using namespace tree;
+
+constexpr int kThreads = 256;
+constexpr uint32_t kThreadMax = 8;   // leaves handled by one thread per node
+constexpr uint32_t kUnit = 1024;     // leaves per warp unit
+
+struct Ctl {
+    uint32_t error;
+    uint32_t unit_counter;
+    uint32_t total_units;
+    uint32_t pad[61];
+};
+
+// Per internal node after the candidate search (96 bytes):
+// axes b0 b1 b2, initial OBB extents lo/hi, AABB lo/hi.
+struct Cand {
+    float ax[9];
+    float olo[3], ohi[3];
+    float alo[3], ahi[3];
+    float pad[3];
+};
+static_assert(sizeof(Cand) == 96, "Cand is 96 bytes");
+
+__device__ __forceinline__ uint32_t count_of(const uint32_t* counts, uint32_t node, uint32_t internal) {
+    return node >= internal ? 1u : __ldcg(counts + node);
+}
+
+__device__ __forceinline__ uint4 leaf_face(const kr_bvh_node* nodes, const kr_uvec4* faces, uint32_t leaf) {
+    const uint32_t prim = __ldg(reinterpret_cast<const uint32_t*>(nodes + leaf) + 6);
+    return __ldg(reinterpret_cast<const uint4*>(faces) + prim);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) summary_up_kernel(const kr_bvh_node* nodes, const uint32_t* parents,
+                                                              const kr_vec3* verts, const kr_uvec4* faces,
+                                                              uint32_t n, uint32_t internal, uint4* summary,
+                                                              uint32_t* counts, uint32_t* visits, kr_obb3* obbs,
+                                                              kr_mat4* xfs, uint32_t* err) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t leaf = internal + j;
+    const uint4 face = leaf_face(nodes, faces, leaf);
+    leaf_box(load_vertex(verts, face.x), load_vertex(verts, face.y), load_vertex(verts, face.z), obbs + leaf,
+             xfs + leaf);
+    if (internal == 0) return;
+    Summary own;
+    leaf_summary(verts, face, own);
+    uint32_t child = leaf;
+    uint32_t p = parents[leaf];
+    for (uint32_t steps = 0; p != kNoParent; ++steps) {
+        if (steps > internal || p >= internal) {
+            atomicOr(err, kErrCycle);
+            return;
+        }
+        __threadfence();
+        if (atomicAdd(visits + p, 1u) == 0) return;
+        __threadfence();
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(nodes + p);
+        const uint32_t L = __ldg(w + 6), R = __ldg(w + 7);
+        const uint32_t other = (L == child) ? R : L;
+        if ((L != child && R != child) || other >= internal + n) {
+            atomicOr(err, kErrBadInput);
+            return;
+        }
+        Summary o;
+        if (other >= internal) leaf_summary(verts, leaf_face(nodes, faces, other), o);
+        else load_summary(summary + 7 * static_cast<size_t>(other), o);
+        if (L == child) {
+            merge_right(own, o);
+        } else {
+            merge_right(o, own);
+            own = o;
+        }
+        store_summary(summary + 7 * static_cast<size_t>(p), own);
+        __stcg(counts + p, count_of(counts, L, internal) + count_of(counts, R, internal));
+        child = p;
+        p = parents[p];
+    }
+}
+
+// DFS rank of every leaf (left subtree first); the leaf's triangle goes to
+// that slot of `tris`; the leaf is the first of every ancestor it reaches
+// through left children only.
+__global__ void __launch_bounds__(kThreads) dfs_rank_kernel(const kr_bvh_node* nodes, const uint32_t* parents,
+                                                            const uint32_t* counts, const kr_vec3* verts,
+                                                            const kr_uvec4* faces, uint32_t n, uint32_t internal,
+                                                            uint32_t* first, float* tris, uint32_t* err) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n || *err) return;  // an earlier pass found a malformed tree
+    const uint32_t leaf = internal + j;
+    uint32_t rank = 0;
+    uint32_t child = leaf, p = parents[leaf];
+    for (uint32_t steps = 0; p != kNoParent; ++steps) {
+        if (steps > internal || p >= internal) {
+            atomicOr(err, kErrCycle);
+            return;
+        }
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(nodes + p);
+        const uint32_t L = __ldg(w + 6);
+        if (L != child) rank += count_of(counts, L, internal);
+        child = p;
+        p = parents[p];
+    }
+    if (rank >= n) {
+        atomicOr(err, kErrBadInput);
+        return;
+    }
+    const uint4 face = leaf_face(nodes, faces, leaf);
+    const f3 a = load_vertex(verts, face.x), b = load_vertex(verts, face.y), c = load_vertex(verts, face.z);
+    float* t = tris + 9 * static_cast<size_t>(rank);
+    t[0] = a.x; t[1] = a.y; t[2] = a.z; t[3] = b.x; t[4] = b.y; t[5] = b.z; t[6] = c.x; t[7] = c.y; t[8] = c.z;
+    child = leaf;
+    p = parents[leaf];
+    while (p != kNoParent && __ldg(reinterpret_cast<const uint32_t*>(nodes + p) + 6) == child) {
+        first[p] = rank;
+        child = p;
+        p = parents[p];
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) candidate_kernel(const uint4* summary, const kr_vec3* verts,
+                                                             const uint32_t* counts, uint32_t internal, Cand* cand,
+                                                             uint32_t* nunits, uint32_t* keys, const uint32_t* err) {
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= internal) return;
+    if (*err) {  // malformed tree: no summaries to read; nothing is scheduled after this
+        nunits[a] = 0;
+        return;
+    }
+    Summary s;
+    load_summary(summary + 7 * static_cast<size_t>(a), s);
+    f3 P[14];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        P[2 * k] = load_vertex(verts, s.ilo[k]);
+        P[2 * k + 1] = load_vertex(verts, s.ihi[k]);
+    }
+    const Candidate c = node_candidate(P, s);
+    Cand out;
+    out.ax[0] = c.b0.x; out.ax[1] = c.b0.y; out.ax[2] = c.b0.z;
+    out.ax[3] = c.b1.x; out.ax[4] = c.b1.y; out.ax[5] = c.b1.z;
+    out.ax[6] = c.b2.x; out.ax[7] = c.b2.y; out.ax[8] = c.b2.z;
+    out.olo[0] = c.lo.x; out.olo[1] = c.lo.y; out.olo[2] = c.lo.z;
+    out.ohi[0] = c.hi.x; out.ohi[1] = c.hi.y; out.ohi[2] = c.hi.z;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { out.alo[k] = s.lo[k]; out.ahi[k] = s.hi[k]; }
+    out.pad[0] = out.pad[1] = out.pad[2] = 0.f;
+    float4* dst = reinterpret_cast<float4*>(cand + a);
+    const float4* src = reinterpret_cast<const float4*>(&out);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) dst[q] = src[q];
+    const uint32_t cnt = counts[a];
+    const uint32_t units = cnt > kThreadMax ? (cnt + kUnit - 1) / kUnit : 0u;
+    nunits[a] = units;
+    if (units > 1) {
+        uint32_t* k = keys + 6 * static_cast<size_t>(a);
+        k[0] = f2key(c.lo.x); k[1] = f2key(c.lo.y); k[2] = f2key(c.lo.z);
+        k[3] = f2key(c.hi.x); k[4] = f2key(c.hi.y); k[5] = f2key(c.hi.z);
+    }
+}
+
+// The box of an internal node from its final extents (finalize_obbs_kernel).
+__device__ __forceinline__ void finalize_node(const Cand& c, f3 lo, f3 hi, kr_obb3* obb, kr_mat4* xf) {
+    const float aq = half_area3(mk3(c.ahi[0] - c.alo[0], c.ahi[1] - c.alo[1], c.ahi[2] - c.alo[2]));
+    const float oq = half_area3(sub3(hi, lo));
+    if (oq < aq)
+        write_box(obb, xf, mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
+                  mk3(c.ax[6], c.ax[7], c.ax[8]), lo, hi);
+    else
+        write_box(obb, xf, mk3(1, 0, 0), mk3(0, 1, 0), mk3(0, 0, 1), mk3(c.alo[0], c.alo[1], c.alo[2]),
+                  mk3(c.ahi[0], c.ahi[1], c.ahi[2]));
+}
+
+__device__ __forceinline__ Cand load_cand(const Cand* cand, uint32_t a) {
+    Cand c;
+    float4* d = reinterpret_cast<float4*>(&c);
+    const float4* s = reinterpret_cast<const float4*>(cand + a);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) d[q] = __ldg(s + q);
+    return c;
+}
+
+// projections of one triangle (9 floats) on the three axes, into lo/hi
+__device__ __forceinline__ void project_tri(const float* t, f3 b0, f3 b1, f3 b2, float lo[3], float hi[3]) {
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const f3 p = mk3(__ldg(t + 3 * v), __ldg(t + 3 * v + 1), __ldg(t + 3 * v + 2));
+        const float q0 = dot3(p, b0), q1 = dot3(p, b1), q2 = dot3(p, b2);
+        lo[0] = fminf(lo[0], q0); hi[0] = fmaxf(hi[0], q0);
+        lo[1] = fminf(lo[1], q1); hi[1] = fmaxf(hi[1], q1);
+        lo[2] = fminf(lo[2], q2); hi[2] = fmaxf(hi[2], q2);
+    }
+}
+
+// Nodes of at most kThreadMax leaves: one thread each, finalised here.
+__global__ void __launch_bounds__(kThreads) extents_small_kernel(const Cand* cand, const uint32_t* counts,
+                                                                 const uint32_t* first, const float* tris,
+                                                                 uint32_t internal, kr_obb3* obbs, kr_mat4* xfs,
+                                                                 const uint32_t* err) {
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= internal || *err) return;
+    const uint32_t cnt = counts[a];
+    if (cnt > kThreadMax) return;
+    const Cand c = load_cand(cand, a);
+    const f3 b0 = mk3(c.ax[0], c.ax[1], c.ax[2]), b1 = mk3(c.ax[3], c.ax[4], c.ax[5]), b2 = mk3(c.ax[6], c.ax[7], c.ax[8]);
+    float lo[3] = {c.olo[0], c.olo[1], c.olo[2]}, hi[3] = {c.ohi[0], c.ohi[1], c.ohi[2]};
+    const float* t = tris + 9 * static_cast<size_t>(first[a]);
+    for (uint32_t i = 0; i < cnt; ++i) project_tri(t + 9 * i, b0, b1, b2, lo, hi);
+    finalize_node(c, mk3(lo[0], lo[1], lo[2]), mk3(hi[0], hi[1], hi[2]), obbs + a, xfs + a);
+}
+
+// Larger nodes: warp-sized units of kUnit leaves taken from a counter.
+__global__ void __launch_bounds__(kThreads) extents_units_kernel(const Cand* cand, const uint32_t* counts,
+                                                                 const uint32_t* first, const float* tris,
+                                                                 const uint32_t* nunits, const uint32_t* unit_start,
+                                                                 uint32_t internal, Ctl* ctl, uint32_t* keys,
+                                                                 kr_obb3* obbs, kr_mat4* xfs) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t total = ctl->error ? 0u : ctl->total_units;
+    for (;;) {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(&ctl->unit_counter, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= total) return;
+        // the last node whose first unit is <= u owns it
+        uint32_t lo_i = 0, hi_i = internal;  // search in [lo_i, hi_i)
+        while (hi_i - lo_i > 1) {
+            const uint32_t mid = (lo_i + hi_i) >> 1;
+            if (__ldg(unit_start + mid) <= u) lo_i = mid; else hi_i = mid;
+        }
+        const uint32_t a = lo_i;
+        const uint32_t chunk = u - __ldg(unit_start + a);
+        const uint32_t cnt = __ldg(counts + a);
+        const uint32_t units = __ldg(nunits + a);
+        const uint32_t begin = chunk * kUnit;
+        const uint32_t end = min(cnt, begin + kUnit);
+        const Cand c = load_cand(cand, a);
+        const f3 b0 = mk3(c.ax[0], c.ax[1], c.ax[2]), b1 = mk3(c.ax[3], c.ax[4], c.ax[5]),
+                 b2 = mk3(c.ax[6], c.ax[7], c.ax[8]);
+        float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+        const float* t = tris + 9 * static_cast<size_t>(__ldg(first + a));
+        for (uint32_t i = begin + lane; i < end; i += 32) project_tri(t + 9 * static_cast<size_t>(i), b0, b1, b2, lo, hi);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = warp_min(lo[k]);
+            hi[k] = warp_max(hi[k]);
+        }
+        if (units == 1) {
+            if (lane == 0)
+                finalize_node(c, mk3(fminf(c.olo[0], lo[0]), fminf(c.olo[1], lo[1]), fminf(c.olo[2], lo[2])),
+                              mk3(fmaxf(c.ohi[0], hi[0]), fmaxf(c.ohi[1], hi[1]), fmaxf(c.ohi[2], hi[2])), obbs + a,
+                              xfs + a);
+        } else if (lane < 6) {
+            const float v = lane < 3 ? lo[lane] : hi[lane - 3];
+            uint32_t* k = keys + 6 * static_cast<size_t>(a) + lane;
+            if (lane < 3) atomicMin(k, f2key(v)); else atomicMax(k, f2key(v));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) finalize_multi_kernel(const Cand* cand, const uint32_t* nunits,
+                                                                  const uint32_t* keys, uint32_t internal,
+                                                                  kr_obb3* obbs, kr_mat4* xfs, const uint32_t* err) {
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= internal || *err || nunits[a] <= 1) return;
+    const uint32_t* k = keys + 6 * static_cast<size_t>(a);
+    finalize_node(load_cand(cand, a), mk3(key2f(k[0]), key2f(k[1]), key2f(k[2])),
+                  mk3(key2f(k[3]), key2f(k[4]), key2f(k[5])), obbs + a, xfs + a);
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+Layout layout(uint32_t n) {
+    const size_t ni = n > 1 ? n - 1 : 1;
+    Layout L;
+    size_t o = 0;
+    L.ctl = o;      o += align256(sizeof(Ctl));
+    L.visits = o;   o += align256(4 * ni);
+    L.counts = o;   o += align256(4 * ni);
+    L.summary = o;  o += align256(112 * ni);
+    L.first = o;    o += align256(4 * ni);
+    L.tris = o;     o += align256(36ull * (n > 0 ? n : 1));
+    L.cand = o;     o += align256(sizeof(Cand) * ni);
+    L.nunits = o;   o += align256(4 * ni);
+    L.ustart = o;   o += align256(4 * ni);
+    L.keys = o;     o += align256(24 * ni);
+    L.scan = o;     o += align256(scan_temp_bytes(ni));
+    L.total = o;
+    return L;
+}
+
+kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec3* verts, const kr_uvec4* faces,
+                 kr_obb3* obbs, kr_mat4* xfs, uint32_t n, uint32_t internal, void* workspace, cudaStream_t s) {
+    if (n == 0) return kr_success;
+    if (!nodes || !parents || !verts || !faces || !obbs || !xfs || !workspace)
+        return "kr_cuda_bvh_obb_tree: null pointer argument";
+    if (internal + 1 != n) return "kr_cuda_bvh_obb_tree: a binary BVH has internal_count == primitive_count - 1";
+    if (reinterpret_cast<uintptr_t>(workspace) & 255) return "kr_cuda_bvh_obb_tree: workspace must be 256-aligned";
+    char* ws = static_cast<char*>(workspace);
+    const Layout L = layout(n);
+    Ctl* ctl = reinterpret_cast<Ctl*>(ws + L.ctl);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(ws + L.counts);
+    uint4* summary = reinterpret_cast<uint4*>(ws + L.summary);
+    uint32_t* first = reinterpret_cast<uint32_t*>(ws + L.first);
+    float* tris = reinterpret_cast<float*>(ws + L.tris);
+    Cand* cand = reinterpret_cast<Cand*>(ws + L.cand);
+    uint32_t* nunits = reinterpret_cast<uint32_t*>(ws + L.nunits);
+    uint32_t* ustart = reinterpret_cast<uint32_t*>(ws + L.ustart);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(ws + L.keys);
+    const unsigned gl = (n + kThreads - 1) / kThreads;
+    const unsigned gi = (internal + kThreads - 1) / kThreads;
+
+    if (internal > 0) OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.visits, 0, 4ull * internal, s));
+    summary_up_kernel<<<gl, kThreads, 0, s>>>(nodes, parents, verts, faces, n, internal, summary, counts,
+                                              reinterpret_cast<uint32_t*>(ws + L.visits), obbs, xfs, &ctl->error);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    if (internal == 0) return kr_success;
+    dfs_rank_kernel<<<gl, kThreads, 0, s>>>(nodes, parents, counts, verts, faces, n, internal, first, tris,
+                                            &ctl->error);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    candidate_kernel<<<gi, kThreads, 0, s>>>(summary, verts, counts, internal, cand, nunits, keys, &ctl->error);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    extents_small_kernel<<<gi, kThreads, 0, s>>>(cand, counts, first, tris, internal, obbs, xfs, &ctl->error);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    OBVH_TRY(exclusive_scan_u32(nunits, ustart, internal, &ctl->total_units, ws + L.scan, s));
+    OBVH_TRY_CUDA(cudaMemsetAsync(&ctl->unit_counter, 0, sizeof(uint32_t), s));
+    const int grid = 4 * device_info().sm_count;
+    extents_units_kernel<<<grid, kThreads, 0, s>>>(cand, counts, first, tris, nunits, ustart, internal, ctl, keys,
+                                                   obbs, xfs);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    finalize_multi_kernel<<<gi, kThreads, 0, s>>>(cand, nunits, keys, internal, obbs, xfs, &ctl->error);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    return kr_success;
+}
+
+uint32_t* error_word(void* workspace) { return &reinterpret_cast<Ctl*>(workspace)->error; }
+
+struct SyncContext {
+    std::mutex mutex;
+    DeviceBuffer ws;
+    uint32_t prims = 0;
+};
+
+SyncContext& sync_context() {
+    static std::mutex m;
+    static std::unordered_map<int, SyncContext*> ctxs;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(m);
+    SyncContext*& c = ctxs[dev];
+    if (!c) c = new SyncContext();
+    return *c;
+}
+
+kr_error run_sync(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec3* verts, const kr_uvec4* faces,
+                  kr_obb3* obbs, kr_mat4* xfs, uint32_t n, uint32_t internal) {
+    SyncContext& c = sync_context();
+    std::lock_guard<std::mutex> lock(c.mutex);
+    const size_t need = layout(n).total;
+    OBVH_TRY(c.ws.reserve(need));
+    OBVH_TRY_CUDA(cudaMemsetAsync(c.ws.ptr, 0, sizeof(Ctl), nullptr));
+    OBVH_TRY(enqueue(nodes, parents, verts, faces, obbs, xfs, n, internal, c.ws.ptr, nullptr));
+    uint32_t err = 0;
+    OBVH_TRY_CUDA(cudaMemcpyAsync(&err, error_word(c.ws.ptr), sizeof err, cudaMemcpyDeviceToHost, nullptr));
+    OBVH_TRY_CUDA(cudaStreamSynchronize(nullptr));
+    if (err & kErrCycle) return "kr_cuda_bvh_obb_tree: parent walk longer than the tree (cycle?)";
+    if (err) return "kr_cuda_bvh_obb_tree: malformed tree";
+    return kr_success;
+}
+
+}  // namespace obbtree
+}  // namespace obvh
+
+using namespace obvh;
+
+extern "C" kr_error kr_cuda_bvh_obb_tree(kr_bvh_node* nodes, const kr_u32* parents, const kr_u32* primitive_counts,
+                                         const kr_scalar* costs, const kr_vec3* vertices, const kr_uvec4* faces,
+                                         const kr_u32* primitives, kr_obb3* obbs, kr_mat4* transforms, kr_scalar ci,
+                                         kr_scalar ct, kr_scalar obb_cost, kr_u32 primitive_count,
+                                         kr_u32 internal_count, kr_u32 primitive_threshold) {
+    // primitive_counts, costs, primitives, ci, ct, obb_cost and
+    // primitive_threshold are accepted and unused, as in the reference.
+    (void)primitive_counts; (void)costs; (void)primitives; (void)ci; (void)ct; (void)obb_cost;
+    (void)primitive_threshold;
+    kr_error e = obbtree::run_sync(nodes, parents, vertices, faces, obbs, transforms, primitive_count, internal_count);
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_size obvh_obb_tree_workspace_bytes(kr_u32 primitive_count) {
+    return obbtree::layout(primitive_count).total;
+}
+
+extern "C" kr_error obvh_bvh_obb_tree_async(const kr_bvh_node* d_nodes, const kr_u32* d_parents,
+                                            const kr_vec3* d_vertices, const kr_uvec4* d_faces, kr_obb3* d_obbs,
+                                            kr_mat4* d_transforms, kr_u32 primitive_count, kr_u32 internal_count,
+                                            void* d_workspace, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    kr_error e = kr_success;
+    if (d_workspace) {
+        cudaError_t ce = cudaMemsetAsync(d_workspace, 0, sizeof(obbtree::Ctl), s);
+        if (ce != cudaSuccess) e = cuda_error(ce);
+    }
+    if (!e)
+        e = obbtree::enqueue(d_nodes, d_parents, d_vertices, d_faces, d_obbs, d_transforms, primitive_count,
+                             internal_count, d_workspace, s);
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error obvh_obb_tree_error(const void* d_workspace, void* stream, kr_u32* device_error) {
+    if (!d_workspace || !device_error) return "obvh_obb_tree_error: null pointer argument";
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(device_error, d_workspace, sizeof(kr_u32), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? kr_success : cuda_error(e);
+}
