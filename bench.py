@@ -3,16 +3,21 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
-Workloads (synthetic inputs with the reference scenes' shapes; the reference
-publishes no numbers, so vs_baseline is null):
+Workloads (seeded synthetic inputs with the reference scenes' shapes; the
+reference publishes no numbers, so vs_baseline is null):
 
-* ``dito``     - DiTO-14 fit of 100,000,000 points on an ellipsoid surface
-                 (semi-axes 4, 1, 0.25; rotated, noised, offset).  A step is
-                 one fit: two streaming passes.  Metric Mpoints/s.
+* ``lbvh_obb_tree`` (default) - LBVH (30-bit Morton, Karras, 1 primitive per
+  leaf) over 2,000,000 thin random triangles (centroids uniform in [0,1]^3,
+  vertices at log-uniform radius 0.002..0.02), then the AABB->OBB-tree
+  transform, then the node collapse.  A step is one such build.  Metric
+  Mnodes/s = (2N-1) nodes per step.
+* ``dito`` - DiTO-14 fit of 100,000,000 points on an ellipsoid surface
+  (semi-axes 4, 1, 0.25; rotated, noised, offset).  A step is one fit (two
+  streaming passes).  Metric Mpoints/s.
 
-Multi-GPU: every rank fits its own point set (independent units, no
-collective); ``value`` is the points of all ranks over the slowest rank's
-device time ("scaling": "weak").
+Multi-GPU: every rank builds/fits its own input (independent units, no
+collective); ``value`` = units of all ranks / the slowest rank's device time
+("scaling": "weak").
 """
 from __future__ import annotations
 
@@ -25,7 +30,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -37,13 +41,14 @@ FALLBACK_HBM_GBS = 6650.0
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["dito"], default="dito")
-    ap.add_argument("--points", type=int, default=100_000_000)
+    ap.add_argument("--workload", choices=["lbvh_obb_tree", "dito"], default="lbvh_obb_tree")
+    ap.add_argument("--points", type=int, default=100_000_000, help="dito: points per fit")
+    ap.add_argument("--tris", type=int, default=2_000_000, help="lbvh_obb_tree: triangles per build")
     ap.add_argument("--profile", action="store_true",
-                    help="only warm-up + timed fits, no clock soak, e2e or CPU legs (for ncu captures)")
+                    help="only warm-up + timed steps, no clock soak, e2e or CPU legs (for ncu captures)")
     return ap.parse_args()
 
 
@@ -64,12 +69,15 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, enabled: bool = True):
         self.gpu = gpu_index
+        self.enabled = enabled
         self.proc = None
         self.file = None
 
     def start(self):
+        if not self.enabled:
+            return
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.proc = subprocess.Popen(
@@ -80,6 +88,8 @@ class ClockSampler:
         time.sleep(0.3)
 
     def stop(self):
+        if not self.enabled or self.file is None:
+            return None
         if self.proc is not None:
             time.sleep(0.25)
             self.proc.terminate()
@@ -112,7 +122,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-# ---------------------------------------------------------------------------
 class Dist:
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -120,15 +129,14 @@ class Dist:
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = False
 
-    def init(self, backend="nccl"):
+    def init(self):
         import torch
         if self.world > 1:
             import torch.distributed as dist
-            if backend == "nccl":
-                torch.cuda.set_device(self.local)
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
             self.pg = True
-        elif backend == "nccl":
+        else:
             torch.cuda.set_device(0)
 
     def barrier(self):
@@ -151,139 +159,299 @@ class Dist:
             dist.destroy_process_group()
 
 
-# ---------------------------------------------------------------------------
-def cpu_reference_dito(points_np, repeats: int):
-    """The reference's own DiTO_14 (oracle/_ref) on host cores: Mpoints/s."""
-    import oracle
-    oracle.ref_dito14(points_np[:1000])
-    t0 = time.perf_counter()
-    for _ in range(repeats):
-        oracle.ref_dito14(points_np)
-    dt = time.perf_counter() - t0
-    return points_np.shape[0] * repeats / dt / 1e6, dt
+def profile_summary():
+    from obvh_b200 import _native
+    buf = ctypes.create_string_buffer(1 << 16)
+    _native.check(_native.lib().obvh_profile_summary(buf, len(buf)))
+    return json.loads(buf.value.decode())
 
 
-def bench_dito_ours(a, dist: Dist):
+def profile_enable(on: bool):
+    from obvh_b200 import _native
+    _native.check(_native.lib().obvh_profile_enable(1 if on else 0))
+
+
+def timed_steps(a, dist, step_fn, sampler, stream):
+    """Warm-up, then exactly a.steps steps between barriers; returns the max-over-ranks
+    device time (ms), the per-kernel profile of the timed region and the clocks."""
     import torch
-    from obvh_b200 import DitoFitter, points_obb, workloads
-
-    n = a.points
-    dev = torch.device("cuda", torch.cuda.current_device())
-    # Two independent point sets, alternated between steps: a step never finds
-    # the previous step's data in L2 (each set is 1.2 GB, the L2 126 MB).
-    sets = [workloads.ellipsoid_points_torch(n, seed=1234 + 2 * dist.rank + j, device=dev) for j in range(2)]
-    pts = sets[0]
-    fitter = DitoFitter(dev)
-    out = torch.empty(15, dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream(dev)
-
-    sampler = ClockSampler(dev.index if dist.world == 1 else dist.local)
     if not a.profile:
         sampler.start()
-        # settle clocks: ~1 s of back-to-back fits before the warm-up
-        t_end = time.time() + 1.0
+        t_end = time.time() + 1.0  # settle clocks
+        j = 0
         while time.time() < t_end:
-            for j in range(20):
-                fitter.fit(sets[j & 1], out)
+            step_fn(j)
+            j += 1
             torch.cuda.synchronize()
     for j in range(a.warmup):
-        fitter.fit(sets[j & 1], out)
+        step_fn(j)
     torch.cuda.synchronize()
     dist.barrier()
     torch.cuda.synchronize()
-
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-            torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    profile_enable(True)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
-    for j, (e0, e1, e2) in enumerate(evs):
-        p = sets[(j + a.warmup) & 1]
-        e0.record(stream)
-        fitter.fit_pass(p, out, 1)
-        e1.record(stream)
-        fitter.fit_pass(p, out, 2)
-        e2.record(stream)
+    for j in range(a.steps):
+        step_fn(a.warmup + j)
     stop.record(stream)
     torch.cuda.synchronize()
     dist.barrier()
     torch.cuda.synchronize()
     clocks = sampler.stop() if not a.profile else None
+    prof = profile_summary()
+    profile_enable(False)
+    return dist.max(start.elapsed_time(stop)), prof, clocks
 
-    total_ms = dist.max(start.elapsed_time(stop))
-    p1 = [e0.elapsed_time(e1) for e0, e1, _ in evs]
-    p2 = [e1.elapsed_time(e2) for _, e1, e2 in evs]
+
+def roofline(prof, bytes_per_launch, peak, peak_kind, traffic_file=None):
+    """The roofline object of the kernel with the largest device time."""
+    name, (launches, total_ms) = max(prof.items(), key=lambda kv: kv[1][1])
+    per_launch_ms = total_ms / max(launches, 1)
+    algo = bytes_per_launch.get(name)
+    achieved = algo / (per_launch_ms / 1e3) / 1e9 if algo else None
+    traffic = None
+    if traffic_file and os.path.exists(traffic_file):
+        with open(traffic_file) as f:
+            traffic = json.load(f).get(name)
+    return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1) if achieved else None, "peak": peak,
+            "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None, "traffic": traffic,
+            "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo,
+            "launches": launches, "ms_per_launch": round(per_launch_ms, 5)}
+
+
+# ---------------------------------------------------------------------------
+def tree_bytes_per_launch(n):
+    """Algorithmic (compulsory HBM) bytes per launch of each kernel of the
+    LBVH -> OBB-tree -> collapse step for n triangles (nn = 2n-1 nodes):
+    every input read once and every output written once."""
+    ni = n - 1
+    nn = 2 * n - 1
+    return {
+        "tri_bounds_kernel": 52 * n + 24 * n,          # face + 3 vertices in, triangle box out
+        "morton_kernel": 24 * n + 8 * n,               # box in, key + index out
+        "radix_hist": 4 * n,                           # keys in
+        "radix_scatter": 16 * n,                       # key + value in and out
+        "leaves_kernel": 4 * n + 24 * n + 36 * n,      # order, box in; leaf node out
+        "karras_kernel": 4 * n + 36 * ni + 8 * ni,     # codes in; internal nodes + parents out
+        "aabb_up_kernel": 36 * nn + 8 * nn + 32 * ni,  # nodes in; counts, costs, bounds out
+        # faces + vertices in, leaf boxes + transforms out, summaries out and read once
+        "summary_up_kernel": 52 * n + 124 * n + 112 * ni * 2 + 4 * ni,
+        "dfs_rank_kernel": 52 * n + 36 * n + 4 * ni,   # faces + vertices in; ordered triangles + firsts out
+        "candidate_kernel": 112 * ni + 168 * ni + 96 * ni + 8 * ni,  # summary + 14 vertices in; frame out
+        "extents_small_kernel": 96 * ni + 124 * ni,    # frame in; box + transform out
+        "extents_units_kernel": 36 * n,                # ordered triangles in
+        "mark_up_kernel": 36 * nn + 16 * nn + 36 * n,
+        "roots_kernel": 14 * nn,
+        "gather_kernel": 8 * nn,
+        "scan_tile_sums": 4 * nn,
+        "scan_tiles": 8 * nn,
+    }
+
+
+def bench_tree_ours(a, dist):
+    import numpy as np
+    import torch
+    from obvh_b200 import _native, bvh, workloads
+
+    n = a.tris
+    nn = 2 * n - 1
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lib = _native.lib()
+    # two meshes alternated between steps (2 x 104 MB > 126 MB L2)
+    host_meshes = [workloads.triangle_soup(n, seed=1 + 2 * dist.rank + j) for j in range(2)]
+    meshes = [bvh.Mesh(v, f, device=dev) for v, f in host_meshes]
+    ws_bytes = max(int(lib.obvh_lbvh_workspace_bytes(n)), int(lib.obvh_obb_tree_workspace_bytes(n)),
+                   int(lib.obvh_collapse_workspace_bytes(n)))
+    ws = torch.zeros(ws_bytes, dtype=torch.uint8, device=dev)
+    u8, i32, f32 = torch.uint8, torch.int32, torch.float32
+    out = {"nodes": torch.empty(nn * 36, dtype=u8, device=dev), "parents": torch.empty(nn, dtype=i32, device=dev),
+           "counts": torch.empty(nn, dtype=i32, device=dev), "costs": torch.empty(nn, dtype=f32, device=dev),
+           "bounds": torch.empty(12, dtype=f32, device=dev), "obbs": torch.empty(nn * 15, dtype=f32, device=dev),
+           "xfs": torch.empty(nn * 16, dtype=f32, device=dev), "collapsed": torch.empty(nn * 36, dtype=u8, device=dev),
+           "prims": torch.empty(n, dtype=i32, device=dev)}
+    P = {k: ctypes.c_void_p(t.data_ptr()) for k, t in out.items()}
+    W = ctypes.c_void_p(ws.data_ptr())
+    stream = torch.cuda.current_stream(dev)
+    S = ctypes.c_void_p(stream.cuda_stream)
+
+    def step(j, mesh=None):
+        m = mesh or meshes[j & 1]
+        V, F = ctypes.c_void_p(m.verts.data_ptr()), ctypes.c_void_p(m.faces.data_ptr())
+        _native.check(lib.obvh_lbvh_build_async(V, F, n, P["nodes"], P["parents"], P["counts"], P["costs"],
+                                                P["bounds"], W, S))
+        _native.check(lib.obvh_bvh_obb_tree_async(P["nodes"], P["parents"], V, F, P["obbs"], P["xfs"], n, n - 1, W, S))
+        _native.check(lib.obvh_bvh_collapse_async(P["nodes"], P["parents"], P["collapsed"], P["counts"], P["prims"],
+                                                  P["costs"], 1.2, 1.0, n, n - 1, W, S))
+
+    sampler = ClockSampler(dev.index, enabled=not a.profile)
+    total_ms, prof, clocks = timed_steps(a, dist, step, sampler, stream)
+    err = int(ws[:4].view(i32).item())
+    if err != 0:
+        raise RuntimeError(f"device error word {err}")
+    if a.profile:
+        return {"profile": "lbvh_obb_tree", "tris": n, "ms_per_step": total_ms / a.steps, "kernels": prof}
+
     ms_step = total_ms / a.steps
-    value = dist.world * n * a.steps / (total_ms / 1e3) / 1e6
+    value = dist.world * nn * a.steps / (total_ms / 1e3) / 1e6
+    peak, peak_kind = peaks()
+    kern = {k: {"launches": v[0], "ms_per_step": round(v[1] / a.steps, 5)} for k, v in prof.items()}
+    roof = roofline(prof, tree_bytes_per_launch(n), peak, peak_kind,
+                    os.path.join(ROOT, "profiles", "lbvh_obb_tree_traffic.json"))
+    launches = sum(v[0] for v in prof.values())
 
+    # End to end through the C ABI: the pinned host mesh copied in, the tree
+    # built, transformed and collapsed, and the root box + root cost read back.
+    pinned = [(torch.from_numpy(v).pin_memory(), torch.from_numpy(bvh.as_faces4(f).view(np.int32)).pin_memory())
+              for v, f in host_meshes]
+    staging = bvh.Mesh(host_meshes[0][0], host_meshes[0][1], device=dev)
+    result = torch.empty(16, dtype=f32).pin_memory()
+    e2e_steps = max(3, min(a.steps, 10))
+
+    def e2e_step(j):
+        pv, pf = pinned[j & 1]
+        staging.verts.copy_(pv, non_blocking=True)
+        staging.faces.copy_(pf, non_blocking=True)
+        step(j, staging)
+        result[:15].copy_(out["obbs"][:15], non_blocking=True)
+        result[15:].copy_(out["costs"][:1], non_blocking=True)
+        stream.synchronize()
+
+    e2e_step(0)
+    t0 = time.perf_counter()
+    for j in range(e2e_steps):
+        e2e_step(j)
+    e2e_s = time.perf_counter() - t0
+    e2e_min = -dist.max(-(nn * e2e_steps / e2e_s / 1e6))
+
+    line = {
+        "metric": "LBVH + OBB-tree + collapse build throughput (Mnodes/s)",
+        "value": round(value, 3), "unit": "Mnodes/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": round(ms_step, 5), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: thin random triangles (centroid U[0,1]^3, vertex radius log-U[0.002,0.02]), seeded",
+        "config": {"workload": "lbvh_obb_tree_collapse", "triangles_per_gpu": n, "nodes_per_gpu": nn,
+                   "morton_bits": 30, "ci": 1.2, "ct": 1.0,
+                   "l2": "two 104 MB meshes alternated between steps; each step writes ~1 GB",
+                   "parallelism": f"replicas{dist.world}"},
+        "kernels": kern, "gpu_launches": launches, "roofline": roof,
+        "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mnodes/s",
+                "h2d_bytes_per_step": int(host_meshes[0][0].nbytes + n * 16), "d2h_bytes_per_step": 64,
+                "api": "obvh_lbvh_build_async + obvh_bvh_obb_tree_async + obvh_bvh_collapse_async, pinned host mesh"},
+        "clocks": clocks,
+    }
+    if dist.rank == 0 and dist.world == 1:
+        line["cpu_baseline"] = cpu_tree_baseline()
+    return line
+
+
+def cpu_tree_baseline(n=200_000):
+    """The oracle port of the same build on one host core (the reference has
+    no CPU implementation of this GPU path)."""
+    from oracle import bvh as ref
+    from obvh_b200 import workloads
+    v, f = workloads.triangle_soup(n, seed=77)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        r = ref.lbvh_build(v, f)
+        ref.obb_tree(r["nodes"], r["parents"], v, f)
+        ref.collapse(r["nodes"], r["parents"], r["counts"], r["costs"])
+        reps += 1
+        dt = time.perf_counter() - t0
+        if dt > 8.0 or reps >= 20:
+            break
+    return {"value": round((2 * n - 1) * reps / dt / 1e6, 4), "unit": "Mnodes/s", "cores": 1, "kind": "port",
+            "sample": f"{reps} builds of {n} triangles ({dt:.1f} s), oracle C restatement"}
+
+
+def bench_tree_reference(a, dist):
+    """The CPU restatement of the path (oracle port) on this host: the
+    reference has no CPU implementation of its GPU build to run."""
+    from oracle import bvh as ref
+    from obvh_b200 import workloads
+    n = min(a.tris, 500_000)
+    v, f = workloads.triangle_soup(n, seed=1)
+    times = []
+    for j in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
+        r = ref.lbvh_build(v, f)
+        ref.obb_tree(r["nodes"], r["parents"], v, f)
+        ref.collapse(r["nodes"], r["parents"], r["counts"], r["costs"])
+        if j >= a.warmup:
+            times.append(time.perf_counter() - t0)
+    nn = 2 * n - 1
+    value = nn * len(times) / sum(times) / 1e6
+    return {"metric": "LBVH + OBB-tree + collapse build throughput (Mnodes/s)", "impl": "reference",
+            "value": round(value, 4), "unit": "Mnodes/s", "n_gpus": dist.world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (same generator as the ours arm)",
+            "config": {"workload": "lbvh_obb_tree_collapse", "triangles_per_gpu": a.tris, "sample_triangles": n},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mnodes/s", "cores": 1, "kind": "port",
+                             "sample": f"{n}-triangle builds per step (oracle C restatement, single-threaded)"},
+            "e2e": {"value": round(value, 4), "unit": "Mnodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# ---------------------------------------------------------------------------
+def bench_dito_ours(a, dist):
+    import torch
+    from obvh_b200 import DitoFitter, points_obb, workloads
+
+    n = a.points
+    dev = torch.device("cuda", torch.cuda.current_device())
+    # two independent point sets alternated between steps (1.2 GB each > 126 MB L2)
+    sets = [workloads.ellipsoid_points_torch(n, seed=1234 + 2 * dist.rank + j, device=dev) for j in range(2)]
+    fitter = DitoFitter(dev)
+    out = torch.empty(15, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sampler = ClockSampler(dev.index, enabled=not a.profile)
+    total_ms, prof, clocks = timed_steps(a, dist, lambda j: fitter.fit(sets[j & 1], out), sampler, stream)
     path, _, err = fitter.report()
     if err:
         raise RuntimeError(f"device error word {err}")
     if a.profile:
-        return {"profile": "dito", "points": n, "pass1_ms": statistics.mean(p1), "pass2_ms": statistics.mean(p2),
-                "path": path}
-
+        return {"profile": "dito", "points": n, "ms_per_step": total_ms / a.steps, "kernels": prof}
     peak, peak_kind = peaks()
-    t1, t2 = statistics.mean(p1), statistics.mean(p2)
-    dom_name, dom_ms = ("dito_extremal_pass", t1) if t1 >= t2 else ("dito_extent_pass", t2)
-    algo_bytes = 12.0 * n  # one pass reads every point once
-    achieved = algo_bytes / (dom_ms / 1e3) / 1e9
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "dito_traffic.json")
-    if os.path.exists(prof):
-        with open(prof) as f:
-            tj = json.load(f)
-        if dom_name in tj:
-            traffic = tj[dom_name]["bytes_per_point"] * n
+    value = dist.world * n * a.steps / (total_ms / 1e3) / 1e6
+    roof = roofline(prof, {"dito_extremal_pass": 12 * n, "dito_extent_pass": 12 * n}, peak, peak_kind,
+                    os.path.join(ROOT, "profiles", "dito_traffic.json"))
 
-    # End to end through the reference-facing call: host (pinned) points in,
-    # box out; the H2D copy of the points and the read-back are inside.
     host = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
-    host.copy_(pts)
+    host.copy_(sets[0])
     host_np = host.numpy()
-    points_obb(host_np)  # warm
+    points_obb(host_np)
     e2e_steps = max(3, min(a.steps, 10))
-    torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         points_obb(host_np)
     e2e_s = time.perf_counter() - t0
-    e2e_local = n * e2e_steps / e2e_s / 1e6
-    e2e_min = -dist.max(-e2e_local)
-
+    e2e_min = -dist.max(-(n * e2e_steps / e2e_s / 1e6))
     line = {
-        "metric": "DiTO-14 fit throughput (Mpoints/s)",
-        "value": round(value, 3),
-        "unit": "Mpoints/s",
-        "n_gpus": dist.world,
-        "steps": a.steps,
-        "warmup": a.warmup,
-        "ms_per_step": round(ms_step, 5),
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f32",
+        "metric": "DiTO-14 fit throughput (Mpoints/s)", "value": round(value, 3), "unit": "Mpoints/s",
+        "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(total_ms / a.steps, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: ellipsoid surface points (4,1,0.25), Haar rotation, N(0,0.01^2) noise, U[-10,10]^3 offset",
         "config": {"workload": "dito_plain_fit", "points_per_gpu": n, "point_bytes": 12,
-                   "l2": "two 1.2 GB point sets alternated between steps (> 126 MB L2), no flush", "parallelism": f"replicas{dist.world}",
-                   "path": path},
-        "kernels_ms": {"dito_extremal_pass": round(t1, 5), "dito_extent_pass": round(t2, 5)},
-        "gpu_launches": 2 * a.steps,
-        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo_bytes},
+                   "l2": "two 1.2 GB point sets alternated between steps (> 126 MB L2), no flush",
+                   "parallelism": f"replicas{dist.world}", "path": path},
+        "kernels": {k: {"launches": v[0], "ms_per_step": round(v[1] / a.steps, 5)} for k, v in prof.items()},
+        "gpu_launches": sum(v[0] for v in prof.values()), "roofline": roof,
         "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mpoints/s", "h2d_bytes_per_step": 12 * n,
                 "d2h_bytes_per_step": 316, "api": "obvh_points_obb (kr_cuda_points_obb with errors), pinned host"},
         "clocks": clocks,
     }
     if dist.rank == 0 and dist.world == 1:
-        sample = host_np[: min(n, 100_000_000)]
-        v, dt = cpu_reference_dito(sample, repeats=3)
-        line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpoints/s", "cores": 1, "kind": "reference",
-                                "sample": f"3 fits of the first {sample.shape[0]} points ({dt:.1f} s)"}
+        import oracle
+        oracle.ref_dito14(host_np[:1000])
+        t0 = time.perf_counter()
+        for _ in range(3):
+            oracle.ref_dito14(host_np)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(3 * n / dt / 1e6, 3), "unit": "Mpoints/s", "cores": 1,
+                                "kind": "reference",
+                                "sample": f"3 fits of the {n}-point set ({dt:.1f} s), reference DiTO_14 (oracle/_ref)"}
     return line
 
 
-def bench_dito_reference(a, dist: Dist):
+def bench_dito_reference(a, dist):
     """The reference's own CPU DiTO_14 (single-threaded, as shipped) on this host."""
     import numpy as np
     import oracle
@@ -291,8 +459,8 @@ def bench_dito_reference(a, dist: Dist):
     n = a.points
     try:
         import torch
-        pts = workloads.ellipsoid_points_torch(n, seed=1234, device="cuda" if torch.cuda.is_available() else "cpu")
-        host = pts.cpu().numpy()
+        host = workloads.ellipsoid_points_torch(n, seed=1234, device="cuda" if torch.cuda.is_available() else "cpu")
+        host = host.cpu().numpy()
     except Exception:
         host = workloads.ellipsoid_points(n, seed=1234)
     host = np.ascontiguousarray(host, dtype=np.float32)
@@ -303,18 +471,15 @@ def bench_dito_reference(a, dist: Dist):
         t0 = time.perf_counter()
         oracle.ref_dito14(host)
         times.append(time.perf_counter() - t0)
-    total = sum(times)
-    value = n * a.steps / total / 1e6
-    return {
-        "metric": "DiTO-14 fit throughput (Mpoints/s)", "impl": "reference", "value": round(value, 3),
-        "unit": "Mpoints/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": round(1e3 * total / a.steps, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (same generator as the ours arm)",
-        "config": {"workload": "dito_plain_fit", "points_per_gpu": n},
-        "cpu_baseline": {"value": round(value, 3), "unit": "Mpoints/s", "cores": 1, "kind": "reference",
-                         "sample": f"full {n}-point fit per step; DiTO_14<float> is single-threaded"},
-        "e2e": {"value": round(value, 3), "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    value = n * len(times) / sum(times) / 1e6
+    return {"metric": "DiTO-14 fit throughput (Mpoints/s)", "impl": "reference", "value": round(value, 3),
+            "unit": "Mpoints/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (same generator as the ours arm)",
+            "config": {"workload": "dito_plain_fit", "points_per_gpu": n},
+            "cpu_baseline": {"value": round(value, 3), "unit": "Mpoints/s", "cores": 1, "kind": "reference",
+                             "sample": f"full {n}-point fit per step; DiTO_14<float> is single-threaded"},
+            "e2e": {"value": round(value, 3), "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
@@ -323,15 +488,18 @@ def main():
     if a.impl == "reference":
         if dist.world > 1 and dist.rank != 0:
             return
-        import oracle
-        if not oracle.ref_available():
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_dito.so was not built"}))
-            return
-        print(json.dumps(bench_dito_reference(a, dist)), flush=True)
+        if a.workload == "dito":
+            import oracle
+            if not oracle.ref_available():
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_dito.so was not built"}))
+                return
+            print(json.dumps(bench_dito_reference(a, dist)), flush=True)
+        else:
+            print(json.dumps(bench_tree_reference(a, dist)), flush=True)
         return
-    dist.init("nccl")
+    dist.init()
     try:
-        line = bench_dito_ours(a, dist)
+        line = bench_tree_ours(a, dist) if a.workload == "lbvh_obb_tree" else bench_dito_ours(a, dist)
         if dist.rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -21,6 +21,18 @@ OBVH_EXPORT const char* obvh_version(void);
  */
 OBVH_EXPORT kr_error obvh_last_error(void);
 
+/*
+ * Per-kernel device timing.  While enabled, every kernel the library launches
+ * is bracketed by CUDA events on its stream; obvh_profile_summary()
+ * synchronises the device and writes a JSON object
+ * {"kernel name": [launches, total ms], ...} into buf.  Enabling clears the
+ * record.  The reference logs per-kernel times with kr_log after
+ * synchronising every launch (src/common/cuda/util.h:27-57); here timing is
+ * opt-in and launches stay asynchronous.
+ */
+OBVH_EXPORT kr_error obvh_profile_enable(int on);
+OBVH_EXPORT kr_error obvh_profile_summary(char* buf, kr_size cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -176,16 +176,25 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, kr_bvh_node*
     OBVH_TRY_CUDA(cudaMemcpyAsync(collapsed, nodes, sizeof(kr_bvh_node) * nn, cudaMemcpyDeviceToDevice, s));
     OBVH_TRY_CUDA(cudaMemsetAsync(flags, 0, nn, s));
     OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.visits, 0, 4ull * nn, s));
-    mark_up_kernel<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(
-        nodes, parents, collapsed, counts, costs, flags, reinterpret_cast<uint32_t*>(ws + L.visits), ci, ct, n,
-        internal, &ctl->error);
+    {
+        ProfScope prof_scope_("mark_up_kernel", s);
+        mark_up_kernel<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+            nodes, parents, collapsed, counts, costs, flags, reinterpret_cast<uint32_t*>(ws + L.visits), ci, ct, n,
+            internal, &ctl->error);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     if (mid_event) OBVH_TRY_CUDA(cudaEventRecord(mid_event, s));
     const unsigned gn = (nn + kThreads - 1) / kThreads;
-    roots_kernel<<<gn, kThreads, 0, s>>>(parents, flags, counts, nn, sizes, &ctl->error);
+    {
+        ProfScope prof_scope_("roots_kernel", s);
+        roots_kernel<<<gn, kThreads, 0, s>>>(parents, flags, counts, nn, sizes, &ctl->error);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     OBVH_TRY(exclusive_scan_u32(sizes, offsets, nn, &ctl->total, ws + L.scan, s));
-    gather_kernel<<<gn, kThreads, 0, s>>>(nodes, sizes, offsets, nn, collapsed, counts, primitives, &ctl->error);
+    {
+        ProfScope prof_scope_("gather_kernel", s);
+        gather_kernel<<<gn, kThreads, 0, s>>>(nodes, sizes, offsets, nn, collapsed, counts, primitives, &ctl->error);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     return kr_success;
 }

@@ -444,11 +444,17 @@ kr_error enqueue(const kr_vec3* d_points, uint64_t count, uint32_t flags, kr_obb
     Split sp = make_split(reinterpret_cast<const float*>(d_points), count);
     int grid = grid_for(sp);
     if (passes & 1) {
-        dito_extremal_pass<<<grid, kThreads, kSmemBytes, stream>>>(sp, static_cast<char*>(ws), d_obb, flags);
+        {
+            ProfScope prof_scope_("dito_extremal_pass", stream);
+            dito_extremal_pass<<<grid, kThreads, kSmemBytes, stream>>>(sp, static_cast<char*>(ws), d_obb, flags);
+        }
         OBVH_TRY_CUDA(cudaGetLastError());
     }
     if (passes & 2) {
-        dito_extent_pass<<<grid, kThreads, kSmemBytes, stream>>>(sp, static_cast<char*>(ws), d_obb, flags);
+        {
+            ProfScope prof_scope_("dito_extent_pass", stream);
+            dito_extent_pass<<<grid, kThreads, kSmemBytes, stream>>>(sp, static_cast<char*>(ws), d_obb, flags);
+        }
         OBVH_TRY_CUDA(cudaGetLastError());
     }
     return kr_success;

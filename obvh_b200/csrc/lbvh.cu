@@ -301,10 +301,13 @@ int bounds_grid(uint32_t n) {
 kr_error enqueue_bounds(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, float* tri_boxes, char* ws,
                         kr_aabb3* scene_out, kr_aabb3* centroid_out, bool overwrite, cudaStream_t s) {
     const Layout L = layout(0);
-    tri_bounds_kernel<<<bounds_grid(n), kThreads, 0, s>>>(verts, reinterpret_cast<const uint4*>(faces), n, tri_boxes,
-                                                          reinterpret_cast<BoundsRec*>(ws + L.recs),
-                                                          reinterpret_cast<Ctl*>(ws + L.ctl), scene_out, centroid_out,
-                                                          overwrite);
+    {
+        ProfScope prof_scope_("tri_bounds_kernel", s);
+        tri_bounds_kernel<<<bounds_grid(n), kThreads, 0, s>>>(verts, reinterpret_cast<const uint4*>(faces), n, tri_boxes,
+                                                              reinterpret_cast<BoundsRec*>(ws + L.recs),
+                                                              reinterpret_cast<Ctl*>(ws + L.ctl), scene_out, centroid_out,
+                                                              overwrite);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     return kr_success;
 }
@@ -324,25 +327,37 @@ kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, 
     const unsigned grid_n = (n + kThreads - 1) / kThreads;
 
     OBVH_TRY(enqueue_bounds(verts, faces, n, tri, ws, boxes, boxes + 1, true, s));
-    morton_kernel<<<grid_n, kThreads, 0, s>>>(tri, n, boxes, reinterpret_cast<uint32_t*>(ws + L.keys0),
-                                              reinterpret_cast<uint32_t*>(ws + L.vals0));
+    {
+        ProfScope prof_scope_("morton_kernel", s);
+        morton_kernel<<<grid_n, kThreads, 0, s>>>(tri, n, boxes, reinterpret_cast<uint32_t*>(ws + L.keys0),
+                                                  reinterpret_cast<uint32_t*>(ws + L.vals0));
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     bool alt = false;
     OBVH_TRY(radix_sort_pairs(ws + L.keys0, ws + L.keys1, reinterpret_cast<uint32_t*>(ws + L.vals0),
                               reinterpret_cast<uint32_t*>(ws + L.vals1), n, 4, 0, 30, ws + L.sort, s, &alt));
     const uint32_t* codes = reinterpret_cast<const uint32_t*>(ws + (alt ? L.keys1 : L.keys0));
     const uint32_t* order = reinterpret_cast<const uint32_t*>(ws + (alt ? L.vals1 : L.vals0));
-    leaves_kernel<<<grid_n, kThreads, 0, s>>>(tri, order, n, nodes);
+    {
+        ProfScope prof_scope_("leaves_kernel", s);
+        leaves_kernel<<<grid_n, kThreads, 0, s>>>(tri, order, n, nodes);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     if (n >= 2) {
-        karras_kernel<<<(n - 1 + kThreads - 1) / kThreads, kThreads, 0, s>>>(codes, n, nodes, parents);
+        {
+            ProfScope prof_scope_("karras_kernel", s);
+            karras_kernel<<<(n - 1 + kThreads - 1) / kThreads, kThreads, 0, s>>>(codes, n, nodes, parents);
+        }
         OBVH_TRY_CUDA(cudaGetLastError());
         OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.visits, 0, 4ull * (n - 1), s));
     } else {
         OBVH_TRY_CUDA(cudaMemsetAsync(parents, 0xff, sizeof(uint32_t), s));
     }
-    aabb_up_kernel<<<grid_n, kThreads, 0, s>>>(nodes, parents, counts, costs, reinterpret_cast<uint32_t*>(ws + L.visits),
-                                               n, err);
+    {
+        ProfScope prof_scope_("aabb_up_kernel", s);
+        aabb_up_kernel<<<grid_n, kThreads, 0, s>>>(nodes, parents, counts, costs, reinterpret_cast<uint32_t*>(ws + L.visits),
+                                                   n, err);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     if (bounds_out)
         OBVH_TRY_CUDA(cudaMemcpyAsync(bounds_out, boxes, 2 * sizeof(kr_aabb3), cudaMemcpyDeviceToDevice, s));

@@ -353,24 +353,42 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec
     const unsigned gi = (internal + kThreads - 1) / kThreads;
 
     if (internal > 0) OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.visits, 0, 4ull * internal, s));
-    summary_up_kernel<<<gl, kThreads, 0, s>>>(nodes, parents, verts, faces, n, internal, summary, counts,
-                                              reinterpret_cast<uint32_t*>(ws + L.visits), obbs, xfs, &ctl->error);
+    {
+        ProfScope prof_scope_("summary_up_kernel", s);
+        summary_up_kernel<<<gl, kThreads, 0, s>>>(nodes, parents, verts, faces, n, internal, summary, counts,
+                                                  reinterpret_cast<uint32_t*>(ws + L.visits), obbs, xfs, &ctl->error);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     if (internal == 0) return kr_success;
-    dfs_rank_kernel<<<gl, kThreads, 0, s>>>(nodes, parents, counts, verts, faces, n, internal, first, tris,
-                                            &ctl->error);
+    {
+        ProfScope prof_scope_("dfs_rank_kernel", s);
+        dfs_rank_kernel<<<gl, kThreads, 0, s>>>(nodes, parents, counts, verts, faces, n, internal, first, tris,
+                                                &ctl->error);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
-    candidate_kernel<<<gi, kThreads, 0, s>>>(summary, verts, counts, internal, cand, nunits, keys, &ctl->error);
+    {
+        ProfScope prof_scope_("candidate_kernel", s);
+        candidate_kernel<<<gi, kThreads, 0, s>>>(summary, verts, counts, internal, cand, nunits, keys, &ctl->error);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
-    extents_small_kernel<<<gi, kThreads, 0, s>>>(cand, counts, first, tris, internal, obbs, xfs, &ctl->error);
+    {
+        ProfScope prof_scope_("extents_small_kernel", s);
+        extents_small_kernel<<<gi, kThreads, 0, s>>>(cand, counts, first, tris, internal, obbs, xfs, &ctl->error);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     OBVH_TRY(exclusive_scan_u32(nunits, ustart, internal, &ctl->total_units, ws + L.scan, s));
     OBVH_TRY_CUDA(cudaMemsetAsync(&ctl->unit_counter, 0, sizeof(uint32_t), s));
     const int grid = 4 * device_info().sm_count;
-    extents_units_kernel<<<grid, kThreads, 0, s>>>(cand, counts, first, tris, nunits, ustart, internal, ctl, keys,
-                                                   obbs, xfs);
+    {
+        ProfScope prof_scope_("extents_units_kernel", s);
+        extents_units_kernel<<<grid, kThreads, 0, s>>>(cand, counts, first, tris, nunits, ustart, internal, ctl, keys,
+                                                       obbs, xfs);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
-    finalize_multi_kernel<<<gi, kThreads, 0, s>>>(cand, nunits, keys, internal, obbs, xfs, &ctl->error);
+    {
+        ProfScope prof_scope_("finalize_multi_kernel", s);
+        finalize_multi_kernel<<<gi, kThreads, 0, s>>>(cand, nunits, keys, internal, obbs, xfs, &ctl->error);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     return kr_success;
 }

@@ -1,8 +1,15 @@
 // runtime.cu - host runtime helpers (errors, device info, cached buffers).
 #include "runtime.h"
 
+#include <cstring>
+
+#include <atomic>
+#include <cstdio>
+#include <map>
 #include <mutex>
+#include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "obvh_api.h"
 
@@ -67,7 +74,79 @@ void PinnedBuffer::release() {
     bytes = 0;
 }
 
+namespace {
+std::atomic<bool> g_prof{false};
+std::mutex g_prof_mutex;
+struct ProfEvent {
+    const char* name;
+    cudaEvent_t ev;
+    bool begin;
+};
+std::vector<ProfEvent> g_prof_events;
+std::vector<cudaEvent_t> g_prof_pool;
+size_t g_prof_used = 0;
+}  // namespace
+
+bool profiling() { return g_prof.load(std::memory_order_relaxed); }
+
+void prof_record(const char* name, cudaStream_t s, bool begin) {
+    std::lock_guard<std::mutex> lock(g_prof_mutex);
+    if (g_prof_used == g_prof_pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        g_prof_pool.push_back(e);
+    }
+    cudaEvent_t e = g_prof_pool[g_prof_used++];
+    cudaEventRecord(e, s);
+    g_prof_events.push_back({name, e, begin});
+}
+
 }  // namespace obvh
+
+extern "C" kr_error obvh_profile_enable(int on) {
+    std::lock_guard<std::mutex> lock(obvh::g_prof_mutex);
+    obvh::g_prof_events.clear();
+    obvh::g_prof_used = 0;
+    obvh::g_prof.store(on != 0);
+    return kr_success;
+}
+
+extern "C" kr_error obvh_profile_summary(char* buf, kr_size cap) {
+    if (!buf || cap == 0) return "obvh_profile_summary: null buffer";
+    std::lock_guard<std::mutex> lock(obvh::g_prof_mutex);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return obvh::cuda_error(e);
+    // pair each begin with the next end of the same name (launch sites nest nothing)
+    std::map<std::string, std::pair<int, double>> agg;
+    std::map<std::string, std::vector<cudaEvent_t>> open;
+    for (const auto& r : obvh::g_prof_events) {
+        if (r.begin) {
+            open[r.name].push_back(r.ev);
+            continue;
+        }
+        auto& st = open[r.name];
+        if (st.empty()) continue;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, st.back(), r.ev);
+        st.pop_back();
+        auto& a = agg[r.name];
+        a.first += 1;
+        a.second += ms;
+    }
+    std::string out = "{";
+    bool first = true;
+    for (const auto& kv : agg) {
+        char item[256];
+        std::snprintf(item, sizeof item, "%s\"%s\": [%d, %.6f]", first ? "" : ", ", kv.first.c_str(), kv.second.first,
+                      kv.second.second);
+        out += item;
+        first = false;
+    }
+    out += "}";
+    if (out.size() + 1 > cap) return "obvh_profile_summary: buffer too small";
+    std::memcpy(buf, out.c_str(), out.size() + 1);
+    return kr_success;
+}
 
 extern "C" kr_error obvh_last_error(void) { return obvh::t_last_error; }
 

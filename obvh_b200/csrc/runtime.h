@@ -53,4 +53,22 @@ struct PinnedBuffer {
     void release();
 };
 
+// ---------------------------------------------------------------------------
+// Per-kernel timing, off by default (obvh_profile_enable).  A ProfScope around
+// a launch records an event pair on the launching stream; the summary gives
+// launches and total device time per kernel name.
+bool profiling();
+void prof_record(const char* name, cudaStream_t s, bool begin);
+
+struct ProfScope {
+    const char* name;
+    cudaStream_t s;
+    ProfScope(const char* n, cudaStream_t st) : name(n), s(st) {
+        if (profiling()) prof_record(name, s, true);
+    }
+    ~ProfScope() {
+        if (profiling()) prof_record(name, s, false);
+    }
+};
+
 }  // namespace obvh

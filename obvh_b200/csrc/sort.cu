@@ -209,11 +209,17 @@ kr_error sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt, uin
     uint32_t* src_v = vals;
     uint32_t* dst_v = vals_alt;
     for (int shift = begin_bit; shift < end_bit; shift += 8) {
-        radix_hist<K><<<ntiles, kSortThreads, 0, stream>>>(src_k, n, shift, counts, ntiles);
+        {
+            ProfScope prof_scope_("radix_hist", stream);
+            radix_hist<K><<<ntiles, kSortThreads, 0, stream>>>(src_k, n, shift, counts, ntiles);
+        }
         OBVH_TRY_CUDA(cudaGetLastError());
         OBVH_TRY(exclusive_scan_u32(counts, counts, ncounts, nullptr, scan_temp, stream));
-        radix_scatter<K><<<ntiles, kSortThreads, sizeof(ScatterSmem<K>), stream>>>(src_k, src_v, dst_k, dst_v, n,
-                                                                                   shift, counts, ntiles);
+        {
+            ProfScope prof_scope_("radix_scatter", stream);
+            radix_scatter<K><<<ntiles, kSortThreads, sizeof(ScatterSmem<K>), stream>>>(src_k, src_v, dst_k, dst_v, n,
+                                                                                       shift, counts, ntiles);
+        }
         OBVH_TRY_CUDA(cudaGetLastError());
         std::swap(src_k, dst_k);
         std::swap(src_v, dst_v);
@@ -242,16 +248,25 @@ kr_error exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint3
     }
     const uint64_t nb = div_up(n, kScanTile);
     if (nb == 1) {
-        scan_tiles<<<1, kScanThreads, 0, stream>>>(in, out, n, nullptr, total);
+        {
+            ProfScope prof_scope_("scan_tiles", stream);
+            scan_tiles<<<1, kScanThreads, 0, stream>>>(in, out, n, nullptr, total);
+        }
         OBVH_TRY_CUDA(cudaGetLastError());
         return kr_success;
     }
     uint32_t* sums = static_cast<uint32_t*>(temp);
     void* rest = sums + ((nb + 63) & ~63ull);
-    scan_tile_sums<<<static_cast<unsigned>(nb), kScanThreads, 0, stream>>>(in, n, sums);
+    {
+        ProfScope prof_scope_("scan_tile_sums", stream);
+        scan_tile_sums<<<static_cast<unsigned>(nb), kScanThreads, 0, stream>>>(in, n, sums);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     OBVH_TRY(exclusive_scan_u32(sums, sums, nb, nullptr, rest, stream));
-    scan_tiles<<<static_cast<unsigned>(nb), kScanThreads, 0, stream>>>(in, out, n, sums, total);
+    {
+        ProfScope prof_scope_("scan_tiles", stream);
+        scan_tiles<<<static_cast<unsigned>(nb), kScanThreads, 0, stream>>>(in, out, n, sums, total);
+    }
     OBVH_TRY_CUDA(cudaGetLastError());
     return kr_success;
 }
