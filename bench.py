@@ -241,6 +241,10 @@ def tree_bytes_per_launch(n):
         "extents_small_kernel": 96 * ni + 124 * ni,    # frame in; box + transform out
         "extents_units_kernel": 36 * n,                # ordered triangles in
         "mark_up_kernel": 36 * nn + 16 * nn + 36 * n,
+        # fused build: leaf node (x2), ordered triangle, leaf box + transform out; box, face, vertices in
+        "leaves_fused_kernel": 4 * n + 24 * n + 52 * n + 72 * n + 36 * n + 124 * n,
+        # fused leaf-to-root pass: children in, bounds/counts/costs/collapsed node/summary out
+        "fused_up_kernel": 36 * n + 8 * n + 36 * n + 72 * ni + 16 * ni + 24 * ni + 36 * ni + 8 * ni + 224 * ni,
         "roots_kernel": 14 * nn,
         "gather_kernel": 8 * nn,
         "scan_tile_sums": 4 * nn,
@@ -260,9 +264,8 @@ def bench_tree_ours(a, dist):
     # two meshes alternated between steps (2 x 104 MB > 126 MB L2)
     host_meshes = [workloads.triangle_soup(n, seed=1 + 2 * dist.rank + j) for j in range(2)]
     meshes = [bvh.Mesh(v, f, device=dev) for v, f in host_meshes]
-    ws_bytes = max(int(lib.obvh_lbvh_workspace_bytes(n)), int(lib.obvh_obb_tree_workspace_bytes(n)),
-                   int(lib.obvh_collapse_workspace_bytes(n)))
-    ws = torch.zeros(ws_bytes, dtype=torch.uint8, device=dev)
+    ws = torch.empty(int(lib.obvh_build_workspace_bytes(n)), dtype=torch.uint8, device=dev)
+    _native.check(lib.obvh_build_workspace_init(ctypes.c_void_p(ws.data_ptr()), n, None))
     u8, i32, f32 = torch.uint8, torch.int32, torch.float32
     out = {"nodes": torch.empty(nn * 36, dtype=u8, device=dev), "parents": torch.empty(nn, dtype=i32, device=dev),
            "counts": torch.empty(nn, dtype=i32, device=dev), "costs": torch.empty(nn, dtype=f32, device=dev),
@@ -277,17 +280,16 @@ def bench_tree_ours(a, dist):
     def step(j, mesh=None):
         m = mesh or meshes[j & 1]
         V, F = ctypes.c_void_p(m.verts.data_ptr()), ctypes.c_void_p(m.faces.data_ptr())
-        _native.check(lib.obvh_lbvh_build_async(V, F, n, P["nodes"], P["parents"], P["counts"], P["costs"],
-                                                P["bounds"], W, S))
-        _native.check(lib.obvh_bvh_obb_tree_async(P["nodes"], P["parents"], V, F, P["obbs"], P["xfs"], n, n - 1, W, S))
-        _native.check(lib.obvh_bvh_collapse_async(P["nodes"], P["parents"], P["collapsed"], P["counts"], P["prims"],
-                                                  P["costs"], 1.2, 1.0, n, n - 1, W, S))
+        _native.check(lib.obvh_build_async(V, F, n, bvh.BUILD_OBBS | bvh.BUILD_COLLAPSE, 1.2, 1.0, P["nodes"],
+                                           P["parents"], P["counts"], P["costs"], P["bounds"], P["obbs"], P["xfs"],
+                                           P["collapsed"], P["prims"], W, S))
 
     sampler = ClockSampler(dev.index, enabled=not a.profile)
     total_ms, prof, clocks = timed_steps(a, dist, step, sampler, stream)
-    err = int(ws[:4].view(i32).item())
-    if err != 0:
-        raise RuntimeError(f"device error word {err}")
+    err, slots = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    _native.check(lib.obvh_build_status(W, n, S, ctypes.byref(err), ctypes.byref(slots)))
+    if err.value != 0:
+        raise RuntimeError(f"device error word {err.value}")
     if a.profile:
         return {"profile": "lbvh_obb_tree", "tris": n, "ms_per_step": total_ms / a.steps, "kernels": prof}
 
@@ -336,7 +338,7 @@ def bench_tree_ours(a, dist):
         "kernels": kern, "gpu_launches": launches, "roofline": roof,
         "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mnodes/s",
                 "h2d_bytes_per_step": int(host_meshes[0][0].nbytes + n * 16), "d2h_bytes_per_step": 64,
-                "api": "obvh_lbvh_build_async + obvh_bvh_obb_tree_async + obvh_bvh_collapse_async, pinned host mesh"},
+                "api": "obvh_build_async (LBVH + OBB tree + collapse), pinned host mesh"},
         "clocks": clocks,
     }
     if dist.rank == 0 and dist.world == 1:

@@ -1,0 +1,52 @@
+/*
+ * obvh_build.h - the full commit of the reference's lbvh_gpu intersector on
+ * the GPU in one chain of kernels: LBVH build, AABB-BVH -> OBB-tree transform
+ * of the uncollapsed tree, and node collapse (src/ads/lbvh_gpu/lbvh.cu:
+ * 1646-1723, which calls the steps of obvh_lbvh.h and obvh_transforms.h one
+ * after the other).  The results are those of the separate steps:
+ * obvh_lbvh_build_async, then kr_cuda_bvh_obb_tree, then kr_cuda_bvh_collapse
+ * (with the collapse's costs and counts replacing the build's when
+ * OBVH_BUILD_COLLAPSE is set).  No single reference entry point corresponds.
+ */
+#ifndef OBVH_BUILD_H
+#define OBVH_BUILD_H
+
+#include "obvh_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OBVH_BUILD_OBBS 0x1u     /* fill d_obbs / d_transforms */
+#define OBVH_BUILD_COLLAPSE 0x2u /* fill d_collapsed / d_primitives */
+
+/* Device workspace bytes for `face_count` triangles. */
+OBVH_EXPORT kr_size obvh_build_workspace_bytes(kr_u32 face_count);
+
+/* Zeroes what must start at zero; once, before the first build. */
+OBVH_EXPORT kr_error obvh_build_workspace_init(void* d_workspace, kr_u32 face_count, void* stream);
+
+/*
+ * Enqueues the build on `stream`.  Device pointers; the node arrays have
+ * 2n-1 entries (n = face_count), d_primitives n entries, d_bounds (nullable)
+ * 2 boxes (scene, centroid).  ci/ct are the collapse's SAH constants.
+ */
+OBVH_EXPORT kr_error obvh_build_async(const kr_vec3* d_vertices, const kr_uvec4* d_faces, kr_u32 face_count,
+                                      kr_u32 flags, kr_scalar ci, kr_scalar ct, kr_bvh_node* d_nodes,
+                                      kr_u32* d_parents, kr_u32* d_primitive_counts, kr_scalar* d_costs,
+                                      kr_aabb3* d_bounds, kr_obb3* d_obbs, kr_mat4* d_transforms,
+                                      kr_bvh_node* d_collapsed, kr_u32* d_primitives, void* d_workspace,
+                                      void* stream);
+
+/*
+ * After a build (synchronises `stream`): the device error word (0 = none) and
+ * the number of primitive slots the collapsed leaves use.
+ */
+OBVH_EXPORT kr_error obvh_build_status(const void* d_workspace, kr_u32 face_count, void* stream,
+                                       kr_u32* device_error, kr_u32* primitive_slots);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OBVH_BUILD_H */

@@ -57,6 +57,10 @@ def _declare(lib: ctypes.CDLL) -> None:
                                           vp, vp]),
         "obvh_profile_enable": (err, [c.c_int]),
         "obvh_profile_summary": (err, [c.c_char_p, c.c_uint64]),
+        "obvh_build_workspace_bytes": (c.c_uint64, [c.c_uint32]),
+        "obvh_build_workspace_init": (err, [vp, c.c_uint32, vp]),
+        "obvh_build_async": (err, [vp, vp, c.c_uint32, c.c_uint32, c.c_float, c.c_float] + [vp] * 11),
+        "obvh_build_status": (err, [vp, c.c_uint32, vp, c.POINTER(c.c_uint32), c.POINTER(c.c_uint32)]),
         "obvh_dito_workspace_report": (err, [vp, vp, c.POINTER(c.c_uint32), c.POINTER(c.c_float),
                                              c.POINTER(c.c_uint32)]),
     }

@@ -170,3 +170,59 @@ def collapse(tree: dict, ci: float = 1.2, ct: float = 1.0, metrics: bool = False
     if metrics:
         out["metrics"] = (m[0], m[1])
     return out
+
+
+BUILD_OBBS = 0x1
+BUILD_COLLAPSE = 0x2
+
+
+class ObvhBuilder:
+    """obvh_build_async: LBVH + OBB tree + collapse in one chain of kernels,
+    with the workspace kept between builds."""
+
+    def __init__(self, device="cuda"):
+        import torch
+        self.torch = torch
+        self.device = torch.device(device)
+        self.lib = _native.lib()
+        self.ws = None
+        self.ws_faces = -1
+
+    def _workspace(self, n, s):
+        if self.ws is None or n > self.ws_faces:
+            self.ws = self.torch.empty(int(self.lib.obvh_build_workspace_bytes(n)), dtype=self.torch.uint8,
+                                       device=self.device)
+            self.ws_faces = n
+            _native.check(self.lib.obvh_build_workspace_init(_ptr(self.ws), n, s))
+        return self.ws
+
+    def outputs(self, n):
+        t = self.torch
+        nn = 2 * n - 1
+        d = self.device
+        return {"nodes": t.empty(nn * NODE_BYTES, dtype=t.uint8, device=d),
+                "parents": t.empty(nn, dtype=t.int32, device=d), "counts": t.empty(nn, dtype=t.int32, device=d),
+                "costs": t.empty(nn, dtype=t.float32, device=d), "bounds": t.empty(12, dtype=t.float32, device=d),
+                "obbs": t.empty((nn, 15), dtype=t.float32, device=d),
+                "transforms": t.empty((nn, 16), dtype=t.float32, device=d),
+                "collapsed": t.empty(nn * NODE_BYTES, dtype=t.uint8, device=d),
+                "primitives": t.zeros(n, dtype=t.int32, device=d)}
+
+    def build(self, mesh: Mesh, flags=BUILD_OBBS | BUILD_COLLAPSE, ci=1.2, ct=1.0, stream=None, out=None):
+        n = mesh.n_faces
+        s = _stream(self.torch, stream)
+        ws = self._workspace(n, s)
+        o = out if out is not None else self.outputs(n)
+        e = self.lib.obvh_build_async(_ptr(mesh.verts), _ptr(mesh.faces), n, flags, ci, ct, _ptr(o["nodes"]),
+                                      _ptr(o["parents"]), _ptr(o["counts"]), _ptr(o["costs"]), _ptr(o["bounds"]),
+                                      _ptr(o["obbs"]), _ptr(o["transforms"]), _ptr(o["collapsed"]),
+                                      _ptr(o["primitives"]), _ptr(ws), s)
+        _native.check(e)
+        return o
+
+    def status(self, n, stream=None):
+        err = ctypes.c_uint32(0)
+        slots = ctypes.c_uint32(0)
+        _native.check(self.lib.obvh_build_status(_ptr(self.ws), n, _stream(self.torch, stream), ctypes.byref(err),
+                                                 ctypes.byref(slots)))
+        return err.value, slots.value

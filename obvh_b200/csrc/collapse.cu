@@ -63,9 +63,7 @@ __global__ void __launch_bounds__(kThreads) mark_up_kernel(const kr_bvh_node* no
             atomicOr(err, kErrCycle);
             return;
         }
-        __threadfence();
-        if (atomicAdd(visits + p, 1u) == 0) return;
-        __threadfence();
+        if (arrive(visits + p) == 0) return;
         const NodeView pn = load_node(nodes, p);
         const uint32_t count = __ldcg(counts + pn.left) + __ldcg(counts + pn.right);
         __stcg(counts + p, count);

@@ -191,8 +191,10 @@ __device__ __forceinline__ int delta(const uint32_t* codes, int i, int j, uint32
 
 __device__ __forceinline__ int halve_up(int x) { return x == 1 ? 0 : ((x % 2) == 1 ? x / 2 + 1 : x / 2); }
 
+// first (nullable) receives each internal node's first leaf in depth-first
+// order: the lower end of its key range.
 __global__ void __launch_bounds__(kThreads) karras_kernel(const uint32_t* codes, uint32_t n, kr_bvh_node* nodes,
-                                                          uint32_t* parents) {
+                                                          uint32_t* parents, uint32_t* first) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t internal = n - 1;
     if (i >= static_cast<int>(internal)) return;
@@ -222,6 +224,7 @@ __global__ void __launch_bounds__(kThreads) karras_kernel(const uint32_t* codes,
     w[6] = left;
     w[7] = right;
     w[8] = 0;  // nPrimitives 0, axis 0
+    if (first) first[i] = static_cast<uint32_t>(lo);
     if (i == 0) parents[0] = tree::kNoParent;
 }
 
@@ -245,9 +248,7 @@ __global__ void __launch_bounds__(kThreads) aabb_up_kernel(kr_bvh_node* nodes, c
             atomicOr(err, kErrCycle);
             return;
         }
-        __threadfence();
-        if (atomicAdd(visits + p, 1u) == 0) return;
-        __threadfence();
+        if (tree::arrive(visits + p) == 0) return;
         const tree::NodeView pn = tree::load_node(nodes, p);
         const tree::NodeView L = tree::load_node(nodes, pn.left), R = tree::load_node(nodes, pn.right);
         float lo[3], hi[3];
@@ -312,20 +313,13 @@ kr_error enqueue_bounds(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n,
     return kr_success;
 }
 
-kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, kr_bvh_node* nodes,
-                       uint32_t* parents, uint32_t* counts, float* costs, kr_aabb3* bounds_out, void* workspace,
-                       cudaStream_t s) {
-    if (n < 1) return "obvh_lbvh_build: at least one primitive is needed";
-    if (!verts || !faces || !nodes || !parents || !counts || !costs || !workspace)
-        return "obvh_lbvh_build: null pointer argument";
-    if (reinterpret_cast<uintptr_t>(workspace) & 255) return "obvh_lbvh_build: workspace must be 256-byte aligned";
+kr_error enqueue_codes(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, void* workspace, cudaStream_t s,
+                       Codes* out) {
     char* ws = static_cast<char*>(workspace);
     const Layout L = layout(n);
     float* tri = reinterpret_cast<float*>(ws + L.tri);
     kr_aabb3* boxes = reinterpret_cast<kr_aabb3*>(ws + L.boxes);
-    uint32_t* err = &reinterpret_cast<Ctl*>(ws + L.ctl)->error;
     const unsigned grid_n = (n + kThreads - 1) / kThreads;
-
     OBVH_TRY(enqueue_bounds(verts, faces, n, tri, ws, boxes, boxes + 1, true, s));
     {
         ProfScope prof_scope_("morton_kernel", s);
@@ -336,31 +330,51 @@ kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, 
     bool alt = false;
     OBVH_TRY(radix_sort_pairs(ws + L.keys0, ws + L.keys1, reinterpret_cast<uint32_t*>(ws + L.vals0),
                               reinterpret_cast<uint32_t*>(ws + L.vals1), n, 4, 0, 30, ws + L.sort, s, &alt));
-    const uint32_t* codes = reinterpret_cast<const uint32_t*>(ws + (alt ? L.keys1 : L.keys0));
-    const uint32_t* order = reinterpret_cast<const uint32_t*>(ws + (alt ? L.vals1 : L.vals0));
-    {
-        ProfScope prof_scope_("leaves_kernel", s);
-        leaves_kernel<<<grid_n, kThreads, 0, s>>>(tri, order, n, nodes);
-    }
-    OBVH_TRY_CUDA(cudaGetLastError());
+    out->codes = reinterpret_cast<const uint32_t*>(ws + (alt ? L.keys1 : L.keys0));
+    out->order = reinterpret_cast<const uint32_t*>(ws + (alt ? L.vals1 : L.vals0));
+    out->tri_boxes = tri;
+    out->boxes = boxes;
+    out->visits = reinterpret_cast<uint32_t*>(ws + L.visits);
+    out->err = &reinterpret_cast<Ctl*>(ws + L.ctl)->error;
+    return kr_success;
+}
+
+kr_error enqueue_karras(const uint32_t* codes, uint32_t n, kr_bvh_node* nodes, uint32_t* parents, uint32_t* first,
+                        cudaStream_t s) {
     if (n >= 2) {
-        {
-            ProfScope prof_scope_("karras_kernel", s);
-            karras_kernel<<<(n - 1 + kThreads - 1) / kThreads, kThreads, 0, s>>>(codes, n, nodes, parents);
-        }
+        ProfScope prof_scope_("karras_kernel", s);
+        karras_kernel<<<(n - 1 + kThreads - 1) / kThreads, kThreads, 0, s>>>(codes, n, nodes, parents, first);
         OBVH_TRY_CUDA(cudaGetLastError());
-        OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.visits, 0, 4ull * (n - 1), s));
     } else {
         OBVH_TRY_CUDA(cudaMemsetAsync(parents, 0xff, sizeof(uint32_t), s));
     }
+    return kr_success;
+}
+
+kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, kr_bvh_node* nodes,
+                       uint32_t* parents, uint32_t* counts, float* costs, kr_aabb3* bounds_out, void* workspace,
+                       cudaStream_t s) {
+    if (n < 1) return "obvh_lbvh_build: at least one primitive is needed";
+    if (!verts || !faces || !nodes || !parents || !counts || !costs || !workspace)
+        return "obvh_lbvh_build: null pointer argument";
+    if (reinterpret_cast<uintptr_t>(workspace) & 255) return "obvh_lbvh_build: workspace must be 256-byte aligned";
+    const unsigned grid_n = (n + kThreads - 1) / kThreads;
+    Codes c;
+    OBVH_TRY(enqueue_codes(verts, faces, n, workspace, s, &c));
+    {
+        ProfScope prof_scope_("leaves_kernel", s);
+        leaves_kernel<<<grid_n, kThreads, 0, s>>>(c.tri_boxes, c.order, n, nodes);
+    }
+    OBVH_TRY_CUDA(cudaGetLastError());
+    OBVH_TRY(enqueue_karras(c.codes, n, nodes, parents, nullptr, s));
+    if (n >= 2) OBVH_TRY_CUDA(cudaMemsetAsync(c.visits, 0, 4ull * (n - 1), s));
     {
         ProfScope prof_scope_("aabb_up_kernel", s);
-        aabb_up_kernel<<<grid_n, kThreads, 0, s>>>(nodes, parents, counts, costs, reinterpret_cast<uint32_t*>(ws + L.visits),
-                                                   n, err);
+        aabb_up_kernel<<<grid_n, kThreads, 0, s>>>(nodes, parents, counts, costs, c.visits, n, c.err);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     if (bounds_out)
-        OBVH_TRY_CUDA(cudaMemcpyAsync(bounds_out, boxes, 2 * sizeof(kr_aabb3), cudaMemcpyDeviceToDevice, s));
+        OBVH_TRY_CUDA(cudaMemcpyAsync(bounds_out, c.boxes, 2 * sizeof(kr_aabb3), cudaMemcpyDeviceToDevice, s));
     return kr_success;
 }
 

@@ -23,6 +23,21 @@ Layout layout(uint32_t n);
 kr_error enqueue_bounds(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, float* tri_boxes, char* ws,
                         kr_aabb3* scene_out, kr_aabb3* centroid_out, bool overwrite, cudaStream_t s);
 
+// Bounds, Morton codes and the stable sort; pointers into the workspace.
+struct Codes {
+    const uint32_t* codes;   // sorted codes
+    const uint32_t* order;   // primitive of sorted position j
+    const float* tri_boxes;  // 6 floats per primitive (unsorted)
+    kr_aabb3* boxes;         // scene, centroid
+    uint32_t* visits;        // n zero-able arrival counters
+    uint32_t* err;
+};
+kr_error enqueue_codes(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, void* workspace, cudaStream_t s,
+                       Codes* out);
+// Karras tree over sorted codes; first (nullable) gets each internal node's first leaf.
+kr_error enqueue_karras(const uint32_t* codes, uint32_t n, kr_bvh_node* nodes, uint32_t* parents, uint32_t* first,
+                        cudaStream_t s);
+
 // Full build into caller buffers (nodes/parents/counts/costs of 2n-1 entries).
 kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, kr_bvh_node* nodes,
                        uint32_t* parents, uint32_t* counts, float* costs, kr_aabb3* bounds_out, void* workspace,

@@ -17,8 +17,8 @@
 //                vertices (:676-756) and the initial extents along them.
 //   extents      min/max of every subtree vertex on the node's axes, read
 //                from the contiguous run: one thread per node up to 8 leaves,
-//                one warp per 1024-leaf unit above that (a persistent grid
-//                takes units from a counter); only nodes of more than one unit
+//                one warp per 1024-leaf unit above that (units dealt to the
+//                warps of a persistent grid); only nodes of more than one unit
 //                combine partial results, with 6 integer atomics per unit.
 //                Nodes finished here are finalised in place (:903-964).
 //   finalize     the multi-unit nodes.
@@ -46,9 +46,8 @@ constexpr uint32_t kUnit = 1024;     // leaves per warp unit
 
 struct Ctl {
     uint32_t error;
-    uint32_t unit_counter;
     uint32_t total_units;
-    uint32_t pad[61];
+    uint32_t pad[62];
 };
 
 // Per internal node after the candidate search (96 bytes):
@@ -92,9 +91,7 @@ __global__ void __launch_bounds__(kThreads) summary_up_kernel(const kr_bvh_node*
             atomicOr(err, kErrCycle);
             return;
         }
-        __threadfence();
-        if (atomicAdd(visits + p, 1u) == 0) return;
-        __threadfence();
+        if (arrive(visits + p) == 0) return;
         const uint32_t* w = reinterpret_cast<const uint32_t*>(nodes + p);
         const uint32_t L = __ldg(w + 6), R = __ldg(w + 7);
         const uint32_t other = (L == child) ? R : L;
@@ -158,7 +155,9 @@ __global__ void __launch_bounds__(kThreads) dfs_rank_kernel(const kr_bvh_node* n
     }
 }
 
-__global__ void __launch_bounds__(kThreads) candidate_kernel(const uint4* summary, const kr_vec3* verts,
+// `points` is the packed xyz array the summary's vertex ids index: the mesh
+// vertices, or the depth-first triangle slots of the fused build.
+__global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* summary, const kr_vec3* verts,
                                                              const uint32_t* counts, uint32_t internal, Cand* cand,
                                                              uint32_t* nunits, uint32_t* keys, const uint32_t* err) {
     const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -253,15 +252,14 @@ __global__ void __launch_bounds__(kThreads) extents_small_kernel(const Cand* can
 __global__ void __launch_bounds__(kThreads) extents_units_kernel(const Cand* cand, const uint32_t* counts,
                                                                  const uint32_t* first, const float* tris,
                                                                  const uint32_t* nunits, const uint32_t* unit_start,
-                                                                 uint32_t internal, Ctl* ctl, uint32_t* keys,
+                                                                 uint32_t internal, const uint32_t* err,
+                                                                 const uint32_t* total_units, uint32_t* keys,
                                                                  kr_obb3* obbs, kr_mat4* xfs) {
     const int lane = threadIdx.x & 31;
-    const uint32_t total = ctl->error ? 0u : ctl->total_units;
-    for (;;) {
-        uint32_t u = 0;
-        if (lane == 0) u = atomicAdd(&ctl->unit_counter, 1u);
-        u = __shfl_sync(0xffffffffu, u, 0);
-        if (u >= total) return;
+    const uint32_t total = *err ? 0u : *total_units;
+    // Units are dealt round-robin to the warps of the grid: no shared counter.
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t u = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < total; u += warps) {
         // the last node whose first unit is <= u owns it
         uint32_t lo_i = 0, hi_i = internal;  // search in [lo_i, hi_i)
         while (hi_i - lo_i > 1) {
@@ -350,7 +348,6 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec
     uint32_t* ustart = reinterpret_cast<uint32_t*>(ws + L.ustart);
     uint32_t* keys = reinterpret_cast<uint32_t*>(ws + L.keys);
     const unsigned gl = (n + kThreads - 1) / kThreads;
-    const unsigned gi = (internal + kThreads - 1) / kThreads;
 
     if (internal > 0) OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.visits, 0, 4ull * internal, s));
     {
@@ -366,28 +363,50 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec
                                                 &ctl->error);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
+    FrameBuffers fb;
+    fb.summary = summary;
+    fb.points = verts;
+    fb.counts = counts;
+    fb.first = first;
+    fb.tris = tris;
+    fb.cand = cand;
+    fb.nunits = nunits;
+    fb.ustart = ustart;
+    fb.keys = keys;
+    fb.scan = ws + L.scan;
+    fb.err = &ctl->error;
+    fb.total_units = &ctl->total_units;
+    return enqueue_frames(fb, internal, obbs, xfs, s);
+}
+
+size_t cand_bytes(uint32_t internal) { return sizeof(Cand) * (internal > 0 ? internal : 1); }
+
+kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs, kr_mat4* xfs, cudaStream_t s) {
+    if (internal == 0) return kr_success;
+    const unsigned gi = (internal + kThreads - 1) / kThreads;
+    Cand* cand = static_cast<Cand*>(b.cand);
     {
         ProfScope prof_scope_("candidate_kernel", s);
-        candidate_kernel<<<gi, kThreads, 0, s>>>(summary, verts, counts, internal, cand, nunits, keys, &ctl->error);
+        candidate_kernel<<<gi, kThreads, 0, s>>>(b.summary, b.points, b.counts, internal, cand, b.nunits, b.keys,
+                                                 b.err);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     {
         ProfScope prof_scope_("extents_small_kernel", s);
-        extents_small_kernel<<<gi, kThreads, 0, s>>>(cand, counts, first, tris, internal, obbs, xfs, &ctl->error);
+        extents_small_kernel<<<gi, kThreads, 0, s>>>(cand, b.counts, b.first, b.tris, internal, obbs, xfs, b.err);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
-    OBVH_TRY(exclusive_scan_u32(nunits, ustart, internal, &ctl->total_units, ws + L.scan, s));
-    OBVH_TRY_CUDA(cudaMemsetAsync(&ctl->unit_counter, 0, sizeof(uint32_t), s));
+    OBVH_TRY(exclusive_scan_u32(b.nunits, b.ustart, internal, b.total_units, b.scan, s));
     const int grid = 4 * device_info().sm_count;
     {
         ProfScope prof_scope_("extents_units_kernel", s);
-        extents_units_kernel<<<grid, kThreads, 0, s>>>(cand, counts, first, tris, nunits, ustart, internal, ctl, keys,
-                                                       obbs, xfs);
+        extents_units_kernel<<<grid, kThreads, 0, s>>>(cand, b.counts, b.first, b.tris, b.nunits, b.ustart, internal,
+                                                       b.err, b.total_units, b.keys, obbs, xfs);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     {
         ProfScope prof_scope_("finalize_multi_kernel", s);
-        finalize_multi_kernel<<<gi, kThreads, 0, s>>>(cand, nunits, keys, internal, obbs, xfs, &ctl->error);
+        finalize_multi_kernel<<<gi, kThreads, 0, s>>>(cand, b.nunits, b.keys, internal, obbs, xfs, b.err);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     return kr_success;

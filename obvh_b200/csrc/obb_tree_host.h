@@ -22,5 +22,26 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec
                  kr_obb3* obbs, kr_mat4* xfs, uint32_t n, uint32_t internal, void* workspace, cudaStream_t s);
 uint32_t* error_word(void* workspace);
 
+// The stages after the subtree summaries: candidate frames, extents and the
+// final boxes of the internal nodes [0, internal).  points[id] (packed xyz)
+// resolves the summaries' vertex ids; tris holds each subtree's triangles
+// contiguously in depth-first order, node a's starting at first[a].
+struct FrameBuffers {
+    const uint4* summary;      // 7 x uint4 per internal node
+    const kr_vec3* points;
+    const uint32_t* counts;    // leaves under each internal node
+    const uint32_t* first;
+    const float* tris;         // 9 floats per leaf, depth-first
+    void* cand;                // cand_bytes(internal)
+    uint32_t* nunits;          // internal entries each
+    uint32_t* ustart;
+    uint32_t* keys;            // 6 per internal node
+    void* scan;                // scan_temp_bytes(internal)
+    uint32_t* err;
+    uint32_t* total_units;
+};
+size_t cand_bytes(uint32_t internal);
+kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs, kr_mat4* xfs, cudaStream_t s);
+
 }  // namespace obbtree
 }  // namespace obvh

@@ -19,6 +19,15 @@ namespace tree {
 
 constexpr uint32_t kNoParent = 0xffffffffu;
 
+// Arrival at a node in a bottom-up pass: returns how many threads arrived
+// before.  Release orders this thread's writes of its child's data before the
+// count; acquire makes the other child's data visible to the second arrival.
+__device__ __forceinline__ uint32_t arrive(uint32_t* counter) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
+    return old;
+}
+
 // kr_bvh_node field access through 4-byte words (the struct is 36 bytes,
 // 4-byte aligned): words 0..5 bounds, 6 left|primitivesOffset, 7 right,
 // 8 nPrimitives | axis << 16.
@@ -256,13 +265,14 @@ struct Candidate {
     f3 lo, hi;  // slots 3..5
 };
 
+// kr_min/kr_max over finite values equal fminf/fmaxf up to the sign of a zero.
 __device__ __forceinline__ void extent_proj(const f3* P, f3 d, float& lo, float& hi) {
     lo = hi = dot3(P[0], d);
 #pragma unroll
     for (int i = 1; i < 14; ++i) {
         float q = dot3(P[i], d);
-        lo = kmin(lo, q);
-        hi = kmax(hi, q);
+        lo = fminf(lo, q);
+        hi = fmaxf(hi, q);
     }
 }
 
@@ -331,7 +341,6 @@ __device__ inline Candidate node_candidate(const f3* P, const Summary& s) {
     const f3 e1 = unit3(sub3(p1, p2));
     const f3 e2 = unit3(sub3(p2, p0));
     const f3 n = unit3(cross3(e1, e0));
-    score_frames(P, n, e0, e1, e2, b, blen, bmid, best);
 
     float qlo = dot3(P[0], n), qhi = qlo;
     f3 q1 = P[0], q0 = P[0];
@@ -343,19 +352,27 @@ __device__ inline Candidate node_candidate(const f3* P, const Summary& s) {
     }
     const float tri = dot3(p0, n);
     const bool up = qhi - eps > tri, down = qlo + eps < tri;
+    // A flat set returns before the reference's scores are used (:737-743),
+    // so the test can come first and all frames go through one scorer loop
+    // in the reference's order: base triangle, upper faces, lower faces.
     if (!up && !down) return stale;
+    f3 tn[7], te[7][3];
+    int nt = 0;
+    tn[nt] = n; te[nt][0] = e0; te[nt][1] = e1; te[nt][2] = e2; ++nt;
     if (up) {
         const f3 f0 = unit3(sub3(q0, p0)), f1 = unit3(sub3(q0, p1)), f2 = unit3(sub3(q0, p2));
-        score_frames(P, unit3(cross3(f1, e0)), e0, f1, f0, b, blen, bmid, best);
-        score_frames(P, unit3(cross3(f2, e1)), e1, f2, f1, b, blen, bmid, best);
-        score_frames(P, unit3(cross3(f0, e2)), e2, f0, f2, b, blen, bmid, best);
+        tn[nt] = unit3(cross3(f1, e0)); te[nt][0] = e0; te[nt][1] = f1; te[nt][2] = f0; ++nt;
+        tn[nt] = unit3(cross3(f2, e1)); te[nt][0] = e1; te[nt][1] = f2; te[nt][2] = f1; ++nt;
+        tn[nt] = unit3(cross3(f0, e2)); te[nt][0] = e2; te[nt][1] = f0; te[nt][2] = f2; ++nt;
     }
     if (down) {
         const f3 g0 = unit3(sub3(q1, p0)), g1 = unit3(sub3(q1, p1)), g2 = unit3(sub3(q1, p2));
-        score_frames(P, unit3(cross3(g1, e0)), e0, g1, g0, b, blen, bmid, best);
-        score_frames(P, unit3(cross3(g2, e1)), e1, g2, g1, b, blen, bmid, best);
-        score_frames(P, unit3(cross3(g0, e2)), e2, g0, g2, b, blen, bmid, best);
+        tn[nt] = unit3(cross3(g1, e0)); te[nt][0] = e0; te[nt][1] = g1; te[nt][2] = g0; ++nt;
+        tn[nt] = unit3(cross3(g2, e1)); te[nt][0] = e1; te[nt][1] = g2; te[nt][2] = g1; ++nt;
+        tn[nt] = unit3(cross3(g0, e2)); te[nt][0] = e2; te[nt][1] = g0; te[nt][2] = g2; ++nt;
     }
+#pragma unroll 1
+    for (int t = 0; t < nt; ++t) score_frames(P, tn[t], te[t][0], te[t][1], te[t][2], b, blen, bmid, best);
     c.b0 = b[0]; c.b1 = b[1]; c.b2 = b[2];
     c.lo = blen;
     c.hi = bmid;

@@ -1,0 +1,92 @@
+"""GPU parity of the fused commit (obvh_build_async: LBVH + OBB tree +
+collapse in one chain) against the oracle running the three steps in turn."""
+import numpy as np
+import pytest
+
+from conftest import same_bits
+from oracle import bvh as ref
+from obvh_b200 import bvh, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def builder():
+    import torch
+    assert torch.cuda.is_available()
+    return bvh.ObvhBuilder()
+
+
+def _run(builder, v, f, flags, ci=1.2, ct=1.0):
+    import torch
+    mesh = bvh.Mesh(v, f)
+    o = builder.build(mesh, flags=flags, ci=ci, ct=ct)
+    torch.cuda.synchronize()
+    err, slots = builder.status(mesh.n_faces)
+    assert err == 0
+    return o, slots
+
+
+def _expect(v, f, ci=1.2, ct=1.0):
+    r = ref.lbvh_build(v, f)
+    obbs, xfs, _ = ref.obb_tree(r["nodes"], r["parents"], v, f)
+    col, cnt, prims, cst, used = ref.collapse(r["nodes"], r["parents"], r["counts"], r["costs"], ci, ct)
+    return r, obbs, xfs, col, cnt, prims, cst, used
+
+
+def _check(o, slots, exp, n, flags):
+    r, obbs, xfs, col, cnt, prims, cst, used = exp
+    nodes = bvh.nodes_numpy(o["nodes"])
+    ni = n - 1
+    assert same_bits(nodes["b"], r["nodes"]["b"])
+    assert np.array_equal(nodes["left"], r["nodes"]["left"])
+    assert np.array_equal(nodes["right"][:ni], r["nodes"]["right"][:ni])
+    assert np.array_equal(nodes["n_prims"], r["nodes"]["n_prims"])
+    assert np.array_equal(o["parents"].cpu().numpy().view(np.uint32), r["parents"])
+    assert same_bits(o["bounds"].cpu().numpy(), np.concatenate([r["scene"], r["centroid"]]))
+    if flags & bvh.BUILD_OBBS:
+        assert same_bits(o["obbs"].cpu().numpy(), obbs)
+        assert same_bits(o["transforms"].cpu().numpy(), xfs)
+    counts = o["counts"].cpu().numpy().view(np.uint32)
+    costs = o["costs"].cpu().numpy()
+    if flags & bvh.BUILD_COLLAPSE:
+        c = bvh.nodes_numpy(o["collapsed"])
+        assert same_bits(c["b"], col["b"])
+        assert np.array_equal(c["left"], col["left"])
+        assert np.array_equal(c["right"][:ni], col["right"][:ni])
+        assert np.array_equal(c["n_prims"], col["n_prims"])
+        assert np.array_equal(counts, cnt)
+        assert same_bits(costs, cst)
+        assert slots == used
+        assert np.array_equal(o["primitives"].cpu().numpy().view(np.uint32)[:used], prims[:used])
+    else:
+        assert np.array_equal(counts, r["counts"])
+        assert same_bits(costs, r["costs"])
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 17, 1000, 65_537])
+def test_fused_build_matches_the_three_steps(builder, n):
+    v, f = workloads.triangle_soup(n, seed=300 + n)
+    o, slots = _run(builder, v, f, 3)
+    _check(o, slots, _expect(v, f), n, 3)
+
+
+def test_fused_build_full_size(builder):
+    v, f = workloads.triangle_soup(2_000_000, seed=1)
+    o, slots = _run(builder, v, f, 3)
+    _check(o, slots, _expect(v, f), 2_000_000, 3)
+
+
+def test_fused_build_mesh_and_other_sah_constants(builder):
+    v, f = workloads.torus_knot_mesh(segments=256, around=112)
+    n = f.shape[0]
+    o, slots = _run(builder, v, f, 3, ci=0.8, ct=1.3)
+    _check(o, slots, _expect(v, f, 0.8, 1.3), n, 3)
+
+
+@pytest.mark.parametrize("flags", [0, 1, 2])
+def test_fused_build_partial_flags(builder, flags):
+    n = 20_000
+    v, f = workloads.triangle_soup(n, seed=41)
+    o, slots = _run(builder, v, f, flags)
+    _check(o, slots, _expect(v, f), n, flags)
