@@ -14,6 +14,12 @@ reference publishes no numbers, so vs_baseline is null):
 * ``dito`` - DiTO-14 fit of 100,000,000 points on an ellipsoid surface
   (semi-axes 4, 1, 0.25; rotated, noised, offset).  A step is one fit (two
   streaming passes).  Metric Mpoints/s.
+* ``dito_batch`` - DiTO-14 fits of 4,096 anisotropic Gaussian clouds of
+  log-uniform sizes 64..262,144 (about 129M points in one CSR buffer) in one
+  persistent work-stealing launch replayed from a CUDA graph, knobs picked by
+  the autotuner first.  A step is the whole batch.  Metric Mpoints/s; the line
+  also carries the plain per-call throughput (one obvh_dito_fit_async per set)
+  on the same device-resident buffer.
 
 Multi-GPU: every rank builds/fits its own input (independent units, no
 collective); ``value`` = units of all ranks / the slowest rank's device time
@@ -44,7 +50,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["lbvh_obb_tree", "dito"], default="lbvh_obb_tree")
+    ap.add_argument("--workload", choices=["lbvh_obb_tree", "dito", "dito_batch"], default="lbvh_obb_tree")
+    ap.add_argument("--sets", type=int, default=4096, help="dito_batch: point sets per batch")
+    ap.add_argument("--no-autotune", action="store_true", help="dito_batch: default knobs")
     ap.add_argument("--points", type=int, default=100_000_000, help="dito: points per fit")
     ap.add_argument("--tris", type=int, default=2_000_000, help="lbvh_obb_tree: triangles per build")
     ap.add_argument("--profile", action="store_true",
@@ -484,24 +492,157 @@ def bench_dito_reference(a, dist):
             "e2e": {"value": round(value, 3), "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def bench_batch_ours(a, dist):
+    import numpy as np
+    import torch
+    from obvh_b200 import _native, workloads
+    from obvh_b200.batch import DitoBatch, points_obb_batch
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    pts, offsets = workloads.gaussian_sets_torch(a.sets, seed=3 + dist.rank, device=dev)
+    total = int(offsets[-1])
+    out = torch.empty((a.sets, 15), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    batch = DitoBatch(offsets)
+    tuning, tuned_ms = (batch.tuning, None) if (a.no_autotune or a.profile) else batch.autotune(pts, out, repeats=3)
+    batch.capture(pts, out)
+    sampler = ClockSampler(dev.index, enabled=not a.profile)
+    total_ms, prof, clocks = timed_steps(a, dist, lambda j: batch.launch(stream), sampler, stream)
+    if batch.status(stream):
+        raise RuntimeError("device error word set")
+    if a.profile:
+        return {"profile": "dito_batch", "sets": a.sets, "points": total, "ms_per_step": total_ms / a.steps,
+                "kernels": prof}
+    peak, peak_kind = peaks()
+    value = dist.world * total * a.steps / (total_ms / 1e3) / 1e6
+    # every set (at most 3 MB) fits in L2 between its two passes: 12 B/point compulsory
+    roof = roofline(prof, {"dito_batch_kernel": 12 * total}, peak, peak_kind,
+                    os.path.join(ROOT, "profiles", "dito_batch_traffic.json"))
+
+    # plain per-call path on the same device-resident buffer: one fit per set
+    lib = _native.lib()
+    ws = torch.zeros(int(lib.obvh_dito_workspace_bytes()), dtype=torch.uint8, device=dev)
+    W, S = ctypes.c_void_p(ws.data_ptr()), ctypes.c_void_p(stream.cuda_stream)
+    base, obase = pts.data_ptr(), out.data_ptr()
+    calls = [(ctypes.c_void_p(base + 12 * int(offsets[s])), int(offsets[s + 1] - offsets[s]),
+              ctypes.c_void_p(obase + 60 * s)) for s in range(a.sets)]
+
+    def per_call():
+        for p, n, o in calls:
+            e = lib.obvh_dito_fit_async(p, n, 0, o, W, S)
+            if e:
+                _native.check(e)
+    per_call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 2
+    e0.record(stream)
+    for _ in range(reps):
+        per_call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    pc_ms = e0.elapsed_time(e1) / reps
+    pc_value = -dist.max(-(total / (pc_ms / 1e3) / 1e6)) * dist.world
+
+    host = torch.empty((total, 3), dtype=torch.float32, pin_memory=True)
+    host.copy_(pts)
+    host_np = host.numpy()
+    points_obb_batch(host_np, offsets)
+    e2e_steps = max(3, min(a.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        points_obb_batch(host_np, offsets)
+    e2e_s = time.perf_counter() - t0
+    e2e_min = -dist.max(-(total * e2e_steps / e2e_s / 1e6))
+    line = {
+        "metric": "Batched DiTO-14 fit throughput (Mpoints/s)", "value": round(value, 3), "unit": "Mpoints/s",
+        "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(total_ms / a.steps, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: anisotropic Gaussian clouds (sigma log-U[0.01,5] per axis), Haar rotation, "
+                "U[-100,100]^3 offset; sizes log-U[64,262144]",
+        "config": {"workload": "dito_batch", "sets_per_gpu": a.sets, "points_per_gpu": total, "point_bytes": 12,
+                   "l2": f"{12 * total / 1e9:.2f} GB of points per step (> 126 MB L2), no flush",
+                   "launch": "one graph: memset + one persistent kernel", "tuning": tuning,
+                   "autotuned_ms": tuned_ms, "parallelism": f"replicas{dist.world}"},
+        "kernels": {k: {"launches": v[0], "ms_per_step": round(v[1] / a.steps, 5)} for k, v in prof.items()},
+        "gpu_launches": sum(v[0] for v in prof.values()), "roofline": roof,
+        "per_call": {"value": round(pc_value, 3), "unit": "Mpoints/s", "ms_per_batch": round(pc_ms, 3),
+                     "api": "obvh_dito_fit_async per set (2 kernels per set), same device buffer",
+                     "speedup": round(value / pc_value, 2)},
+        "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mpoints/s", "h2d_bytes_per_step": 12 * total,
+                "d2h_bytes_per_step": 60 * a.sets + 4, "api": "obvh_points_obb_batch, pinned host"},
+        "clocks": clocks,
+    }
+    if dist.rank == 0 and dist.world == 1:
+        import oracle
+        threads = os.cpu_count() or 1
+        off = np.asarray(offsets, np.int64)
+        oracle.ref_dito14_batch(host_np, off[:65], threads)
+        t0 = time.perf_counter()
+        oracle.ref_dito14_batch(host_np, off, threads)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(total / dt / 1e6, 3), "unit": "Mpoints/s", "cores": threads,
+                                "kind": "reference",
+                                "sample": f"the whole {a.sets}-set batch once ({dt:.1f} s), reference DiTO_14 "
+                                          f"(oracle/_ref), one set per thread"}
+    return line
+
+
+def bench_batch_reference(a, dist):
+    """The reference's CPU DiTO_14 over the batch, one set per host thread."""
+    import numpy as np
+    import oracle
+    from obvh_b200 import workloads
+    try:
+        import torch
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        pts, offsets = workloads.gaussian_sets_torch(a.sets, seed=3, device=dev)
+        host = pts.cpu().numpy()
+    except Exception:
+        host, offsets = workloads.gaussian_sets(a.sets, seed=3)
+    host = np.ascontiguousarray(host, dtype=np.float32)
+    off = np.asarray(offsets, np.int64)
+    total = int(off[-1])
+    threads = os.cpu_count() or 1
+    for _ in range(a.warmup):
+        oracle.ref_dito14_batch(host, off[:65], threads)
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        oracle.ref_dito14_batch(host, off, threads)
+        times.append(time.perf_counter() - t0)
+    value = total * len(times) / sum(times) / 1e6
+    return {"metric": "Batched DiTO-14 fit throughput (Mpoints/s)", "impl": "reference", "value": round(value, 3),
+            "unit": "Mpoints/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (same generator as the ours arm)",
+            "config": {"workload": "dito_batch", "sets_per_gpu": a.sets, "points_per_gpu": total},
+            "cpu_baseline": {"value": round(value, 3), "unit": "Mpoints/s", "cores": threads, "kind": "reference",
+                             "sample": f"the whole {a.sets}-set batch per step, one set per thread "
+                                       f"(warm-up steps on the first 64 sets)"},
+            "e2e": {"value": round(value, 3), "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     a = parse_args()
     dist = Dist()
     if a.impl == "reference":
         if dist.world > 1 and dist.rank != 0:
             return
-        if a.workload == "dito":
+        if a.workload in ("dito", "dito_batch"):
             import oracle
             if not oracle.ref_available():
                 print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_dito.so was not built"}))
                 return
-            print(json.dumps(bench_dito_reference(a, dist)), flush=True)
+            ref = bench_dito_reference if a.workload == "dito" else bench_batch_reference
+            print(json.dumps(ref(a, dist)), flush=True)
         else:
             print(json.dumps(bench_tree_reference(a, dist)), flush=True)
         return
     dist.init()
     try:
-        line = bench_tree_ours(a, dist) if a.workload == "lbvh_obb_tree" else bench_dito_ours(a, dist)
+        run = {"lbvh_obb_tree": bench_tree_ours, "dito": bench_dito_ours, "dito_batch": bench_batch_ours}
+        line = run[a.workload](a, dist)
         if dist.rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -27,6 +27,16 @@ class Obb3(ctypes.Structure):
     _fields_ = [("v", ctypes.c_float * 15)]
 
 
+class DitoBatchTuning(ctypes.Structure):
+    """obvh_dito_batch_tuning (include/obvh_batch.h)."""
+    _fields_ = [(name, ctypes.c_uint32) for name in
+                ("points_per_thread", "chunk_points", "warp_max_points", "cta_max_points", "lag_tasks",
+                 "ctas_per_sm")]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 def _declare(lib: ctypes.CDLL) -> None:
     c = ctypes
     vp = c.c_void_p
@@ -61,6 +71,18 @@ def _declare(lib: ctypes.CDLL) -> None:
         "obvh_build_workspace_init": (err, [vp, c.c_uint32, vp]),
         "obvh_build_async": (err, [vp, vp, c.c_uint32, c.c_uint32, c.c_float, c.c_float] + [vp] * 11),
         "obvh_build_status": (err, [vp, c.c_uint32, vp, c.POINTER(c.c_uint32), c.POINTER(c.c_uint32)]),
+        "obvh_dito_batch_create": (err, [vp, c.c_uint64, c.c_uint32, vp, c.POINTER(vp)]),
+        "obvh_dito_batch_destroy": (err, [vp]),
+        "obvh_dito_batch_get_tuning": (err, [vp, c.POINTER(DitoBatchTuning)]),
+        "obvh_dito_batch_set_tuning": (err, [vp, c.POINTER(DitoBatchTuning)]),
+        "obvh_dito_batch_enqueue": (err, [vp, vp, vp, vp]),
+        "obvh_dito_batch_capture": (err, [vp, vp, vp]),
+        "obvh_dito_batch_launch": (err, [vp, vp]),
+        "obvh_dito_batch_autotune": (err, [vp, vp, vp, vp, c.c_uint32, c.POINTER(DitoBatchTuning),
+                                           c.POINTER(c.c_float)]),
+        "obvh_dito_batch_status": (err, [vp, vp, c.POINTER(c.c_uint32)]),
+        "obvh_dito_batch_info": (err, [vp] + [c.POINTER(c.c_uint32)] * 4),
+        "obvh_points_obb_batch": (err, [vp, vp, c.c_uint64, c.c_uint32, vp, c.POINTER(c.c_float)]),
         "obvh_dito_workspace_report": (err, [vp, vp, c.POINTER(c.c_uint32), c.POINTER(c.c_float),
                                              c.POINTER(c.c_uint32)]),
     }

@@ -75,84 +75,6 @@ __host__ __device__ inline Split make_split(const float* xyz, uint64_t n) {
     return s;
 }
 
-// Slab projection k of the 7 fixed DiTO directions, in the reference's
-// evaluation order (dito.cpp:115-172); k is a compile-time constant after unrolling.
-__device__ __forceinline__ float slab(int k, float x, float y, float z) {
-    switch (k) {
-        case 0: return x;
-        case 1: return y;
-        case 2: return z;
-        case 3: return x + y + z;
-        case 4: return x + y - z;
-        case 5: return x - y + z;
-        default: return x - y - z;
-    }
-}
-
-// Per-thread running extremes.  For each direction the thread keeps the
-// extreme value and the CTA-local index of the first point of the first
-// 4-point group reaching it (groups are visited in increasing index order and
-// replaced only on strict improvement).  The hot loop is branch-free; the
-// exact point inside a winning group is resolved once per CTA.
-struct Extremes {
-    float mn[7], mx[7];
-    uint32_t gmn[7], gmx[7];
-    __device__ void init() {
-#pragma unroll
-        for (int k = 0; k < 7; ++k) {
-            mn[k] = kInf;
-            mx[k] = -kInf;
-            gmn[k] = 0xffffffffu;
-            gmx[k] = 0xffffffffu;
-        }
-    }
-    // the 4 points x/y/z[0..4) with indices g, g+1, g+2, g+3
-    __device__ __forceinline__ void group(const float* x, const float* y, const float* z, uint32_t g) {
-#pragma unroll
-        for (int k = 0; k < 7; ++k) {
-            float v0 = slab(k, x[0], y[0], z[0]), v1 = slab(k, x[1], y[1], z[1]);
-            float v2 = slab(k, x[2], y[2], z[2]), v3 = slab(k, x[3], y[3], z[3]);
-            float lo = fminf(fminf(v0, v1), fminf(v2, v3));
-            float hi = fmaxf(fmaxf(v0, v1), fmaxf(v2, v3));
-            bool a = lo < mn[k];
-            mn[k] = a ? lo : mn[k];
-            gmn[k] = a ? g : gmn[k];
-            bool b = hi > mx[k];
-            mx[k] = b ? hi : mx[k];
-            gmx[k] = b ? g : gmx[k];
-        }
-    }
-};
-
-// Extents along three axes (values only).
-struct Extents {
-    f3 b0, b1, b2;
-    float lo[3], hi[3];
-    __device__ void init(const float* axes) {
-        b0 = mk3(axes[0], axes[1], axes[2]);
-        b1 = mk3(axes[3], axes[4], axes[5]);
-        b2 = mk3(axes[6], axes[7], axes[8]);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) { lo[k] = kInf; hi[k] = -kInf; }
-    }
-    __device__ __forceinline__ void point(float x, float y, float z) {
-        f3 p = mk3(x, y, z);
-        float q0 = dot3(p, b0), q1 = dot3(p, b1), q2 = dot3(p, b2);
-        lo[0] = fminf(lo[0], q0); hi[0] = fmaxf(hi[0], q0);
-        lo[1] = fminf(lo[1], q1); hi[1] = fmaxf(hi[1], q1);
-        lo[2] = fminf(lo[2], q2); hi[2] = fmaxf(hi[2], q2);
-    }
-};
-
-// Unpacks 4-point groups (3 float4 each) into coordinate arrays.
-__device__ __forceinline__ void unpack4(const float4& a, const float4& b, const float4& c, float* x, float* y,
-                                        float* z) {
-    x[0] = a.x; y[0] = a.y; z[0] = a.z;
-    x[1] = a.w; y[1] = b.x; z[1] = b.y;
-    x[2] = b.z; y[2] = b.w; z[2] = c.x;
-    x[3] = c.y; y[3] = c.z; z[3] = c.w;
-}
-
 __device__ __forceinline__ void cta_tiles(uint64_t ntiles, uint64_t& b, uint64_t& e) {
     b = ntiles * blockIdx.x / gridDim.x;
     e = ntiles * (blockIdx.x + 1) / gridDim.x;

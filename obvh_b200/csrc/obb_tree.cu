@@ -42,7 +42,8 @@ using namespace tree;
 
 constexpr int kThreads = 256;
 constexpr uint32_t kThreadMax = 8;   // leaves handled by one thread per node
-constexpr uint32_t kUnit = 1024;     // leaves per warp unit
+constexpr uint32_t kUnit = 1024;    // leaves per warp unit
+constexpr uint32_t kUnitRun = 4;   // consecutive units per warp visit
 
 struct Ctl {
     uint32_t error;
@@ -257,41 +258,49 @@ __global__ void __launch_bounds__(kThreads) extents_units_kernel(const Cand* can
                                                                  kr_obb3* obbs, kr_mat4* xfs) {
     const int lane = threadIdx.x & 31;
     const uint32_t total = *err ? 0u : *total_units;
-    // Units are dealt round-robin to the warps of the grid: no shared counter.
+    // Warps take runs of kUnitRun consecutive units round-robin: one binary
+    // search per run, and big and small nodes spread evenly over the warps.
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t u = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < total; u += warps) {
-        // the last node whose first unit is <= u owns it
-        uint32_t lo_i = 0, hi_i = internal;  // search in [lo_i, hi_i)
-        while (hi_i - lo_i > 1) {
-            const uint32_t mid = (lo_i + hi_i) >> 1;
-            if (__ldg(unit_start + mid) <= u) lo_i = mid; else hi_i = mid;
+    const uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    for (uint32_t u0 = w * kUnitRun; u0 < total; u0 += warps * kUnitRun) {
+        const uint32_t u1 = min(total, u0 + kUnitRun);
+        uint32_t a;
+        {
+            uint32_t lo_i = 0, hi_i = internal;  // the last node whose first unit is <= u0 owns it
+            while (hi_i - lo_i > 1) {
+                const uint32_t mid = (lo_i + hi_i) >> 1;
+                if (__ldg(unit_start + mid) <= u0) lo_i = mid; else hi_i = mid;
+            }
+            a = lo_i;
         }
-        const uint32_t a = lo_i;
-        const uint32_t chunk = u - __ldg(unit_start + a);
-        const uint32_t cnt = __ldg(counts + a);
-        const uint32_t units = __ldg(nunits + a);
-        const uint32_t begin = chunk * kUnit;
-        const uint32_t end = min(cnt, begin + kUnit);
-        const Cand c = load_cand(cand, a);
-        const f3 b0 = mk3(c.ax[0], c.ax[1], c.ax[2]), b1 = mk3(c.ax[3], c.ax[4], c.ax[5]),
-                 b2 = mk3(c.ax[6], c.ax[7], c.ax[8]);
-        float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
-        const float* t = tris + 9 * static_cast<size_t>(__ldg(first + a));
-        for (uint32_t i = begin + lane; i < end; i += 32) project_tri(t + 9 * static_cast<size_t>(i), b0, b1, b2, lo, hi);
+        for (uint32_t u = u0; u < u1; ++u) {
+            while (__ldg(unit_start + a) + __ldg(nunits + a) <= u) ++a;
+            const uint32_t chunk = u - __ldg(unit_start + a);
+            const uint32_t cnt = __ldg(counts + a);
+            const uint32_t units = __ldg(nunits + a);
+            const uint32_t begin = chunk * kUnit;
+            const uint32_t end = min(cnt, begin + kUnit);
+            const Cand c = load_cand(cand, a);
+            const f3 b0 = mk3(c.ax[0], c.ax[1], c.ax[2]), b1 = mk3(c.ax[3], c.ax[4], c.ax[5]),
+                     b2 = mk3(c.ax[6], c.ax[7], c.ax[8]);
+            float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+            const float* t = tris + 9 * static_cast<size_t>(__ldg(first + a));
+            for (uint32_t i = begin + lane; i < end; i += 32) project_tri(t + 9 * static_cast<size_t>(i), b0, b1, b2, lo, hi);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            lo[k] = warp_min(lo[k]);
-            hi[k] = warp_max(hi[k]);
-        }
-        if (units == 1) {
-            if (lane == 0)
-                finalize_node(c, mk3(fminf(c.olo[0], lo[0]), fminf(c.olo[1], lo[1]), fminf(c.olo[2], lo[2])),
-                              mk3(fmaxf(c.ohi[0], hi[0]), fmaxf(c.ohi[1], hi[1]), fmaxf(c.ohi[2], hi[2])), obbs + a,
-                              xfs + a);
-        } else if (lane < 6) {
-            const float v = lane < 3 ? lo[lane] : hi[lane - 3];
-            uint32_t* k = keys + 6 * static_cast<size_t>(a) + lane;
-            if (lane < 3) atomicMin(k, f2key(v)); else atomicMax(k, f2key(v));
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = warp_min(lo[k]);
+                hi[k] = warp_max(hi[k]);
+            }
+            if (units == 1) {
+                if (lane == 0)
+                    finalize_node(c, mk3(fminf(c.olo[0], lo[0]), fminf(c.olo[1], lo[1]), fminf(c.olo[2], lo[2])),
+                                  mk3(fmaxf(c.ohi[0], hi[0]), fmaxf(c.ohi[1], hi[1]), fmaxf(c.ohi[2], hi[2])), obbs + a,
+                                  xfs + a);
+            } else if (lane < 6) {
+                const float v = lane < 3 ? lo[lane] : hi[lane - 3];
+                uint32_t* k = keys + 6 * static_cast<size_t>(a) + lane;
+                if (lane < 3) atomicMin(k, f2key(v)); else atomicMax(k, f2key(v));
+            }
         }
     }
 }

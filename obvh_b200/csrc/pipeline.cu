@@ -90,10 +90,17 @@ __global__ void __launch_bounds__(kThreads) fused_up_kernel(kr_bvh_node* nodes, 
     const uint32_t internal = n - 1;
     const uint32_t leaf = internal + j;
     const bool collapse = flags != nullptr;
+    // The arriving thread carries its own child's bounds, count and cost; only
+    // the sibling's are read from memory.
+    float olo[3], ohi[3];
+    uint32_t ocount = 1;
+    float ocost;
     {
         const NodeView lf = load_node(nodes, leaf);
+        for (int k = 0; k < 3; ++k) { olo[k] = lf.lo[k]; ohi[k] = lf.hi[k]; }
         // leaf cost: ct * area in the collapse (transforms.cu:97), 1 * area in the LBVH (lbvh.cu:427)
-        __stcg(costs + leaf, (collapse ? ct : 1.0f) * box_area(lf.lo, lf.hi));
+        ocost = (collapse ? ct : 1.0f) * box_area(lf.lo, lf.hi);
+        __stcg(costs + leaf, ocost);
         __stcg(counts + leaf, 1u);
     }
     Summary own;
@@ -108,12 +115,21 @@ __global__ void __launch_bounds__(kThreads) fused_up_kernel(kr_bvh_node* nodes, 
         if (arrive(visits + p) == 0) return;
         const uint32_t* pw = reinterpret_cast<const uint32_t*>(nodes + p);
         const uint32_t L = __ldg(pw + 6), R = __ldg(pw + 7);
-        const NodeView ln = load_node(nodes, L), rn = load_node(nodes, R);
+        const bool from_left = (L == child);
+        const uint32_t other = from_left ? R : L;
+        const NodeView sib = load_node(nodes, other);
+        const uint32_t scount = __ldcg(counts + other);
+        const float scost = __ldcg(costs + other);
+        // left/right views of the two children
+        const float* llo = from_left ? olo : sib.lo;
+        const float* lhi = from_left ? ohi : sib.hi;
+        const float* rlo = from_left ? sib.lo : olo;
+        const float* rhi = from_left ? sib.hi : ohi;
         float lo[3], hi[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {  // kr_aabb_expand(left, right)
-            lo[k] = kmin(kmin(ln.lo[k], rn.lo[k]), rn.hi[k]);
-            hi[k] = kmax(kmax(ln.hi[k], rn.lo[k]), rn.hi[k]);
+            lo[k] = kmin(kmin(llo[k], rlo[k]), rhi[k]);
+            hi[k] = kmax(kmax(lhi[k], rlo[k]), rhi[k]);
         }
         uint32_t w[9];
         for (int k = 0; k < 3; ++k) { w[k] = __float_as_uint(lo[k]); w[3 + k] = __float_as_uint(hi[k]); }
@@ -122,10 +138,10 @@ __global__ void __launch_bounds__(kThreads) fused_up_kernel(kr_bvh_node* nodes, 
         w[8] = 0;
         store_words(nodes, p, w, 6);
         if (collapsed) store_words(collapsed, p, w, 9);
-        const uint32_t count = __ldcg(counts + L) + __ldcg(counts + R);
+        const uint32_t count = ocount + scount;
         __stcg(counts + p, count);
         const float area = box_area(lo, hi);
-        const float cl = __ldcg(costs + L), cr = __ldcg(costs + R);
+        const float cl = from_left ? ocost : scost, cr = from_left ? scost : ocost;
         float cost;
         if (collapse) {
             // bvh_mark_collapse_kernel (transforms.cu:111-133)
@@ -146,9 +162,11 @@ __global__ void __launch_bounds__(kThreads) fused_up_kernel(kr_bvh_node* nodes, 
         } else {
             cost = 1.2f * area + cr + cl;  // calculate_aabbs_kernel (lbvh.cu:452)
         }
+        for (int k = 0; k < 3; ++k) { olo[k] = lo[k]; ohi[k] = hi[k]; }
+        ocount = count;
+        ocost = cost;
         __stcg(costs + p, cost);
         if (summary) {
-            const uint32_t other = (L == child) ? R : L;
             Summary o;
             if (other >= internal) slot_summary(tris, other - internal, o);
             else load_summary(summary + 7 * static_cast<size_t>(other), o);

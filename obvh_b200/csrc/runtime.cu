@@ -90,6 +90,8 @@ size_t g_prof_used = 0;
 bool profiling() { return g_prof.load(std::memory_order_relaxed); }
 
 void prof_record(const char* name, cudaStream_t s, bool begin) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
     std::lock_guard<std::mutex> lock(g_prof_mutex);
     if (g_prof_used == g_prof_pool.size()) {
         cudaEvent_t e;

@@ -167,3 +167,35 @@ def gaussian_sets(n_sets: int = 4096, seed: int = 3, size_min: int = 64, size_ma
         x = rng.normal(size=(sizes[s], 3)) * sig
         pts[offsets[s]:offsets[s + 1]] = x @ rot.T + off
     return pts, offsets
+
+
+def gaussian_sets_torch(n_sets: int = 4096, seed: int = 3, size_min: int = 64, size_max: int = 262144,
+                        sigma_min: float = 0.01, sigma_max: float = 5.0, offset_range: float = 100.0,
+                        device="cuda"):
+    """Same distribution as gaussian_sets, generated with torch on `device`
+    (fast enough for the 4,096-set runs; a different random stream for the
+    points).  Returns (points [total x 3] float32 tensor, offsets int64 numpy)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(math.log(size_min), math.log(size_max), size=n_sets)).astype(np.int64)
+    offsets = np.zeros(n_sets + 1, np.int64)
+    np.cumsum(sizes, out=offsets[1:])
+    sig = np.exp(rng.uniform(math.log(sigma_min), math.log(sigma_max), size=(n_sets, 3)))
+    rot = np.stack([random_rotation(rng) for _ in range(n_sets)])
+    off = rng.uniform(-offset_range, offset_range, size=(n_sets, 3))
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    out = torch.empty((int(offsets[-1]), 3), dtype=torch.float32, device=device)
+    # a few thousand sets per slab keeps the temporaries small
+    step = 256
+    for s0 in range(0, n_sets, step):
+        s1 = min(n_sets, s0 + step)
+        a, b = int(offsets[s0]), int(offsets[s1])
+        ids = torch.repeat_interleave(torch.arange(s1 - s0, device=device),
+                                      torch.tensor(sizes[s0:s1], device=device))
+        x = torch.randn((b - a, 3), generator=g, device=device, dtype=torch.float64)
+        x = x * torch.tensor(sig[s0:s1], device=device)[ids]
+        r = torch.tensor(rot[s0:s1], device=device)[ids]
+        y = torch.einsum("nij,nj->ni", r, x) + torch.tensor(off[s0:s1], device=device)[ids]
+        out[a:b] = y.to(torch.float32)
+    return out, offsets
