@@ -11,6 +11,10 @@ reference publishes no numbers, so vs_baseline is null):
   vertices at log-uniform radius 0.002..0.02), then the AABB->OBB-tree
   transform, then the node collapse.  A step is one such build.  Metric
   Mnodes/s = (2N-1) nodes per step.
+* ``atrbvh_obb_tree`` - ATRBVH (63-bit Morton LBVH, then agglomerative
+  treelet optimisation, treelet size 7, 2 iterations) over the 917,504-triangle
+  (2,3) torus-knot tube, then the OBB-tree transform and the collapse.  A step
+  is one such build.  Metric Mnodes/s.
 * ``dito`` - DiTO-14 fit of 100,000,000 points on an ellipsoid surface
   (semi-axes 4, 1, 0.25; rotated, noised, offset).  A step is one fit (two
   streaming passes).  Metric Mpoints/s.
@@ -50,7 +54,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["lbvh_obb_tree", "dito", "dito_batch"], default="lbvh_obb_tree")
+    ap.add_argument("--workload", choices=["lbvh_obb_tree", "atrbvh_obb_tree", "dito", "dito_batch"],
+                    default="lbvh_obb_tree")
+    ap.add_argument("--treelet", type=int, default=7, help="atrbvh_obb_tree: treelet size")
     ap.add_argument("--sets", type=int, default=4096, help="dito_batch: point sets per batch")
     ap.add_argument("--no-autotune", action="store_true", help="dito_batch: default knobs")
     ap.add_argument("--points", type=int, default=100_000_000, help="dito: points per fit")
@@ -253,6 +259,13 @@ def tree_bytes_per_launch(n):
         "leaves_fused_kernel": 4 * n + 24 * n + 52 * n + 72 * n + 36 * n + 124 * n,
         # fused leaf-to-root pass: children in, bounds/counts/costs/collapsed node/summary out
         "fused_up_kernel": 36 * n + 8 * n + 36 * n + 72 * ni + 16 * ni + 24 * ni + 36 * ni + 8 * ni + 224 * ni,
+        # ATRBVH: triangle in, 63-bit key + index out; sorted keys in, working nodes out;
+        # leaf triangles + nodes in/out bottom-up; one pass over the working tree per iteration
+        "morton63_kernel": 52 * n + 12 * n,
+        "karras63_kernel": 12 * n + 48 * nn,
+        "boxes_up_kernel": 52 * n + 48 * nn * 2,
+        "treelet_kernel": 48 * nn * 2 + 8 * nn * 2,
+        "emit_kernel": 48 * nn + 36 * nn + 4 * nn,
         "roots_kernel": 14 * nn,
         "gather_kernel": 8 * nn,
         "scan_tile_sums": 4 * nn,
@@ -260,20 +273,28 @@ def tree_bytes_per_launch(n):
     }
 
 
-def bench_tree_ours(a, dist):
+def bench_tree_ours(a, dist, atrbvh=False):
     import numpy as np
     import torch
     from obvh_b200 import _native, bvh, workloads
 
-    n = a.tris
-    nn = 2 * n - 1
     dev = torch.device("cuda", torch.cuda.current_device())
     lib = _native.lib()
-    # two meshes alternated between steps (2 x 104 MB > 126 MB L2)
-    host_meshes = [workloads.triangle_soup(n, seed=1 + 2 * dist.rank + j) for j in range(2)]
+    if atrbvh:
+        # two knots alternated between steps (different surface noise)
+        host_meshes = [workloads.torus_knot_mesh(seed=2 + 2 * dist.rank + j) for j in range(2)]
+        ws_bytes, ws_init, status_fn = lib.obvh_atrbvh_workspace_bytes, lib.obvh_atrbvh_workspace_init, \
+            lib.obvh_atrbvh_status
+    else:
+        # two meshes alternated between steps (2 x 104 MB > 126 MB L2)
+        host_meshes = [workloads.triangle_soup(a.tris, seed=1 + 2 * dist.rank + j) for j in range(2)]
+        ws_bytes, ws_init, status_fn = lib.obvh_build_workspace_bytes, lib.obvh_build_workspace_init, \
+            lib.obvh_build_status
+    n = host_meshes[0][1].shape[0]
+    nn = 2 * n - 1
     meshes = [bvh.Mesh(v, f, device=dev) for v, f in host_meshes]
-    ws = torch.empty(int(lib.obvh_build_workspace_bytes(n)), dtype=torch.uint8, device=dev)
-    _native.check(lib.obvh_build_workspace_init(ctypes.c_void_p(ws.data_ptr()), n, None))
+    ws = torch.empty(int(ws_bytes(n)), dtype=torch.uint8, device=dev)
+    _native.check(ws_init(ctypes.c_void_p(ws.data_ptr()), n, None))
     u8, i32, f32 = torch.uint8, torch.int32, torch.float32
     out = {"nodes": torch.empty(nn * 36, dtype=u8, device=dev), "parents": torch.empty(nn, dtype=i32, device=dev),
            "counts": torch.empty(nn, dtype=i32, device=dev), "costs": torch.empty(nn, dtype=f32, device=dev),
@@ -285,28 +306,36 @@ def bench_tree_ours(a, dist):
     stream = torch.cuda.current_stream(dev)
     S = ctypes.c_void_p(stream.cuda_stream)
 
+    flags = bvh.BUILD_OBBS | bvh.BUILD_COLLAPSE
+
     def step(j, mesh=None):
         m = mesh or meshes[j & 1]
         V, F = ctypes.c_void_p(m.verts.data_ptr()), ctypes.c_void_p(m.faces.data_ptr())
-        _native.check(lib.obvh_build_async(V, F, n, bvh.BUILD_OBBS | bvh.BUILD_COLLAPSE, 1.2, 1.0, P["nodes"],
-                                           P["parents"], P["counts"], P["costs"], P["bounds"], P["obbs"], P["xfs"],
-                                           P["collapsed"], P["prims"], W, S))
+        if atrbvh:
+            e = lib.obvh_build_atrbvh_async(V, F, n, flags, a.treelet, 2, 1.2, 1.0, P["nodes"], P["parents"],
+                                            P["counts"], P["costs"], P["bounds"], P["obbs"], P["xfs"],
+                                            P["collapsed"], P["prims"], W, S)
+        else:
+            e = lib.obvh_build_async(V, F, n, flags, 1.2, 1.0, P["nodes"], P["parents"], P["counts"], P["costs"],
+                                     P["bounds"], P["obbs"], P["xfs"], P["collapsed"], P["prims"], W, S)
+        _native.check(e)
 
     sampler = ClockSampler(dev.index, enabled=not a.profile)
     total_ms, prof, clocks = timed_steps(a, dist, step, sampler, stream)
     err, slots = ctypes.c_uint32(0), ctypes.c_uint32(0)
-    _native.check(lib.obvh_build_status(W, n, S, ctypes.byref(err), ctypes.byref(slots)))
+    _native.check(status_fn(W, n, S, ctypes.byref(err), ctypes.byref(slots)))
     if err.value != 0:
         raise RuntimeError(f"device error word {err.value}")
+    wname = "atrbvh_obb_tree" if atrbvh else "lbvh_obb_tree"
     if a.profile:
-        return {"profile": "lbvh_obb_tree", "tris": n, "ms_per_step": total_ms / a.steps, "kernels": prof}
+        return {"profile": wname, "tris": n, "ms_per_step": total_ms / a.steps, "kernels": prof}
 
     ms_step = total_ms / a.steps
     value = dist.world * nn * a.steps / (total_ms / 1e3) / 1e6
     peak, peak_kind = peaks()
     kern = {k: {"launches": v[0], "ms_per_step": round(v[1] / a.steps, 5)} for k, v in prof.items()}
     roof = roofline(prof, tree_bytes_per_launch(n), peak, peak_kind,
-                    os.path.join(ROOT, "profiles", "lbvh_obb_tree_traffic.json"))
+                    os.path.join(ROOT, "profiles", f"{wname}_traffic.json"))
     launches = sum(v[0] for v in prof.values())
 
     # End to end through the C ABI: the pinned host mesh copied in, the tree
@@ -333,24 +362,36 @@ def bench_tree_ours(a, dist):
     e2e_s = time.perf_counter() - t0
     e2e_min = -dist.max(-(nn * e2e_steps / e2e_s / 1e6))
 
+    if atrbvh:
+        metric = "ATRBVH + OBB-tree + collapse build throughput (Mnodes/s)"
+        data = ("synthetic: (2,3) torus-knot tube, 1024 segments x 448 around, radius 0.15, radial bump "
+                "0.02 sin(13 theta) cos(7 phi) + U[0,0.005] noise")
+        config = {"workload": "atrbvh_obb_tree_collapse", "triangles_per_gpu": n, "nodes_per_gpu": nn,
+                  "morton_bits": 63, "treelet_size": a.treelet, "iterations": 2, "ci": 1.2, "ct": 1.0,
+                  "l2": "two 26 MB knots alternated; each step writes ~0.6 GB after reading its input, no flush",
+                  "parallelism": f"replicas{dist.world}"}
+        api = "obvh_build_atrbvh_async (ATRBVH + OBB tree + collapse), pinned host mesh"
+    else:
+        metric = "LBVH + OBB-tree + collapse build throughput (Mnodes/s)"
+        data = "synthetic: thin random triangles (centroid U[0,1]^3, vertex radius log-U[0.002,0.02]), seeded"
+        config = {"workload": "lbvh_obb_tree_collapse", "triangles_per_gpu": n, "nodes_per_gpu": nn,
+                  "morton_bits": 30, "ci": 1.2, "ct": 1.0,
+                  "l2": "two 104 MB meshes alternated between steps; each step writes ~1 GB",
+                  "parallelism": f"replicas{dist.world}"}
+        api = "obvh_build_async (LBVH + OBB tree + collapse), pinned host mesh"
     line = {
-        "metric": "LBVH + OBB-tree + collapse build throughput (Mnodes/s)",
+        "metric": metric,
         "value": round(value, 3), "unit": "Mnodes/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": round(ms_step, 5), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32",
-        "data": "synthetic: thin random triangles (centroid U[0,1]^3, vertex radius log-U[0.002,0.02]), seeded",
-        "config": {"workload": "lbvh_obb_tree_collapse", "triangles_per_gpu": n, "nodes_per_gpu": nn,
-                   "morton_bits": 30, "ci": 1.2, "ct": 1.0,
-                   "l2": "two 104 MB meshes alternated between steps; each step writes ~1 GB",
-                   "parallelism": f"replicas{dist.world}"},
+        "dtype": "f32", "data": data, "config": config,
         "kernels": kern, "gpu_launches": launches, "roofline": roof,
         "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mnodes/s",
                 "h2d_bytes_per_step": int(host_meshes[0][0].nbytes + n * 16), "d2h_bytes_per_step": 64,
-                "api": "obvh_build_async (LBVH + OBB tree + collapse), pinned host mesh"},
+                "api": api},
         "clocks": clocks,
     }
     if dist.rank == 0 and dist.world == 1:
-        line["cpu_baseline"] = cpu_tree_baseline()
+        line["cpu_baseline"] = cpu_atrbvh_baseline(a.treelet) if atrbvh else cpu_tree_baseline()
     return line
 
 
@@ -371,6 +412,55 @@ def cpu_tree_baseline(n=200_000):
             break
     return {"value": round((2 * n - 1) * reps / dt / 1e6, 4), "unit": "Mnodes/s", "cores": 1, "kind": "port",
             "sample": f"{reps} builds of {n} triangles ({dt:.1f} s), oracle C restatement"}
+
+
+def _atrbvh_port_build(v, f, tau):
+    from oracle import bvh as ref
+    r = ref.atrbvh_build(v, f, tau, 2)
+    ref.obb_tree(r["nodes"], r["parents"], v, f)
+    ref.collapse(r["nodes"], r["parents"], r["counts"], r["costs"])
+
+
+def cpu_atrbvh_baseline(tau, segments=256, around=112):
+    """The oracle port of the ATRBVH commit on one host core, on a smaller
+    knot of the same shape (the reference has no CPU implementation)."""
+    from obvh_b200 import workloads
+    v, f = workloads.torus_knot_mesh(segments, around, seed=77)
+    n = f.shape[0]
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        _atrbvh_port_build(v, f, tau)
+        reps += 1
+        dt = time.perf_counter() - t0
+        if dt > 8.0 or reps >= 20:
+            break
+    return {"value": round((2 * n - 1) * reps / dt / 1e6, 4), "unit": "Mnodes/s", "cores": 1, "kind": "port",
+            "sample": f"{reps} builds of a {n}-triangle knot ({segments}x{around}, {dt:.1f} s), oracle C restatement"}
+
+
+def bench_atrbvh_reference(a, dist):
+    """The CPU restatement of the ATRBVH commit (oracle port) on this host, on
+    a bounded knot of the benchmark's shape."""
+    from obvh_b200 import workloads
+    segments, around = 512, 224
+    v, f = workloads.torus_knot_mesh(segments, around, seed=2)
+    n = f.shape[0]
+    times = []
+    for j in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
+        _atrbvh_port_build(v, f, a.treelet)
+        if j >= a.warmup:
+            times.append(time.perf_counter() - t0)
+    value = (2 * n - 1) * len(times) / sum(times) / 1e6
+    return {"metric": "ATRBVH + OBB-tree + collapse build throughput (Mnodes/s)", "impl": "reference",
+            "value": round(value, 4), "unit": "Mnodes/s", "n_gpus": dist.world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (same generator as the ours arm)",
+            "config": {"workload": "atrbvh_obb_tree_collapse", "treelet_size": a.treelet, "iterations": 2,
+                       "sample_triangles": n},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mnodes/s", "cores": 1, "kind": "port",
+                             "sample": f"{segments}x{around} knot ({n} triangles) per step, oracle C restatement"},
+            "e2e": {"value": round(value, 4), "unit": "Mnodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def bench_tree_reference(a, dist):
@@ -636,12 +726,15 @@ def main():
                 return
             ref = bench_dito_reference if a.workload == "dito" else bench_batch_reference
             print(json.dumps(ref(a, dist)), flush=True)
+        elif a.workload == "atrbvh_obb_tree":
+            print(json.dumps(bench_atrbvh_reference(a, dist)), flush=True)
         else:
             print(json.dumps(bench_tree_reference(a, dist)), flush=True)
         return
     dist.init()
     try:
-        run = {"lbvh_obb_tree": bench_tree_ours, "dito": bench_dito_ours, "dito_batch": bench_batch_ours}
+        run = {"lbvh_obb_tree": bench_tree_ours, "atrbvh_obb_tree": lambda a, d: bench_tree_ours(a, d, atrbvh=True),
+               "dito": bench_dito_ours, "dito_batch": bench_batch_ours}
         line = run[a.workload](a, dist)
         if dist.rank == 0:
             print(json.dumps(line), flush=True)

@@ -226,3 +226,46 @@ class ObvhBuilder:
         _native.check(self.lib.obvh_build_status(_ptr(self.ws), n, _stream(self.torch, stream), ctypes.byref(err),
                                                  ctypes.byref(slots)))
         return err.value, slots.value
+
+
+ATRBVH_TREELET_SIZE = 9  # OBVH_ATRBVH_TREELET_SIZE: the reference intersector's treelet size
+ATRBVH_ITERATIONS = 2
+
+
+class AtrbvhBuilder(ObvhBuilder):
+    """obvh_build_atrbvh_async: ATRBVH (LBVH-63 + agglomerative treelets), then
+    the OBB tree and the collapse, with the workspace kept between builds."""
+
+    def _workspace(self, n, s):
+        if self.ws is None or n > self.ws_faces:
+            self.ws = self.torch.empty(int(self.lib.obvh_atrbvh_workspace_bytes(n)), dtype=self.torch.uint8,
+                                       device=self.device)
+            self.ws_faces = n
+            _native.check(self.lib.obvh_atrbvh_workspace_init(_ptr(self.ws), n, s))
+        return self.ws
+
+    def outputs(self, n):
+        o = super().outputs(n)
+        o["bounds"] = self.torch.empty(6, dtype=self.torch.float32, device=self.device)  # scene box only
+        return o
+
+    def build(self, mesh: Mesh, flags=BUILD_OBBS | BUILD_COLLAPSE, ci=1.2, ct=1.0, stream=None, out=None,
+              treelet_size=ATRBVH_TREELET_SIZE, iterations=ATRBVH_ITERATIONS):
+        n = mesh.n_faces
+        s = _stream(self.torch, stream)
+        ws = self._workspace(n, s)
+        o = out if out is not None else self.outputs(n)
+        e = self.lib.obvh_build_atrbvh_async(_ptr(mesh.verts), _ptr(mesh.faces), n, flags, treelet_size, iterations,
+                                             ci, ct, _ptr(o["nodes"]), _ptr(o["parents"]), _ptr(o["counts"]),
+                                             _ptr(o["costs"]), _ptr(o["bounds"]), _ptr(o["obbs"]),
+                                             _ptr(o["transforms"]), _ptr(o["collapsed"]), _ptr(o["primitives"]),
+                                             _ptr(ws), s)
+        _native.check(e)
+        return o
+
+    def status(self, n, stream=None):
+        err = ctypes.c_uint32(0)
+        slots = ctypes.c_uint32(0)
+        _native.check(self.lib.obvh_atrbvh_status(_ptr(self.ws), n, _stream(self.torch, stream), ctypes.byref(err),
+                                                  ctypes.byref(slots)))
+        return err.value, slots.value

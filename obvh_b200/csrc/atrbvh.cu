@@ -1,0 +1,717 @@
+// atrbvh.cu - the reference's ATRBVH builder on the GPU: an LBVH over 63-bit
+// Morton codes, restructured by agglomerative treelet optimisation, handed on
+// as kr_bvh_node records (src/ads/atrbvh_gpu/atrbvh.cu:258-380 with
+// LBVHBuilder.cpp:33-139 and AgglomerativeTreeletOptimizer.cpp:22-117).
+//
+//   scene box        union of the triangle boxes (atrbvh.cu:282-298)
+//   morton63_kernel  centroid of the triangle box in the scene box, 21 bits
+//                    per axis (LBVH.cu:72-93, Commons.cuh:422-430,602-638)
+//   radix sort       stable, 64-bit keys with the triangle index as value
+//   karras63_kernel  Karras tree with index tie-break and the doubling-divisor
+//                    split search (LBVH.cu:156-300)
+//   boxes_up_kernel  leaf boxes and bottom-up node boxes and areas
+//                    (LBVH.cu:414-447,551-648)
+//   treelet_kernel   one bottom-up pass per iteration (gamma = tau, 2 tau,
+//                    ...): at every node whose subtree holds at least gamma
+//                    triangles, the warp forms a treelet of tau leaves by
+//                    largest area, merges them agglomeratively by smallest
+//                    union area, and keeps the result if its SAH is lower
+//                    (AgglomerativeTreelet.cu:405-570, Treelet.cuh:55-129)
+//   emit_kernel      SoA tree -> kr_bvh_node + parents (atrbvh.cu:95-123),
+//                    then the LBVH refit for bounds, counts and costs.
+//
+// The reference runs its treelet kernel with __syncthreads() inside
+// warp-divergent loops; every shared array it touches there is per warp, so
+// here each warp synchronises only itself (__syncwarp).  The two warp
+// reductions that pick the leaf to expand and the pair to merge use the
+// reference's shuffle-down order and strict comparisons, so ties resolve as
+// there.  Node data written by other warps is read through L2 (__ldcg) after
+// the arrival counter's acquire.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+#include <mutex>
+#include <unordered_map>
+
+#include "collapse_host.h"
+#include "device_common.cuh"
+#include "lbvh_host.h"
+#include "obb_tree_host.h"
+#include "obvh_atrbvh.h"
+#include "obvh_build.h"
+#include "runtime.h"
+#include "sort.h"
+#include "tree_device.cuh"
+
+namespace obvh {
+namespace atrbvh {
+
+constexpr int kThreads = 256;
+constexpr int kTreeletThreads = 128;
+constexpr int kTreeletWarps = kTreeletThreads / 32;
+constexpr int kMinTau = 3;
+constexpr int kMaxTau = 20;
+constexpr int kMaxDist = (kMaxTau - 1) * kMaxTau / 2;
+
+// One node of the working tree (48 bytes).
+struct TNode {
+    float lo[3], hi[3];
+    int32_t left, right;
+    float area;
+    int32_t parent;
+    int32_t data;  // triangle of a leaf, -1 for an internal node
+    int32_t pad;
+};
+static_assert(sizeof(TNode) == 48, "TNode is 48 bytes");
+
+struct Ctl {
+    uint32_t error;
+    uint32_t pad[63];
+};
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float box_area(const float* lo, const float* hi) {  // Commons.cuh:95-139
+    const float sx = hi[0] - lo[0], sy = hi[1] - lo[1], sz = hi[2] - lo[2];
+    return 2 * (sx * sy + sx * sz + sy * sz);
+}
+
+__device__ __forceinline__ float union_area(const float* alo, const float* ahi, const float* blo, const float* bhi) {
+    const float sx = fmaxf(ahi[0], bhi[0]) - fminf(alo[0], blo[0]);  // Commons.cuh:173-190
+    const float sy = fmaxf(ahi[1], bhi[1]) - fminf(alo[1], blo[1]);
+    const float sz = fmaxf(ahi[2], bhi[2]) - fminf(alo[2], blo[2]);
+    return 2 * (sx * sy + sx * sz + sy * sz);
+}
+
+__device__ __forceinline__ uint64_t expand_bits64(uint64_t v) {  // 21 bits -> every third of 63
+    v &= 0x1fffffu;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+}
+
+__global__ void __launch_bounds__(kThreads) morton63_kernel(const kr_vec3* verts, const uint4* faces, uint32_t n,
+                                                            const kr_aabb3* scene, uint64_t* keys, uint32_t* vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint4 f = __ldg(faces + i);
+    const f3 a = tree::load_vertex(verts, f.x), b = tree::load_vertex(verts, f.y), c = tree::load_vertex(verts, f.z);
+    const float* sb = reinterpret_cast<const float*>(scene);
+    const float va[3] = {a.x, a.y, a.z}, vb[3] = {b.x, b.y, b.z}, vc[3] = {c.x, c.y, c.z};
+    uint64_t code = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float lo = fminf(fminf(va[k], vb[k]), vc[k]);
+        const float hi = fmaxf(fmaxf(va[k], vb[k]), vc[k]);
+        const float centre = (hi + lo) * 0.5f;
+        const float u = (centre - sb[k]) / (sb[3 + k] - sb[k]);
+        const uint64_t q = static_cast<uint64_t>(fminf(fmaxf(u * 2097152.0f, 0.0f), 2097151.0f));
+        code |= expand_bits64(q) << (2 - k);
+    }
+    keys[i] = code;
+    vals[i] = i;
+}
+
+// longestCommonPrefix over 64-bit keys with the index tie-break (LBVH.cu:171-185).
+__device__ __forceinline__ int lcp64(const uint64_t* keys, uint32_t n, int i, int j, uint64_t ki) {
+    if (j < 0 || j >= static_cast<int>(n)) return -1;
+    const uint64_t kj = __ldg(keys + j);
+    if (ki == kj) return 64 + __clz(i ^ j);
+    return __clzll(ki ^ kj);
+}
+
+__global__ void __launch_bounds__(kThreads) karras63_kernel(const uint64_t* keys, const uint32_t* order, uint32_t n,
+                                                            TNode* t, uint32_t* err) {
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    const int internal = static_cast<int>(n) - 1;
+    if (i >= internal) return;
+    const uint64_t k1 = __ldg(keys + i);
+    const int l1 = lcp64(keys, n, i, i + 1, k1), l2 = lcp64(keys, n, i, i - 1, k1);
+    const int d = (l1 - l2 > 0) - (l1 - l2 < 0);
+    if (d == 0) {  // cannot happen with the index tie-break; guards the searches below
+        atomicOr(err, kErrBadInput);
+        return;
+    }
+    const int minlcp = lcp64(keys, n, i, i - d, k1);
+    int lmax = 2;
+    while (lcp64(keys, n, i, i + lmax * d, k1) > minlcp) lmax <<= 1;
+    int l = 0;
+    for (int s = lmax >> 1; s >= 1; s >>= 1)
+        if (lcp64(keys, n, i, i + (l + s) * d, k1) > minlcp) l += s;
+    const int j = i + l * d;
+    const int nodelcp = lcp64(keys, n, i, j, k1);
+    int s = 0;
+    const int maxdiv = 1 << (32 - __clz(l));
+    for (int divisor = 2; divisor <= maxdiv; divisor <<= 1) {
+        const int step = (l + divisor - 1) / divisor;
+        if (lcp64(keys, n, i, i + (s + step) * d, k1) > nodelcp) s += step;
+    }
+    const int split = i + s * d + min(d, 0);
+    int li = split, ri = split + 1;
+    if (min(i, j) == split) {
+        li = split + internal;
+        t[li].data = static_cast<int32_t>(__ldg(order + split));
+    }
+    if (max(i, j) == split + 1) {
+        ri = split + 1 + internal;
+        t[ri].data = static_cast<int32_t>(__ldg(order + split + 1));
+    }
+    t[i].left = li;
+    t[i].right = ri;
+    t[i].data = -1;
+    t[li].parent = i;
+    t[ri].parent = i;
+    if (i == 0) t[0].parent = -1;
+}
+
+__device__ __forceinline__ void store_box(TNode* t, int32_t i, const float* lo, const float* hi) {
+    float* d = t[i].lo;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        __stcg(d + k, lo[k]);
+        __stcg(d + 3 + k, hi[k]);
+    }
+    __stcg(&t[i].area, box_area(lo, hi));
+}
+
+__device__ __forceinline__ void load_box(const TNode* t, int32_t i, float* lo, float* hi) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = __ldcg(t[i].lo + k);
+        hi[k] = __ldcg(t[i].hi + k);
+    }
+}
+
+// Leaf boxes, then node boxes bottom-up (the second thread to arrive merges).
+__global__ void __launch_bounds__(kThreads) boxes_up_kernel(const kr_vec3* verts, const uint4* faces, uint32_t n,
+                                                            TNode* t, uint32_t* visits, uint32_t* err) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int32_t internal = static_cast<int32_t>(n) - 1;
+    int32_t child = internal + static_cast<int32_t>(j);
+    const int32_t tri = t[child].data;
+    if (tri < 0 || tri >= static_cast<int32_t>(n)) {
+        atomicOr(err, kErrBadInput);
+        return;
+    }
+    const uint4 f = __ldg(faces + tri);
+    const f3 a = tree::load_vertex(verts, f.x), b = tree::load_vertex(verts, f.y), c = tree::load_vertex(verts, f.z);
+    float lo[3] = {fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z)};
+    float hi[3] = {fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z)};
+    t[child].left = -1;
+    t[child].right = -1;
+    store_box(t, child, lo, hi);
+    int32_t p = t[child].parent;
+    for (uint32_t steps = 0; p >= 0; ++steps) {
+        if (steps > n || p >= internal) {
+            atomicOr(err, kErrCycle);
+            return;
+        }
+        if (tree::arrive(visits + p) == 0) return;
+        const int32_t L = __ldcg(&t[p].left), R = __ldcg(&t[p].right);
+        const int32_t sib = L == child ? R : L;
+        if (sib < 0 || sib >= static_cast<int32_t>(2 * n - 1)) {
+            atomicOr(err, kErrCycle);
+            return;
+        }
+        float slo[3], shi[3];
+        load_box(t, sib, slo, shi);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = fminf(lo[k], slo[k]);
+            hi[k] = fmaxf(hi[k], shi[k]);
+        }
+        store_box(t, p, lo, hi);
+        child = p;
+        p = __ldcg(&t[p].parent);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Treelet optimisation.
+
+struct WarpSmem {
+    int32_t internal[32];
+    int32_t leaves[32];
+    float areas[32];
+    float dist[kMaxDist];
+};
+
+// The reference's shuffle-down reductions (Treelet.cuh:21-37 keeps the larger
+// area, AgglomerativeTreelet.cu:59-74 the smaller distance; strict, so on a tie
+// the lane's own value stays).  Uniform across the warp.
+__device__ __forceinline__ void reduce_down(int count, int& idx, float& val, bool want_max) {
+    int amount = count / 2;
+    while (count > 1) {
+        const int oi = __shfl_down_sync(0xffffffffu, idx, amount);
+        const float ov = __shfl_down_sync(0xffffffffu, val, amount);
+        if (want_max ? (ov > val) : (ov < val)) {
+            val = ov;
+            idx = oi;
+        }
+        count = (count + 1) / 2;
+        amount = count / 2;
+    }
+}
+
+__device__ __forceinline__ int trm_index(int row, int col) { return ((row - 1) * row) / 2 + col; }
+__device__ __forceinline__ int trm_row(int index) {  // TriangularMatrix.cuh:40-44
+    return static_cast<int>((-1 + sqrtf(8.0f * index + 1)) / 2) + 1;
+}
+__device__ __forceinline__ int trm_col(int index) {
+    const int y = trm_row(index);
+    return index - (y * (y - 1)) / 2;
+}
+
+__device__ __forceinline__ void shfl_box(const float* lo, const float* hi, int src, float* olo, float* ohi) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        olo[k] = __shfl_sync(0xffffffffu, lo[k], src);
+        ohi[k] = __shfl_sync(0xffffffffu, hi[k], src);
+    }
+}
+
+// The treelet rooted at `root`, by the whole warp.  False on a malformed tree.
+__device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, float ci, int32_t root, WarpSmem& w) {
+    const int lane = threadIdx.x & 31;
+    const int32_t internal_count = n - 1;
+
+    const int32_t node_count = 2 * n - 1;
+    auto valid = [&](int32_t x) { return x >= 0 && x < node_count; };
+    // formTreelet: grow by the frontier node of largest area (Treelet.cuh:55-129)
+    int bad = 0;
+    if (lane == 0) {
+        const int32_t L = __ldcg(&t[root].left), R = __ldcg(&t[root].right);
+        if (!valid(L) || !valid(R)) {
+            bad = 1;
+        } else {
+            w.internal[0] = root;
+            w.leaves[0] = L;
+            w.leaves[1] = R;
+            w.areas[0] = __ldcg(&t[L].area);
+            w.areas[1] = __ldcg(&t[R].area);
+        }
+    }
+    if (__shfl_sync(0xffffffffu, bad, 0)) return false;
+    __syncwarp();
+    for (int it = 0; it < tau - 2; ++it) {
+        int idx = -1;
+        float a = -FLT_MAX;
+        if (lane < 2 + it) {
+            idx = lane;
+            a = w.areas[lane];
+            if (w.leaves[lane] >= internal_count) a = -FLT_MAX;
+        }
+        reduce_down(2 + it, idx, a, true);
+        __syncwarp();
+        if (lane == 0) {
+            const int32_t rep = idx >= 0 ? w.leaves[idx] : -1;
+            const bool internal_node = rep >= 0 && rep < internal_count;
+            const int32_t L = internal_node ? __ldcg(&t[rep].left) : -1;
+            const int32_t R = internal_node ? __ldcg(&t[rep].right) : -1;
+            if (!internal_node || !valid(L) || !valid(R)) {
+                bad = 1;
+            } else {
+                w.internal[it + 1] = rep;
+                w.leaves[idx] = L;
+                w.leaves[it + 2] = R;
+                w.areas[idx] = __ldcg(&t[L].area);
+                w.areas[it + 2] = __ldcg(&t[R].area);
+            }
+        }
+        bad = __shfl_sync(0xffffffffu, bad, 0);
+        __syncwarp();
+        if (bad) return false;
+    }
+
+    // Lane l < tau holds treelet leaf l: its node, SAH and box.
+    int32_t node = -1;
+    float sah = 0.f, lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+    if (lane < tau) {
+        node = w.leaves[lane];
+        sah = __ldcg(sah_arr + node);
+        load_box(t, node, lo, hi);
+    }
+    const int nd = (tau - 1) * tau / 2;
+    for (int k0 = 0; k0 < nd; k0 += 32) {  // every pair row > col
+        const int k = k0 + lane;
+        const int r = k < nd ? trm_row(k) : 0, c = k < nd ? trm_col(k) : 0;
+        float rlo[3], rhi[3], clo[3], chi[3];
+        shfl_box(lo, hi, r, rlo, rhi);
+        shfl_box(lo, hi, c, clo, chi);
+        if (k < nd) w.dist[k] = union_area(rlo, rhi, clo, chi);
+    }
+    __syncwarp();
+
+    for (int last = tau - 1; last > 0; --last) {
+        // pair of smallest union area (findMinimumDistance)
+        const int size = last * (1 + last) / 2;
+        int mi = 0;
+        float md = FLT_MAX;
+        for (int j = lane; j < size; j += 32) {
+            const float d = w.dist[j];
+            if (d < md) {
+                md = d;
+                mi = j;
+            }
+        }
+        reduce_down(32, mi, md, false);
+        mi = __shfl_sync(0xffffffffu, mi, 0);
+        const int jr = trm_row(mi), jc = trm_col(mi);
+
+        // updateState (AgglomerativeTreelet.cu:92-147)
+        const float s = __shfl_sync(0xffffffffu, sah, jr) + __shfl_sync(0xffffffffu, sah, jc);
+        const int32_t li = __shfl_sync(0xffffffffu, node, jr), ri = __shfl_sync(0xffffffffu, node, jc);
+        float alo[3], ahi[3], blo[3], bhi[3];
+        shfl_box(lo, hi, jr, alo, ahi);
+        shfl_box(lo, hi, jc, blo, bhi);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            alo[k] = fminf(blo[k], alo[k]);
+            ahi[k] = fmaxf(bhi[k], ahi[k]);
+        }
+        if (lane == jc) {
+            node = w.internal[last - 1];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { lo[k] = alo[k]; hi[k] = ahi[k]; }
+            w.areas[last] = s + ci * box_area(alo, ahi);
+            sah = w.areas[last];
+        }
+        const int32_t last_node = __shfl_sync(0xffffffffu, node, last);
+        const float last_sah = __shfl_sync(0xffffffffu, sah, last);
+        float llo[3], lhi[3];
+        shfl_box(lo, hi, last, llo, lhi);
+        if (lane == jr) {
+            node = last_node;
+            sah = last_sah;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { lo[k] = llo[k]; hi[k] = lhi[k]; }
+        }
+        if (lane == last) {
+            node = li;
+            w.leaves[last] = ri;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { lo[k] = alo[k]; hi[k] = ahi[k]; }
+        }
+        __syncwarp();
+
+        // updateDistancesMatrix (AgglomerativeTreelet.cu:149-186)
+        if (last > 1) {
+            float cp = 0.f;
+            int dst = -1;
+            if (lane < last && lane != jr) {
+                cp = w.dist[trm_index(last, lane)];
+                dst = trm_index(max(jr, lane), min(jr, lane));
+            }
+            __syncwarp();
+            if (dst >= 0) w.dist[dst] = cp;
+            __syncwarp();
+            int dr = lane, dc = lane;
+            const bool upd = lane < last && lane != jc;
+            if (upd) {
+                dr = max(jc, lane);
+                dc = min(jc, lane);
+            }
+            float rlo[3], rhi[3], clo[3], chi[3];
+            shfl_box(lo, hi, dr, rlo, rhi);
+            shfl_box(lo, hi, dc, clo, chi);
+            const float d = union_area(rlo, rhi, clo, chi);
+            if (upd) w.dist[trm_index(dr, dc)] = d;
+            __syncwarp();
+        }
+    }
+
+    // updateTreelet: keep the new topology if its SAH is lower
+    const bool better = w.areas[1] < __ldcg(sah_arr + w.internal[0]);
+    if (better && lane >= 1 && lane < tau) {
+        const int32_t ni = w.internal[lane - 1];
+        const int32_t right = w.leaves[lane];
+        __stcg(&t[ni].left, node);
+        __stcg(&t[ni].right, right);
+        __stcg(&t[node].parent, ni);
+        __stcg(&t[right].parent, ni);
+        __stcg(sah_arr + ni, w.areas[lane]);
+        store_box(t, ni, lo, hi);
+    }
+    __threadfence();
+    __syncwarp();
+    return true;
+}
+
+__global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, float* sah_arr, int32_t* tris,
+                                                                  uint32_t* counters, int32_t n, int tau,
+                                                                  int32_t gamma, float ci, float ct, uint32_t* err) {
+    __shared__ WarpSmem smem[kTreeletWarps];
+    WarpSmem& w = smem[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int32_t i = static_cast<int32_t>(blockIdx.x * blockDim.x + threadIdx.x);
+    const int32_t internal = n - 1;
+    int32_t cur = -1;
+    if (i < n) {
+        const int32_t leaf = internal + i;
+        __stcg(tris + leaf, 1);
+        __stcg(sah_arr + leaf, ct * __ldcg(&t[leaf].area));
+        cur = __ldcg(&t[leaf].parent);
+    }
+    uint32_t rounds = 0;
+    while (__ballot_sync(0xffffffffu, cur >= 0) != 0) {
+        if (++rounds > static_cast<uint32_t>(n) + 2) {  // deeper than any tree of n leaves
+            if (lane == 0) atomicOr(err, kErrCycle);
+            break;
+        }
+        __threadfence();
+        int32_t count = 0;
+        if (cur >= 0) {
+            if (cur >= internal) {
+                atomicOr(err, kErrCycle);
+                cur = -1;
+            } else if (tree::arrive(counters + cur) == 0) {
+                cur = -1;  // the first child to arrive stops; the second carries on
+            } else {
+                const int32_t L = __ldcg(&t[cur].left), R = __ldcg(&t[cur].right);
+                if (L < 0 || L >= 2 * n - 1 || R < 0 || R >= 2 * n - 1) {
+                    atomicOr(err, kErrCycle);
+                    cur = -1;
+                } else {
+                    const float area = __ldcg(&t[cur].area);
+                    count = __ldcg(tris + L) + __ldcg(tris + R);
+                    __stcg(tris + cur, count);
+                    __stcg(sah_arr + cur, ci * area + __ldcg(sah_arr + L) + __ldcg(sah_arr + R));
+                }
+            }
+        }
+        uint32_t vote = __ballot_sync(0xffffffffu, count >= gamma);
+        while (vote != 0) {
+            const int src = __ffs(vote) - 1;
+            const int32_t root = __shfl_sync(0xffffffffu, cur, src);
+            if (!process_treelet(t, sah_arr, n, tau, ci, root, w) && lane == 0) atomicOr(err, kErrBadInput);
+            vote &= vote - 1;
+        }
+        if (cur >= 0) cur = __ldcg(&t[cur].parent);
+    }
+}
+
+// SoA tree -> kr_bvh_node and parents (copyTree_kernel, atrbvh.cu:95-123):
+// internal nodes get their children and zero bounds, leaves their box, one
+// primitive and the triangle index.
+__global__ void __launch_bounds__(kThreads) emit_kernel(const TNode* t, uint32_t n, kr_bvh_node* nodes,
+                                                        uint32_t* parents) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * n - 1) return;
+    const TNode& s = t[i];
+    parents[i] = static_cast<uint32_t>(s.parent);
+    uint32_t w[9];
+    if (i < n - 1) {
+        for (int k = 0; k < 6; ++k) w[k] = 0u;
+        w[6] = static_cast<uint32_t>(s.left);
+        w[7] = static_cast<uint32_t>(s.right);
+        w[8] = 0u;
+    } else {
+        for (int k = 0; k < 3; ++k) {
+            w[k] = __float_as_uint(s.lo[k]);
+            w[3 + k] = __float_as_uint(s.hi[k]);
+        }
+        w[6] = static_cast<uint32_t>(s.data);
+        w[7] = 0u;
+        w[8] = 1u;
+    }
+    uint32_t* d = reinterpret_cast<uint32_t*>(nodes + i);
+    for (int k = 0; k < 9; ++k) d[k] = w[k];
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+struct Layout {
+    size_t ctl, bounds_ws, scene, keys0, keys1, vals0, vals1, sort, tnodes, counters, tris, sah, obb_ws, col_ws,
+        total;
+};
+
+Layout layout(uint32_t n) {
+    const size_t nn = n > 0 ? 2ull * n - 1 : 1;
+    Layout L;
+    size_t o = 0;
+    L.ctl = o;       o += align256(sizeof(Ctl));
+    L.bounds_ws = o; o += align256(lbvh::layout(0).total);
+    L.scene = o;     o += align256(2 * sizeof(kr_aabb3));
+    L.keys0 = o;     o += align256(8ull * n);
+    L.keys1 = o;     o += align256(8ull * n);
+    L.vals0 = o;     o += align256(4ull * n);
+    L.vals1 = o;     o += align256(4ull * n);
+    L.sort = o;      o += align256(radix_sort_temp_bytes(n));
+    L.tnodes = o;    o += align256(sizeof(TNode) * nn);
+    L.counters = o;  o += align256(4ull * nn);
+    L.tris = o;      o += align256(4ull * nn);
+    L.sah = o;       o += align256(4ull * nn);
+    L.obb_ws = o;    o += align256(obbtree::layout(n).total);
+    L.col_ws = o;    o += align256(collapse::layout(n).total);
+    L.total = o;
+    return L;
+}
+
+kr_error check_args(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32_t tau, const void* ws) {
+    if (n < 2) return "obvh_atrbvh: at least two triangles are needed";
+    if (n > (1u << 30)) return "obvh_atrbvh: more than 2^30 triangles";
+    if (!verts || !faces || !ws) return "obvh_atrbvh: null pointer argument";
+    if (reinterpret_cast<uintptr_t>(ws) & 255) return "obvh_atrbvh: workspace must be 256-byte aligned";
+    if (tau < static_cast<uint32_t>(kMinTau) || tau > static_cast<uint32_t>(kMaxTau))
+        return "obvh_atrbvh: treelet size must be 3..20";
+    return kr_success;
+}
+
+kr_error enqueue_tree(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32_t tau, uint32_t iterations,
+                      float ci, float ct, kr_bvh_node* nodes, uint32_t* parents, uint32_t* counts, float* costs,
+                      kr_aabb3* scene_out, void* workspace, cudaStream_t s) {
+    OBVH_TRY(check_args(verts, faces, n, tau, workspace));
+    if (!nodes || !parents || !counts || !costs) return "obvh_atrbvh: null pointer argument";
+    char* ws = static_cast<char*>(workspace);
+    const Layout L = layout(n);
+    uint32_t* err = &reinterpret_cast<Ctl*>(ws + L.ctl)->error;
+    kr_aabb3* scene = reinterpret_cast<kr_aabb3*>(ws + L.scene);
+    TNode* t = reinterpret_cast<TNode*>(ws + L.tnodes);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(ws + L.counters);
+    const unsigned grid_n = (n + kThreads - 1) / kThreads;
+    const uint32_t internal = n - 1;
+
+    // the transform's and the collapse's control blocks start at zero on every
+    // build, so the status reads zero for the steps that do not run
+    OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.obb_ws, 0, 256, s));
+    OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.col_ws, 0, 256, s));
+    OBVH_TRY(lbvh::enqueue_bounds(verts, faces, n, nullptr, ws + L.bounds_ws, scene, nullptr, true, s));
+    {
+        ProfScope prof_scope_("morton63_kernel", s);
+        morton63_kernel<<<grid_n, kThreads, 0, s>>>(verts, reinterpret_cast<const uint4*>(faces), n, scene,
+                                                    reinterpret_cast<uint64_t*>(ws + L.keys0),
+                                                    reinterpret_cast<uint32_t*>(ws + L.vals0));
+    }
+    OBVH_TRY_CUDA(cudaGetLastError());
+    bool alt = false;
+    OBVH_TRY(radix_sort_pairs(ws + L.keys0, ws + L.keys1, reinterpret_cast<uint32_t*>(ws + L.vals0),
+                              reinterpret_cast<uint32_t*>(ws + L.vals1), n, 8, 0, 63, ws + L.sort, s, &alt));
+    const uint64_t* keys = reinterpret_cast<const uint64_t*>(ws + (alt ? L.keys1 : L.keys0));
+    const uint32_t* order = reinterpret_cast<const uint32_t*>(ws + (alt ? L.vals1 : L.vals0));
+    {
+        ProfScope prof_scope_("karras63_kernel", s);
+        karras63_kernel<<<(internal + kThreads - 1) / kThreads, kThreads, 0, s>>>(keys, order, n, t, err);
+    }
+    OBVH_TRY_CUDA(cudaGetLastError());
+    OBVH_TRY_CUDA(cudaMemsetAsync(counters, 0, 4ull * internal, s));
+    {
+        ProfScope prof_scope_("boxes_up_kernel", s);
+        boxes_up_kernel<<<grid_n, kThreads, 0, s>>>(verts, reinterpret_cast<const uint4*>(faces), n, t, counters, err);
+    }
+    OBVH_TRY_CUDA(cudaGetLastError());
+    int32_t gamma = static_cast<int32_t>(tau);
+    const unsigned grid_t = (n + kTreeletThreads - 1) / kTreeletThreads;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        OBVH_TRY_CUDA(cudaMemsetAsync(counters, 0, 4ull * internal, s));
+        {
+            ProfScope prof_scope_("treelet_kernel", s);
+            treelet_kernel<<<grid_t, kTreeletThreads, 0, s>>>(
+                t, reinterpret_cast<float*>(ws + L.sah), reinterpret_cast<int32_t*>(ws + L.tris), counters,
+                static_cast<int32_t>(n), static_cast<int>(tau), gamma, ci, ct, err);
+        }
+        OBVH_TRY_CUDA(cudaGetLastError());
+        gamma = gamma > (1 << 29) ? gamma : 2 * gamma;
+    }
+    {
+        ProfScope prof_scope_("emit_kernel", s);
+        emit_kernel<<<(2 * n - 1 + kThreads - 1) / kThreads, kThreads, 0, s>>>(t, n, nodes, parents);
+    }
+    OBVH_TRY_CUDA(cudaGetLastError());
+    OBVH_TRY(lbvh::enqueue_refit(nodes, parents, counts, costs, counters, n, err, s));
+    if (scene_out) OBVH_TRY_CUDA(cudaMemcpyAsync(scene_out, scene, sizeof(kr_aabb3), cudaMemcpyDeviceToDevice, s));
+    return kr_success;
+}
+
+kr_error enqueue_full(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32_t flags, uint32_t tau,
+                      uint32_t iterations, float ci, float ct, kr_bvh_node* nodes, uint32_t* parents,
+                      uint32_t* counts, float* costs, kr_aabb3* scene_out, kr_obb3* obbs, kr_mat4* xfs,
+                      kr_bvh_node* collapsed, uint32_t* prims, void* workspace, cudaStream_t s) {
+    OBVH_TRY(enqueue_tree(verts, faces, n, tau, iterations, ci, ct, nodes, parents, counts, costs, scene_out,
+                          workspace, s));
+    char* ws = static_cast<char*>(workspace);
+    const Layout L = layout(n);
+    if (flags & OBVH_BUILD_OBBS) {
+        if (!obbs || !xfs) return "obvh_build_atrbvh: OBVH_BUILD_OBBS needs obbs and transforms";
+        OBVH_TRY(obbtree::enqueue(nodes, parents, verts, faces, obbs, xfs, n, n - 1, ws + L.obb_ws, s));
+    }
+    if (flags & OBVH_BUILD_COLLAPSE) {
+        if (!collapsed || !prims) return "obvh_build_atrbvh: OBVH_BUILD_COLLAPSE needs collapsed and primitives";
+        OBVH_TRY(collapse::enqueue(nodes, parents, collapsed, counts, prims, costs, ci, ct, n, n - 1, ws + L.col_ws, s,
+                                   nullptr));
+    }
+    return kr_success;
+}
+
+kr_error status(const void* workspace, uint32_t n, cudaStream_t s, uint32_t* device_error, uint32_t* slots) {
+    const char* ws = static_cast<const char*>(workspace);
+    const Layout L = layout(n);
+    uint32_t e[2] = {0, 0};
+    uint32_t col[2] = {0, 0};  // collapse error word, primitive slots
+    OBVH_TRY_CUDA(cudaMemcpyAsync(&e[0], ws + L.ctl, 4, cudaMemcpyDeviceToHost, s));
+    OBVH_TRY_CUDA(cudaMemcpyAsync(&e[1], ws + L.obb_ws, 4, cudaMemcpyDeviceToHost, s));  // transform error word
+    OBVH_TRY_CUDA(cudaMemcpyAsync(col, ws + L.col_ws, 8, cudaMemcpyDeviceToHost, s));
+    OBVH_TRY_CUDA(cudaStreamSynchronize(s));
+    if (device_error) *device_error = e[0] | e[1] | col[0];
+    if (slots) *slots = col[1];
+    return kr_success;
+}
+
+}  // namespace atrbvh
+}  // namespace obvh
+
+namespace {
+kr_error fail(kr_error e) {
+    obvh::set_last_error(e);
+    return e;
+}
+}  // namespace
+
+extern "C" kr_size obvh_atrbvh_workspace_bytes(kr_u32 face_count) {
+    return obvh::atrbvh::layout(face_count).total;
+}
+
+extern "C" kr_error obvh_atrbvh_workspace_init(void* d_workspace, kr_u32 face_count, void* stream) {
+    if (!d_workspace) return fail("obvh_atrbvh_workspace_init: null workspace");
+    cudaError_t e = cudaMemsetAsync(d_workspace, 0, obvh::atrbvh::layout(face_count).total,
+                                    static_cast<cudaStream_t>(stream));
+    return e != cudaSuccess ? fail(obvh::cuda_error(e)) : kr_success;
+}
+
+extern "C" kr_error obvh_atrbvh_build_async(const kr_vec3* d_vertices, const kr_uvec4* d_faces, kr_u32 face_count,
+                                            kr_u32 treelet_size, kr_u32 iterations, kr_scalar ci, kr_scalar ct,
+                                            kr_bvh_node* d_nodes, kr_u32* d_parents, kr_u32* d_primitive_counts,
+                                            kr_scalar* d_costs, kr_aabb3* d_scene, void* d_workspace,
+                                            void* stream) {
+    kr_error e = obvh::atrbvh::enqueue_tree(d_vertices, d_faces, face_count, treelet_size, iterations, ci, ct, d_nodes,
+                                            d_parents, d_primitive_counts, d_costs, d_scene, d_workspace,
+                                            static_cast<cudaStream_t>(stream));
+    return e ? fail(e) : kr_success;
+}
+
+extern "C" kr_error obvh_build_atrbvh_async(const kr_vec3* d_vertices, const kr_uvec4* d_faces, kr_u32 face_count,
+                                            kr_u32 flags, kr_u32 treelet_size, kr_u32 iterations, kr_scalar ci,
+                                            kr_scalar ct, kr_bvh_node* d_nodes, kr_u32* d_parents,
+                                            kr_u32* d_primitive_counts, kr_scalar* d_costs, kr_aabb3* d_scene,
+                                            kr_obb3* d_obbs, kr_mat4* d_transforms, kr_bvh_node* d_collapsed,
+                                            kr_u32* d_primitives, void* d_workspace, void* stream) {
+    kr_error e = obvh::atrbvh::enqueue_full(d_vertices, d_faces, face_count, flags, treelet_size, iterations, ci, ct,
+                                            d_nodes, d_parents, d_primitive_counts, d_costs, d_scene, d_obbs,
+                                            d_transforms, d_collapsed, d_primitives, d_workspace,
+                                            static_cast<cudaStream_t>(stream));
+    return e ? fail(e) : kr_success;
+}
+
+extern "C" kr_error obvh_atrbvh_status(const void* d_workspace, kr_u32 face_count, void* stream, kr_u32* device_error,
+                                       kr_u32* primitive_slots) {
+    if (!d_workspace) return fail("obvh_atrbvh_status: null workspace");
+    kr_error e = obvh::atrbvh::status(d_workspace, face_count, static_cast<cudaStream_t>(stream), device_error,
+                                      primitive_slots);
+    return e ? fail(e) : kr_success;
+}

@@ -378,6 +378,17 @@ kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, 
     return kr_success;
 }
 
+kr_error enqueue_refit(kr_bvh_node* nodes, const uint32_t* parents, uint32_t* counts, float* costs, uint32_t* visits,
+                       uint32_t n, uint32_t* err, cudaStream_t s) {
+    if (n >= 2) OBVH_TRY_CUDA(cudaMemsetAsync(visits, 0, 4ull * (n - 1), s));
+    {
+        ProfScope prof_scope_("aabb_up_kernel", s);
+        aabb_up_kernel<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(nodes, parents, counts, costs, visits, n, err);
+    }
+    OBVH_TRY_CUDA(cudaGetLastError());
+    return kr_success;
+}
+
 const uint32_t* sorted_codes(const void* workspace, uint32_t n) {
     // the radix sort of 30-bit keys makes 4 passes: the result is in keys0/vals0
     return reinterpret_cast<const uint32_t*>(static_cast<const char*>(workspace) + layout(n).keys0);

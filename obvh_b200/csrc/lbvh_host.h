@@ -43,6 +43,11 @@ kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, 
                        uint32_t* parents, uint32_t* counts, float* costs, kr_aabb3* bounds_out, void* workspace,
                        cudaStream_t s);
 
+// Bottom-up bounds, counts and costs (ct = 1, ci = 1.2) of a tree whose
+// leaves [n-1, 2n-1) hold their boxes; `visits` is n-1 words of scratch.
+kr_error enqueue_refit(kr_bvh_node* nodes, const uint32_t* parents, uint32_t* counts, float* costs, uint32_t* visits,
+                       uint32_t n, uint32_t* err, cudaStream_t s);
+
 // The sorted Morton codes left in the workspace by the last build of n primitives.
 const uint32_t* sorted_codes(const void* workspace, uint32_t n);
 uint32_t* error_word(void* workspace);

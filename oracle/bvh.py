@@ -16,6 +16,8 @@ assert NODE.itemsize == 36
 _f32 = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _u32 = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _node = np.ctypeslib.ndpointer(dtype=NODE, flags="C_CONTIGUOUS")
+_u64 = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+_i32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _bound = False
 
 
@@ -39,6 +41,17 @@ def _bind():
         "oracle_obb_tree": (c.c_int, [_node, _u32, _f32, _u32, c.c_uint32, c.c_uint32, _f32, _f32, _f32]),
         "oracle_collapse": (c.c_int, [_node, _u32, _node, _u32, _u32, _f32, c.c_float, c.c_float, c.c_uint32,
                                       c.c_uint32]),
+        "oracle_aabb_refit": (c.c_int, [_node, c.c_uint32, _u32, _f32]),
+        "oracle_morton63": (c.c_uint64, [_f32, _f32]),
+        "oracle_morton63_unit": (c.c_uint64, [c.c_float, c.c_float, c.c_float]),
+        "oracle_atrbvh_box_area": (c.c_float, [_f32, _f32]),
+        "oracle_atrbvh_union_area": (c.c_float, [_f32, _f32, _f32, _f32]),
+        "oracle_trm_row": (c.c_int, [c.c_int]),
+        "oracle_trm_col": (c.c_int, [c.c_int]),
+        "oracle_stable_order64": (None, [_u64, c.c_uint32, _u32]),
+        "oracle_karras63": (None, [_u64, _u32, c.c_uint32, _i32, _i32, _i32, _i32]),
+        "oracle_atrbvh_build": (c.c_int, [_f32, _u32, c.c_uint32, c.c_int, c.c_int, c.c_float, c.c_float, _node,
+                                          _u32, _u32, _f32, _u64, _f32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(l, name)
@@ -164,3 +177,59 @@ def ref_vecmath():
 
 def ref_vecmath_available() -> bool:
     return os.path.exists(os.path.join(HERE, "_ref", "libref_vecmath.so"))
+
+
+def morton63(tri9, scene):
+    """63-bit Morton code of one triangle (9 floats) in the scene box (6 floats)."""
+    l = _bind()
+    return int(l.oracle_morton63(np.ascontiguousarray(tri9, np.float32), np.ascontiguousarray(scene, np.float32)))
+
+
+def karras63(sorted_codes, order):
+    """SoA tree of the 63-bit Karras build: (left, right, parent, data) int32 arrays."""
+    l = _bind()
+    k = np.ascontiguousarray(sorted_codes, np.uint64)
+    o = np.ascontiguousarray(order, np.uint32)
+    n = k.shape[0]
+    arrs = [np.full(2 * n - 1, -1, np.int32) for _ in range(4)]
+    l.oracle_karras63(k, o, n, *arrs)
+    return tuple(arrs)
+
+
+def atrbvh_build(verts, faces, treelet_size=9, iterations=2, ci=1.2, ct=1.0):
+    """LBVH-63 + agglomerative treelet optimisation, as kr_bvh_node records:
+    dict of nodes, parents, counts, costs, sorted codes, and the optimiser's
+    root SAH after each iteration."""
+    l = _bind()
+    v, f, n = _mesh(verts, faces)
+    nn = 2 * n - 1
+    out = {"nodes": np.zeros(nn, NODE), "parents": np.zeros(nn, np.uint32), "counts": np.zeros(nn, np.uint32),
+           "costs": np.zeros(nn, np.float32), "codes": np.zeros(n, np.uint64),
+           "sah": np.zeros(max(iterations, 1), np.float32)}
+    rc = l.oracle_atrbvh_build(v, f, n, treelet_size, iterations, ci, ct, out["nodes"], out["parents"],
+                               out["counts"], out["costs"], out["codes"], out["sah"])
+    if rc != 0:
+        raise ValueError("oracle_atrbvh_build failed")
+    return out
+
+
+def ref_atrbvh():
+    """The reference's host-callable ATRBVH helpers (oracle/_ref/libref_atrbvh.so), or None."""
+    path = os.path.join(HERE, "_ref", "libref_atrbvh.so")
+    if not os.path.exists(path):
+        return None
+    r = ctypes.CDLL(path)
+    c = ctypes
+    for name, (res, args) in {
+        "ref_morton63": (c.c_uint64, [c.c_float, c.c_float, c.c_float]),
+        "ref_expand_bits64": (c.c_uint64, [c.c_uint64]),
+        "ref_box_area": (c.c_float, [_f32, _f32]),
+        "ref_union_area": (c.c_float, [_f32, _f32, _f32, _f32]),
+        "ref_trm_index": (c.c_int, [c.c_int, c.c_int]),
+        "ref_trm_row": (c.c_int, [c.c_int]),
+        "ref_trm_col": (c.c_int, [c.c_int]),
+    }.items():
+        f = getattr(r, name)
+        f.restype = res
+        f.argtypes = args
+    return r

@@ -300,6 +300,35 @@ static int64_t post_order(const obvh_oracle_node* nodes, uint32_t internal, uint
     return k;
 }
 
+/* Bottom-up bounds, primitive counts and SAH costs of a tree whose leaves
+ * (at [n-1, 2n-1)) already hold their boxes: calculate_aabbs_kernel
+ * (src/ads/lbvh_gpu/lbvh.cu:399-457, and its copy in
+ * src/ads/atrbvh_gpu/atrbvh.cu:127-183), with ct = 1 and ci = 1.2 hard-coded
+ * there.  Returns 0, or -1 for a malformed tree. */
+int oracle_aabb_refit(obvh_oracle_node* nodes, uint32_t n, uint32_t* counts, float* costs) {
+    const uint32_t internal = n - 1;
+    const float ct = 1.0f, ci = 1.2f;
+    for (uint32_t j = 0; j < n; j++) {
+        costs[internal + j] = ct * area(nodes[internal + j].b);
+        counts[internal + j] = 1;
+    }
+    uint32_t* po = malloc(sizeof(uint32_t) * (internal + 1));
+    int64_t m = post_order(nodes, internal, po);
+    for (int64_t k = 0; k < m; k++) {
+        obvh_oracle_node* p = &nodes[po[k]];
+        const float* l = nodes[p->left].b;
+        const float* r = nodes[p->right].b;
+        /* kr_aabb_expand(left, right) = expand3(expand3(left, right.min), right.max) */
+        v3 lo = vmin(vmin(mk(l[0], l[1], l[2]), mk(r[0], r[1], r[2])), mk(r[3], r[4], r[5]));
+        v3 hi = vmax(vmax(mk(l[3], l[4], l[5]), mk(r[0], r[1], r[2])), mk(r[3], r[4], r[5]));
+        p->b[0] = lo.x; p->b[1] = lo.y; p->b[2] = lo.z; p->b[3] = hi.x; p->b[4] = hi.y; p->b[5] = hi.z;
+        counts[po[k]] = counts[p->left] + counts[p->right];
+        costs[po[k]] = ci * area(p->b) + costs[p->right] + costs[p->left];
+    }
+    free(po);
+    return (m == (int64_t)internal) ? 0 : -1;
+}
+
 void oracle_lbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, obvh_oracle_node* nodes,
                        uint32_t* parents, uint32_t* codes_sorted, uint32_t* counts, float* costs,
                        float scene[6], float centroid[6]) {
@@ -320,26 +349,7 @@ void oracle_lbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, o
     }
     if (n >= 2) oracle_karras(codes_sorted, n, nodes, parents);
     else parents[0] = 0xffffffffu;
-    /* calculate_aabbs_kernel (lbvh.cu:399-457): ct = 1, ci = 1.2 hard-coded */
-    const float ct = 1.0f, ci = 1.2f;
-    for (uint32_t j = 0; j < n; j++) {
-        costs[internal + j] = ct * area(nodes[internal + j].b);
-        counts[internal + j] = 1;
-    }
-    uint32_t* po = malloc(sizeof(uint32_t) * (internal + 1));
-    int64_t m = post_order(nodes, internal, po);
-    for (int64_t k = 0; k < m; k++) {
-        obvh_oracle_node* p = &nodes[po[k]];
-        const float* l = nodes[p->left].b;
-        const float* r = nodes[p->right].b;
-        /* kr_aabb_expand(left, right) = expand3(expand3(left, right.min), right.max) */
-        v3 lo = vmin(vmin(mk(l[0], l[1], l[2]), mk(r[0], r[1], r[2])), mk(r[3], r[4], r[5]));
-        v3 hi = vmax(vmax(mk(l[3], l[4], l[5]), mk(r[0], r[1], r[2])), mk(r[3], r[4], r[5]));
-        p->b[0] = lo.x; p->b[1] = lo.y; p->b[2] = lo.z; p->b[3] = hi.x; p->b[4] = hi.y; p->b[5] = hi.z;
-        counts[po[k]] = counts[p->left] + counts[p->right];
-        costs[po[k]] = ci * area(p->b) + costs[p->right] + costs[p->left];
-    }
-    free(po);
+    oracle_aabb_refit(nodes, n, counts, costs);
     free(codes);
     free(order);
 }

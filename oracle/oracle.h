@@ -48,6 +48,7 @@ void oracle_karras(const uint32_t* codes, uint32_t n, obvh_oracle_node* nodes, u
 void oracle_lbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, obvh_oracle_node* nodes,
                        uint32_t* parents, uint32_t* codes_sorted, uint32_t* counts, float* costs,
                        float scene[6], float centroid[6]);
+int oracle_aabb_refit(obvh_oracle_node* nodes, uint32_t n, uint32_t* counts, float* costs);
 void oracle_leaf_obb(const float* tri9, float obb[15], float xf[16]);
 int oracle_obb_tree(const obvh_oracle_node* nodes, const uint32_t* parents, const float* verts,
                     const uint32_t* faces4, uint32_t n_leaves, uint32_t n_internal, float* obbs, float* xfs,
@@ -55,6 +56,24 @@ int oracle_obb_tree(const obvh_oracle_node* nodes, const uint32_t* parents, cons
 int oracle_collapse(const obvh_oracle_node* nodes, const uint32_t* parents, obvh_oracle_node* collapsed,
                     uint32_t* counts, uint32_t* prims, float* costs, float ci, float ct, uint32_t n_leaves,
                     uint32_t n_internal);
+
+/* ATRBVH path (atrbvh_oracle.c) */
+uint64_t oracle_morton63(const float tri9[9], const float scene[6]);
+uint64_t oracle_morton63_unit(float x, float y, float z);  /* a point already in the unit cube */
+float oracle_atrbvh_box_area(const float* lo, const float* hi);
+float oracle_atrbvh_union_area(const float* alo, const float* ahi, const float* blo, const float* bhi);
+int oracle_trm_row(int index);
+int oracle_trm_col(int index);
+void oracle_stable_order64(const uint64_t* keys, uint32_t n, uint32_t* order);
+/* SoA tree of the 63-bit Karras build: left/right/parent/data per node (-1 = none). */
+void oracle_karras63(const uint64_t* sorted, const uint32_t* order, uint32_t n, int32_t* left, int32_t* right,
+                     int32_t* parent, int32_t* data);
+/* LBVH-63 + agglomerative treelet optimisation + copy to kr_bvh_node + refit.
+ * codes_sorted (nullable) receives the sorted Morton codes, sah_out (nullable)
+ * the root's treelet-optimiser SAH after each iteration.  Returns 0 or -1. */
+int oracle_atrbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, int treelet_size, int iterations,
+                        float ci, float ct, obvh_oracle_node* nodes, uint32_t* parents, uint32_t* counts,
+                        float* costs, uint64_t* codes_sorted, float* sah_out);
 
 #ifdef __cplusplus
 }
