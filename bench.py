@@ -54,9 +54,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["lbvh_obb_tree", "atrbvh_obb_tree", "dito", "dito_batch"],
+    ap.add_argument("--workload", choices=["lbvh_obb_tree", "atrbvh_obb_tree", "dito", "dito_batch", "serve"],
                     default="lbvh_obb_tree")
     ap.add_argument("--treelet", type=int, default=7, help="atrbvh_obb_tree: treelet size")
+    ap.add_argument("--requests", type=int, default=300, help="serve: requests in the stream")
     ap.add_argument("--sets", type=int, default=4096, help="dito_batch: point sets per batch")
     ap.add_argument("--no-autotune", action="store_true", help="dito_batch: default knobs")
     ap.add_argument("--points", type=int, default=100_000_000, help="dito: points per fit")
@@ -713,6 +714,160 @@ def bench_batch_reference(a, dist):
             "e2e": {"value": round(value, 3), "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def _serve_requests(n_req, seed, dev):
+    """The served mix: 70% DiTO fits of Gaussian clouds (1k..4M points,
+    log-uniform), 30% LBVH + OBB-tree + collapse builds of thin-triangle
+    soups (10k..2M triangles, log-uniform); inputs resident on the device."""
+    import math
+    import numpy as np
+    from obvh_b200 import workloads
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(n_req):
+        if rng.uniform() < 0.7:
+            n = int(math.exp(rng.uniform(math.log(1e3), math.log(4e6))))
+            reqs.append(("fit", workloads.gaussian_cloud_torch(n, rng, device=dev), n))
+        else:
+            n = int(math.exp(rng.uniform(math.log(1e4), math.log(2e6))))
+            v, f = workloads.triangle_soup_torch(n, seed=int(rng.integers(0, 2 ** 31)), device=dev)
+            reqs.append(("build", (v, f), n))
+    return reqs
+
+
+def bench_serve_ours(a, dist):
+    import threading
+    import numpy as np
+    import torch
+    from obvh_b200 import _native, bvh
+    from obvh_b200.server import Server
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lib = _native.lib()
+    reqs = _serve_requests(a.requests, 4 + dist.rank, dev)
+    torch.cuda.synchronize()
+    n_fit = sum(1 for r in reqs if r[0] == "fit")
+    pts = sum(r[2] for r in reqs if r[0] == "fit")
+    nodes = sum(2 * r[2] - 1 for r in reqs if r[0] == "build")
+    stream = torch.cuda.current_stream(dev)
+    S = ctypes.c_void_p(stream.cuda_stream)
+
+    # serial plain per-call: one request at a time through the plain paths, each
+    # call waited for before the next (the reference's kr_cuda_points_obb /
+    # commit are blocking calls); inputs already on the device
+    ws_fit = torch.zeros(int(lib.obvh_dito_workspace_bytes()), dtype=torch.uint8, device=dev)
+    _native.check(lib.obvh_dito_workspace_init(ctypes.c_void_p(ws_fit.data_ptr()), S))
+    nmax = max([r[2] for r in reqs if r[0] == "build"] or [1])
+    builder = bvh.ObvhBuilder(dev)
+    outs = builder.outputs(nmax)
+    obb = torch.empty(15, dtype=torch.float32, device=dev)
+
+    def plain(r):
+        if r[0] == "fit":
+            p = r[1]
+            _native.check(lib.obvh_dito_fit_async(ctypes.c_void_p(p.data_ptr()), r[2], 0, ctypes.c_void_p(obb.data_ptr()),
+                                                  ctypes.c_void_p(ws_fit.data_ptr()), S))
+        else:
+            v, f = r[1]
+            builder.build(bvh.Mesh.from_device(v, f), flags=3, ci=1.2, ct=1.0, stream=stream, out=outs)
+        stream.synchronize()
+
+    for r in reqs[:4]:
+        plain(r)
+    t0 = time.perf_counter()
+    for r in reqs:
+        plain(r)
+    serial_s = time.perf_counter() - t0
+    serial_rps = len(reqs) / serial_s
+    del outs
+    torch.cuda.empty_cache()
+
+    free, _ = torch.cuda.mem_get_info(dev)
+    budget = int(min(120 << 30, free - (4 << 30)))
+
+    def run(rate, host=None):
+        """Submits every request (Poisson arrivals at `rate` req/s, or all at
+        once for rate None), releases results in order; returns stats."""
+        srv = Server(budget_bytes=budget, build_lanes=4)
+        ids = [None] * len(reqs)
+        ready = threading.Semaphore(0)
+
+        def producer():
+            rng = np.random.default_rng(99)
+            t_next = time.perf_counter()
+            for k, r in enumerate(reqs):
+                if rate:
+                    t_next += rng.exponential(1.0 / rate)
+                    delay = t_next - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                if r[0] == "fit":
+                    ids[k] = srv.submit_fit(host[k] if host else r[1])
+                else:
+                    ids[k] = srv.submit_build(*(host[k] if host else r[1]), flags=3, ci=1.2, ct=1.0)
+                ready.release()
+
+        t = threading.Thread(target=producer)
+        t0 = time.perf_counter()
+        t.start()
+        for k in range(len(reqs)):
+            ready.acquire()
+            srv.wait(ids[k], 600_000)
+            srv.release(ids[k])
+        t.join()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        return st, wall
+
+    run(None)  # warm-up (plans, arena)
+    profile_enable(True)
+    sat, sat_wall = run(None)
+    prof = profile_summary()
+    profile_enable(False)
+    served_rps = len(reqs) / sat["span_s"]
+    sweep = {}
+    for frac in (0.5, 1.0, 2.0, 4.0):
+        rate = frac * serial_rps
+        st, wall = run(rate)
+        sweep[f"{frac:g}x_serial_rate"] = {"offered_rps": round(rate, 2), "served_rps": round(len(reqs) / wall, 2),
+                                           "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+                                           "max_ms": round(st["max_ms"], 3), "fit_batches": st["fit_batches"]}
+    # end to end: the same mix from pinned host memory, copied in by the server
+    host = []
+    for r in reqs:
+        if r[0] == "fit":
+            host.append(r[1].cpu().pin_memory().numpy())
+        else:
+            host.append((r[1][0].cpu().pin_memory().numpy(), r[1][1].cpu().pin_memory().numpy().view(np.uint32)))
+    e2e, e2e_wall = run(None, host)
+    h2d = sum(12 * r[2] if r[0] == "fit" else 12 * 3 * r[2] + 16 * r[2] for r in reqs)
+    return {
+        "metric": "Served mixed requests throughput (requests/s)", "value": round(served_rps, 3), "unit": "requests/s",
+        "n_gpus": dist.world, "steps": 1, "warmup": 1, "ms_per_step": round(1e3 * sat["span_s"], 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: 70% Gaussian-cloud fits (1k..4M points), 30% thin-triangle soup builds (10k..2M), "
+                "log-uniform sizes, seeded",
+        "config": {"workload": "serve_mixed", "requests": len(reqs), "fits": n_fit, "builds": len(reqs) - n_fit,
+                   "points": pts, "build_nodes": nodes, "hbm_budget_bytes": budget, "build_lanes": 4,
+                   "inputs": "device-resident", "l2": "GBs of inputs per run (> 126 MB L2)",
+                   "parallelism": f"replicas{dist.world}"},
+        "served": {"p50_ms": round(sat["p50_ms"], 3), "p99_ms": round(sat["p99_ms"], 3),
+                   "fit_batches": sat["fit_batches"], "peak_arena_bytes": sat["peak_bytes"],
+                   "mpoints_per_s": round(pts / sat["span_s"] / 1e6, 2),
+                   "mnodes_per_s": round(nodes / sat["span_s"] / 1e6, 2)},
+        "per_call": {"value": round(serial_rps, 3), "unit": "requests/s", "seconds": round(serial_s, 4),
+                     "api": "obvh_dito_fit_async / obvh_build_async, one request at a time, each waited for",
+                     "speedup": round(served_rps / serial_rps, 2)},
+        "poisson_sweep": sweep,
+        "kernels": {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()},
+        "gpu_launches": sum(v[0] for v in prof.values()),
+        "roofline": None,
+        "e2e": {"value": round(len(reqs) / e2e["span_s"], 3), "unit": "requests/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 60 * n_fit, "api": "obvh_server_submit_fit / _build from pinned host memory",
+                "p50_ms": round(e2e["p50_ms"], 3), "p99_ms": round(e2e["p99_ms"], 3)},
+    }
+
+
 def main():
     a = parse_args()
     dist = Dist()
@@ -734,7 +889,7 @@ def main():
     dist.init()
     try:
         run = {"lbvh_obb_tree": bench_tree_ours, "atrbvh_obb_tree": lambda a, d: bench_tree_ours(a, d, atrbvh=True),
-               "dito": bench_dito_ours, "dito_batch": bench_batch_ours}
+               "dito": bench_dito_ours, "dito_batch": bench_batch_ours, "serve": bench_serve_ours}
         line = run[a.workload](a, dist)
         if dist.rank == 0:
             print(json.dumps(line), flush=True)

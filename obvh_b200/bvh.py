@@ -50,6 +50,16 @@ class Mesh:
         self.verts = torch.from_numpy(v).to(device)
         self.faces = torch.from_numpy(f.view(np.int32)).to(device)
 
+    @classmethod
+    def from_device(cls, verts, faces):
+        """Wraps CUDA tensors already on the device (float32 [V,3], int32/uint32 [F,4])."""
+        m = cls.__new__(cls)
+        m.verts = verts.contiguous()
+        m.faces = faces.contiguous()
+        m.n_vertices = m.verts.shape[0]
+        m.n_faces = m.faces.shape[0]
+        return m
+
 
 class LbvhBuilder:
     """obvh_lbvh_build_async with a workspace kept between builds."""

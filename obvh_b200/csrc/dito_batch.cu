@@ -38,6 +38,7 @@
 #include "device_common.cuh"
 #include "dito_device.cuh"
 #include "obvh_api.h"
+#include "dito_batch_host.h"
 #include "obvh_batch.h"
 #include "runtime.h"
 
@@ -57,7 +58,8 @@ enum : uint32_t { kPending = 0, kNeedsPass2 = 1, kFinal = 2, kGaveUp = 3 };
 // Device view of a planned batch.
 struct Params {
     const float* xyz;           // all points, packed xyz
-    const uint64_t* offsets;    // [sets + 1]
+    const int64_t* first;       // [sets]: first coordinate of each set, in floats from xyz
+    const uint64_t* count;      // [sets]: its points
     const uint4* tasks;         // {kind, set or first list slot, chunk or set count, large-set slot}
     const uint32_t* warp_sets;  // sets of the warp tasks, 8 per task
     const uint2* chunks;        // per large set: first record, chunk count
@@ -94,10 +96,9 @@ struct SetView {
 };
 
 __device__ __forceinline__ SetView set_view(const Params& p, uint32_t s) {
-    const uint64_t o0 = p.offsets[s], o1 = p.offsets[s + 1];
     SetView v;
-    v.base = p.xyz + 3 * o0;
-    v.n = static_cast<uint32_t>(o1 - o0);
+    v.base = p.xyz + p.first[s];
+    v.n = static_cast<uint32_t>(p.count[s]);
     // A point is 12 bytes: base misaligned by 4*m bytes becomes aligned after m points.
     const uint32_t m = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(v.base) & 15u) >> 2);
     v.head = m < v.n ? m : v.n;
@@ -514,15 +515,19 @@ struct Batch {
     std::mutex mutex;
     int device = 0;
     uint32_t flags = 0;
-    std::vector<uint64_t> offsets;  // host copy
+    std::vector<int64_t> first;    // host copy of the sets: first coordinate (floats from the base)
+    std::vector<uint64_t> count;   // and points
+    uint64_t size(size_t s) const { return count[s]; }
+    size_t sets() const { return first.size(); }
     obvh_dito_batch_tuning tuning{};
     // plan
     std::vector<uint4> tasks;
     std::vector<uint32_t> warp_sets;
     std::vector<uint2> chunks;
     uint32_t nlarge = 0, nchunks = 0;
-    // device memory: offsets | tasks | warp_sets | chunks | ctl | large | rec1_val | rec1_idx | rec2
+    // device memory: first | count | tasks | warp_sets | chunks | ctl | large | rec1_val | rec1_idx | rec2
     DeviceBuffer dev;
+    PinnedBuffer staging;  // the plan on its way up
     size_t off_tasks = 0, off_warp = 0, off_chunks = 0, off_ctl = 0, off_large = 0, off_r1v = 0, off_r1i = 0,
            off_r2 = 0, ctl_bytes = 0;
     int grid = 0;
@@ -532,7 +537,11 @@ struct Batch {
     const void* graph_points = nullptr;
     void* graph_obbs = nullptr;
 
-    ~Batch() { drop_graph(); dev.release(); }
+    ~Batch() {
+        drop_graph();
+        dev.release();
+        staging.release();
+    }
     void drop_graph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -566,18 +575,18 @@ kr_error check_tuning(const obvh_dito_batch_tuning& t) {
 // Orders the tasks: large sets' pass-1 chunks (largest set first), CTA sets,
 // then warp tasks (both largest first), with each large set's pass-2 chunks
 // inserted `lag` tasks after its last pass-1 chunk (or at the end).
-kr_error plan(Batch& B) {
+kr_error plan(Batch& B, cudaStream_t s = nullptr, bool sync = true) {
     const obvh_dito_batch_tuning& t = B.tuning;
-    const size_t S = B.offsets.size() - 1;
+    const size_t S = B.sets();
     std::vector<uint32_t> warp_ids, cta_ids, large_ids;
     for (size_t s = 0; s < S; ++s) {
-        const uint64_t n = B.offsets[s + 1] - B.offsets[s];
+        const uint64_t n = B.size(s);
         if (n <= t.warp_max_points) warp_ids.push_back(static_cast<uint32_t>(s));
         else if (n <= t.cta_max_points) cta_ids.push_back(static_cast<uint32_t>(s));
         else large_ids.push_back(static_cast<uint32_t>(s));
     }
     auto by_size = [&](uint32_t a, uint32_t b) {
-        const uint64_t na = B.offsets[a + 1] - B.offsets[a], nb = B.offsets[b + 1] - B.offsets[b];
+        const uint64_t na = B.size(a), nb = B.size(b);
         return na != nb ? na > nb : a < b;
     };
     std::sort(warp_ids.begin(), warp_ids.end(), by_size);
@@ -595,7 +604,7 @@ kr_error plan(Batch& B) {
     uint32_t rec = 0;
     for (uint32_t b = 0; b < B.nlarge; ++b) {
         const uint32_t s = large_ids[b];
-        const uint64_t n = B.offsets[s + 1] - B.offsets[s];
+        const uint64_t n = B.size(s);
         const uint32_t nch = static_cast<uint32_t>((n + t.chunk_points - 1) / t.chunk_points);
         B.chunks.push_back(make_uint2(rec, nch));
         rec += nch;
@@ -642,7 +651,7 @@ kr_error plan(Batch& B) {
     }
 
     // device layout
-    size_t off = align256((S + 1) * sizeof(uint64_t));
+    size_t off = 2 * align256((S + 1) * sizeof(uint64_t));
     B.off_tasks = off;
     off = align256(off + B.tasks.size() * sizeof(uint4));
     B.off_warp = off;
@@ -662,16 +671,18 @@ kr_error plan(Batch& B) {
     off = align256(off + (B.nchunks + 1) * 6 * sizeof(float));
     B.drop_graph();
     OBVH_TRY(B.dev.reserve(off));
-    char* d = static_cast<char*>(B.dev.ptr);
-    OBVH_TRY_CUDA(cudaMemcpy(d, B.offsets.data(), (S + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice));
-    if (!B.tasks.empty())
-        OBVH_TRY_CUDA(cudaMemcpy(d + B.off_tasks, B.tasks.data(), B.tasks.size() * sizeof(uint4), cudaMemcpyHostToDevice));
-    if (!B.warp_sets.empty())
-        OBVH_TRY_CUDA(cudaMemcpy(d + B.off_warp, B.warp_sets.data(), B.warp_sets.size() * sizeof(uint32_t),
-                                 cudaMemcpyHostToDevice));
-    if (!B.chunks.empty())
-        OBVH_TRY_CUDA(cudaMemcpy(d + B.off_chunks, B.chunks.data(), B.chunks.size() * sizeof(uint2),
-                                 cudaMemcpyHostToDevice));
+    // the plan goes up in one copy from pinned staging (everything before the control words)
+    OBVH_TRY(B.staging.reserve(B.off_ctl));
+    char* h = static_cast<char*>(B.staging.ptr);
+    if (S) {
+        std::memcpy(h, B.first.data(), S * sizeof(int64_t));
+        std::memcpy(h + align256((S + 1) * sizeof(uint64_t)), B.count.data(), S * sizeof(uint64_t));
+    }
+    if (!B.tasks.empty()) std::memcpy(h + B.off_tasks, B.tasks.data(), B.tasks.size() * sizeof(uint4));
+    if (!B.warp_sets.empty()) std::memcpy(h + B.off_warp, B.warp_sets.data(), B.warp_sets.size() * sizeof(uint32_t));
+    if (!B.chunks.empty()) std::memcpy(h + B.off_chunks, B.chunks.data(), B.chunks.size() * sizeof(uint2));
+    OBVH_TRY_CUDA(cudaMemcpyAsync(B.dev.ptr, h, B.off_ctl, cudaMemcpyHostToDevice, s));
+    if (sync) OBVH_TRY_CUDA(cudaStreamSynchronize(s));
     return kr_success;
 }
 
@@ -686,13 +697,15 @@ kr_error launch_u(const Batch& B, const Params& prm, cudaStream_t s) {
 }
 
 kr_error enqueue(Batch& B, const kr_vec3* d_points, kr_obb3* d_obbs, cudaStream_t s) {
-    if (B.offsets.size() > 1 && B.offsets.back() > 0 && !d_points) return "obvh_dito_batch: null points";
-    if (B.offsets.size() > 1 && !d_obbs) return "obvh_dito_batch: null output";
+    if (B.sets() > 0 && !d_points) return "obvh_dito_batch: null points";
+    if (B.sets() > 0 && !d_obbs) return "obvh_dito_batch: null output";
     if (reinterpret_cast<uintptr_t>(d_points) & 3u) return "obvh_dito_batch: points must be 4-byte aligned";
+    // (sets may also lie outside d_points' allocation: each set is d_points + first[s] floats)
     char* d = static_cast<char*>(B.dev.ptr);
     Params prm;
     prm.xyz = reinterpret_cast<const float*>(d_points);
-    prm.offsets = reinterpret_cast<const uint64_t*>(d);
+    prm.first = reinterpret_cast<const int64_t*>(d);
+    prm.count = reinterpret_cast<const uint64_t*>(d + align256((B.sets() + 1) * sizeof(uint64_t)));
     prm.tasks = reinterpret_cast<const uint4*>(d + B.off_tasks);
     prm.warp_sets = reinterpret_cast<const uint32_t*>(d + B.off_warp);
     prm.chunks = reinterpret_cast<const uint2*>(d + B.off_chunks);
@@ -711,6 +724,30 @@ kr_error enqueue(Batch& B, const kr_vec3* d_points, kr_obb3* d_obbs, cudaStream_
         case 8: return launch_u<2>(B, prm, s);
         default: return launch_u<4>(B, prm, s);
     }
+}
+
+Batch* make_batch(uint32_t flags, const obvh_dito_batch_tuning* tuning) {
+    Batch* b = new (std::nothrow) Batch();
+    if (!b) return nullptr;
+    cudaGetDevice(&b->device);
+    b->flags = flags;
+    b->tuning = tuning ? *tuning : default_tuning();
+    return b;
+}
+
+void free_batch(Batch* b) { delete b; }
+
+kr_error enqueue_status(Batch& B, uint32_t* host_word, cudaStream_t s) {
+    OBVH_TRY_CUDA(cudaMemcpyAsync(host_word, static_cast<char*>(B.dev.ptr) + B.off_ctl + 4, 4, cudaMemcpyDeviceToHost, s));
+    return kr_success;
+}
+
+kr_error replan(Batch& B, const int64_t* first, const uint64_t* count, size_t sets, cudaStream_t s) {
+    for (size_t i = 0; i < sets; ++i)
+        if (count[i] >= (1ull << 32) - 4) return "dito_batch: a set holds 2^32 points or more";
+    B.first.assign(first, first + sets);
+    B.count.assign(count, count + sets);
+    return plan(B, s, false);
 }
 
 kr_error status(Batch& B, cudaStream_t s, uint32_t* err) {
@@ -780,7 +817,12 @@ extern "C" kr_error obvh_dito_batch_create(const kr_size* offsets, kr_size sets,
     Batch& B = h->b;
     cudaGetDevice(&B.device);
     B.flags = flags;
-    B.offsets.assign(offsets, offsets + sets + 1);
+    B.first.resize(sets);
+    B.count.resize(sets);
+    for (kr_size i = 0; i < sets; ++i) {
+        B.first[i] = static_cast<int64_t>(3 * offsets[i]);
+        B.count[i] = offsets[i + 1] - offsets[i];
+    }
     B.tuning = tuning ? *tuning : obvh::dito_batch::default_tuning();
     kr_error e = obvh::dito_batch::check_tuning(B.tuning);
     if (!e) e = obvh::dito_batch::plan(B);

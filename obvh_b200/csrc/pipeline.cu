@@ -18,12 +18,14 @@
 //     is its leaf range read backwards, so no tree walk is needed to gather it.
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 
 #include "device_common.cuh"
 #include "lbvh_host.h"
 #include "obb_tree_host.h"
 #include "obvh_build.h"
+#include "pipeline_host.h"
 #include "runtime.h"
 #include "sort.h"
 #include "tree_device.cuh"
@@ -264,6 +266,15 @@ Layout layout(uint32_t n) {
     L.scan = o;     o += align256(scan_temp_bytes(nn));
     L.total = o;
     return L;
+}
+
+StatusWords status_words(uint32_t n) {
+    const Layout L = layout(n);
+    StatusWords w;
+    w.error = L.ctl + offsetof(Ctl, error);
+    w.slots = L.ctl + offsetof(Ctl, total_slots);
+    w.lbvh_error = L.lbvh + 4;  // lbvh::Ctl {ticket, error}
+    return w;
 }
 
 kr_error enqueue(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32_t flags, float ci, float ct,

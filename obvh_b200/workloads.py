@@ -199,3 +199,39 @@ def gaussian_sets_torch(n_sets: int = 4096, seed: int = 3, size_min: int = 64, s
         y = torch.einsum("nij,nj->ni", r, x) + torch.tensor(off[s0:s1], device=device)[ids]
         out[a:b] = y.to(torch.float32)
     return out, offsets
+
+
+def triangle_soup_torch(n_tris: int, seed: int = 1, rmin: float = 0.002, rmax: float = 0.02, device="cuda"):
+    """Same distribution as triangle_soup, generated with torch on `device` (a
+    different random stream): (vertices [3n x 3] float32, faces [n x 4] int32
+    with face i = (3i, 3i+1, 3i+2, 0))."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    c = torch.rand((n_tris, 1, 3), generator=g, device=device, dtype=torch.float64)
+    u = torch.randn((n_tris, 3, 3), generator=g, device=device, dtype=torch.float64)
+    u = u / u.norm(dim=2, keepdim=True)
+    r = torch.exp(torch.rand((n_tris, 3, 1), generator=g, device=device, dtype=torch.float64)
+                  * (math.log(rmax) - math.log(rmin)) + math.log(rmin))
+    v = (c + r * u).reshape(-1, 3).to(torch.float32)
+    f = torch.zeros((n_tris, 4), dtype=torch.int32, device=device)
+    base = torch.arange(0, 3 * n_tris, 3, dtype=torch.int32, device=device)
+    f[:, 0] = base
+    f[:, 1] = base + 1
+    f[:, 2] = base + 2
+    return v, f
+
+
+def gaussian_cloud_torch(n: int, rng: np.random.Generator, device="cuda", sigma_min: float = 0.01,
+                         sigma_max: float = 5.0, offset_range: float = 100.0):
+    """One anisotropic Gaussian cloud (the gaussian_sets generator for a single
+    set): per-axis sigma log-uniform, Haar rotation, uniform offset."""
+    import torch
+    sig = np.exp(rng.uniform(math.log(sigma_min), math.log(sigma_max), size=3))
+    rot = random_rotation(rng)
+    off = rng.uniform(-offset_range, offset_range, size=3)
+    g = torch.Generator(device=device)
+    g.manual_seed(int(rng.integers(0, 2 ** 62)))
+    x = torch.randn((n, 3), generator=g, device=device, dtype=torch.float64) * torch.tensor(sig, device=device)
+    y = x @ torch.tensor(rot.T, device=device) + torch.tensor(off, device=device)
+    return y.to(torch.float32).contiguous()
