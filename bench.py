@@ -138,21 +138,25 @@ class ClockSampler:
 
 
 class Dist:
+    """One process per GPU (replicas): a barrier and a max over ranks, nothing
+    on the data path.  NCCL on GPUs; gloo when OBVH_DIST_BACKEND=gloo (the CPU
+    tests of this plumbing)."""
+
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = os.environ.get("OBVH_DIST_BACKEND", "nccl")
         self.pg = False
 
     def init(self):
         import torch
+        if self.backend != "gloo":
+            torch.cuda.set_device(self.local if self.world > 1 else 0)
         if self.world > 1:
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            dist.init_process_group(self.backend, timeout=datetime.timedelta(seconds=120))
             self.pg = True
-        else:
-            torch.cuda.set_device(0)
 
     def barrier(self):
         if self.pg:
@@ -164,7 +168,7 @@ class Dist:
             return x
         import torch
         import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device="cpu" if self.backend == "gloo" else "cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
