@@ -114,6 +114,19 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 // ---------------------------------------------------------------------------
 // Lexicographic (value, index) selection: smaller value wins, ties go to the
 // smaller index -- the "first point wins" rule of a sequential strict scan.
+// Three-input min/max (one instruction on sm_100a).  Over finite values the
+// result is that of two kr_min/kr_max steps up to the sign of a zero.
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 __device__ __forceinline__ bool better_min(float v, uint64_t i, float bv, uint64_t bi) {
     return v < bv || (v == bv && i < bi);
 }

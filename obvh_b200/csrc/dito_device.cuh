@@ -75,8 +75,8 @@ struct Extremes {
         for (int k = 0; k < 7; ++k) {
             float v0 = slab(k, x[0], y[0], z[0]), v1 = slab(k, x[1], y[1], z[1]);
             float v2 = slab(k, x[2], y[2], z[2]), v3 = slab(k, x[3], y[3], z[3]);
-            float lo = fminf(fminf(v0, v1), fminf(v2, v3));
-            float hi = fmaxf(fmaxf(v0, v1), fmaxf(v2, v3));
+            float lo = min3f(v0, v1, fminf(v2, v3));
+            float hi = max3f(v0, v1, fmaxf(v2, v3));
             bool a = lo < mn[k];
             mn[k] = a ? lo : mn[k];
             gmn[k] = a ? g : gmn[k];

@@ -221,14 +221,24 @@ __device__ __forceinline__ Cand load_cand(const Cand* cand, uint32_t a) {
 }
 
 // projections of one triangle (9 floats) on the three axes, into lo/hi
-__device__ __forceinline__ void project_tri(const float* t, f3 b0, f3 b1, f3 b2, float lo[3], float hi[3]) {
+// (three-input min/max over the three vertices).
+struct Axes {
+    f3 b0, b1, b2;
+};
+__device__ __forceinline__ Axes make_axes(f3 b0, f3 b1, f3 b2) { return Axes{b0, b1, b2}; }
+__device__ __forceinline__ void project_tri(const float* t, const Axes& ax, float lo[3], float hi[3]) {
+    float q[3][3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
         const f3 p = mk3(__ldg(t + 3 * v), __ldg(t + 3 * v + 1), __ldg(t + 3 * v + 2));
-        const float q0 = dot3(p, b0), q1 = dot3(p, b1), q2 = dot3(p, b2);
-        lo[0] = fminf(lo[0], q0); hi[0] = fmaxf(hi[0], q0);
-        lo[1] = fminf(lo[1], q1); hi[1] = fmaxf(hi[1], q1);
-        lo[2] = fminf(lo[2], q2); hi[2] = fmaxf(hi[2], q2);
+        q[0][v] = dot3(p, ax.b0);
+        q[1][v] = dot3(p, ax.b1);
+        q[2][v] = dot3(p, ax.b2);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = fminf(min3f(lo[k], q[k][0], q[k][1]), q[k][2]);
+        hi[k] = fmaxf(max3f(hi[k], q[k][0], q[k][1]), q[k][2]);
     }
 }
 
@@ -245,7 +255,8 @@ __global__ void __launch_bounds__(kThreads) extents_small_kernel(const Cand* can
     const f3 b0 = mk3(c.ax[0], c.ax[1], c.ax[2]), b1 = mk3(c.ax[3], c.ax[4], c.ax[5]), b2 = mk3(c.ax[6], c.ax[7], c.ax[8]);
     float lo[3] = {c.olo[0], c.olo[1], c.olo[2]}, hi[3] = {c.ohi[0], c.ohi[1], c.ohi[2]};
     const float* t = tris + 9 * static_cast<size_t>(first[a]);
-    for (uint32_t i = 0; i < cnt; ++i) project_tri(t + 9 * i, b0, b1, b2, lo, hi);
+    const Axes ax = make_axes(b0, b1, b2);
+    for (uint32_t i = 0; i < cnt; ++i) project_tri(t + 9 * i, ax, lo, hi);
     finalize_node(c, mk3(lo[0], lo[1], lo[2]), mk3(hi[0], hi[1], hi[2]), obbs + a, xfs + a);
 }
 
@@ -285,7 +296,8 @@ __global__ void __launch_bounds__(kThreads) extents_units_kernel(const Cand* can
                      b2 = mk3(c.ax[6], c.ax[7], c.ax[8]);
             float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
             const float* t = tris + 9 * static_cast<size_t>(__ldg(first + a));
-            for (uint32_t i = begin + lane; i < end; i += 32) project_tri(t + 9 * static_cast<size_t>(i), b0, b1, b2, lo, hi);
+            const Axes ax = make_axes(b0, b1, b2);
+            for (uint32_t i = begin + lane; i < end; i += 32) project_tri(t + 9 * static_cast<size_t>(i), ax, lo, hi);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 lo[k] = warp_min(lo[k]);

@@ -51,28 +51,86 @@ __device__ __forceinline__ void store_words(kr_bvh_node* nodes, uint32_t i, cons
     for (int k = 0; k < count; ++k) __stcg(d + k, w[k]);
 }
 
-// Sorted leaf j: node internal + j, its triangle at slot j, its own box.
+// Writes `words` staged words to dst with coalesced stores: 4-byte stores up
+// to the first 16-byte boundary, 16-byte stores after it.  src (shared) and
+// dst (global) have the same address modulo 16.
+__device__ __forceinline__ void copy_out(uint32_t* dst, const uint32_t* src, uint32_t words) {
+    const uint32_t lead = min(words, static_cast<uint32_t>(((16 - (reinterpret_cast<uintptr_t>(dst) & 15)) & 15) / 4));
+    for (uint32_t t = threadIdx.x; t < lead; t += blockDim.x) dst[t] = src[t];
+    const uint32_t n4 = (words - lead) / 4;
+    float4* d4 = reinterpret_cast<float4*>(dst + lead);
+    const float4* s4 = reinterpret_cast<const float4*>(src + lead);
+    for (uint32_t t = threadIdx.x; t < n4; t += blockDim.x) d4[t] = s4[t];
+    for (uint32_t t = lead + 4 * n4 + threadIdx.x; t < words; t += blockDim.x) dst[t] = src[t];
+}
+
+// The staging slot in shared memory for a record of `rw` words of this thread
+// whose run of records starts at dst (same address phase modulo 16).
+__device__ __forceinline__ uint32_t* stage_at(uint32_t* stage, const void* dst, uint32_t rw) {
+    return stage + (reinterpret_cast<uintptr_t>(dst) & 15) / 4 + threadIdx.x * rw;
+}
+
+// Sorted leaf j: node internal + j, its triangle at slot j, its own box.  The
+// CTA's leaves are consecutive, so every output is one contiguous run per CTA:
+// records are staged in shared memory and written out coalesced.
 __global__ void __launch_bounds__(kThreads) leaves_fused_kernel(const float* tri_boxes, const uint32_t* order,
                                                                 const kr_vec3* verts, const uint4* faces, uint32_t n,
                                                                 kr_bvh_node* nodes, kr_bvh_node* collapsed,
                                                                 float* tris, kr_obb3* obbs, kr_mat4* xfs) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
+    __shared__ __align__(16) uint32_t stage_a[kThreads * 15 + 4];  // node (9), triangle (9) or box (15) records
+    __shared__ __align__(16) uint32_t stage_x[kThreads * 16 + 4];  // transforms
+    const uint32_t j0 = blockIdx.x * blockDim.x;
+    const uint32_t j = j0 + threadIdx.x;
+    const uint32_t count = min(static_cast<uint32_t>(blockDim.x), n - j0);
+    const bool live = j < n;
     const uint32_t internal = n - 1;
-    const uint32_t i = order[j];
-    const float* b = tri_boxes + 6 * static_cast<size_t>(i);
     uint32_t w[9];
-    for (int k = 0; k < 6; ++k) w[k] = __float_as_uint(b[k]);
-    w[6] = i;  // primitivesOffset
-    w[7] = 0;
-    w[8] = 1;  // one primitive, axis 0
-    store_words(nodes, internal + j, w, 9);
-    if (collapsed) store_words(collapsed, internal + j, w, 9);
-    const uint4 f = __ldg(faces + i);
-    const f3 v0 = load_vertex(verts, f.x), v1 = load_vertex(verts, f.y), v2 = load_vertex(verts, f.z);
-    float* t = tris + 9 * static_cast<size_t>(j);
-    t[0] = v0.x; t[1] = v0.y; t[2] = v0.z; t[3] = v1.x; t[4] = v1.y; t[5] = v1.z; t[6] = v2.x; t[7] = v2.y; t[8] = v2.z;
-    if (obbs) leaf_box(v0, v1, v2, obbs + internal + j, xfs + internal + j);
+    f3 v0 = mk3(0, 0, 0), v1 = v0, v2 = v0;
+    if (live) {
+        const uint32_t i = order[j];
+        const float* b = tri_boxes + 6 * static_cast<size_t>(i);
+        for (int k = 0; k < 6; ++k) w[k] = __float_as_uint(b[k]);
+        w[6] = i;  // primitivesOffset
+        w[7] = 0;
+        w[8] = 1;  // one primitive, axis 0
+        const uint4 f = __ldg(faces + i);
+        v0 = load_vertex(verts, f.x);
+        v1 = load_vertex(verts, f.y);
+        v2 = load_vertex(verts, f.z);
+    }
+    for (int out = 0; out < 2; ++out) {
+        kr_bvh_node* dst = out == 0 ? nodes : collapsed;
+        if (!dst) continue;
+        uint32_t* d = reinterpret_cast<uint32_t*>(dst + internal + j0);
+        if (live) {
+            uint32_t* st = stage_at(stage_a, d, 9);
+            for (int k = 0; k < 9; ++k) st[k] = w[k];
+        }
+        __syncthreads();
+        copy_out(d, stage_a + (reinterpret_cast<uintptr_t>(d) & 15) / 4, 9 * count);
+        __syncthreads();
+    }
+    {
+        uint32_t* d = reinterpret_cast<uint32_t*>(tris + 9 * static_cast<size_t>(j0));
+        if (live) {
+            float* st = reinterpret_cast<float*>(stage_at(stage_a, d, 9));
+            st[0] = v0.x; st[1] = v0.y; st[2] = v0.z; st[3] = v1.x; st[4] = v1.y; st[5] = v1.z;
+            st[6] = v2.x; st[7] = v2.y; st[8] = v2.z;
+        }
+        __syncthreads();
+        copy_out(d, stage_a + (reinterpret_cast<uintptr_t>(d) & 15) / 4, 9 * count);
+        __syncthreads();
+    }
+    if (obbs) {
+        uint32_t* db = reinterpret_cast<uint32_t*>(obbs + internal + j0);
+        uint32_t* dx = reinterpret_cast<uint32_t*>(xfs + internal + j0);
+        if (live)
+            leaf_box(v0, v1, v2, reinterpret_cast<kr_obb3*>(stage_at(stage_a, db, 15)),
+                     reinterpret_cast<kr_mat4*>(stage_at(stage_x, dx, 16)));
+        __syncthreads();
+        copy_out(db, stage_a + (reinterpret_cast<uintptr_t>(db) & 15) / 4, 15 * count);
+        copy_out(dx, stage_x + (reinterpret_cast<uintptr_t>(dx) & 15) / 4, 16 * count);
+    }
 }
 
 // Summary of sorted leaf j; its vertex ids are the triangle slots 3j..3j+2.
@@ -287,6 +345,10 @@ kr_error enqueue(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32
     if (!verts || !faces || !nodes || !parents || !counts || !costs || !workspace)
         return "obvh_build: null pointer argument";
     if (want_obbs && (!obbs || !xfs)) return "obvh_build: OBVH_BUILD_OBBS needs obbs and transforms";
+    if (want_obbs && ((reinterpret_cast<uintptr_t>(xfs) & 15) || (reinterpret_cast<uintptr_t>(obbs) & 3)))
+        return "obvh_build: transforms must be 16-byte and boxes 4-byte aligned";
+    if ((reinterpret_cast<uintptr_t>(nodes) & 3) || (collapsed && (reinterpret_cast<uintptr_t>(collapsed) & 3)))
+        return "obvh_build: node arrays must be 4-byte aligned";
     if (want_collapse && (!collapsed || !primitives)) return "obvh_build: OBVH_BUILD_COLLAPSE needs collapsed nodes and primitives";
     if (reinterpret_cast<uintptr_t>(workspace) & 255) return "obvh_build: workspace must be 256-byte aligned";
     char* ws = static_cast<char*>(workspace);

@@ -265,19 +265,38 @@ struct Candidate {
     f3 lo, hi;  // slots 3..5
 };
 
-// kr_min/kr_max over finite values equal fminf/fmaxf up to the sign of a zero.
-__device__ __forceinline__ void extent_proj(const f3* P, f3 d, float& lo, float& hi) {
-    lo = hi = dot3(P[0], d);
+// The 14 summary points.  (Packed two-wide multiplies and adds are each exact,
+// but a packed multiply feeding a packed add is contracted into a fused
+// multiply-add by the code generator even when both carry .rn, which changes
+// the rounding; the projections therefore stay scalar.)
+struct Points14 {
+    f3 p[14];
+};
+
+__device__ __forceinline__ Points14 pack14(const f3* P) {
+    Points14 q;
 #pragma unroll
-    for (int i = 1; i < 14; ++i) {
-        float q = dot3(P[i], d);
-        lo = fminf(lo, q);
-        hi = fmaxf(hi, q);
+    for (int k = 0; k < 14; ++k) q.p[k] = P[k];
+    return q;
+}
+
+// Extent of the 14 points along d: min and max of their projections, two
+// points per three-input min/max.
+__device__ __forceinline__ void extent_proj(const Points14& Q, f3 d, float& lo, float& hi) {
+    float a = dot3(Q.p[0], d), b = dot3(Q.p[1], d);
+    lo = fminf(a, b);
+    hi = fmaxf(a, b);
+#pragma unroll
+    for (int k = 1; k < 7; ++k) {
+        a = dot3(Q.p[2 * k], d);
+        b = dot3(Q.p[2 * k + 1], d);
+        lo = min3f(lo, a, b);
+        hi = max3f(hi, a, b);
     }
 }
 
-__device__ __forceinline__ void score_frames(const f3* P, f3 n, f3 e0, f3 e1, f3 e2, f3* b, f3& blen, f3& bmid,
-                                             float& best) {
+__device__ __forceinline__ void score_frames(const Points14& P, f3 n, f3 e0, f3 e1, f3 e2, f3* b, f3& blen,
+                                             f3& bmid, float& best) {
     const f3 e[3] = {e0, e1, e2};
     float nlo, nhi;
     extent_proj(P, n, nlo, nhi);
@@ -371,8 +390,9 @@ __device__ inline Candidate node_candidate(const f3* P, const Summary& s) {
         tn[nt] = unit3(cross3(g2, e1)); te[nt][0] = e1; te[nt][1] = g2; te[nt][2] = g1; ++nt;
         tn[nt] = unit3(cross3(g0, e2)); te[nt][0] = e2; te[nt][1] = g0; te[nt][2] = g2; ++nt;
     }
+    const Points14 Q = pack14(P);
 #pragma unroll 1
-    for (int t = 0; t < nt; ++t) score_frames(P, tn[t], te[t][0], te[t][1], te[t][2], b, blen, bmid, best);
+    for (int t = 0; t < nt; ++t) score_frames(Q, tn[t], te[t][0], te[t][1], te[t][2], b, blen, bmid, best);
     c.b0 = b[0]; c.b1 = b[1]; c.b2 = b[2];
     c.lo = blen;
     c.hi = bmid;
