@@ -63,8 +63,11 @@ __global__ void __launch_bounds__(kThreads) mark_up_kernel(const kr_bvh_node* no
             atomicOr(err, kErrCycle);
             return;
         }
-        if (arrive(visits + p) == 0) return;
+        // p's box and children and its parent are final before this kernel:
+        // read them ahead of the arrival
         const NodeView pn = load_node(nodes, p);
+        const uint32_t grand = __ldg(parents + p);
+        if (arrive(visits + p) == 0) return;
         const uint32_t count = __ldcg(counts + pn.left) + __ldcg(counts + pn.right);
         __stcg(counts + p, count);
         const float area = box_area(pn.lo, pn.hi);
@@ -80,7 +83,7 @@ __global__ void __launch_bounds__(kThreads) mark_up_kernel(const kr_bvh_node* no
         } else {
             __stcg(costs + p, node_cost);
         }
-        p = parents[p];
+        p = grand;
     }
 }
 

@@ -248,9 +248,13 @@ __global__ void __launch_bounds__(kThreads) aabb_up_kernel(kr_bvh_node* nodes, c
             atomicOr(err, kErrCycle);
             return;
         }
+        // p's children and its parent are final before this kernel: read them
+        // ahead of the arrival
+        const uint32_t* pw = reinterpret_cast<const uint32_t*>(nodes + p);
+        const uint32_t left = __ldg(pw + 6), right = __ldg(pw + 7);
+        const uint32_t grand = __ldg(parents + p);
         if (tree::arrive(visits + p) == 0) return;
-        const tree::NodeView pn = tree::load_node(nodes, p);
-        const tree::NodeView L = tree::load_node(nodes, pn.left), R = tree::load_node(nodes, pn.right);
+        const tree::NodeView L = tree::load_node(nodes, left), R = tree::load_node(nodes, right);
         float lo[3], hi[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {  // kr_aabb_expand(left, right)
@@ -263,9 +267,9 @@ __global__ void __launch_bounds__(kThreads) aabb_up_kernel(kr_bvh_node* nodes, c
             __stcg(w + k, __float_as_uint(lo[k]));
             __stcg(w + 3 + k, __float_as_uint(hi[k]));
         }
-        __stcg(counts + p, __ldcg(counts + pn.left) + __ldcg(counts + pn.right));
-        __stcg(costs + p, 1.2f * tree::box_area(lo, hi) + __ldcg(costs + pn.right) + __ldcg(costs + pn.left));
-        p = parents[p];
+        __stcg(counts + p, __ldcg(counts + left) + __ldcg(counts + right));
+        __stcg(costs + p, 1.2f * tree::box_area(lo, hi) + __ldcg(costs + right) + __ldcg(costs + left));
+        p = grand;
     }
 }
 

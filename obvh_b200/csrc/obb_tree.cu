@@ -41,7 +41,7 @@ namespace obbtree {
 using namespace tree;
 
 constexpr int kThreads = 256;
-constexpr uint32_t kThreadMax = 8;   // leaves handled by one thread per node
+constexpr uint32_t kThreadMax = 32;  // leaves handled by one thread per node
 constexpr uint32_t kUnit = 1024;    // leaves per warp unit
 constexpr uint32_t kUnitRun = 4;   // consecutive units per warp visit
 
@@ -92,9 +92,12 @@ __global__ void __launch_bounds__(kThreads) summary_up_kernel(const kr_bvh_node*
             atomicOr(err, kErrCycle);
             return;
         }
-        if (arrive(visits + p) == 0) return;
+        // p's children and its parent are final before this kernel: read them
+        // ahead of the arrival
         const uint32_t* w = reinterpret_cast<const uint32_t*>(nodes + p);
         const uint32_t L = __ldg(w + 6), R = __ldg(w + 7);
+        const uint32_t grand = __ldg(parents + p);
+        if (arrive(visits + p) == 0) return;
         const uint32_t other = (L == child) ? R : L;
         if ((L != child && R != child) || other >= internal + n) {
             atomicOr(err, kErrBadInput);
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(kThreads) summary_up_kernel(const kr_bvh_node*
         store_summary(summary + 7 * static_cast<size_t>(p), own);
         __stcg(counts + p, count_of(counts, L, internal) + count_of(counts, R, internal));
         child = p;
-        p = parents[p];
+        p = grand;
     }
 }
 
@@ -304,10 +307,12 @@ __global__ void __launch_bounds__(kThreads) extents_units_kernel(const Cand* can
                 hi[k] = warp_max(hi[k]);
             }
             if (units == 1) {
-                if (lane == 0)
-                    finalize_node(c, mk3(fminf(c.olo[0], lo[0]), fminf(c.olo[1], lo[1]), fminf(c.olo[2], lo[2])),
-                                  mk3(fmaxf(c.ohi[0], hi[0]), fmaxf(c.ohi[1], hi[1]), fmaxf(c.ohi[2], hi[2])), obbs + a,
-                                  xfs + a);
+                // the whole node in this unit: its extents go straight to the
+                // keys; finalize_multi_kernel builds the box, one thread per node
+                if (lane < 6) {
+                    const float v = lane < 3 ? fminf(c.olo[lane], lo[lane]) : fmaxf(c.ohi[lane - 3], hi[lane - 3]);
+                    __stcg(keys + 6 * static_cast<size_t>(a) + lane, f2key(v));
+                }
             } else if (lane < 6) {
                 const float v = lane < 3 ? lo[lane] : hi[lane - 3];
                 uint32_t* k = keys + 6 * static_cast<size_t>(a) + lane;
@@ -317,11 +322,13 @@ __global__ void __launch_bounds__(kThreads) extents_units_kernel(const Cand* can
     }
 }
 
+// Nodes handled in warp units: the box from the extents in the keys (one unit:
+// written by it; several: the atomic min/max over the units).
 __global__ void __launch_bounds__(kThreads) finalize_multi_kernel(const Cand* cand, const uint32_t* nunits,
                                                                   const uint32_t* keys, uint32_t internal,
                                                                   kr_obb3* obbs, kr_mat4* xfs, const uint32_t* err) {
     const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= internal || *err || nunits[a] <= 1) return;
+    if (a >= internal || *err || nunits[a] == 0) return;
     const uint32_t* k = keys + 6 * static_cast<size_t>(a);
     finalize_node(load_cand(cand, a), mk3(key2f(k[0]), key2f(k[1]), key2f(k[2])),
                   mk3(key2f(k[3]), key2f(k[4]), key2f(k[5])), obbs + a, xfs + a);

@@ -172,9 +172,13 @@ __global__ void __launch_bounds__(kThreads) fused_up_kernel(kr_bvh_node* nodes, 
             atomicOr(err, kErrCycle);
             return;
         }
-        if (arrive(visits + p) == 0) return;
+        // The parent's children and its own parent were written before this
+        // kernel: read them before the arrival so they are not on the
+        // dependent chain of the walk.
         const uint32_t* pw = reinterpret_cast<const uint32_t*>(nodes + p);
         const uint32_t L = __ldg(pw + 6), R = __ldg(pw + 7);
+        const uint32_t grand = __ldg(parents + p);
+        if (arrive(visits + p) == 0) return;
         const bool from_left = (L == child);
         const uint32_t other = from_left ? R : L;
         const NodeView sib = load_node(nodes, other);
@@ -239,7 +243,7 @@ __global__ void __launch_bounds__(kThreads) fused_up_kernel(kr_bvh_node* nodes, 
             store_summary(summary + 7 * static_cast<size_t>(p), own);
         }
         child = p;
-        p = parents[p];
+        p = grand;
     }
 }
 

@@ -295,17 +295,19 @@ __device__ __forceinline__ void extent_proj(const Points14& Q, f3 d, float& lo, 
     }
 }
 
-__device__ __forceinline__ void score_frames(const Points14& P, f3 n, f3 e0, f3 e1, f3 e2, f3* b, f3& blen,
-                                             f3& bmid, float& best) {
-    const f3 e[3] = {e0, e1, e2};
+// One candidate frame: normal n and its three edges, whose extents (elo/ehi)
+// are computed once per node (an edge is shared by up to three frames).
+__device__ __forceinline__ void score_frames(const Points14& P, f3 n, const f3* E, const float* ELO, const float* EHI,
+                                             const int* ids, f3* b, f3& blen, f3& bmid, float& best) {
     float nlo, nhi;
     extent_proj(P, n, nlo, nhi);
     const float dy = nhi - nlo;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const f3 m = cross3(e[k], n);
-        float elo, ehi, mlo, mhi;
-        extent_proj(P, e[k], elo, ehi);
+        const f3 e = E[ids[k]];
+        const f3 m = cross3(e, n);
+        const float elo = ELO[ids[k]], ehi = EHI[ids[k]];
+        float mlo, mhi;
         extent_proj(P, m, mlo, mhi);
         const f3 dlen = mk3(ehi - elo, dy, mhi - mlo);
         const float q = half_area3(dlen);
@@ -313,7 +315,7 @@ __device__ __forceinline__ void score_frames(const Points14& P, f3 n, f3 e0, f3 
             best = q;
             bmid = mk3(ehi, nhi, mhi);
             blen = mk3(elo, nlo, mlo);
-            b[0] = e[k]; b[1] = n; b[2] = m;
+            b[0] = e; b[1] = n; b[2] = m;
         }
     }
 }
@@ -375,24 +377,36 @@ __device__ inline Candidate node_candidate(const f3* P, const Summary& s) {
     // so the test can come first and all frames go through one scorer loop
     // in the reference's order: base triangle, upper faces, lower faces.
     if (!up && !down) return stale;
-    f3 tn[7], te[7][3];
+    // Edge table: base triangle e0..e2, upper faces f0..f2, lower faces g0..g2.
+    f3 E[9];
+    float ELO[9], EHI[9];
+    E[0] = e0; E[1] = e1; E[2] = e2;
+    f3 tn[7];
+    int ids[7][3];
     int nt = 0;
-    tn[nt] = n; te[nt][0] = e0; te[nt][1] = e1; te[nt][2] = e2; ++nt;
+    tn[nt] = n; ids[nt][0] = 0; ids[nt][1] = 1; ids[nt][2] = 2; ++nt;
     if (up) {
         const f3 f0 = unit3(sub3(q0, p0)), f1 = unit3(sub3(q0, p1)), f2 = unit3(sub3(q0, p2));
-        tn[nt] = unit3(cross3(f1, e0)); te[nt][0] = e0; te[nt][1] = f1; te[nt][2] = f0; ++nt;
-        tn[nt] = unit3(cross3(f2, e1)); te[nt][0] = e1; te[nt][1] = f2; te[nt][2] = f1; ++nt;
-        tn[nt] = unit3(cross3(f0, e2)); te[nt][0] = e2; te[nt][1] = f0; te[nt][2] = f2; ++nt;
+        E[3] = f0; E[4] = f1; E[5] = f2;
+        tn[nt] = unit3(cross3(f1, e0)); ids[nt][0] = 0; ids[nt][1] = 4; ids[nt][2] = 3; ++nt;
+        tn[nt] = unit3(cross3(f2, e1)); ids[nt][0] = 1; ids[nt][1] = 5; ids[nt][2] = 4; ++nt;
+        tn[nt] = unit3(cross3(f0, e2)); ids[nt][0] = 2; ids[nt][1] = 3; ids[nt][2] = 5; ++nt;
     }
     if (down) {
         const f3 g0 = unit3(sub3(q1, p0)), g1 = unit3(sub3(q1, p1)), g2 = unit3(sub3(q1, p2));
-        tn[nt] = unit3(cross3(g1, e0)); te[nt][0] = e0; te[nt][1] = g1; te[nt][2] = g0; ++nt;
-        tn[nt] = unit3(cross3(g2, e1)); te[nt][0] = e1; te[nt][1] = g2; te[nt][2] = g1; ++nt;
-        tn[nt] = unit3(cross3(g0, e2)); te[nt][0] = e2; te[nt][1] = g0; te[nt][2] = g2; ++nt;
+        E[6] = g0; E[7] = g1; E[8] = g2;
+        tn[nt] = unit3(cross3(g1, e0)); ids[nt][0] = 0; ids[nt][1] = 7; ids[nt][2] = 6; ++nt;
+        tn[nt] = unit3(cross3(g2, e1)); ids[nt][0] = 1; ids[nt][1] = 8; ids[nt][2] = 7; ++nt;
+        tn[nt] = unit3(cross3(g0, e2)); ids[nt][0] = 2; ids[nt][1] = 6; ids[nt][2] = 8; ++nt;
     }
     const Points14 Q = pack14(P);
 #pragma unroll 1
-    for (int t = 0; t < nt; ++t) score_frames(Q, tn[t], te[t][0], te[t][1], te[t][2], b, blen, bmid, best);
+    for (int k = 0; k < 9; ++k) {
+        if ((k >= 3 && k < 6 && !up) || (k >= 6 && !down)) continue;
+        extent_proj(Q, E[k], ELO[k], EHI[k]);
+    }
+#pragma unroll 1
+    for (int t = 0; t < nt; ++t) score_frames(Q, tn[t], E, ELO, EHI, ids[t], b, blen, bmid, best);
     c.b0 = b[0]; c.b1 = b[1]; c.b2 = b[2];
     c.lo = blen;
     c.hi = bmid;
