@@ -233,21 +233,36 @@ __global__ void __launch_bounds__(kThreads) boxes_up_kernel(const kr_vec3* verts
 // ---------------------------------------------------------------------------
 // Treelet optimisation.
 
-struct WarpSmem {
+// Per-treelet shared state (one per segment of a warp).
+struct SegSmem {
     int32_t internal[32];
     int32_t leaves[32];
     float areas[32];
     float dist[kMaxDist];
 };
 
-// The reference's shuffle-down reductions (Treelet.cuh:21-37 keeps the larger
-// area, AgglomerativeTreelet.cu:59-74 the smaller distance; strict, so on a tie
-// the lane's own value stays).  Uniform across the warp.
-__device__ __forceinline__ void reduce_down(int count, int& idx, float& val, bool want_max) {
+// A treelet of tau <= W leaves is processed by a segment of W lanes (W = 8,
+// 16 or 32), so a warp works on 32 / W treelets at once.  The reference uses a
+// whole warp per treelet; its two reductions are replayed exactly:
+//   - the leaf to expand (Treelet.cuh:21-37): a shuffle-down over the first
+//     2 + it <= tau lanes, larger area wins, ties keep the lane's own value;
+//     within W lanes every shuffle source that matters exists, and a source
+//     past the segment returns the lane's own value, which never wins, as the
+//     reference's lanes past the count (area -FLT_MAX) do not;
+//   - the pair to merge (AgglomerativeTreelet.cu:59-90): 32 "virtual lanes"
+//     v scan the distance entries v, v + 32, ...; lane sl of the segment holds
+//     the virtual lanes sl + W q.  Shuffle steps of 16 and 8 that stay inside
+//     one physical lane (W <= 16) are folds of its own virtual lanes; the rest
+//     are segment-wide shuffles.  Same pairs, same order, same strict '<'.
+template <int W>
+__device__ __forceinline__ int seg_lane() { return threadIdx.x & (W - 1); }
+
+template <int W>
+__device__ __forceinline__ void reduce_down_seg(int count, int& idx, float& val, bool want_max) {
     int amount = count / 2;
     while (count > 1) {
-        const int oi = __shfl_down_sync(0xffffffffu, idx, amount);
-        const float ov = __shfl_down_sync(0xffffffffu, val, amount);
+        const int oi = __shfl_down_sync(0xffffffffu, idx, amount, W);
+        const float ov = __shfl_down_sync(0xffffffffu, val, amount, W);
         if (want_max ? (ov > val) : (ov < val)) {
             val = ov;
             idx = oi;
@@ -255,6 +270,49 @@ __device__ __forceinline__ void reduce_down(int count, int& idx, float& val, boo
         count = (count + 1) / 2;
         amount = count / 2;
     }
+}
+
+// findMinimumDistance over `size` entries, the reference's 32-lane tree.
+template <int W>
+__device__ __forceinline__ int min_distance_seg(const float* dist, int size) {
+    constexpr int Q = 32 / W;
+    const int sl = seg_lane<W>();
+    float val[Q];
+    int idx[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        val[q] = FLT_MAX;
+        idx[q] = 0;
+        for (int j = sl + W * q; j < size; j += 32) {
+            const float d = dist[j];
+            if (d < val[q]) {
+                val[q] = d;
+                idx[q] = j;
+            }
+        }
+    }
+#pragma unroll
+    for (int amount = 16; amount >= W && amount >= 1; amount >>= 1) {
+        const int step = amount / W;  // virtual lanes v and v + amount share this physical lane
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (q + step < Q && val[q + step] < val[q]) {
+                val[q] = val[q + step];
+                idx[q] = idx[q + step];
+            }
+    }
+    int i0 = idx[0];
+    float v0 = val[0];
+#pragma unroll
+    for (int amount = W / 2; amount >= 1; amount >>= 1) {
+        const int oi = __shfl_down_sync(0xffffffffu, i0, amount, W);
+        const float ov = __shfl_down_sync(0xffffffffu, v0, amount, W);
+        if (ov < v0) {
+            v0 = ov;
+            i0 = oi;
+        }
+    }
+    return __shfl_sync(0xffffffffu, i0, 0, W);
 }
 
 __device__ __forceinline__ int trm_index(int row, int col) { return ((row - 1) * row) / 2 + col; }
@@ -266,24 +324,30 @@ __device__ __forceinline__ int trm_col(int index) {
     return index - (y * (y - 1)) / 2;
 }
 
+template <int W>
 __device__ __forceinline__ void shfl_box(const float* lo, const float* hi, int src, float* olo, float* ohi) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        olo[k] = __shfl_sync(0xffffffffu, lo[k], src);
-        ohi[k] = __shfl_sync(0xffffffffu, hi[k], src);
+        olo[k] = __shfl_sync(0xffffffffu, lo[k], src, W);
+        ohi[k] = __shfl_sync(0xffffffffu, hi[k], src, W);
     }
 }
 
-// The treelet rooted at `root`, by the whole warp.  False on a malformed tree.
-__device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, float ci, int32_t root, WarpSmem& w) {
-    const int lane = threadIdx.x & 31;
+// The treelet rooted at `root`, by a segment of W lanes.  Every lane of the
+// warp calls this together (the shuffles span the warp); a segment with
+// `active` false computes nothing that is stored.  Returns false (for the
+// segment) on a malformed tree.
+template <int W>
+__device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, float ci, int32_t root, bool active,
+                                SegSmem& w) {
+    const int sl = seg_lane<W>();
     const int32_t internal_count = n - 1;
-
     const int32_t node_count = 2 * n - 1;
     auto valid = [&](int32_t x) { return x >= 0 && x < node_count; };
+
     // formTreelet: grow by the frontier node of largest area (Treelet.cuh:55-129)
-    int bad = 0;
-    if (lane == 0) {
+    int bad = active ? 0 : 1;
+    if (sl == 0 && active) {
         const int32_t L = __ldcg(&t[root].left), R = __ldcg(&t[root].right);
         if (!valid(L) || !valid(R)) {
             bad = 1;
@@ -295,19 +359,19 @@ __device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, fl
             w.areas[1] = __ldcg(&t[R].area);
         }
     }
-    if (__shfl_sync(0xffffffffu, bad, 0)) return false;
+    bad = __shfl_sync(0xffffffffu, bad, 0, W);
     __syncwarp();
     for (int it = 0; it < tau - 2; ++it) {
         int idx = -1;
         float a = -FLT_MAX;
-        if (lane < 2 + it) {
-            idx = lane;
-            a = w.areas[lane];
-            if (w.leaves[lane] >= internal_count) a = -FLT_MAX;
+        if (!bad && sl < 2 + it) {
+            idx = sl;
+            a = w.areas[sl];
+            if (w.leaves[sl] >= internal_count) a = -FLT_MAX;
         }
-        reduce_down(2 + it, idx, a, true);
+        reduce_down_seg<W>(2 + it, idx, a, true);
         __syncwarp();
-        if (lane == 0) {
+        if (sl == 0 && !bad) {
             const int32_t rep = idx >= 0 ? w.leaves[idx] : -1;
             const bool internal_node = rep >= 0 && rep < internal_count;
             const int32_t L = internal_node ? __ldcg(&t[rep].left) : -1;
@@ -322,75 +386,62 @@ __device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, fl
                 w.areas[it + 2] = __ldcg(&t[R].area);
             }
         }
-        bad = __shfl_sync(0xffffffffu, bad, 0);
+        bad = __shfl_sync(0xffffffffu, bad, 0, W);
         __syncwarp();
-        if (bad) return false;
     }
 
-    // Lane l < tau holds treelet leaf l: its node, SAH and box.
+    // Lane sl < tau holds treelet leaf sl: its node, SAH and box.
     int32_t node = -1;
     float sah = 0.f, lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
-    if (lane < tau) {
-        node = w.leaves[lane];
+    if (!bad && sl < tau) {
+        node = w.leaves[sl];
         sah = __ldcg(sah_arr + node);
         load_box(t, node, lo, hi);
     }
     const int nd = (tau - 1) * tau / 2;
-    for (int k0 = 0; k0 < nd; k0 += 32) {  // every pair row > col
-        const int k = k0 + lane;
+    for (int k0 = 0; k0 < nd; k0 += W) {  // every pair row > col
+        const int k = k0 + sl;
         const int r = k < nd ? trm_row(k) : 0, c = k < nd ? trm_col(k) : 0;
         float rlo[3], rhi[3], clo[3], chi[3];
-        shfl_box(lo, hi, r, rlo, rhi);
-        shfl_box(lo, hi, c, clo, chi);
+        shfl_box<W>(lo, hi, r, rlo, rhi);
+        shfl_box<W>(lo, hi, c, clo, chi);
         if (k < nd) w.dist[k] = union_area(rlo, rhi, clo, chi);
     }
     __syncwarp();
 
     for (int last = tau - 1; last > 0; --last) {
-        // pair of smallest union area (findMinimumDistance)
-        const int size = last * (1 + last) / 2;
-        int mi = 0;
-        float md = FLT_MAX;
-        for (int j = lane; j < size; j += 32) {
-            const float d = w.dist[j];
-            if (d < md) {
-                md = d;
-                mi = j;
-            }
-        }
-        reduce_down(32, mi, md, false);
-        mi = __shfl_sync(0xffffffffu, mi, 0);
+        const int mi = min_distance_seg<W>(w.dist, last * (1 + last) / 2);
         const int jr = trm_row(mi), jc = trm_col(mi);
 
         // updateState (AgglomerativeTreelet.cu:92-147)
-        const float s = __shfl_sync(0xffffffffu, sah, jr) + __shfl_sync(0xffffffffu, sah, jc);
-        const int32_t li = __shfl_sync(0xffffffffu, node, jr), ri = __shfl_sync(0xffffffffu, node, jc);
+        const float s = __shfl_sync(0xffffffffu, sah, jr, W) + __shfl_sync(0xffffffffu, sah, jc, W);
+        const int32_t li = __shfl_sync(0xffffffffu, node, jr, W), ri = __shfl_sync(0xffffffffu, node, jc, W);
         float alo[3], ahi[3], blo[3], bhi[3];
-        shfl_box(lo, hi, jr, alo, ahi);
-        shfl_box(lo, hi, jc, blo, bhi);
+        shfl_box<W>(lo, hi, jr, alo, ahi);
+        shfl_box<W>(lo, hi, jc, blo, bhi);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             alo[k] = fminf(blo[k], alo[k]);
             ahi[k] = fmaxf(bhi[k], ahi[k]);
         }
-        if (lane == jc) {
+        if (sl == jc) {
             node = w.internal[last - 1];
 #pragma unroll
             for (int k = 0; k < 3; ++k) { lo[k] = alo[k]; hi[k] = ahi[k]; }
             w.areas[last] = s + ci * box_area(alo, ahi);
             sah = w.areas[last];
         }
-        const int32_t last_node = __shfl_sync(0xffffffffu, node, last);
-        const float last_sah = __shfl_sync(0xffffffffu, sah, last);
+        const int32_t last_node = __shfl_sync(0xffffffffu, node, last, W);
+        const float last_sah = __shfl_sync(0xffffffffu, sah, last, W);
         float llo[3], lhi[3];
-        shfl_box(lo, hi, last, llo, lhi);
-        if (lane == jr) {
+        shfl_box<W>(lo, hi, last, llo, lhi);
+        if (sl == jr) {
             node = last_node;
             sah = last_sah;
 #pragma unroll
             for (int k = 0; k < 3; ++k) { lo[k] = llo[k]; hi[k] = lhi[k]; }
         }
-        if (lane == last) {
+        if (sl == last) {
             node = li;
             w.leaves[last] = ri;
 #pragma unroll
@@ -402,22 +453,22 @@ __device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, fl
         if (last > 1) {
             float cp = 0.f;
             int dst = -1;
-            if (lane < last && lane != jr) {
-                cp = w.dist[trm_index(last, lane)];
-                dst = trm_index(max(jr, lane), min(jr, lane));
+            if (sl < last && sl != jr) {
+                cp = w.dist[trm_index(last, sl)];
+                dst = trm_index(max(jr, sl), min(jr, sl));
             }
             __syncwarp();
             if (dst >= 0) w.dist[dst] = cp;
             __syncwarp();
-            int dr = lane, dc = lane;
-            const bool upd = lane < last && lane != jc;
+            int dr = sl, dc = sl;
+            const bool upd = sl < last && sl != jc;
             if (upd) {
-                dr = max(jc, lane);
-                dc = min(jc, lane);
+                dr = max(jc, sl);
+                dc = min(jc, sl);
             }
             float rlo[3], rhi[3], clo[3], chi[3];
-            shfl_box(lo, hi, dr, rlo, rhi);
-            shfl_box(lo, hi, dc, clo, chi);
+            shfl_box<W>(lo, hi, dr, rlo, rhi);
+            shfl_box<W>(lo, hi, dc, clo, chi);
             const float d = union_area(rlo, rhi, clo, chi);
             if (upd) w.dist[trm_index(dr, dc)] = d;
             __syncwarp();
@@ -425,28 +476,31 @@ __device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, fl
     }
 
     // updateTreelet: keep the new topology if its SAH is lower
-    const bool better = w.areas[1] < __ldcg(sah_arr + w.internal[0]);
-    if (better && lane >= 1 && lane < tau) {
-        const int32_t ni = w.internal[lane - 1];
-        const int32_t right = w.leaves[lane];
+    const bool better = !bad && w.areas[1] < __ldcg(sah_arr + w.internal[0]);
+    if (better && sl >= 1 && sl < tau) {
+        const int32_t ni = w.internal[sl - 1];
+        const int32_t right = w.leaves[sl];
         __stcg(&t[ni].left, node);
         __stcg(&t[ni].right, right);
         __stcg(&t[node].parent, ni);
         __stcg(&t[right].parent, ni);
-        __stcg(sah_arr + ni, w.areas[lane]);
+        __stcg(sah_arr + ni, w.areas[sl]);
         store_box(t, ni, lo, hi);
     }
     __threadfence();
     __syncwarp();
-    return true;
+    return !(active && bad);
 }
 
+template <int W>
 __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, float* sah_arr, int32_t* tris,
                                                                   uint32_t* counters, int32_t n, int tau,
                                                                   int32_t gamma, float ci, float ct, uint32_t* err) {
-    __shared__ WarpSmem smem[kTreeletWarps];
-    WarpSmem& w = smem[threadIdx.x >> 5];
+    constexpr int S = 32 / W;  // segments (treelets in flight) per warp
+    __shared__ SegSmem smem[kTreeletWarps * S];
     const int lane = threadIdx.x & 31;
+    const int seg = lane / W;
+    SegSmem& w = smem[(threadIdx.x >> 5) * S + seg];
     const int32_t i = static_cast<int32_t>(blockIdx.x * blockDim.x + threadIdx.x);
     const int32_t internal = n - 1;
     int32_t cur = -1;
@@ -485,10 +539,17 @@ __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, floa
         }
         uint32_t vote = __ballot_sync(0xffffffffu, count >= gamma);
         while (vote != 0) {
-            const int src = __ffs(vote) - 1;
-            const int32_t root = __shfl_sync(0xffffffffu, cur, src);
-            if (!process_treelet(t, sah_arr, n, tau, ci, root, w) && lane == 0) atomicOr(err, kErrBadInput);
-            vote &= vote - 1;
+            // the next S treelet roots of the warp, lowest lanes first, one per segment
+            int src = -1;
+#pragma unroll
+            for (int q = 0; q < S; ++q) {
+                const int b = vote ? __ffs(vote) - 1 : -1;
+                if (q == seg) src = b;
+                vote = vote ? (vote & (vote - 1)) : 0u;
+            }
+            const int32_t root = __shfl_sync(0xffffffffu, cur, src < 0 ? 0 : src);
+            if (!process_treelet<W>(t, sah_arr, n, tau, ci, root, src >= 0, w) && (lane & (W - 1)) == 0)
+                atomicOr(err, kErrBadInput);
         }
         if (cur >= 0) cur = __ldcg(&t[cur].parent);
     }
@@ -612,9 +673,16 @@ kr_error enqueue_tree(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, u
         OBVH_TRY_CUDA(cudaMemsetAsync(counters, 0, 4ull * internal, s));
         {
             ProfScope prof_scope_("treelet_kernel", s);
-            treelet_kernel<<<grid_t, kTreeletThreads, 0, s>>>(
-                t, reinterpret_cast<float*>(ws + L.sah), reinterpret_cast<int32_t*>(ws + L.tris), counters,
-                static_cast<int32_t>(n), static_cast<int>(tau), gamma, ci, ct, err);
+            float* sah = reinterpret_cast<float*>(ws + L.sah);
+            int32_t* tris = reinterpret_cast<int32_t*>(ws + L.tris);
+            const int32_t nn = static_cast<int32_t>(n);
+            const int tt = static_cast<int>(tau);
+            if (tau <= 8)
+                treelet_kernel<8><<<grid_t, kTreeletThreads, 0, s>>>(t, sah, tris, counters, nn, tt, gamma, ci, ct, err);
+            else if (tau <= 16)
+                treelet_kernel<16><<<grid_t, kTreeletThreads, 0, s>>>(t, sah, tris, counters, nn, tt, gamma, ci, ct, err);
+            else
+                treelet_kernel<32><<<grid_t, kTreeletThreads, 0, s>>>(t, sah, tris, counters, nn, tt, gamma, ci, ct, err);
         }
         OBVH_TRY_CUDA(cudaGetLastError());
         gamma = gamma > (1 << 29) ? gamma : 2 * gamma;
