@@ -33,7 +33,8 @@ typedef struct obvh_dito_batch_tuning {
     kr_u32 chunk_points;      /* points per task of a large set (>= 1024) */
     kr_u32 warp_max_points;   /* sets up to this size are fitted by one warp */
     kr_u32 cta_max_points;    /* sets up to this size by one CTA; larger ones in chunks */
-    kr_u32 lag_tasks;         /* tasks between a large set's pass 1 and pass 2 (0: 2 per CTA) */
+    kr_u32 lag_tasks;         /* 0: the CTA completing a large set's pass 1 runs its pass 2 (from L2);
+                                 n > 0: pass 2 in chunk tasks queued n tasks after the set's pass 1 */
     kr_u32 ctas_per_sm;       /* 1 or 2 */
 } obvh_dito_batch_tuning;
 

@@ -65,6 +65,7 @@ struct Params {
     const uint2* chunks;        // per large set: first record, chunk count
     uint32_t ntasks;
     uint32_t flags;
+    uint32_t finisher;          // 1: the CTA completing a large set's pass 1 runs its pass 2
     kr_obb3* out;               // [sets]
     uint32_t* ctl;              // [0] queue head, [1] error, then per large set 2 tickets + release word
     Ctl* large;                 // per large set: candidate frame and plan
@@ -413,6 +414,29 @@ __device__ void chunk_pass1(const Params& p, uint32_t s, uint32_t c, uint32_t b,
         }
     }
     __syncthreads();
+    if (p.finisher) {
+        // This CTA also runs pass 2 over the whole set: its chunks were read
+        // moments ago by the CTAs that took them, so it comes from L2.
+        if (warp == 0)
+            candidate_from_lanes(v, lane < 14 ? sh.val[lane] : 0.f, lane < 14 ? sh.idx[lane] : kNoIndex, p.flags,
+                                 &sh.ctl, p.out + s, error_word(p));
+        __syncthreads();
+        if (sh.ctl.plan == 0) return;
+        Extents e2;
+        e2.init(sh.ctl.axes);
+        scan_extents<U>(v, 0, v.groups, tid, kThreads, e2);
+        if (static_cast<uint32_t>(tid) < v.head) {
+            const float* q = v.base + 3 * tid;
+            e2.point(q[0], q[1], q[2]);
+        }
+        if (static_cast<uint32_t>(tid) < v.n - v.tail0()) {
+            const float* q = v.base + 3 * static_cast<uint64_t>(v.tail0() + tid);
+            e2.point(q[0], q[1], q[2]);
+        }
+        cta_reduce_extents(e2, sh);
+        if (tid == 0) finalize_extents(&sh.ctl, sh.glohi, p.flags, p.out + s);
+        return;
+    }
     if (warp == 0) {
         Ctl* ctl = p.large + b;
         candidate_from_lanes(v, lane < 14 ? sh.val[lane] : 0.f, lane < 14 ? sh.idx[lane] : kNoIndex, p.flags, ctl,
@@ -554,11 +578,13 @@ struct Batch {
 
 obvh_dito_batch_tuning default_tuning() {
     obvh_dito_batch_tuning t;
-    t.points_per_thread = 8;
-    t.chunk_points = 16384;
-    t.warp_max_points = 1024;
-    t.cta_max_points = 16384;
-    t.lag_tasks = 0;
+    // measured best among the robust settings (sets of any size) on Gaussian
+    // clouds of 64..262,144 points; obvh_dito_batch_autotune refines per batch
+    t.points_per_thread = 16;
+    t.chunk_points = 65536;
+    t.warp_max_points = 4096;
+    t.cta_max_points = 65536;
+    t.lag_tasks = 0;  // pass 2 of a large set by the CTA completing its pass 1
     t.ctas_per_sm = 2;
     return t;
 }
@@ -595,7 +621,9 @@ kr_error plan(Batch& B, cudaStream_t s = nullptr, bool sync = true) {
 
     const DeviceInfo& info = device_info();
     B.grid = static_cast<int>(t.ctas_per_sm) * info.sm_count;
-    const uint32_t lag = t.lag_tasks ? t.lag_tasks : 2u * static_cast<uint32_t>(B.grid);
+    // lag 0: no pass-2 tasks, the CTA completing a set's pass 1 runs its pass 2
+    const bool finisher = t.lag_tasks == 0;
+    const uint32_t lag = t.lag_tasks;
 
     B.tasks.clear();
     B.warp_sets.clear();
@@ -628,7 +656,7 @@ kr_error plan(Batch& B, cudaStream_t s = nullptr, bool sync = true) {
     for (uint32_t b = 0; b < B.nlarge; ++b) {
         for (uint32_t c = 0; c < B.chunks[b].y; ++c) {
             B.tasks.push_back(make_uint4(kPass1, large_ids[b], c, b));
-            if (c + 1 == B.chunks[b].y) pending.push_back({B.tasks.size() + lag, b});
+            if (c + 1 == B.chunks[b].y && !finisher) pending.push_back({B.tasks.size() + lag, b});
             // release the pass-2 chunks of sets whose lag has passed
             while (next_pending < pending.size() && pending[next_pending].due <= B.tasks.size()) {
                 const uint32_t bb = pending[next_pending].b;
@@ -711,6 +739,7 @@ kr_error enqueue(Batch& B, const kr_vec3* d_points, kr_obb3* d_obbs, cudaStream_
     prm.chunks = reinterpret_cast<const uint2*>(d + B.off_chunks);
     prm.ntasks = static_cast<uint32_t>(B.tasks.size());
     prm.flags = B.flags;
+    prm.finisher = B.tuning.lag_tasks == 0 ? 1u : 0u;
     prm.out = d_obbs;
     prm.ctl = reinterpret_cast<uint32_t*>(d + B.off_ctl);
     prm.large = reinterpret_cast<Ctl*>(d + B.off_large);
@@ -969,7 +998,7 @@ kr_error autotune(Batch& B, const kr_vec3* d_points, kr_obb3* d_obbs, cudaStream
             auto t = best; t.cta_max_points = v; OBVH_TRY(trial(t));
         }
         for (uint32_t v : {256u, 512u, 1024u, 2048u, 4096u}) { auto t = best; t.warp_max_points = v; OBVH_TRY(trial(t)); }
-        for (uint32_t v : {grid / 2, grid, 2 * grid, 4 * grid}) { auto t = best; t.lag_tasks = v; OBVH_TRY(trial(t)); }
+        for (uint32_t v : {0u, grid, 2 * grid, 4 * grid}) { auto t = best; t.lag_tasks = v; OBVH_TRY(trial(t)); }
     }
     B.tuning = best;
     OBVH_TRY(plan(B));

@@ -25,6 +25,9 @@ TUNINGS = {
                        lag_tasks=1, ctas_per_sm=2),
     "chunks_no_lag": dict(points_per_thread=4, chunk_points=1024, warp_max_points=16, cta_max_points=2048,
                           lag_tasks=1, ctas_per_sm=1),
+    # pass 2 of a chunked set by the CTA that completes its pass 1
+    "chunks_finisher": dict(points_per_thread=8, chunk_points=1024, warp_max_points=0, cta_max_points=0,
+                            lag_tasks=0, ctas_per_sm=2),
 }
 
 
