@@ -248,8 +248,8 @@ def tree_bytes_per_launch(n):
     return {
         "tri_bounds_kernel": 52 * n + 24 * n,          # face + 3 vertices in, triangle box out
         "morton_kernel": 24 * n + 8 * n,               # box in, key + index out
-        "radix_hist": 4 * n,                           # keys in
-        "radix_scatter": 16 * n,                       # key + value in and out
+        "radix_digit_counts": 4 * n,                   # keys in (every pass's digits at once)
+        "radix_onesweep": 16 * n,                      # key + value in and out (u32 keys)
         "leaves_kernel": 4 * n + 24 * n + 36 * n,      # order, box in; leaf node out
         "karras_kernel": 4 * n + 36 * ni + 8 * ni,     # codes in; internal nodes + parents out
         "aabb_up_kernel": 36 * nn + 8 * nn + 32 * ni,  # nodes in; counts, costs, bounds out

@@ -653,7 +653,7 @@ kr_error enqueue_tree(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, u
     OBVH_TRY_CUDA(cudaGetLastError());
     bool alt = false;
     OBVH_TRY(radix_sort_pairs(ws + L.keys0, ws + L.keys1, reinterpret_cast<uint32_t*>(ws + L.vals0),
-                              reinterpret_cast<uint32_t*>(ws + L.vals1), n, 8, 0, 63, ws + L.sort, s, &alt));
+                              reinterpret_cast<uint32_t*>(ws + L.vals1), n, 8, 0, 63, ws + L.sort, s, &alt, err));
     const uint64_t* keys = reinterpret_cast<const uint64_t*>(ws + (alt ? L.keys1 : L.keys0));
     const uint32_t* order = reinterpret_cast<const uint32_t*>(ws + (alt ? L.vals1 : L.vals0));
     {

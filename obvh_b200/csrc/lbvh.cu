@@ -333,7 +333,8 @@ kr_error enqueue_codes(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, 
     OBVH_TRY_CUDA(cudaGetLastError());
     bool alt = false;
     OBVH_TRY(radix_sort_pairs(ws + L.keys0, ws + L.keys1, reinterpret_cast<uint32_t*>(ws + L.vals0),
-                              reinterpret_cast<uint32_t*>(ws + L.vals1), n, 4, 0, 30, ws + L.sort, s, &alt));
+                              reinterpret_cast<uint32_t*>(ws + L.vals1), n, 4, 0, 30, ws + L.sort, s, &alt,
+                              &reinterpret_cast<Ctl*>(ws + L.ctl)->error));
     out->codes = reinterpret_cast<const uint32_t*>(ws + (alt ? L.keys1 : L.keys0));
     out->order = reinterpret_cast<const uint32_t*>(ws + (alt ? L.vals1 : L.vals0));
     out->tri_boxes = tri;

@@ -181,7 +181,15 @@ __global__ void __launch_bounds__(kThreads) fused_up_kernel(kr_bvh_node* nodes, 
         if (arrive(visits + p) == 0) return;
         const bool from_left = (L == child);
         const uint32_t other = from_left ? R : L;
-        const NodeView sib = load_node(nodes, other);
+        NodeView sib;  // the sibling's bounds only
+        {
+            const uint32_t* sw = reinterpret_cast<const uint32_t*>(nodes + other);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                sib.lo[k] = __uint_as_float(__ldcg(sw + k));
+                sib.hi[k] = __uint_as_float(__ldcg(sw + 3 + k));
+            }
+        }
         const uint32_t scount = __ldcg(counts + other);
         const float scost = __ldcg(costs + other);
         // left/right views of the two children
@@ -216,10 +224,10 @@ __global__ void __launch_bounds__(kThreads) fused_up_kernel(kr_bvh_node* nodes, 
                 flags[p] = 1;
                 flags[L] = 1;
                 flags[R] = 1;
-                uint32_t* lw = reinterpret_cast<uint32_t*>(collapsed + L) + 8;
-                uint32_t* rw = reinterpret_cast<uint32_t*>(collapsed + R) + 8;
-                __stcg(lw, (__ldcg(lw) & 0xffff0000u) | kHidden);
-                __stcg(rw, (__ldcg(rw) & 0xffff0000u) | kHidden);
+                // nPrimitives = 0xFFFF; the axis byte and the pad of every node
+                // record are zero here, so the whole word is written
+                __stcg(reinterpret_cast<uint32_t*>(collapsed + L) + 8, kHidden);
+                __stcg(reinterpret_cast<uint32_t*>(collapsed + R) + 8, kHidden);
             } else {
                 cost = node_cost;
             }

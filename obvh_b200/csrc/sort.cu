@@ -96,42 +96,106 @@ constexpr int kRounds = 16;                       // keys per lane
 constexpr int kSortTile = kSortThreads * kRounds;  // 4096 keys per CTA
 constexpr int kRadix = 256;
 
+// ---------------------------------------------------------------------------
+// Stable LSD radix sort, one sweep per 8-bit digit (the single-pass scheme of
+// decoupled look-back): one kernel first counts every pass's digits over all
+// keys (order does not matter for global counts); then each pass is one
+// kernel whose CTAs take tiles from an atomic counter, rank their keys inside
+// the tile (stable: warps in order, lanes in order), publish their per-digit
+// counts, and add up the counts of the tiles before them from those tiles'
+// published words ("aggregate" = this tile's own count, "prefix" = inclusive
+// of all tiles before it).  A tile only waits on tiles taken before it, by
+// CTAs that are running, so the waits end; each is also bounded by the
+// global timer and reports a timeout in the error word.
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPre = 2u << 30;
+constexpr uint32_t kFlagMask = 3u << 30;
+constexpr uint32_t kCountMask = kFlagAgg - 1;
+constexpr int kMaxPasses = 8;
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* a) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(uint32_t* a, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(a), "r"(v) : "memory");
+}
+
+// Sort workspace: [0, 8 KB) digit counts then exclusive digit offsets per
+// pass, [8 KB, 8 KB + 64) tile counters and the error word, then the
+// per-pass tile status words.
+struct SortTemp {
+    uint32_t* digits;   // [kMaxPasses][kRadix]
+    uint32_t* tiles;    // [kMaxPasses] tile counters, [kMaxPasses] error word
+    uint32_t* err;
+    uint32_t* status;   // [passes][ntiles][kRadix]
+};
+constexpr size_t kSortHeader = kMaxPasses * kRadix * 4 + 256;
+
+__host__ __device__ inline SortTemp sort_temp(void* temp) {
+    SortTemp t;
+    char* c = static_cast<char*>(temp);
+    t.digits = reinterpret_cast<uint32_t*>(c);
+    t.tiles = reinterpret_cast<uint32_t*>(c + kMaxPasses * kRadix * 4);
+    t.err = t.tiles + kMaxPasses;
+    t.status = reinterpret_cast<uint32_t*>(c + kSortHeader);
+    return t;
+}
+
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads) radix_hist(const K* keys, uint64_t n, int shift, uint32_t* counts,
-                                                           uint32_t ntiles) {
-    __shared__ uint32_t h[kRadix];
-    h[threadIdx.x] = 0;
+__global__ void __launch_bounds__(kSortThreads) radix_digit_counts(const K* keys, uint64_t n, int begin_bit,
+                                                                   int passes, uint32_t* digits) {
+    __shared__ uint32_t h[kMaxPasses][kRadix];
+    for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += kSortThreads) (&h[0][0])[i] = 0;
     __syncthreads();
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile;
-#pragma unroll 4
-    for (int i = threadIdx.x; i < kSortTile; i += kSortThreads) {
-        const uint64_t idx = base + i;
-        if (idx < n) atomicAdd(&h[static_cast<uint32_t>(keys[idx] >> shift) & (kRadix - 1)], 1u);
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * kSortThreads;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * kSortThreads + threadIdx.x; i < n; i += stride) {
+        const K k = keys[i];
+        for (int p = 0; p < passes; ++p) atomicAdd(&h[p][static_cast<uint32_t>(k >> (begin_bit + 8 * p)) & (kRadix - 1)], 1u);
     }
     __syncthreads();
-    counts[static_cast<uint64_t>(threadIdx.x) * ntiles + blockIdx.x] = h[threadIdx.x];
+    for (int p = 0; p < passes; ++p)
+        if (h[p][threadIdx.x]) atomicAdd(&digits[p * kRadix + threadIdx.x], h[p][threadIdx.x]);
+}
+
+// Global digit counts -> exclusive digit offsets, in place (one CTA).
+__global__ void __launch_bounds__(kSortThreads) radix_digit_offsets(uint32_t* digits, int passes) {
+    __shared__ uint32_t total;
+    for (int p = 0; p < passes; ++p) {
+        const uint32_t c = digits[p * kRadix + threadIdx.x];
+        const uint32_t e = block_exclusive_sum(c, &total);
+        __syncthreads();
+        digits[p * kRadix + threadIdx.x] = e;
+        __syncthreads();
+    }
 }
 
 template <typename K>
 struct ScatterSmem {
     uint32_t wcount[kSortWarps][kRadix];
     uint32_t tstart[kRadix];
+    uint32_t gbase[kRadix];
     uint32_t total;
+    uint32_t tile;
     K keys[kSortTile];
     uint32_t vals[kSortTile];
 };
 
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads) radix_scatter(const K* keys_in, const uint32_t* vals_in, K* keys_out,
-                                                              uint32_t* vals_out, uint64_t n, int shift,
-                                                              const uint32_t* offsets, uint32_t ntiles) {
+__global__ void __launch_bounds__(kSortThreads) radix_onesweep(const K* keys_in, const uint32_t* vals_in, K* keys_out,
+                                                               uint32_t* vals_out, uint64_t n, int shift,
+                                                               const uint32_t* offsets, uint32_t* status,
+                                                               uint32_t* tile_counter, uint32_t* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ScatterSmem<K>& sm = *reinterpret_cast<ScatterSmem<K>*>(smem_raw);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&sm.wcount[0][0])[i] = 0;
+    if (threadIdx.x == 0) sm.tile = atomicAdd(tile_counter, 1u);
     __syncthreads();
+    const uint32_t tile = sm.tile;
 
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+    const uint64_t base = static_cast<uint64_t>(tile) * kSortTile;
     const uint32_t lt = (1u << lane) - 1u;
     K k[kRounds];
     uint32_t v[kRounds], pos[kRounds];
@@ -152,19 +216,42 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(const K* keys_in, 
         __syncwarp();
     }
     __syncthreads();
-    // per digit: warp bases (exclusive over warps) and the tile's count
     {
         const int d = threadIdx.x;
-        uint32_t s = 0;
+        uint32_t c = 0;  // this tile's count of digit d; warp bases exclusive over warps
 #pragma unroll
         for (int w = 0; w < kSortWarps; ++w) {
-            uint32_t c = sm.wcount[w][d];
-            sm.wcount[w][d] = s;
-            s += c;
+            const uint32_t x = sm.wcount[w][d];
+            sm.wcount[w][d] = c;
+            c += x;
         }
-        // exclusive scan of the tile's digit counts -> tile-local digit starts
-        const uint32_t start = block_exclusive_sum(s, &sm.total);
-        sm.tstart[d] = start;
+        sm.tstart[d] = block_exclusive_sum(c, &sm.total);
+        // decoupled look-back over the tiles before this one
+        uint32_t* mine = status + static_cast<uint64_t>(tile) * kRadix + d;
+        uint32_t excl = 0;
+        if (tile == 0) {
+            st_relaxed(mine, kFlagPre | c);
+        } else {
+            st_relaxed(mine, kFlagAgg | c);
+            uint64_t j = tile - 1;
+            const uint64_t t0 = global_ns();
+            for (;;) {
+                const uint32_t w = ld_relaxed(status + j * kRadix + d);
+                if ((w & kFlagMask) == 0) {
+                    if (global_ns() - t0 > kWaitNs || ld_relaxed(err) != 0) {
+                        atomicOr(err, kErrWaitTimeout);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                excl += w & kCountMask;
+                if ((w & kFlagPre) || j == 0) break;
+                --j;
+            }
+            st_relaxed(mine, kFlagPre | (excl + c));
+        }
+        sm.gbase[d] = offsets[d] + excl;
     }
     __syncthreads();
 #pragma unroll
@@ -182,8 +269,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(const K* keys_in, 
     for (uint32_t i = threadIdx.x; i < valid; i += kSortThreads) {
         const K key = sm.keys[i];
         const uint32_t d = static_cast<uint32_t>(key >> shift) & (kRadix - 1);
-        const uint64_t dst = static_cast<uint64_t>(offsets[static_cast<uint64_t>(d) * ntiles + blockIdx.x]) +
-                             (i - sm.tstart[d]);
+        const uint64_t dst = static_cast<uint64_t>(sm.gbase[d]) + (i - sm.tstart[d]);
         keys_out[dst] = key;
         vals_out[dst] = sm.vals[i];
     }
@@ -191,34 +277,44 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(const K* keys_in, 
 
 template <typename K>
 kr_error sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt, uint64_t n, int begin_bit, int end_bit,
-                   void* temp, cudaStream_t stream, bool* in_alt) {
+                   void* temp, cudaStream_t stream, bool* in_alt, uint32_t* err) {
     *in_alt = false;
     if (n <= 1 || end_bit <= begin_bit) return kr_success;
     const uint32_t ntiles = static_cast<uint32_t>(div_up(n, kSortTile));
-    const uint64_t ncounts = static_cast<uint64_t>(kRadix) * ntiles;
-    uint32_t* counts = static_cast<uint32_t*>(temp);
-    void* scan_temp = counts + ((ncounts + 63) & ~63ull);
+    const int passes = (end_bit - begin_bit + 7) / 8;
+    if (passes > kMaxPasses) return "radix_sort_pairs: at most 64 key bits";
+    const SortTemp t = sort_temp(temp);
     static bool configured = false;
     if (!configured) {
-        OBVH_TRY_CUDA(cudaFuncSetAttribute(radix_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        OBVH_TRY_CUDA(cudaFuncSetAttribute(radix_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(sizeof(ScatterSmem<K>))));
         configured = true;
     }
+    // counts, tile counters, error word and this sort's status words start at zero
+    OBVH_TRY_CUDA(cudaMemsetAsync(temp, 0, kSortHeader + static_cast<size_t>(passes) * ntiles * kRadix * 4, stream));
+    {
+        ProfScope prof_scope_("radix_digit_counts", stream);
+        int grid = 2 * device_info().sm_count;
+        const uint64_t need = div_up(n, kSortThreads);
+        if (need < static_cast<uint64_t>(grid)) grid = static_cast<int>(need);
+        radix_digit_counts<K><<<grid, kSortThreads, 0, stream>>>(keys, n, begin_bit, passes, t.digits);
+    }
+    OBVH_TRY_CUDA(cudaGetLastError());
+    {
+        ProfScope prof_scope_("radix_digit_offsets", stream);
+        radix_digit_offsets<<<1, kSortThreads, 0, stream>>>(t.digits, passes);
+    }
+    OBVH_TRY_CUDA(cudaGetLastError());
     K* src_k = keys;
     K* dst_k = keys_alt;
     uint32_t* src_v = vals;
     uint32_t* dst_v = vals_alt;
-    for (int shift = begin_bit; shift < end_bit; shift += 8) {
+    for (int p = 0; p < passes; ++p) {
         {
-            ProfScope prof_scope_("radix_hist", stream);
-            radix_hist<K><<<ntiles, kSortThreads, 0, stream>>>(src_k, n, shift, counts, ntiles);
-        }
-        OBVH_TRY_CUDA(cudaGetLastError());
-        OBVH_TRY(exclusive_scan_u32(counts, counts, ncounts, nullptr, scan_temp, stream));
-        {
-            ProfScope prof_scope_("radix_scatter", stream);
-            radix_scatter<K><<<ntiles, kSortThreads, sizeof(ScatterSmem<K>), stream>>>(src_k, src_v, dst_k, dst_v, n,
-                                                                                       shift, counts, ntiles);
+            ProfScope prof_scope_("radix_onesweep", stream);
+            radix_onesweep<K><<<ntiles, kSortThreads, sizeof(ScatterSmem<K>), stream>>>(
+                src_k, src_v, dst_k, dst_v, n, begin_bit + 8 * p, t.digits + p * kRadix,
+                t.status + static_cast<size_t>(p) * ntiles * kRadix, t.tiles + p, err ? err : t.err);
         }
         OBVH_TRY_CUDA(cudaGetLastError());
         std::swap(src_k, dst_k);
@@ -273,19 +369,20 @@ kr_error exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint3
 
 size_t radix_sort_temp_bytes(uint64_t n) {
     const uint64_t ntiles = div_up(n > 0 ? n : 1, kSortTile);
-    const uint64_t ncounts = static_cast<uint64_t>(kRadix) * ntiles;
-    return ((ncounts + 63) & ~63ull) * sizeof(uint32_t) + scan_temp_bytes(ncounts);
+    return kSortHeader + static_cast<size_t>(kMaxPasses) * ntiles * kRadix * 4;
 }
 
+uint32_t* radix_sort_error_word(void* temp) { return sort_temp(temp).err; }
+
 kr_error radix_sort_pairs(void* keys, void* keys_alt, uint32_t* vals, uint32_t* vals_alt, uint64_t n, int key_bytes,
-                          int begin_bit, int end_bit, void* temp, cudaStream_t stream, bool* in_alt) {
-    if (n >= (1ull << 32)) return "radix_sort_pairs: at most 2^32 - 1 elements";
+                          int begin_bit, int end_bit, void* temp, cudaStream_t stream, bool* in_alt, uint32_t* err) {
+    if (n >= (1ull << 30)) return "radix_sort_pairs: at most 2^30 - 1 elements";
     if (key_bytes == 4)
         return sort_impl(static_cast<uint32_t*>(keys), static_cast<uint32_t*>(keys_alt), vals, vals_alt, n, begin_bit,
-                         end_bit, temp, stream, in_alt);
+                         end_bit, temp, stream, in_alt, err);
     if (key_bytes == 8)
         return sort_impl(static_cast<uint64_t*>(keys), static_cast<uint64_t*>(keys_alt), vals, vals_alt, n, begin_bit,
-                         end_bit, temp, stream, in_alt);
+                         end_bit, temp, stream, in_alt, err);
     return "radix_sort_pairs: key_bytes must be 4 or 8";
 }
 

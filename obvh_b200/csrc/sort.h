@@ -20,11 +20,15 @@ kr_error exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, uint3
                             cudaStream_t stream);
 
 size_t radix_sort_temp_bytes(uint64_t n);
-// Stable sort of keys[0..n) (key_bytes 4 or 8) with their values by bits
+// Stable sort of keys[0..n < 2^30) (key_bytes 4 or 8) with their values by bits
 // [begin_bit, end_bit).  keys/vals hold the input; keys_alt/vals_alt are
 // scratch of the same size.  On return *in_alt says whether the sorted data
 // ended in the *_alt buffers.
+// A bounded wait that times out sets kErrWaitTimeout in *err (a device word of
+// the caller's), or in the sort's own word inside `temp` when err is null.
 kr_error radix_sort_pairs(void* keys, void* keys_alt, uint32_t* vals, uint32_t* vals_alt, uint64_t n, int key_bytes,
-                          int begin_bit, int end_bit, void* temp, cudaStream_t stream, bool* in_alt);
+                          int begin_bit, int end_bit, void* temp, cudaStream_t stream, bool* in_alt,
+                          uint32_t* err = nullptr);
+uint32_t* radix_sort_error_word(void* temp);
 
 }  // namespace obvh
