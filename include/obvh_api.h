@@ -33,6 +33,15 @@ OBVH_EXPORT kr_error obvh_last_error(void);
 OBVH_EXPORT kr_error obvh_profile_enable(int on);
 OBVH_EXPORT kr_error obvh_profile_summary(char* buf, kr_size cap);
 
+/*
+ * Check of the library's bounded waits: one thread waits for a device flag
+ * that nothing sets, gives up after limit_us microseconds (at most 1 s) the
+ * way every wait in the library does, and sets the timeout bit in a device
+ * error word, which is returned in *device_error.  The context stays usable.
+ * No counterpart in the reference.
+ */
+OBVH_EXPORT kr_error obvh_check_bounded_wait(kr_u32 limit_us, kr_u32* device_error);
+
 #ifdef __cplusplus
 }
 #endif

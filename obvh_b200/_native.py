@@ -66,6 +66,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "obvh_bvh_collapse_async": (err, [vp, vp, vp, vp, vp, vp, c.c_float, c.c_float, c.c_uint32, c.c_uint32,
                                           vp, vp]),
         "obvh_profile_enable": (err, [c.c_int]),
+        "obvh_check_bounded_wait": (err, [c.c_uint32, c.POINTER(c.c_uint32)]),
         "obvh_profile_summary": (err, [c.c_char_p, c.c_uint64]),
         "obvh_build_workspace_bytes": (c.c_uint64, [c.c_uint32]),
         "obvh_build_workspace_init": (err, [vp, c.c_uint32, vp]),
