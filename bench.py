@@ -251,7 +251,7 @@ def tree_bytes_per_launch(n):
         "radix_digit_counts": 4 * n,                   # keys in (every pass's digits at once)
         "radix_onesweep": 16 * n,                      # key + value in and out (u32 keys)
         "leaves_kernel": 4 * n + 24 * n + 36 * n,      # order, box in; leaf node out
-        "karras_kernel": 4 * n + 36 * ni + 8 * ni,     # codes in; internal nodes + parents out
+        "karras_kernel": 4 * n + 36 * ni + 16 * ni,    # codes in; internal nodes, parents, first leaves, spans out
         "aabb_up_kernel": 36 * nn + 8 * nn + 32 * ni,  # nodes in; counts, costs, bounds out
         # faces + vertices in, leaf boxes + transforms out, summaries out and read once
         "summary_up_kernel": 52 * n + 124 * n + 112 * ni * 2 + 4 * ni,
@@ -259,11 +259,14 @@ def tree_bytes_per_launch(n):
         "candidate_kernel": 112 * ni + 168 * ni + 96 * ni + 8 * ni,  # summary + 14 vertices in; frame out
         "extents_small_kernel": 96 * ni + 124 * ni,    # frame in; box + transform out
         "extents_units_kernel": 36 * n,                # ordered triangles in
+        # tiles: ordered triangles, frames, first leaves and counts in; boxes + transforms (or extent keys) out
+        "extents_tile_kernel": 36 * n + 104 * ni + 124 * ni,
         "mark_up_kernel": 36 * nn + 16 * nn + 36 * n,
         # fused build: leaf node (x2), ordered triangle, leaf box + transform out; box, face, vertices in
         "leaves_fused_kernel": 4 * n + 24 * n + 52 * n + 72 * n + 36 * n + 124 * n,
-        # fused leaf-to-root pass: children in, bounds/counts/costs/collapsed node/summary out
-        "fused_up_kernel": 36 * n + 8 * n + 36 * n + 72 * ni + 16 * ni + 24 * ni + 36 * ni + 8 * ni + 224 * ni,
+        # fused leaf-to-root pass over the CTA-local nodes: leaf nodes + triangles in, leaf costs + counts out;
+        # children, first leaf, count in; bounds, collapsed node, cost, summary out; collapse marks
+        "fused_up_local_kernel": 36 * n + 36 * n + 8 * n + 16 * ni + 24 * ni + 36 * ni + 4 * ni + 112 * ni + nn,
         # ATRBVH: triangle in, 63-bit key + index out; sorted keys in, working nodes out;
         # leaf triangles + nodes in/out bottom-up; one pass over the working tree per iteration
         "morton63_kernel": 52 * n + 12 * n,

@@ -192,9 +192,10 @@ __device__ __forceinline__ int delta(const uint32_t* codes, int i, int j, uint32
 __device__ __forceinline__ int halve_up(int x) { return x == 1 ? 0 : ((x % 2) == 1 ? x / 2 + 1 : x / 2); }
 
 // first (nullable) receives each internal node's first leaf in depth-first
-// order: the lower end of its key range.
+// order: the lower end of its key range; span (nullable) the number of leaves
+// in the range, which is the node's primitive count (one primitive per leaf).
 __global__ void __launch_bounds__(kThreads) karras_kernel(const uint32_t* codes, uint32_t n, kr_bvh_node* nodes,
-                                                          uint32_t* parents, uint32_t* first) {
+                                                          uint32_t* parents, uint32_t* first, uint32_t* span) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t internal = n - 1;
     if (i >= static_cast<int>(internal)) return;
@@ -225,6 +226,7 @@ __global__ void __launch_bounds__(kThreads) karras_kernel(const uint32_t* codes,
     w[7] = right;
     w[8] = 0;  // nPrimitives 0, axis 0
     if (first) first[i] = static_cast<uint32_t>(lo);
+    if (span) span[i] = static_cast<uint32_t>(hi - lo + 1);
     if (i == 0) parents[0] = tree::kNoParent;
 }
 
@@ -345,10 +347,10 @@ kr_error enqueue_codes(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, 
 }
 
 kr_error enqueue_karras(const uint32_t* codes, uint32_t n, kr_bvh_node* nodes, uint32_t* parents, uint32_t* first,
-                        cudaStream_t s) {
+                        uint32_t* span, cudaStream_t s) {
     if (n >= 2) {
         ProfScope prof_scope_("karras_kernel", s);
-        karras_kernel<<<(n - 1 + kThreads - 1) / kThreads, kThreads, 0, s>>>(codes, n, nodes, parents, first);
+        karras_kernel<<<(n - 1 + kThreads - 1) / kThreads, kThreads, 0, s>>>(codes, n, nodes, parents, first, span);
         OBVH_TRY_CUDA(cudaGetLastError());
     } else {
         OBVH_TRY_CUDA(cudaMemsetAsync(parents, 0xff, sizeof(uint32_t), s));
@@ -371,7 +373,7 @@ kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, 
         leaves_kernel<<<grid_n, kThreads, 0, s>>>(c.tri_boxes, c.order, n, nodes);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
-    OBVH_TRY(enqueue_karras(c.codes, n, nodes, parents, nullptr, s));
+    OBVH_TRY(enqueue_karras(c.codes, n, nodes, parents, nullptr, nullptr, s));
     if (n >= 2) OBVH_TRY_CUDA(cudaMemsetAsync(c.visits, 0, 4ull * (n - 1), s));
     {
         ProfScope prof_scope_("aabb_up_kernel", s);

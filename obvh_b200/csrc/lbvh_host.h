@@ -34,9 +34,10 @@ struct Codes {
 };
 kr_error enqueue_codes(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, void* workspace, cudaStream_t s,
                        Codes* out);
-// Karras tree over sorted codes; first (nullable) gets each internal node's first leaf.
+// Karras tree over sorted codes; first (nullable) gets each internal node's
+// first leaf, span (nullable) its number of leaves.
 kr_error enqueue_karras(const uint32_t* codes, uint32_t n, kr_bvh_node* nodes, uint32_t* parents, uint32_t* first,
-                        cudaStream_t s);
+                        uint32_t* span, cudaStream_t s);
 
 // Full build into caller buffers (nodes/parents/counts/costs of 2n-1 entries).
 kr_error enqueue_build(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, kr_bvh_node* nodes,

@@ -16,12 +16,15 @@
 //   candidate    node-parallel DiTO-14 candidate axes from the 14 summary
 //                vertices (:676-756) and the initial extents along them.
 //   extents      min/max of every subtree vertex on the node's axes, read
-//                from the contiguous run: one thread per node up to 8 leaves,
-//                one warp per 1024-leaf unit above that (units dealt to the
-//                warps of a persistent grid); only nodes of more than one unit
-//                combine partial results, with 6 integer atomics per unit.
-//                Nodes finished here are finalised in place (:903-964).
-//   finalize     the multi-unit nodes.
+//                from the contiguous run: one thread per node up to 32
+//                leaves, one warp per 1024-leaf unit above that (units dealt
+//                to the warps of a persistent grid); only nodes of more than
+//                one unit combine partial results, with 6 integer atomics per
+//                unit.  Nodes finished here are finalised in place (:903-964).
+//                For a Karras tree (the fused build), tiles instead: one CTA
+//                per 1,024 consecutive leaves stages their triangles in shared
+//                memory once and serves every node over them from there.
+//   finalize     the nodes of more than one unit or tile.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -44,6 +47,13 @@ constexpr int kThreads = 256;
 constexpr uint32_t kThreadMax = 32;  // leaves handled by one thread per node
 constexpr uint32_t kUnit = 1024;    // leaves per warp unit
 constexpr uint32_t kUnitRun = 4;   // consecutive units per warp visit
+constexpr int kTileShift = 10;      // tiled extents: 1,024 leaves per tile
+constexpr uint32_t kTile = 1u << kTileShift;
+// Ancestors of a leaf in a Karras tree over 30-bit codes with the index
+// tie-break: each level lengthens the common prefix of the 62-bit (code,
+// index) keys, so there are at most 62.
+constexpr uint32_t kChain = 64;
+constexpr uint32_t kTileItems = 320;  // warp items per tile kept in shared memory
 
 struct Ctl {
     uint32_t error;
@@ -161,10 +171,50 @@ __global__ void __launch_bounds__(kThreads) dfs_rank_kernel(const kr_bvh_node* n
 
 // `points` is the packed xyz array the summary's vertex ids index: the mesh
 // vertices, or the depth-first triangle slots of the fused build.
+struct ChainArgs {
+    const uint32_t* parents;  // null: per-node extents, no chains
+    const uint32_t* first;
+    uint32_t n;
+    uint32_t walker_blocks;   // leading CTAs that walk the tile chains
+    uint32_t* chains;
+    uint32_t* chain_counts;
+    uint32_t* err;
+};
+
+// The ancestors of tile tau's first leaf (side 0) and last leaf (side 1) whose
+// leaf ranges are not inside the tile: the nodes the tile serves partially.
+// A node on both chains is listed on side 0 only.
+__device__ void walk_chain(const ChainArgs& c, const uint32_t* counts, uint32_t w) {
+    const uint32_t ntiles = (c.n + kTile - 1) >> kTileShift;
+    if (w >= 2 * ntiles) return;
+    const uint32_t tau = w >> 1, side = w & 1;
+    const uint32_t t0 = tau << kTileShift, tend = min(t0 + kTile, c.n);
+    const uint32_t internal = c.n - 1;
+    uint32_t* out = c.chains + static_cast<size_t>(w) * kChain;
+    uint32_t count = 0;
+    uint32_t p = c.parents[internal + (side ? tend - 1 : t0)];
+    for (uint32_t steps = 0; p != kNoParent; ++steps) {
+        if (p >= internal || steps >= kChain) {
+            atomicOr(c.err, kErrBadInput);
+            break;
+        }
+        const uint32_t f = __ldg(c.first + p), cnt = __ldg(counts + p);
+        if (side && f <= t0) break;  // from here on the nodes hold the first leaf too
+        if (f < t0 || f + cnt > tend) out[count++] = p;
+        p = __ldg(c.parents + p);
+    }
+    c.chain_counts[w] = count;
+}
+
 __global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* summary, const kr_vec3* verts,
                                                              const uint32_t* counts, uint32_t internal, Cand* cand,
-                                                             uint32_t* nunits, uint32_t* keys, const uint32_t* err) {
-    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+                                                             uint32_t* nunits, uint32_t* keys, const uint32_t* err,
+                                                             ChainArgs chain) {
+    if (blockIdx.x < chain.walker_blocks) {
+        if (!*err) walk_chain(chain, counts, blockIdx.x * blockDim.x + threadIdx.x);
+        return;
+    }
+    const uint32_t a = (blockIdx.x - chain.walker_blocks) * blockDim.x + threadIdx.x;
     if (a >= internal) return;
     if (*err) {  // malformed tree: no summaries to read; nothing is scheduled after this
         nunits[a] = 0;
@@ -193,7 +243,13 @@ __global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* sum
 #pragma unroll
     for (int q = 0; q < 6; ++q) dst[q] = src[q];
     const uint32_t cnt = counts[a];
-    const uint32_t units = cnt > kThreadMax ? (cnt + kUnit - 1) / kUnit : 0u;
+    uint32_t units;
+    if (chain.parents) {  // tiles: 0 in one tile and small, 1 in one tile, 2 over several tiles
+        const uint32_t f = __ldg(chain.first + a);
+        units = (f >> kTileShift) != ((f + cnt - 1) >> kTileShift) ? 2u : (cnt > kThreadMax ? 1u : 0u);
+    } else {
+        units = cnt > kThreadMax ? (cnt + kUnit - 1) / kUnit : 0u;
+    }
     nunits[a] = units;
     if (units > 1) {
         uint32_t* k = keys + 6 * static_cast<size_t>(a);
@@ -234,6 +290,23 @@ __device__ __forceinline__ void project_tri(const float* t, const Axes& ax, floa
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
         const f3 p = mk3(__ldg(t + 3 * v), __ldg(t + 3 * v + 1), __ldg(t + 3 * v + 2));
+        q[0][v] = dot3(p, ax.b0);
+        q[1][v] = dot3(p, ax.b1);
+        q[2][v] = dot3(p, ax.b2);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = fminf(min3f(lo[k], q[k][0], q[k][1]), q[k][2]);
+        hi[k] = fmaxf(max3f(hi[k], q[k][0], q[k][1]), q[k][2]);
+    }
+}
+
+// project_tri for a triangle in shared memory
+__device__ __forceinline__ void project_tri_s(const float* t, const Axes& ax, float lo[3], float hi[3]) {
+    float q[3][3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const f3 p = mk3(t[3 * v], t[3 * v + 1], t[3 * v + 2]);
         q[0][v] = dot3(p, ax.b0);
         q[1][v] = dot3(p, ax.b1);
         q[2][v] = dot3(p, ax.b2);
@@ -317,6 +390,126 @@ __global__ void __launch_bounds__(kThreads) extents_units_kernel(const Cand* can
                 const float v = lane < 3 ? lo[lane] : hi[lane - 3];
                 uint32_t* k = keys + 6 * static_cast<size_t>(a) + lane;
                 if (lane < 3) atomicMin(k, f2key(v)); else atomicMax(k, f2key(v));
+            }
+        }
+    }
+}
+
+// One tile of kTile consecutive leaves: their triangles are staged in shared
+// memory once, then every node over them is served from there.  Nodes inside
+// the tile with at most kThreadMax leaves: one thread each, finalised here.
+// Larger nodes inside the tile: a warp each, extents to the keys.  Nodes
+// crossing the tile's edges (the two chains): a warp each over their part in
+// the tile, combined in the keys with integer atomics.  Warps take items from
+// a shared counter; an item beyond the list's capacity is done by the thread
+// that found it.
+__global__ void __launch_bounds__(kThreads) extents_tile_kernel(const Cand* cand, const uint32_t* counts,
+                                                                const uint32_t* first, const float* tris, uint32_t n,
+                                                                const uint32_t* chains, const uint32_t* chain_counts,
+                                                                uint32_t* keys, kr_obb3* obbs, kr_mat4* xfs,
+                                                                const uint32_t* err) {
+    __shared__ __align__(16) float tri[kTile * 9];
+    __shared__ uint32_t item_node[kTileItems];
+    __shared__ uint16_t item_b[kTileItems], item_e[kTileItems];
+    __shared__ uint32_t nitems, next_item;
+    if (*err) return;
+    const uint32_t t = threadIdx.x, lane = t & 31;
+    const uint32_t t0 = blockIdx.x << kTileShift;
+    const uint32_t tn = min(kTile, n - t0);
+    const uint32_t internal = n - 1;
+    {
+        // 9 * t0 floats = t0 * 36 bytes from a 16-byte aligned base: aligned
+        const float4* src = reinterpret_cast<const float4*>(tris + 9 * static_cast<size_t>(t0));
+        float4* dst = reinterpret_cast<float4*>(tri);
+        const uint32_t n4 = 9 * tn / 4;
+        for (uint32_t i = t; i < n4; i += kThreads) dst[i] = __ldg(src + i);
+        for (uint32_t i = 4 * n4 + t; i < 9 * tn; i += kThreads) tri[i] = __ldg(tris + 9 * static_cast<size_t>(t0) + i);
+    }
+    if (t == 0) {
+        nitems = 0;
+        next_item = 0;
+    }
+    __syncthreads();
+    const auto add_item = [&](uint32_t a, uint32_t b, uint32_t e, bool partial) {
+        const uint32_t idx = atomicAdd(&nitems, 1u);
+        if (idx < kTileItems) {
+            item_node[idx] = a | (partial ? 0x80000000u : 0u);
+            item_b[idx] = static_cast<uint16_t>(b);
+            item_e[idx] = static_cast<uint16_t>(e);
+            return;
+        }
+        // list full: this thread does the item alone
+        const Cand c = load_cand(cand, a);
+        const Axes ax = make_axes(mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
+                                  mk3(c.ax[6], c.ax[7], c.ax[8]));
+        float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+        for (uint32_t i = b; i < e; ++i) project_tri_s(tri + 9 * i, ax, lo, hi);
+        for (int k = 0; k < 3; ++k) {
+            uint32_t* kk = keys + 6 * static_cast<size_t>(a);
+            if (partial) {
+                atomicMin(kk + k, f2key(lo[k]));
+                atomicMax(kk + 3 + k, f2key(hi[k]));
+            } else {
+                __stcg(kk + k, f2key(fminf(c.olo[k], lo[k])));
+                __stcg(kk + 3 + k, f2key(fmaxf(c.ohi[k], hi[k])));
+            }
+        }
+    };
+    // nodes inside the tile: their indices lie in the tile too
+    const uint32_t qn = t0 < internal ? min(tn, internal - t0) : 0u;
+    for (uint32_t i = t; i < qn; i += kThreads) {
+        const uint32_t a = t0 + i;
+        const uint32_t f = __ldg(first + a), cnt = __ldg(counts + a);
+        if (f < t0 || f + cnt > t0 + tn) continue;
+        if (cnt <= kThreadMax) {
+            const Cand c = load_cand(cand, a);
+            float lo[3] = {c.olo[0], c.olo[1], c.olo[2]}, hi[3] = {c.ohi[0], c.ohi[1], c.ohi[2]};
+            const Axes ax = make_axes(mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
+                                      mk3(c.ax[6], c.ax[7], c.ax[8]));
+            const float* tp = tri + 9 * (f - t0);
+            for (uint32_t k = 0; k < cnt; ++k) project_tri_s(tp + 9 * k, ax, lo, hi);
+            finalize_node(c, mk3(lo[0], lo[1], lo[2]), mk3(hi[0], hi[1], hi[2]), obbs + a, xfs + a);
+        } else {
+            add_item(a, f - t0, f - t0 + cnt, false);
+        }
+    }
+    // nodes over the tile's edges
+    for (uint32_t side = 0; side < 2; ++side) {
+        const uint32_t w = 2 * blockIdx.x + side;
+        const uint32_t cnt = min(chain_counts[w], kChain);
+        for (uint32_t i = t; i < cnt; i += kThreads) {
+            const uint32_t a = chains[static_cast<size_t>(w) * kChain + i];
+            const uint32_t f = __ldg(first + a), c = __ldg(counts + a);
+            add_item(a, max(f, t0) - t0, min(f + c, t0 + tn) - t0, true);
+        }
+    }
+    __syncthreads();
+    const uint32_t items = min(nitems, kTileItems);
+    for (;;) {
+        uint32_t it = 0;
+        if (lane == 0) it = atomicAdd(&next_item, 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= items) break;
+        const uint32_t a = item_node[it] & 0x7fffffffu;
+        const bool partial = item_node[it] >> 31;
+        const uint32_t b = item_b[it], e = item_e[it];
+        const Cand c = load_cand(cand, a);
+        const Axes ax = make_axes(mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
+                                  mk3(c.ax[6], c.ax[7], c.ax[8]));
+        float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+        for (uint32_t i = b + lane; i < e; i += 32) project_tri_s(tri + 9 * i, ax, lo, hi);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = warp_min(lo[k]);
+            hi[k] = warp_max(hi[k]);
+        }
+        if (lane < 6) {
+            uint32_t* kk = keys + 6 * static_cast<size_t>(a) + lane;
+            if (partial) {
+                if (lane < 3) atomicMin(kk, f2key(lo[lane])); else atomicMax(kk, f2key(hi[lane - 3]));
+            } else {
+                const float v = lane < 3 ? fminf(c.olo[lane], lo[lane]) : fmaxf(c.ohi[lane - 3], hi[lane - 3]);
+                __stcg(kk, f2key(v));
             }
         }
     }
@@ -408,17 +601,40 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec
 }
 
 size_t cand_bytes(uint32_t internal) { return sizeof(Cand) * (internal > 0 ? internal : 1); }
+size_t chain_bytes(uint32_t n) { return 2ull * kChain * 4 * (((n > 0 ? n : 1) + kTile - 1) >> kTileShift); }
+size_t chain_count_bytes(uint32_t n) { return 2ull * 4 * (((n > 0 ? n : 1) + kTile - 1) >> kTileShift); }
 
 kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs, kr_mat4* xfs, cudaStream_t s) {
     if (internal == 0) return kr_success;
     const unsigned gi = (internal + kThreads - 1) / kThreads;
     Cand* cand = static_cast<Cand*>(b.cand);
+    const uint32_t n = internal + 1;
+    const bool tiled = b.chains != nullptr;
+    const uint32_t ntiles = (n + kTile - 1) >> kTileShift;
+    ChainArgs chain{tiled ? b.parents : nullptr, b.first, n, tiled ? (2 * ntiles + kThreads - 1) / kThreads : 0u,
+                    b.chains, b.chain_counts, b.err};
+    if (tiled && !b.parents) return "enqueue_frames: tiled extents need the parents";
     {
+        // the chain walks go first, so that they overlap the candidate search
         ProfScope prof_scope_("candidate_kernel", s);
-        candidate_kernel<<<gi, kThreads, 0, s>>>(b.summary, b.points, b.counts, internal, cand, b.nunits, b.keys,
-                                                 b.err);
+        candidate_kernel<<<gi + chain.walker_blocks, kThreads, 0, s>>>(b.summary, b.points, b.counts, internal, cand,
+                                                                        b.nunits, b.keys, b.err, chain);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
+    if (tiled) {
+        {
+            ProfScope prof_scope_("extents_tile_kernel", s);
+            extents_tile_kernel<<<ntiles, kThreads, 0, s>>>(cand, b.counts, b.first, b.tris, n, b.chains,
+                                                            b.chain_counts, b.keys, obbs, xfs, b.err);
+        }
+        OBVH_TRY_CUDA(cudaGetLastError());
+        {
+            ProfScope prof_scope_("finalize_multi_kernel", s);
+            finalize_multi_kernel<<<gi, kThreads, 0, s>>>(cand, b.nunits, b.keys, internal, obbs, xfs, b.err);
+        }
+        OBVH_TRY_CUDA(cudaGetLastError());
+        return kr_success;
+    }
     {
         ProfScope prof_scope_("extents_small_kernel", s);
         extents_small_kernel<<<gi, kThreads, 0, s>>>(cand, b.counts, b.first, b.tris, internal, obbs, xfs, b.err);

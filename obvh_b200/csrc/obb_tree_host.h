@@ -39,8 +39,16 @@ struct FrameBuffers {
     void* scan;                // scan_temp_bytes(internal)
     uint32_t* err;
     uint32_t* total_units;
+    // Tiled extents, for a Karras tree over sorted leaves (internal node a's
+    // leaves are [first[a], first[a] + counts[a]) and no leaf has more than
+    // 62 ancestors): null chains selects the per-node path.
+    const uint32_t* parents = nullptr;
+    uint32_t* chains = nullptr;        // chain_bytes(n)
+    uint32_t* chain_counts = nullptr;  // chain_count_bytes(n)
 };
 size_t cand_bytes(uint32_t internal);
+size_t chain_bytes(uint32_t n);
+size_t chain_count_bytes(uint32_t n);
 kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs, kr_mat4* xfs, cudaStream_t s);
 
 }  // namespace obbtree

@@ -20,6 +20,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
 
 #include "device_common.cuh"
 #include "lbvh_host.h"
@@ -43,7 +44,8 @@ struct Ctl {
     uint32_t error;
     uint32_t total_units;
     uint32_t total_slots;
-    uint32_t pad[61];
+    uint32_t frontier;  // walks left for the cross-CTA pass
+    uint32_t pad[60];
 };
 
 __device__ __forceinline__ void store_words(kr_bvh_node* nodes, uint32_t i, const uint32_t* w, int count) {
@@ -139,119 +141,484 @@ __device__ __forceinline__ void slot_summary(const float* tris, uint32_t j, Summ
     leaf_summary(pts, make_uint4(3 * j, 3 * j + 1, 3 * j + 2, 0), s);
 }
 
-// One leaf-to-root pass for bounds, counts, costs, collapse marks and summaries.
-__global__ void __launch_bounds__(kThreads) fused_up_kernel(kr_bvh_node* nodes, kr_bvh_node* collapsed,
-                                                            const uint32_t* parents, const float* tris, uint32_t n,
-                                                            uint32_t* counts, float* costs, uint8_t* flags, float ci,
-                                                            float ct, uint4* summary, uint32_t* visits,
-                                                            uint32_t* err) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    const uint32_t internal = n - 1;
-    const uint32_t leaf = internal + j;
-    const bool collapse = flags != nullptr;
-    // The arriving thread carries its own child's bounds, count and cost; only
-    // the sibling's are read from memory.
-    float olo[3], ohi[3];
-    uint32_t ocount = 1;
-    float ocost;
-    {
-        const NodeView lf = load_node(nodes, leaf);
-        for (int k = 0; k < 3; ++k) { olo[k] = lf.lo[k]; ohi[k] = lf.hi[k]; }
-        // leaf cost: ct * area in the collapse (transforms.cu:97), 1 * area in the LBVH (lbvh.cu:427)
-        ocost = (collapse ? ct : 1.0f) * box_area(lf.lo, lf.hi);
-        __stcg(costs + leaf, ocost);
-        __stcg(counts + leaf, 1u);
+// What a completed node passes to its parent: bounds and SAH cost.
+struct Carry {
+    float lo[3], hi[3];
+    float cost;
+};
+
+// One slab of a 7-direction summary: extreme projections and their vertices.
+struct Slab {
+    float lo, hi;
+    uint32_t ilo, ihi;
+};
+
+// merge_right for one slab: the left child's values, the right child's where
+// strictly better.
+__device__ __forceinline__ Slab merge_slab(const Slab& l, const Slab& r) {
+    Slab o = l;
+    if (l.lo > r.lo) { o.lo = r.lo; o.ilo = r.ilo; }
+    if (l.hi < r.hi) { o.hi = r.hi; o.ihi = r.ihi; }
+    return o;
+}
+
+__device__ __forceinline__ Slab slab_of(const Summary& s, int k) { return Slab{s.lo[k], s.hi[k], s.ilo[k], s.ihi[k]}; }
+__device__ __forceinline__ void set_slab(Summary& s, int k, const Slab& v) {
+    s.lo[k] = v.lo; s.hi[k] = v.hi; s.ilo[k] = v.ilo; s.ihi[k] = v.ihi;
+}
+
+// slab7()[k] of one point, evaluated as slab7 does
+__device__ __forceinline__ float slab_at(f3 p, int k) {
+    switch (k) {
+        case 0: return p.x;
+        case 1: return p.y;
+        case 2: return p.z;
+        case 3: return p.x + p.y + p.z;
+        case 4: return p.x + p.y - p.z;
+        case 5: return p.x - p.y + p.z;
+        default: return p.x - p.y - p.z;
     }
-    Summary own;
-    if (summary) slot_summary(tris, j, own);
-    uint32_t child = leaf;
-    uint32_t p = parents[leaf];
+}
+
+// Slab k of sorted leaf j's summary (leaf_summary over vertex slots 3j..3j+2).
+__device__ __forceinline__ Slab leaf_slab(const f3* v, uint32_t j, int k) {
+    Slab o;
+    o.lo = o.hi = slab_at(v[0], k);
+    o.ilo = o.ihi = 3 * j;
+#pragma unroll
+    for (int i = 1; i < 3; ++i) {
+        const float q = slab_at(v[i], k);
+        if (q < o.lo) { o.lo = q; o.ilo = 3 * j + i; }
+        if (q > o.hi) { o.hi = q; o.ihi = 3 * j + i; }
+    }
+    return o;
+}
+
+// Shared memory of the CTA-local part of the bottom-up pass.  Per internal
+// node: bounds (6), cost (1) and the 7-direction summary (28 words); per leaf:
+// bounds, cost, the 14 slab values and the vertex choices (2 bits each) in one
+// word.  Word-major ([word][node]) so that a warp's accesses spread over banks.
+constexpr int kSlotWords = 35;
+constexpr int kLeafWords = 22;
+constexpr uint16_t kLeafKid = 0x8000u;  // child encoding: leaf j0 + q, else internal node j0 + q
+constexpr uint16_t kNotLocal = 0xffffu;
+
+struct LocalSmem {
+    uint32_t islot[kSlotWords][kThreads];
+    uint32_t lslot[kLeafWords][kThreads];
+    uint32_t deg[kThreads];     // children of local node j0 + q not completed yet
+    uint16_t kid[2][kThreads];  // its children
+    uint16_t cnt[kThreads];     // its primitive count
+    uint16_t up[kThreads];      // its parent's local index, or kNotLocal
+    uint8_t queue[3][kThreads]; // nodes ready in a round
+    uint8_t local[kThreads], iflag[kThreads], lflag[kThreads], hidden[kThreads];
+    uint32_t qn[3];
+    uint32_t nfront, front_base;
+};
+constexpr size_t kFusedSmemBytes = sizeof(LocalSmem);
+
+__device__ __forceinline__ void put_carry(uint32_t (*slots)[kThreads], uint32_t q, const Carry& c) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        slots[k][q] = __float_as_uint(c.lo[k]);
+        slots[3 + k][q] = __float_as_uint(c.hi[k]);
+    }
+    slots[6][q] = __float_as_uint(c.cost);
+}
+
+__device__ __forceinline__ Carry get_carry(const uint32_t (*slots)[kThreads], uint32_t q) {
+    Carry c;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        c.lo[k] = __uint_as_float(slots[k][q]);
+        c.hi[k] = __uint_as_float(slots[3 + k][q]);
+    }
+    c.cost = __uint_as_float(slots[6][q]);
+    return c;
+}
+
+__device__ __forceinline__ void put_slab(uint32_t (*slots)[kThreads], uint32_t q, int k, const Slab& v) {
+    slots[7 + 4 * k][q] = __float_as_uint(v.lo);
+    slots[8 + 4 * k][q] = __float_as_uint(v.hi);
+    slots[9 + 4 * k][q] = v.ilo;
+    slots[10 + 4 * k][q] = v.ihi;
+}
+
+__device__ __forceinline__ Slab get_slab(const uint32_t (*slots)[kThreads], uint32_t q, int k) {
+    return Slab{__uint_as_float(slots[7 + 4 * k][q]), __uint_as_float(slots[8 + 4 * k][q]), slots[9 + 4 * k][q],
+                slots[10 + 4 * k][q]};
+}
+
+// Slab k of leaf j0 + q (vertex slots 3j .. 3j+2).
+__device__ __forceinline__ Slab get_leaf_slab(const LocalSmem& sm, uint32_t q, uint32_t j, int k) {
+    const uint32_t pick = sm.lslot[21][q] >> (4 * k);
+    return Slab{__uint_as_float(sm.lslot[7 + 2 * k][q]), __uint_as_float(sm.lslot[8 + 2 * k][q]), 3 * j + (pick & 3u),
+                3 * j + ((pick >> 2) & 3u)};
+}
+
+__device__ __forceinline__ void store_slab(uint4* summary, uint32_t p, int k, const Slab& v) {
+    __stcg(summary + 7 * static_cast<size_t>(p) + k,
+           make_uint4(__float_as_uint(v.lo), __float_as_uint(v.hi), v.ilo, v.ihi));
+}
+
+struct UpArgs {
+    kr_bvh_node* nodes;
+    kr_bvh_node* collapsed;  // null: no collapse copy
+    const uint32_t* parents;
+    const uint32_t* first;
+    const float* tris;
+    uint32_t n;
+    uint32_t* counts;
+    float* costs;
+    uint8_t* flags;  // null: LBVH costs, no collapse marks
+    float ci, ct;
+    uint4* summary;  // null: no summaries
+    uint32_t* visits;
+    uint32_t* err;
+};
+
+// Completes internal node p (children L, R; count primitives) from its
+// children's carries: writes its bounds, cost and collapse marks and returns
+// its carry.  (The summary is merged by the caller.)
+__device__ __forceinline__ Carry complete_node(const UpArgs& a, uint32_t p, uint32_t L, uint32_t R, uint32_t count,
+                                               const Carry& l, const Carry& r) {
+    Carry o;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {  // kr_aabb_expand(left, right)
+        o.lo[k] = kmin(kmin(l.lo[k], r.lo[k]), r.hi[k]);
+        o.hi[k] = kmax(kmax(l.hi[k], r.lo[k]), r.hi[k]);
+    }
+    uint32_t w[9];
+    for (int k = 0; k < 3; ++k) { w[k] = __float_as_uint(o.lo[k]); w[3 + k] = __float_as_uint(o.hi[k]); }
+    w[6] = L;
+    w[7] = R;
+    w[8] = 0;
+    store_words(a.nodes, p, w, 6);
+    if (a.collapsed) store_words(a.collapsed, p, w, 9);
+    const float area = box_area(o.lo, o.hi);
+    if (a.flags) {
+        // bvh_mark_collapse_kernel (transforms.cu:111-133)
+        const float node_cost = a.ci * area + l.cost + r.cost;
+        const float leaf_cost = a.ct * area * static_cast<float>(count);
+        if (leaf_cost < node_cost && count <= kMaxLeafSize) {
+            o.cost = leaf_cost;
+            a.flags[p] = 1;
+            a.flags[L] = 1;
+            a.flags[R] = 1;
+            // nPrimitives = 0xFFFF; the axis byte and the pad of every node
+            // record are zero here, so the whole word is written
+            __stcg(reinterpret_cast<uint32_t*>(a.collapsed + L) + 8, kHidden);
+            __stcg(reinterpret_cast<uint32_t*>(a.collapsed + R) + 8, kHidden);
+        } else {
+            o.cost = node_cost;
+        }
+    } else {
+        o.cost = 1.2f * area + r.cost + l.cost;  // calculate_aabbs_kernel (lbvh.cu:452)
+    }
+    __stcg(a.costs + p, o.cost);
+    return o;
+}
+
+// Leaf-to-root walk from node x (carry c, summary s) through nodes whose
+// leaf ranges cross a CTA's edge: the second thread to arrive at a node
+// (GPU-scope acquire/release counter) completes it from the sibling's outputs.
+__device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Summary s) {
+    const uint32_t internal = a.n - 1;
+    uint32_t child = x;
+    uint32_t p = a.parents[x];
     for (uint32_t steps = 0; p != kNoParent; ++steps) {
         if (steps > internal || p >= internal) {
-            atomicOr(err, kErrCycle);
+            atomicOr(a.err, kErrCycle);
             return;
         }
-        // The parent's children and its own parent were written before this
-        // kernel: read them before the arrival so they are not on the
-        // dependent chain of the walk.
-        const uint32_t* pw = reinterpret_cast<const uint32_t*>(nodes + p);
+        // written before this kernel: read ahead of the arrival
+        const uint32_t* pw = reinterpret_cast<const uint32_t*>(a.nodes + p);
         const uint32_t L = __ldg(pw + 6), R = __ldg(pw + 7);
-        const uint32_t grand = __ldg(parents + p);
-        if (arrive(visits + p) == 0) return;
+        const uint32_t grand = __ldg(a.parents + p);
+        const uint32_t count = __ldg(a.counts + p);
+        if (arrive(a.visits + p) == 0) return;
         const bool from_left = (L == child);
         const uint32_t other = from_left ? R : L;
-        NodeView sib;  // the sibling's bounds only
+        Carry o;
         {
-            const uint32_t* sw = reinterpret_cast<const uint32_t*>(nodes + other);
+            const uint32_t* sw = reinterpret_cast<const uint32_t*>(a.nodes + other);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                sib.lo[k] = __uint_as_float(__ldcg(sw + k));
-                sib.hi[k] = __uint_as_float(__ldcg(sw + 3 + k));
+                o.lo[k] = __uint_as_float(__ldcg(sw + k));
+                o.hi[k] = __uint_as_float(__ldcg(sw + 3 + k));
             }
         }
-        const uint32_t scount = __ldcg(counts + other);
-        const float scost = __ldcg(costs + other);
-        // left/right views of the two children
-        const float* llo = from_left ? olo : sib.lo;
-        const float* lhi = from_left ? ohi : sib.hi;
-        const float* rlo = from_left ? sib.lo : olo;
-        const float* rhi = from_left ? sib.hi : ohi;
-        float lo[3], hi[3];
+        o.cost = __ldcg(a.costs + other);
+        c = from_left ? complete_node(a, p, L, R, count, c, o) : complete_node(a, p, L, R, count, o, c);
+        if (a.summary) {
+            const bool sleaf = other >= internal;
+            f3 v[3];
+            if (sleaf) {
+                const kr_vec3* pts = reinterpret_cast<const kr_vec3*>(a.tris);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {  // kr_aabb_expand(left, right)
-            lo[k] = kmin(kmin(llo[k], rlo[k]), rhi[k]);
-            hi[k] = kmax(kmax(lhi[k], rlo[k]), rhi[k]);
-        }
-        uint32_t w[9];
-        for (int k = 0; k < 3; ++k) { w[k] = __float_as_uint(lo[k]); w[3 + k] = __float_as_uint(hi[k]); }
-        w[6] = L;
-        w[7] = R;
-        w[8] = 0;
-        store_words(nodes, p, w, 6);
-        if (collapsed) store_words(collapsed, p, w, 9);
-        const uint32_t count = ocount + scount;
-        __stcg(counts + p, count);
-        const float area = box_area(lo, hi);
-        const float cl = from_left ? ocost : scost, cr = from_left ? scost : ocost;
-        float cost;
-        if (collapse) {
-            // bvh_mark_collapse_kernel (transforms.cu:111-133)
-            const float node_cost = ci * area + cl + cr;
-            const float leaf_cost = ct * area * static_cast<float>(count);
-            if (leaf_cost < node_cost && count <= kMaxLeafSize) {
-                cost = leaf_cost;
-                flags[p] = 1;
-                flags[L] = 1;
-                flags[R] = 1;
-                // nPrimitives = 0xFFFF; the axis byte and the pad of every node
-                // record are zero here, so the whole word is written
-                __stcg(reinterpret_cast<uint32_t*>(collapsed + L) + 8, kHidden);
-                __stcg(reinterpret_cast<uint32_t*>(collapsed + R) + 8, kHidden);
-            } else {
-                cost = node_cost;
+                for (int i = 0; i < 3; ++i) v[i] = load_vertex(pts, 3 * (other - internal) + i);
             }
-        } else {
-            cost = 1.2f * area + cr + cl;  // calculate_aabbs_kernel (lbvh.cu:452)
-        }
-        for (int k = 0; k < 3; ++k) { olo[k] = lo[k]; ohi[k] = hi[k]; }
-        ocount = count;
-        ocost = cost;
-        __stcg(costs + p, cost);
-        if (summary) {
-            Summary o;
-            if (other >= internal) slot_summary(tris, other - internal, o);
-            else load_summary(summary + 7 * static_cast<size_t>(other), o);
-            if (L == child) {
-                merge_right(own, o);
-            } else {
-                merge_right(o, own);
-                own = o;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+                Slab sib;
+                if (sleaf) {
+                    sib = leaf_slab(v, other - internal, k);
+                } else {
+                    const uint4 q = __ldcg(a.summary + 7 * static_cast<size_t>(other) + k);
+                    sib = Slab{__uint_as_float(q.x), __uint_as_float(q.y), q.z, q.w};
+                }
+                const Slab own = slab_of(s, k);
+                const Slab m = from_left ? merge_slab(own, sib) : merge_slab(sib, own);
+                set_slab(s, k, m);
+                store_slab(a.summary, p, k, m);
             }
-            store_summary(summary + 7 * static_cast<size_t>(p), own);
         }
         child = p;
         p = grand;
+    }
+}
+
+// Bottom-up pass, part 1 of 2: bounds, costs, collapse marks and summaries of
+// every node whose leaf range lies within one CTA's leaves (the primitive
+// counts of internal nodes are the key-range sizes the tree construction
+// wrote).
+//
+// CTA b takes sorted leaves [j0, jend).  A Karras node lies at one end of its
+// own leaf range, so an internal node whose range lies within these leaves
+// ("local") has its index in [j0, jend) too.  The local nodes are completed
+// in rounds separated by CTA barriers: a round's ready nodes sit in a queue
+// and go to its first threads; a completed node's parent joins the next
+// round's queue once both children are done.  Children are read from shared
+// memory, and the outputs are written at the end as contiguous runs.  The
+// leaves and local nodes whose parents are not local go to a list for part 2.
+__global__ void __launch_bounds__(kThreads, 3) fused_up_local_kernel(UpArgs a, uint32_t* frontier,
+                                                                     uint32_t* frontier_count) {
+    extern __shared__ __align__(16) unsigned char fused_smem[];
+    LocalSmem& sm = *reinterpret_cast<LocalSmem*>(fused_smem);
+    const uint32_t t = threadIdx.x;
+    const uint32_t j0 = blockIdx.x * kThreads;
+    const uint32_t jend = min(j0 + kThreads, a.n);
+    const uint32_t m = jend - j0;
+    const uint32_t internal = a.n - 1;
+    const uint32_t mi = j0 < internal ? min(jend, internal) - j0 : 0u;  // internal node indices in [j0, jend)
+    const bool with_summary = a.summary != nullptr;
+    // leaf cost: ct * area in the collapse (transforms.cu:97), 1 * area in the LBVH (lbvh.cu:427)
+    const float leaf_ct = a.flags ? a.ct : 1.0f;
+    uint32_t leaf_parent = kNoParent;
+    if (t < m) {
+        const uint32_t leaf = internal + j0 + t;
+        leaf_parent = a.parents[leaf];
+        const NodeView lf = load_node(a.nodes, leaf);
+        Carry c;
+        for (int k = 0; k < 3; ++k) { c.lo[k] = lf.lo[k]; c.hi[k] = lf.hi[k]; }
+        c.cost = leaf_ct * box_area(lf.lo, lf.hi);
+        __stcg(a.costs + leaf, c.cost);
+        __stcg(a.counts + leaf, 1u);
+        put_carry(sm.lslot, t, c);
+        if (with_summary) {
+            const kr_vec3* pts = reinterpret_cast<const kr_vec3*>(a.tris);
+            f3 v[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) v[i] = load_vertex(pts, 3 * (j0 + t) + i);
+            uint32_t picks = 0;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+                const Slab sl = leaf_slab(v, j0 + t, k);
+                sm.lslot[7 + 2 * k][t] = __float_as_uint(sl.lo);
+                sm.lslot[8 + 2 * k][t] = __float_as_uint(sl.hi);
+                picks |= ((sl.ilo - 3 * (j0 + t)) | ((sl.ihi - 3 * (j0 + t)) << 2)) << (4 * k);
+            }
+            sm.lslot[21][t] = picks;
+        }
+    }
+    const uint32_t p = j0 + t;
+    bool mine = false;
+    bool bad = false;
+    uint32_t parent = kNoParent;
+    if (t < mi) {
+        const uint32_t* pw = reinterpret_cast<const uint32_t*>(a.nodes + p);
+        const uint32_t L = __ldg(pw + 6), R = __ldg(pw + 7);
+        const uint32_t f = __ldg(a.first + p), count = __ldg(a.counts + p);
+        parent = __ldg(a.parents + p);
+        if (f >= j0 && f + count <= jend) {
+            const bool lleaf = L >= internal, rleaf = R >= internal;
+            const uint32_t lq = (lleaf ? L - internal : L) - j0, rq = (rleaf ? R - internal : R) - j0;
+            if (lq < m && rq < m) {
+                mine = true;
+                sm.kid[0][t] = static_cast<uint16_t>(lq | (lleaf ? kLeafKid : 0u));
+                sm.kid[1][t] = static_cast<uint16_t>(rq | (rleaf ? kLeafKid : 0u));
+                sm.cnt[t] = static_cast<uint16_t>(count);
+                sm.deg[t] = (lleaf ? 0u : 1u) + (rleaf ? 0u : 1u);
+            } else {
+                bad = true;  // a child outside its parent's range
+            }
+        }
+    }
+    sm.local[t] = mine;
+    sm.iflag[t] = 0;
+    sm.lflag[t] = 0;
+    sm.hidden[t] = 0;
+    if (t < 3) sm.qn[t] = 0;
+    if (t == 0) sm.nfront = 0;
+    __syncthreads();
+    const auto is_local = [&](uint32_t x) { return x != kNoParent && x - j0 < m && sm.local[x - j0]; };
+    if (mine) {
+        sm.up[t] = is_local(parent) ? static_cast<uint16_t>(parent - j0) : kNotLocal;
+        if (sm.deg[t] == 0) sm.queue[0][atomicAdd(&sm.qn[0], 1u)] = static_cast<uint8_t>(t);
+    }
+    __syncthreads();
+    // Rounds.  Counters rotate over three slots: a round reads one, appends
+    // to the next and clears the one read the round before.
+    for (uint32_t r = 0;; ++r) {
+        const uint32_t cur = r % 3, nxt = (r + 1) % 3, old = (r + 2) % 3;
+        const uint32_t K = sm.qn[cur];
+        if (K == 0) break;
+        if (r > m) {  // unreachable for a well-formed tree
+            bad = true;
+            break;
+        }
+        if (t == 0) sm.qn[old] = 0;
+        if (t < K) {
+            const uint32_t q = sm.queue[cur][t];
+            const uint32_t kl = sm.kid[0][q], kr = sm.kid[1][q];
+            const bool lleaf = kl & kLeafKid, rleaf = kr & kLeafKid;
+            const uint32_t lq = kl & 0xffu, rq = kr & 0xffu;
+            const uint32_t count = sm.cnt[q];
+            const Carry l = get_carry(lleaf ? sm.lslot : sm.islot, lq);
+            const Carry rc = get_carry(rleaf ? sm.lslot : sm.islot, rq);
+            Carry o;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {  // kr_aabb_expand(left, right)
+                o.lo[k] = kmin(kmin(l.lo[k], rc.lo[k]), rc.hi[k]);
+                o.hi[k] = kmax(kmax(l.hi[k], rc.lo[k]), rc.hi[k]);
+            }
+            const float area = box_area(o.lo, o.hi);
+            if (a.flags) {
+                // bvh_mark_collapse_kernel (transforms.cu:111-133)
+                const float node_cost = a.ci * area + l.cost + rc.cost;
+                const float leaf_cost = a.ct * area * static_cast<float>(count);
+                if (leaf_cost < node_cost && count <= kMaxLeafSize) {
+                    o.cost = leaf_cost;
+                    sm.iflag[q] = 1;
+                    // collapsed children: marked, and nPrimitives = 0xFFFF (axis byte and pad are zero)
+                    if (lleaf) {
+                        sm.lflag[lq] = 1;
+                        __stcg(reinterpret_cast<uint32_t*>(a.collapsed + internal + j0 + lq) + 8, kHidden);
+                    } else {
+                        sm.iflag[lq] = 1;
+                        sm.hidden[lq] = 1;
+                    }
+                    if (rleaf) {
+                        sm.lflag[rq] = 1;
+                        __stcg(reinterpret_cast<uint32_t*>(a.collapsed + internal + j0 + rq) + 8, kHidden);
+                    } else {
+                        sm.iflag[rq] = 1;
+                        sm.hidden[rq] = 1;
+                    }
+                } else {
+                    o.cost = node_cost;
+                }
+            } else {
+                o.cost = 1.2f * area + rc.cost + l.cost;  // calculate_aabbs_kernel (lbvh.cu:452)
+            }
+            put_carry(sm.islot, q, o);
+            if (with_summary) {
+#pragma unroll
+                for (int k = 0; k < 7; ++k) {
+                    const Slab ls = lleaf ? get_leaf_slab(sm, lq, j0 + lq, k) : get_slab(sm.islot, lq, k);
+                    const Slab rs = rleaf ? get_leaf_slab(sm, rq, j0 + rq, k) : get_slab(sm.islot, rq, k);
+                    put_slab(sm.islot, q, k, merge_slab(ls, rs));
+                }
+            }
+            const uint32_t u = sm.up[q];
+            if (u != kNotLocal && atomicSub(&sm.deg[u], 1u) == 1u)
+                sm.queue[nxt][atomicAdd(&sm.qn[nxt], 1u)] = static_cast<uint8_t>(u);
+        }
+        __syncthreads();
+    }
+    if (bad) atomicOr(a.err, kErrBadInput);
+    // Outputs of the local nodes, as contiguous runs over [j0, j0 + mi).
+    {
+        uint32_t* nw = reinterpret_cast<uint32_t*>(a.nodes + j0);
+        uint32_t* cw = a.collapsed ? reinterpret_cast<uint32_t*>(a.collapsed + j0) : nullptr;
+        for (uint32_t w = t; w < 9 * mi; w += kThreads) {
+            const uint32_t q = w / 9, k = w - 9 * q;
+            if (!sm.local[q]) continue;
+            uint32_t v;
+            if (k < 6) {
+                v = sm.islot[k][q];
+                __stcg(nw + w, v);  // words 6..8 hold the children and 0 already
+            } else if (k < 8) {
+                const uint32_t kd = sm.kid[k - 6][q];
+                v = (kd & kLeafKid) ? internal + j0 + (kd & 0xffu) : j0 + kd;
+            } else {
+                v = sm.hidden[q] ? kHidden : 0u;
+            }
+            if (cw) __stcg(cw + w, v);
+        }
+        for (uint32_t q = t; q < mi; q += kThreads)
+            if (sm.local[q]) __stcg(a.costs + j0 + q, __uint_as_float(sm.islot[6][q]));
+        if (with_summary) {
+            uint4* sw = a.summary + 7 * static_cast<size_t>(j0);
+            for (uint32_t w = t; w < 7 * mi; w += kThreads) {
+                const uint32_t q = w / 7, k = w - 7 * q;
+                if (sm.local[q])
+                    __stcg(sw + w, make_uint4(sm.islot[7 + 4 * k][q], sm.islot[8 + 4 * k][q], sm.islot[9 + 4 * k][q],
+                                              sm.islot[10 + 4 * k][q]));
+            }
+        }
+        if (a.flags) {
+            for (uint32_t q = t; q < mi; q += kThreads)
+                if (sm.local[q]) a.flags[j0 + q] = sm.iflag[q];
+            for (uint32_t q = t; q < m; q += kThreads) a.flags[internal + j0 + q] = sm.lflag[q];
+        }
+    }
+    // Walks for part 2: this thread's leaf and its local node, where their
+    // parents are not local.
+    const bool leaf_walk = !bad && t < m && leaf_parent != kNoParent && !is_local(leaf_parent);
+    const bool node_walk = !bad && mine && parent != kNoParent && sm.up[t] == kNotLocal;
+    const uint32_t nf = static_cast<uint32_t>(leaf_walk) + static_cast<uint32_t>(node_walk);
+    const uint32_t at = nf ? atomicAdd(&sm.nfront, nf) : 0u;
+    __syncthreads();
+    if (t == 0) sm.front_base = sm.nfront ? atomicAdd(frontier_count, sm.nfront) : 0u;
+    __syncthreads();
+    if (leaf_walk) frontier[sm.front_base + at] = internal + j0 + t;
+    if (node_walk) frontier[sm.front_base + at + (leaf_walk ? 1 : 0)] = p;
+}
+
+// Bottom-up pass, part 2 of 2: the walks from the listed nodes complete the
+// nodes whose leaf ranges cross a CTA's edge.  Part 1 has finished, so a
+// listed node's outputs are in memory.
+__global__ void __launch_bounds__(kThreads) fused_up_cross_kernel(UpArgs a, const uint32_t* frontier,
+                                                                  const uint32_t* frontier_count) {
+    const uint32_t total = *frontier_count;
+    const uint32_t internal = a.n - 1;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const uint32_t x = frontier[i];
+        Carry c;
+        {
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(a.nodes + x);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                c.lo[k] = __uint_as_float(__ldcg(w + k));
+                c.hi[k] = __uint_as_float(__ldcg(w + 3 + k));
+            }
+        }
+        c.cost = __ldcg(a.costs + x);
+        Summary s;
+        if (a.summary) {
+            if (x >= internal) {
+                const kr_vec3* pts = reinterpret_cast<const kr_vec3*>(a.tris);
+                f3 v[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) v[k] = load_vertex(pts, 3 * (x - internal) + k);
+#pragma unroll
+                for (int k = 0; k < 7; ++k) set_slab(s, k, leaf_slab(v, x - internal, k));
+            } else {
+                load_summary(a.summary + 7 * static_cast<size_t>(x), s);
+            }
+        }
+        walk_up(a, x, c, s);
     }
 }
 
@@ -309,11 +676,29 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(const uint32_t* sizes,
     cw[8] = (cw[8] & 0xffff0000u) | pos;
 }
 
+// The bottom-up pass needs more than the default 48 KB of dynamic shared
+// memory; the attribute is set once per device.
+kr_error configure_fused_up() {
+    static std::mutex mu;
+    static uint64_t done = 0;
+    int dev = 0;
+    OBVH_TRY_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64 && ((done >> dev) & 1)) return kr_success;
+    OBVH_TRY_CUDA(cudaFuncSetAttribute(fused_up_local_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(kFusedSmemBytes)));
+    // room for three CTAs per SM
+    OBVH_TRY_CUDA(cudaFuncSetAttribute(fused_up_local_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    if (dev < 64) done |= 1ull << dev;
+    return kr_success;
+}
+
 // ---------------------------------------------------------------------------
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
 struct Layout {
-    size_t lbvh, ctl, first, tris, summary, flags, cand, nunits, ustart, keys, sizes, offsets, scan, total;
+    size_t lbvh, ctl, first, tris, summary, flags, cand, nunits, ustart, keys, sizes, offsets, scan, frontier, chains,
+        chain_counts, total;
 };
 
 Layout layout(uint32_t n) {
@@ -334,6 +719,9 @@ Layout layout(uint32_t n) {
     L.sizes = o;    o += align256(4 * nn);
     L.offsets = o;  o += align256(4 * nn);
     L.scan = o;     o += align256(scan_temp_bytes(nn));
+    L.frontier = o; o += align256(4 * nn);
+    L.chains = o;   o += align256(obbtree::chain_bytes(n));
+    L.chain_counts = o; o += align256(obbtree::chain_count_bytes(n));
     L.total = o;
     return L;
 }
@@ -383,14 +771,27 @@ kr_error enqueue(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32
                                                     want_obbs ? obbs : nullptr, xfs);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
-    OBVH_TRY(lbvh::enqueue_karras(c.codes, n, nodes, parents, first, s));
+    OBVH_TRY(lbvh::enqueue_karras(c.codes, n, nodes, parents, first, counts, s));
     if (internal > 0) OBVH_TRY_CUDA(cudaMemsetAsync(c.visits, 0, 4ull * internal, s));
     if (want_collapse) OBVH_TRY_CUDA(cudaMemsetAsync(cflags, 0, nn, s));
+    OBVH_TRY(configure_fused_up());
     {
-        ProfScope prof_scope_("fused_up_kernel", s);
-        fused_up_kernel<<<gn, kThreads, 0, s>>>(nodes, want_collapse ? collapsed : nullptr, parents, tris, n, counts,
-                                                costs, want_collapse ? cflags : nullptr, ci, ct,
-                                                want_obbs ? summary : nullptr, c.visits, &ctl->error);
+        UpArgs a{nodes, want_collapse ? collapsed : nullptr, parents, first, tris, n, counts, costs,
+                 want_collapse ? cflags : nullptr, ci, ct, want_obbs ? summary : nullptr, c.visits, &ctl->error};
+        uint32_t* frontier = reinterpret_cast<uint32_t*>(ws + L.frontier);
+        {
+            ProfScope prof_scope_("fused_up_local_kernel", s);
+            fused_up_local_kernel<<<gn, kThreads, kFusedSmemBytes, s>>>(a, frontier, &ctl->frontier);
+        }
+        OBVH_TRY_CUDA(cudaGetLastError());
+        // at most one walk per leaf and per internal node; most of the grid
+        // finds nothing to do, so it is capped at a few CTAs per SM
+        const unsigned cap = 8u * static_cast<unsigned>(device_info().sm_count);
+        const unsigned gx = (nn + kThreads - 1) / kThreads;
+        {
+            ProfScope prof_scope_("fused_up_cross_kernel", s);
+            fused_up_cross_kernel<<<gx < cap ? gx : cap, kThreads, 0, s>>>(a, frontier, &ctl->frontier);
+        }
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     if (want_obbs && internal > 0) {
@@ -407,6 +808,9 @@ kr_error enqueue(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32
         fb.scan = ws + L.scan;
         fb.err = &ctl->error;
         fb.total_units = &ctl->total_units;
+        fb.parents = parents;
+        fb.chains = reinterpret_cast<uint32_t*>(ws + L.chains);
+        fb.chain_counts = reinterpret_cast<uint32_t*>(ws + L.chain_counts);
         OBVH_TRY(obbtree::enqueue_frames(fb, internal, obbs, xfs, s));
     }
     if (want_collapse) {

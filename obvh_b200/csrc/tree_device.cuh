@@ -295,27 +295,42 @@ __device__ __forceinline__ void extent_proj(const Points14& Q, f3 d, float& lo, 
     }
 }
 
-// One candidate frame: normal n and its three edges, whose extents (elo/ehi)
-// are computed once per node (an edge is shared by up to three frames).
-__device__ __forceinline__ void score_frames(const Points14& P, f3 n, const f3* E, const float* ELO, const float* EHI,
-                                             const int* ids, f3* b, f3& blen, f3& bmid, float& best) {
+// An edge direction of the candidate frames with its extent over the 14
+// points (computed once per node: an edge is shared by up to three frames).
+struct EdgeX {
+    f3 d;
+    float lo, hi;
+};
+
+__device__ __forceinline__ EdgeX edge_x(const Points14& P, f3 d) {
+    EdgeX e;
+    e.d = d;
+    extent_proj(P, d, e.lo, e.hi);
+    return e;
+}
+
+// One candidate frame: normal n and its three edges in the reference's order.
+// Each edge e spans a box with n and m = e x n; the smallest half area wins,
+// ties to the earlier (frame, edge).
+__device__ __forceinline__ void score_frame(const Points14& P, f3 n, const EdgeX& x0, const EdgeX& x1,
+                                            const EdgeX& x2, f3* b, f3& blen, f3& bmid, float& best) {
     float nlo, nhi;
     extent_proj(P, n, nlo, nhi);
     const float dy = nhi - nlo;
+    const EdgeX* xs[3] = {&x0, &x1, &x2};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const f3 e = E[ids[k]];
-        const f3 m = cross3(e, n);
-        const float elo = ELO[ids[k]], ehi = EHI[ids[k]];
+        const EdgeX& x = *xs[k];
+        const f3 m = cross3(x.d, n);
         float mlo, mhi;
         extent_proj(P, m, mlo, mhi);
-        const f3 dlen = mk3(ehi - elo, dy, mhi - mlo);
+        const f3 dlen = mk3(x.hi - x.lo, dy, mhi - mlo);
         const float q = half_area3(dlen);
         if (q < best) {
             best = q;
-            bmid = mk3(ehi, nhi, mhi);
-            blen = mk3(elo, nlo, mlo);
-            b[0] = e; b[1] = n; b[2] = m;
+            bmid = mk3(x.hi, nhi, mhi);
+            blen = mk3(x.lo, nlo, mlo);
+            b[0] = x.d; b[1] = n; b[2] = m;
         }
     }
 }
@@ -339,25 +354,28 @@ __device__ inline Candidate node_candidate(const f3* P, const Summary& s) {
         float d = len2_3(sub3(P[2 * k + 1], P[2 * k]));
         if (d > far) { far = d; at = k; }
     }
-    const f3 p0 = P[2 * at], p1 = P[2 * at + 1];
+    f3 p0 = P[0], p1 = P[1];
+#pragma unroll
+    for (int k = 1; k < 7; ++k)
+        if (at == k) { p0 = P[2 * k]; p1 = P[2 * k + 1]; }
     if (len2_3(sub3(p1, p0)) < eps) return stale;
     const f3 e0 = unit3(sub3(p0, p1));
     const float l2 = len2_3(e0);
-    int fi = 0;
+    f3 p2;
     float fd;
     {
         f3 u = sub3(P[0], p0);
         float t = dot3(e0, u);
         fd = len2_3(u) - t * t / l2;
+        p2 = P[0];
 #pragma unroll
         for (int i = 1; i < 14; ++i) {
             u = sub3(P[i], p0);
             t = dot3(e0, u);
             float d = len2_3(u) - t * t / l2;
-            if (d > fd) { fd = d; fi = i; }
+            if (d > fd) { fd = d; p2 = P[i]; }
         }
     }
-    const f3 p2 = P[fi];
     if (fd < eps) return stale;
     const f3 e1 = unit3(sub3(p1, p2));
     const f3 e2 = unit3(sub3(p2, p0));
@@ -373,40 +391,33 @@ __device__ inline Candidate node_candidate(const f3* P, const Summary& s) {
     }
     const float tri = dot3(p0, n);
     const bool up = qhi - eps > tri, down = qlo + eps < tri;
-    // A flat set returns before the reference's scores are used (:737-743),
-    // so the test can come first and all frames go through one scorer loop
-    // in the reference's order: base triangle, upper faces, lower faces.
     if (!up && !down) return stale;
-    // Edge table: base triangle e0..e2, upper faces f0..f2, lower faces g0..g2.
-    f3 E[9];
-    float ELO[9], EHI[9];
-    E[0] = e0; E[1] = e1; E[2] = e2;
-    f3 tn[7];
-    int ids[7][3];
-    int nt = 0;
-    tn[nt] = n; ids[nt][0] = 0; ids[nt][1] = 1; ids[nt][2] = 2; ++nt;
-    if (up) {
-        const f3 f0 = unit3(sub3(q0, p0)), f1 = unit3(sub3(q0, p1)), f2 = unit3(sub3(q0, p2));
-        E[3] = f0; E[4] = f1; E[5] = f2;
-        tn[nt] = unit3(cross3(f1, e0)); ids[nt][0] = 0; ids[nt][1] = 4; ids[nt][2] = 3; ++nt;
-        tn[nt] = unit3(cross3(f2, e1)); ids[nt][0] = 1; ids[nt][1] = 5; ids[nt][2] = 4; ++nt;
-        tn[nt] = unit3(cross3(f0, e2)); ids[nt][0] = 2; ids[nt][1] = 3; ids[nt][2] = 5; ++nt;
-    }
-    if (down) {
-        const f3 g0 = unit3(sub3(q1, p0)), g1 = unit3(sub3(q1, p1)), g2 = unit3(sub3(q1, p2));
-        E[6] = g0; E[7] = g1; E[8] = g2;
-        tn[nt] = unit3(cross3(g1, e0)); ids[nt][0] = 0; ids[nt][1] = 7; ids[nt][2] = 6; ++nt;
-        tn[nt] = unit3(cross3(g2, e1)); ids[nt][0] = 1; ids[nt][1] = 8; ids[nt][2] = 7; ++nt;
-        tn[nt] = unit3(cross3(g0, e2)); ids[nt][0] = 2; ids[nt][1] = 6; ids[nt][2] = 8; ++nt;
-    }
+    // A flat set returns before the reference's scores are used (:737-743),
+    // so the test can come first and the frames are scored in the reference's
+    // order: the base triangle (edges e0 e1 e2), then the three faces to the
+    // upper apex q0, then the three to the lower apex q1.  Face r of an apex
+    // (r = 0, 1, 2) has the base edge e_r and the apex edges a_{r+1}, a_r
+    // (a_i = unit(apex - p_i), indices mod 3) and the normal unit(a_{r+1} x e_r).
     const Points14 Q = pack14(P);
+    EdgeX x0 = edge_x(Q, e0), x1 = edge_x(Q, e1), x2 = edge_x(Q, e2);
+    score_frame(Q, n, x0, x1, x2, b, blen, bmid, best);
 #pragma unroll 1
-    for (int k = 0; k < 9; ++k) {
-        if ((k >= 3 && k < 6 && !up) || (k >= 6 && !down)) continue;
-        extent_proj(Q, E[k], ELO[k], EHI[k]);
+    for (int side = 0; side < 2; ++side) {
+        if (side == 0 ? !up : !down) continue;
+        const f3 apex = side == 0 ? q0 : q1;
+        EdgeX a0 = edge_x(Q, unit3(sub3(apex, p0)));
+        EdgeX a1 = edge_x(Q, unit3(sub3(apex, p1)));
+        EdgeX a2 = edge_x(Q, unit3(sub3(apex, p2)));
+#pragma unroll 1
+        for (int r = 0; r < 3; ++r) {
+            score_frame(Q, unit3(cross3(a1.d, x0.d)), x0, a1, a0, b, blen, bmid, best);
+            // rotate to face r + 1; after three faces x0 x1 x2 are back in order
+            const EdgeX t = x0;
+            x0 = x1; x1 = x2; x2 = t;
+            const EdgeX u = a0;
+            a0 = a1; a1 = a2; a2 = u;
+        }
     }
-#pragma unroll 1
-    for (int t = 0; t < nt; ++t) score_frames(Q, tn[t], E, ELO, EHI, ids[t], b, blen, bmid, best);
     c.b0 = b[0]; c.b1 = b[1]; c.b2 = b[2];
     c.lo = blen;
     c.hi = bmid;
