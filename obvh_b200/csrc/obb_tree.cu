@@ -259,15 +259,15 @@ __global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* sum
 }
 
 // The box of an internal node from its final extents (finalize_obbs_kernel).
+// The OBB if its half area is strictly smaller than the AABB's, else the AABB
+// (arguments selected first, so that a warp whose lanes differ makes one call).
 __device__ __forceinline__ void finalize_node(const Cand& c, f3 lo, f3 hi, kr_obb3* obb, kr_mat4* xf) {
     const float aq = half_area3(mk3(c.ahi[0] - c.alo[0], c.ahi[1] - c.alo[1], c.ahi[2] - c.alo[2]));
     const float oq = half_area3(sub3(hi, lo));
-    if (oq < aq)
-        write_box(obb, xf, mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
-                  mk3(c.ax[6], c.ax[7], c.ax[8]), lo, hi);
-    else
-        write_box(obb, xf, mk3(1, 0, 0), mk3(0, 1, 0), mk3(0, 0, 1), mk3(c.alo[0], c.alo[1], c.alo[2]),
-                  mk3(c.ahi[0], c.ahi[1], c.ahi[2]));
+    const bool o = oq < aq;
+    write_box(obb, xf, o ? mk3(c.ax[0], c.ax[1], c.ax[2]) : mk3(1, 0, 0),
+              o ? mk3(c.ax[3], c.ax[4], c.ax[5]) : mk3(0, 1, 0), o ? mk3(c.ax[6], c.ax[7], c.ax[8]) : mk3(0, 0, 1),
+              o ? lo : mk3(c.alo[0], c.alo[1], c.alo[2]), o ? hi : mk3(c.ahi[0], c.ahi[1], c.ahi[2]));
 }
 
 __device__ __forceinline__ Cand load_cand(const Cand* cand, uint32_t a) {

@@ -20,7 +20,6 @@
 
 #include <cstddef>
 #include <cstdint>
-#include <mutex>
 
 #include "device_common.cuh"
 #include "lbvh_host.h"
@@ -194,18 +193,21 @@ __device__ __forceinline__ Slab leaf_slab(const f3* v, uint32_t j, int k) {
     return o;
 }
 
-// Shared memory of the CTA-local part of the bottom-up pass.  Per internal
-// node: bounds (6), cost (1) and the 7-direction summary (28 words); per leaf:
-// bounds, cost, the 14 slab values and the vertex choices (2 bits each) in one
-// word.  Word-major ([word][node]) so that a warp's accesses spread over banks.
-constexpr int kSlotWords = 35;
-constexpr int kLeafWords = 22;
+// Shared memory of the CTA-local part of the bottom-up pass, in rows of
+// kRow words (one word per node; the odd row length spreads a node's words
+// over the banks).  Internal node rows: bounds (6), cost, the 14 slab values,
+// then the 14 slab vertices as 16-bit offsets from 3 * j0, two per word (7).
+// Leaf rows: bounds (6) and the three vertices (9); a leaf's cost and slabs
+// are recomputed from them.
+constexpr uint32_t kRow = kThreads + 1;
+constexpr int kSlotRows = 28;
+constexpr int kLeafRows = 15;
 constexpr uint16_t kLeafKid = 0x8000u;  // child encoding: leaf j0 + q, else internal node j0 + q
 constexpr uint16_t kNotLocal = 0xffffu;
 
 struct LocalSmem {
-    uint32_t islot[kSlotWords][kThreads];
-    uint32_t lslot[kLeafWords][kThreads];
+    uint32_t islot[kSlotRows * kRow];
+    uint32_t lslot[kLeafRows * kRow];
     uint32_t deg[kThreads];     // children of local node j0 + q not completed yet
     uint16_t kid[2][kThreads];  // its children
     uint16_t cnt[kThreads];     // its primitive count
@@ -217,43 +219,49 @@ struct LocalSmem {
 };
 constexpr size_t kFusedSmemBytes = sizeof(LocalSmem);
 
-__device__ __forceinline__ void put_carry(uint32_t (*slots)[kThreads], uint32_t q, const Carry& c) {
+__device__ __forceinline__ void put_carry(uint32_t* slots, uint32_t q, const Carry& c) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        slots[k][q] = __float_as_uint(c.lo[k]);
-        slots[3 + k][q] = __float_as_uint(c.hi[k]);
+        slots[k * kRow + q] = __float_as_uint(c.lo[k]);
+        slots[(3 + k) * kRow + q] = __float_as_uint(c.hi[k]);
     }
-    slots[6][q] = __float_as_uint(c.cost);
+    slots[6 * kRow + q] = __float_as_uint(c.cost);
 }
 
-__device__ __forceinline__ Carry get_carry(const uint32_t (*slots)[kThreads], uint32_t q) {
-    Carry c;
+__device__ __forceinline__ void get_bounds(const uint32_t* slots, uint32_t q, Carry& c) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        c.lo[k] = __uint_as_float(slots[k][q]);
-        c.hi[k] = __uint_as_float(slots[3 + k][q]);
+        c.lo[k] = __uint_as_float(slots[k * kRow + q]);
+        c.hi[k] = __uint_as_float(slots[(3 + k) * kRow + q]);
     }
-    c.cost = __uint_as_float(slots[6][q]);
+}
+
+// carry of internal node j0 + q / of leaf j0 + q (its cost: leaf_ct * area)
+__device__ __forceinline__ Carry get_carry(const LocalSmem& sm, uint32_t q, bool leaf, float leaf_ct) {
+    Carry c;
+    get_bounds(leaf ? sm.lslot : sm.islot, q, c);
+    c.cost = leaf ? leaf_ct * box_area(c.lo, c.hi) : __uint_as_float(sm.islot[6 * kRow + q]);
     return c;
 }
 
-__device__ __forceinline__ void put_slab(uint32_t (*slots)[kThreads], uint32_t q, int k, const Slab& v) {
-    slots[7 + 4 * k][q] = __float_as_uint(v.lo);
-    slots[8 + 4 * k][q] = __float_as_uint(v.hi);
-    slots[9 + 4 * k][q] = v.ilo;
-    slots[10 + 4 * k][q] = v.ihi;
+__device__ __forceinline__ void put_slab(uint32_t* islot, uint32_t q, int k, const Slab& v, uint32_t base3) {
+    islot[(7 + 2 * k) * kRow + q] = __float_as_uint(v.lo);
+    islot[(8 + 2 * k) * kRow + q] = __float_as_uint(v.hi);
+    islot[(21 + k) * kRow + q] = (v.ilo - base3) | ((v.ihi - base3) << 16);
 }
 
-__device__ __forceinline__ Slab get_slab(const uint32_t (*slots)[kThreads], uint32_t q, int k) {
-    return Slab{__uint_as_float(slots[7 + 4 * k][q]), __uint_as_float(slots[8 + 4 * k][q]), slots[9 + 4 * k][q],
-                slots[10 + 4 * k][q]};
+__device__ __forceinline__ Slab get_slab(const uint32_t* islot, uint32_t q, int k, uint32_t base3) {
+    const uint32_t ids = islot[(21 + k) * kRow + q];
+    return Slab{__uint_as_float(islot[(7 + 2 * k) * kRow + q]), __uint_as_float(islot[(8 + 2 * k) * kRow + q]),
+                base3 + (ids & 0xffffu), base3 + (ids >> 16)};
 }
 
-// Slab k of leaf j0 + q (vertex slots 3j .. 3j+2).
-__device__ __forceinline__ Slab get_leaf_slab(const LocalSmem& sm, uint32_t q, uint32_t j, int k) {
-    const uint32_t pick = sm.lslot[21][q] >> (4 * k);
-    return Slab{__uint_as_float(sm.lslot[7 + 2 * k][q]), __uint_as_float(sm.lslot[8 + 2 * k][q]), 3 * j + (pick & 3u),
-                3 * j + ((pick >> 2) & 3u)};
+// The vertices of leaf j0 + q, for its slabs (leaf_slab).
+__device__ __forceinline__ void leaf_vertices(const LocalSmem& sm, uint32_t q, f3* v) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        v[i] = mk3(__uint_as_float(sm.lslot[(6 + 3 * i) * kRow + q]), __uint_as_float(sm.lslot[(7 + 3 * i) * kRow + q]),
+                   __uint_as_float(sm.lslot[(8 + 3 * i) * kRow + q]));
 }
 
 __device__ __forceinline__ void store_slab(uint4* summary, uint32_t p, int k, const Slab& v) {
@@ -391,7 +399,7 @@ __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Su
 // round's queue once both children are done.  Children are read from shared
 // memory, and the outputs are written at the end as contiguous runs.  The
 // leaves and local nodes whose parents are not local go to a list for part 2.
-__global__ void __launch_bounds__(kThreads, 3) fused_up_local_kernel(UpArgs a, uint32_t* frontier,
+__global__ void __launch_bounds__(kThreads, 4) fused_up_local_kernel(UpArgs a, uint32_t* frontier,
                                                                      uint32_t* frontier_count) {
     extern __shared__ __align__(16) unsigned char fused_smem[];
     LocalSmem& sm = *reinterpret_cast<LocalSmem*>(fused_smem);
@@ -404,33 +412,29 @@ __global__ void __launch_bounds__(kThreads, 3) fused_up_local_kernel(UpArgs a, u
     const bool with_summary = a.summary != nullptr;
     // leaf cost: ct * area in the collapse (transforms.cu:97), 1 * area in the LBVH (lbvh.cu:427)
     const float leaf_ct = a.flags ? a.ct : 1.0f;
-    uint32_t leaf_parent = kNoParent;
-    if (t < m) {
-        const uint32_t leaf = internal + j0 + t;
-        leaf_parent = a.parents[leaf];
-        const NodeView lf = load_node(a.nodes, leaf);
-        Carry c;
-        for (int k = 0; k < 3; ++k) { c.lo[k] = lf.lo[k]; c.hi[k] = lf.hi[k]; }
-        c.cost = leaf_ct * box_area(lf.lo, lf.hi);
-        __stcg(a.costs + leaf, c.cost);
-        __stcg(a.counts + leaf, 1u);
-        put_carry(sm.lslot, t, c);
-        if (with_summary) {
-            const kr_vec3* pts = reinterpret_cast<const kr_vec3*>(a.tris);
-            f3 v[3];
+    // The CTA's leaf records and triangles are contiguous runs of 9 words
+    // each: read word by word across the CTA (coalesced) into the leaf rows,
+    // every load in flight before the first store.
+    {
+        const uint32_t* nw = reinterpret_cast<const uint32_t*>(a.nodes + internal + j0);
+        const uint32_t* tw = reinterpret_cast<const uint32_t*>(a.tris + 9 * static_cast<size_t>(j0));
+        uint32_t bw[9], vw[9];
 #pragma unroll
-            for (int i = 0; i < 3; ++i) v[i] = load_vertex(pts, 3 * (j0 + t) + i);
-            uint32_t picks = 0;
+        for (int r = 0; r < 9; ++r) {
+            const uint32_t w = t + r * kThreads;
+            bw[r] = w < 9 * m ? __ldcg(nw + w) : 0u;
+            vw[r] = with_summary && w < 9 * m ? __ldg(tw + w) : 0u;
+        }
 #pragma unroll
-            for (int k = 0; k < 7; ++k) {
-                const Slab sl = leaf_slab(v, j0 + t, k);
-                sm.lslot[7 + 2 * k][t] = __float_as_uint(sl.lo);
-                sm.lslot[8 + 2 * k][t] = __float_as_uint(sl.hi);
-                picks |= ((sl.ilo - 3 * (j0 + t)) | ((sl.ihi - 3 * (j0 + t)) << 2)) << (4 * k);
-            }
-            sm.lslot[21][t] = picks;
+        for (int r = 0; r < 9; ++r) {
+            const uint32_t w = t + r * kThreads;
+            if (w >= 9 * m) continue;
+            const uint32_t q = w / 9, k = w - 9 * q;
+            if (k < 6) sm.lslot[k * kRow + q] = bw[r];
+            if (with_summary) sm.lslot[(6 + k) * kRow + q] = vw[r];
         }
     }
+    const uint32_t leaf_parent = t < m ? a.parents[internal + j0 + t] : kNoParent;
     const uint32_t p = j0 + t;
     bool mine = false;
     bool bad = false;
@@ -461,6 +465,12 @@ __global__ void __launch_bounds__(kThreads, 3) fused_up_local_kernel(UpArgs a, u
     if (t < 3) sm.qn[t] = 0;
     if (t == 0) sm.nfront = 0;
     __syncthreads();
+    if (t < m) {
+        Carry c;
+        get_bounds(sm.lslot, t, c);
+        __stcg(a.costs + internal + j0 + t, leaf_ct * box_area(c.lo, c.hi));
+        __stcg(a.counts + internal + j0 + t, 1u);
+    }
     const auto is_local = [&](uint32_t x) { return x != kNoParent && x - j0 < m && sm.local[x - j0]; };
     if (mine) {
         sm.up[t] = is_local(parent) ? static_cast<uint16_t>(parent - j0) : kNotLocal;
@@ -484,8 +494,8 @@ __global__ void __launch_bounds__(kThreads, 3) fused_up_local_kernel(UpArgs a, u
             const bool lleaf = kl & kLeafKid, rleaf = kr & kLeafKid;
             const uint32_t lq = kl & 0xffu, rq = kr & 0xffu;
             const uint32_t count = sm.cnt[q];
-            const Carry l = get_carry(lleaf ? sm.lslot : sm.islot, lq);
-            const Carry rc = get_carry(rleaf ? sm.lslot : sm.islot, rq);
+            const Carry l = get_carry(sm, lq, lleaf, leaf_ct);
+            const Carry rc = get_carry(sm, rq, rleaf, leaf_ct);
             Carry o;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {  // kr_aabb_expand(left, right)
@@ -523,11 +533,14 @@ __global__ void __launch_bounds__(kThreads, 3) fused_up_local_kernel(UpArgs a, u
             }
             put_carry(sm.islot, q, o);
             if (with_summary) {
+                f3 lv[3], rv[3];
+                if (lleaf) leaf_vertices(sm, lq, lv);
+                if (rleaf) leaf_vertices(sm, rq, rv);
 #pragma unroll
                 for (int k = 0; k < 7; ++k) {
-                    const Slab ls = lleaf ? get_leaf_slab(sm, lq, j0 + lq, k) : get_slab(sm.islot, lq, k);
-                    const Slab rs = rleaf ? get_leaf_slab(sm, rq, j0 + rq, k) : get_slab(sm.islot, rq, k);
-                    put_slab(sm.islot, q, k, merge_slab(ls, rs));
+                    const Slab ls = lleaf ? leaf_slab(lv, j0 + lq, k) : get_slab(sm.islot, lq, k, 3 * j0);
+                    const Slab rs = rleaf ? leaf_slab(rv, j0 + rq, k) : get_slab(sm.islot, rq, k, 3 * j0);
+                    put_slab(sm.islot, q, k, merge_slab(ls, rs), 3 * j0);
                 }
             }
             const uint32_t u = sm.up[q];
@@ -546,7 +559,7 @@ __global__ void __launch_bounds__(kThreads, 3) fused_up_local_kernel(UpArgs a, u
             if (!sm.local[q]) continue;
             uint32_t v;
             if (k < 6) {
-                v = sm.islot[k][q];
+                v = sm.islot[k * kRow + q];
                 __stcg(nw + w, v);  // words 6..8 hold the children and 0 already
             } else if (k < 8) {
                 const uint32_t kd = sm.kid[k - 6][q];
@@ -557,14 +570,16 @@ __global__ void __launch_bounds__(kThreads, 3) fused_up_local_kernel(UpArgs a, u
             if (cw) __stcg(cw + w, v);
         }
         for (uint32_t q = t; q < mi; q += kThreads)
-            if (sm.local[q]) __stcg(a.costs + j0 + q, __uint_as_float(sm.islot[6][q]));
+            if (sm.local[q]) __stcg(a.costs + j0 + q, __uint_as_float(sm.islot[6 * kRow + q]));
         if (with_summary) {
             uint4* sw = a.summary + 7 * static_cast<size_t>(j0);
             for (uint32_t w = t; w < 7 * mi; w += kThreads) {
                 const uint32_t q = w / 7, k = w - 7 * q;
-                if (sm.local[q])
-                    __stcg(sw + w, make_uint4(sm.islot[7 + 4 * k][q], sm.islot[8 + 4 * k][q], sm.islot[9 + 4 * k][q],
-                                              sm.islot[10 + 4 * k][q]));
+                if (sm.local[q]) {
+                    const uint32_t ids = sm.islot[(21 + k) * kRow + q];
+                    __stcg(sw + w, make_uint4(sm.islot[(7 + 2 * k) * kRow + q], sm.islot[(8 + 2 * k) * kRow + q],
+                                              3 * j0 + (ids & 0xffffu), 3 * j0 + (ids >> 16)));
+                }
             }
         }
         if (a.flags) {
@@ -676,23 +691,6 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(const uint32_t* sizes,
     cw[8] = (cw[8] & 0xffff0000u) | pos;
 }
 
-// The bottom-up pass needs more than the default 48 KB of dynamic shared
-// memory; the attribute is set once per device.
-kr_error configure_fused_up() {
-    static std::mutex mu;
-    static uint64_t done = 0;
-    int dev = 0;
-    OBVH_TRY_CUDA(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lock(mu);
-    if (dev < 64 && ((done >> dev) & 1)) return kr_success;
-    OBVH_TRY_CUDA(cudaFuncSetAttribute(fused_up_local_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(kFusedSmemBytes)));
-    // room for three CTAs per SM
-    OBVH_TRY_CUDA(cudaFuncSetAttribute(fused_up_local_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    if (dev < 64) done |= 1ull << dev;
-    return kr_success;
-}
-
 // ---------------------------------------------------------------------------
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
@@ -774,7 +772,7 @@ kr_error enqueue(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32
     OBVH_TRY(lbvh::enqueue_karras(c.codes, n, nodes, parents, first, counts, s));
     if (internal > 0) OBVH_TRY_CUDA(cudaMemsetAsync(c.visits, 0, 4ull * internal, s));
     if (want_collapse) OBVH_TRY_CUDA(cudaMemsetAsync(cflags, 0, nn, s));
-    OBVH_TRY(configure_fused_up());
+    OBVH_TRY(allow_dynamic_smem(reinterpret_cast<const void*>(fused_up_local_kernel), kFusedSmemBytes));
     {
         UpArgs a{nodes, want_collapse ? collapsed : nullptr, parents, first, tris, n, counts, costs,
                  want_collapse ? cflags : nullptr, ci, ct, want_obbs ? summary : nullptr, c.visits, &ctl->error};

@@ -44,6 +44,20 @@ const DeviceInfo& device_info() {
     return g_info.emplace(dev, info).first->second;
 }
 
+kr_error allow_dynamic_smem(const void* kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> done;
+    int dev = 0;
+    OBVH_TRY_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = done.find({kernel, dev});
+    if (it != done.end() && it->second >= bytes) return kr_success;
+    OBVH_TRY_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+    OBVH_TRY_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    done[{kernel, dev}] = bytes;
+    return kr_success;
+}
+
 kr_error DeviceBuffer::reserve(size_t need) {
     if (need <= bytes) return kr_success;
     release();

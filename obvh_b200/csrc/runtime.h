@@ -37,6 +37,11 @@ struct DeviceInfo {
 // Properties of the current device (cached per device id).
 const DeviceInfo& device_info();
 
+// Lets `kernel` take `bytes` of dynamic shared memory on the current device
+// and prefers the largest shared-memory carveout; done once per (kernel,
+// device).
+kr_error allow_dynamic_smem(const void* kernel, size_t bytes);
+
 // A device buffer that only grows; not thread-safe on its own.
 struct DeviceBuffer {
     void* ptr = nullptr;
