@@ -395,8 +395,9 @@ __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Su
 // own leaf range, so an internal node whose range lies within these leaves
 // ("local") has its index in [j0, jend) too.  The local nodes are completed
 // in rounds separated by CTA barriers: a round's ready nodes sit in a queue
-// and go to its first threads; a completed node's parent joins the next
-// round's queue once both children are done.  Children are read from shared
+// and go to its first threads (to groups of 8 threads when few are ready); a
+// completed node's parent joins the next round's queue once both children
+// are done.  Children are read from shared
 // memory, and the outputs are written at the end as contiguous runs.  The
 // leaves and local nodes whose parents are not local go to a list for part 2.
 __global__ void __launch_bounds__(kThreads, 4) fused_up_local_kernel(UpArgs a, uint32_t* frontier,
@@ -488,64 +489,78 @@ __global__ void __launch_bounds__(kThreads, 4) fused_up_local_kernel(UpArgs a, u
             break;
         }
         if (t == 0) sm.qn[old] = 0;
-        if (t < K) {
-            const uint32_t q = sm.queue[cur][t];
+        // Up to kThreads / 8 ready nodes: a group of 8 lanes per node (lanes
+        // 0..6 one summary slab each, lane 7 the rest).  More: a thread each.
+        const bool grouped = K <= kThreads / 8;
+        const uint32_t g = grouped ? t >> 3 : t;
+        const uint32_t sub = grouped ? (t & 7) : 8u;  // 8: the whole node
+        if (g < K) {
+            const uint32_t q = sm.queue[cur][g];
             const uint32_t kl = sm.kid[0][q], kr = sm.kid[1][q];
             const bool lleaf = kl & kLeafKid, rleaf = kr & kLeafKid;
             const uint32_t lq = kl & 0xffu, rq = kr & 0xffu;
-            const uint32_t count = sm.cnt[q];
-            const Carry l = get_carry(sm, lq, lleaf, leaf_ct);
-            const Carry rc = get_carry(sm, rq, rleaf, leaf_ct);
-            Carry o;
+            if (sub >= 7) {
+                const uint32_t count = sm.cnt[q];
+                const Carry l = get_carry(sm, lq, lleaf, leaf_ct);
+                const Carry rc = get_carry(sm, rq, rleaf, leaf_ct);
+                Carry o;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {  // kr_aabb_expand(left, right)
-                o.lo[k] = kmin(kmin(l.lo[k], rc.lo[k]), rc.hi[k]);
-                o.hi[k] = kmax(kmax(l.hi[k], rc.lo[k]), rc.hi[k]);
-            }
-            const float area = box_area(o.lo, o.hi);
-            if (a.flags) {
-                // bvh_mark_collapse_kernel (transforms.cu:111-133)
-                const float node_cost = a.ci * area + l.cost + rc.cost;
-                const float leaf_cost = a.ct * area * static_cast<float>(count);
-                if (leaf_cost < node_cost && count <= kMaxLeafSize) {
-                    o.cost = leaf_cost;
-                    sm.iflag[q] = 1;
-                    // collapsed children: marked, and nPrimitives = 0xFFFF (axis byte and pad are zero)
-                    if (lleaf) {
-                        sm.lflag[lq] = 1;
-                        __stcg(reinterpret_cast<uint32_t*>(a.collapsed + internal + j0 + lq) + 8, kHidden);
+                for (int k = 0; k < 3; ++k) {  // kr_aabb_expand(left, right)
+                    o.lo[k] = kmin(kmin(l.lo[k], rc.lo[k]), rc.hi[k]);
+                    o.hi[k] = kmax(kmax(l.hi[k], rc.lo[k]), rc.hi[k]);
+                }
+                const float area = box_area(o.lo, o.hi);
+                if (a.flags) {
+                    // bvh_mark_collapse_kernel (transforms.cu:111-133)
+                    const float node_cost = a.ci * area + l.cost + rc.cost;
+                    const float leaf_cost = a.ct * area * static_cast<float>(count);
+                    if (leaf_cost < node_cost && count <= kMaxLeafSize) {
+                        o.cost = leaf_cost;
+                        sm.iflag[q] = 1;
+                        // collapsed children: marked, and nPrimitives = 0xFFFF (axis byte and pad are zero)
+                        if (lleaf) {
+                            sm.lflag[lq] = 1;
+                            __stcg(reinterpret_cast<uint32_t*>(a.collapsed + internal + j0 + lq) + 8, kHidden);
+                        } else {
+                            sm.iflag[lq] = 1;
+                            sm.hidden[lq] = 1;
+                        }
+                        if (rleaf) {
+                            sm.lflag[rq] = 1;
+                            __stcg(reinterpret_cast<uint32_t*>(a.collapsed + internal + j0 + rq) + 8, kHidden);
+                        } else {
+                            sm.iflag[rq] = 1;
+                            sm.hidden[rq] = 1;
+                        }
                     } else {
-                        sm.iflag[lq] = 1;
-                        sm.hidden[lq] = 1;
-                    }
-                    if (rleaf) {
-                        sm.lflag[rq] = 1;
-                        __stcg(reinterpret_cast<uint32_t*>(a.collapsed + internal + j0 + rq) + 8, kHidden);
-                    } else {
-                        sm.iflag[rq] = 1;
-                        sm.hidden[rq] = 1;
+                        o.cost = node_cost;
                     }
                 } else {
-                    o.cost = node_cost;
+                    o.cost = 1.2f * area + rc.cost + l.cost;  // calculate_aabbs_kernel (lbvh.cu:452)
                 }
-            } else {
-                o.cost = 1.2f * area + rc.cost + l.cost;  // calculate_aabbs_kernel (lbvh.cu:452)
+                put_carry(sm.islot, q, o);
             }
-            put_carry(sm.islot, q, o);
-            if (with_summary) {
+            if (with_summary && sub != 7) {
                 f3 lv[3], rv[3];
                 if (lleaf) leaf_vertices(sm, lq, lv);
                 if (rleaf) leaf_vertices(sm, rq, rv);
-#pragma unroll
-                for (int k = 0; k < 7; ++k) {
+                const auto slab = [&](int k) {
                     const Slab ls = lleaf ? leaf_slab(lv, j0 + lq, k) : get_slab(sm.islot, lq, k, 3 * j0);
                     const Slab rs = rleaf ? leaf_slab(rv, j0 + rq, k) : get_slab(sm.islot, rq, k, 3 * j0);
                     put_slab(sm.islot, q, k, merge_slab(ls, rs), 3 * j0);
+                };
+                if (sub == 8) {
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) slab(k);
+                } else {
+                    slab(static_cast<int>(sub));
                 }
             }
-            const uint32_t u = sm.up[q];
-            if (u != kNotLocal && atomicSub(&sm.deg[u], 1u) == 1u)
-                sm.queue[nxt][atomicAdd(&sm.qn[nxt], 1u)] = static_cast<uint8_t>(u);
+            if (sub >= 7) {
+                const uint32_t u = sm.up[q];
+                if (u != kNotLocal && atomicSub(&sm.deg[u], 1u) == 1u)
+                    sm.queue[nxt][atomicAdd(&sm.qn[nxt], 1u)] = static_cast<uint8_t>(u);
+            }
         }
         __syncthreads();
     }
