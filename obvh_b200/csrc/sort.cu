@@ -199,12 +199,19 @@ __global__ void __launch_bounds__(kSortThreads) radix_onesweep(const K* keys_in,
     const uint32_t lt = (1u << lane) - 1u;
     K k[kRounds];
     uint32_t v[kRounds], pos[kRounds];
+    // every load in flight before the ranking (whose warp barriers would
+    // otherwise hold each round's load back until the round before is done)
 #pragma unroll
     for (int r = 0; r < kRounds; ++r) {
         const uint64_t idx = base + warp * (kRounds * 32) + r * 32 + lane;
         const bool ok = idx < n;
         k[r] = ok ? keys_in[idx] : K(0);
         v[r] = ok ? vals_in[idx] : 0u;
+    }
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+        const uint64_t idx = base + warp * (kRounds * 32) + r * 32 + lane;
+        const bool ok = idx < n;
         const uint32_t d = ok ? (static_cast<uint32_t>(k[r] >> shift) & (kRadix - 1)) : kRadix;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const uint32_t before = sm.wcount[warp][ok ? d : 0];
@@ -233,21 +240,36 @@ __global__ void __launch_bounds__(kSortThreads) radix_onesweep(const K* keys_in,
             st_relaxed(mine, kFlagPre | c);
         } else {
             st_relaxed(mine, kFlagAgg | c);
-            uint64_t j = tile - 1;
+            // Eight predecessors' words per step (independent loads): sum
+            // their counts back to the first inclusive prefix; a word not yet
+            // published stops the step, and the walk resumes from it.
+            constexpr int kLook = 8;
+            int64_t j = static_cast<int64_t>(tile) - 1;
             const uint64_t t0 = global_ns();
-            for (;;) {
-                const uint32_t w = ld_relaxed(status + j * kRadix + d);
-                if ((w & kFlagMask) == 0) {
+            bool done = false;
+            while (!done) {
+                uint32_t w[kLook];
+#pragma unroll
+                for (int q = 0; q < kLook; ++q)
+                    w[q] = j - q >= 0 ? ld_relaxed(status + static_cast<uint64_t>(j - q) * kRadix + d) : kFlagPre;
+                int q = 0;
+                for (; q < kLook; ++q) {
+                    if ((w[q] & kFlagMask) == 0) break;  // not published yet
+                    excl += w[q] & kCountMask;
+                    if ((w[q] & kFlagPre) || j - q == 0) {
+                        done = true;
+                        break;
+                    }
+                }
+                if (done) break;
+                j -= q;
+                if (q < kLook) {  // wait for tile j
                     if (global_ns() - t0 > kWaitNs || ld_relaxed(err) != 0) {
                         atomicOr(err, kErrWaitTimeout);
                         break;
                     }
                     __nanosleep(32);
-                    continue;
                 }
-                excl += w & kCountMask;
-                if ((w & kFlagPre) || j == 0) break;
-                --j;
             }
             st_relaxed(mine, kFlagPre | (excl + c));
         }
