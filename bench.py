@@ -276,6 +276,7 @@ def tree_bytes_per_launch(n):
         "emit_kernel": 48 * nn + 36 * nn + 4 * nn,
         "roots_kernel": 14 * nn,
         "gather_kernel": 8 * nn,
+        "gather_ranked_kernel": 8 * nn,
         "scan_tile_sums": 4 * nn,
         "scan_tiles": 8 * nn,
     }

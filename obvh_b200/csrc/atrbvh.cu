@@ -711,8 +711,11 @@ kr_error enqueue_full(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, u
     }
     if (flags & OBVH_BUILD_COLLAPSE) {
         if (!collapsed || !prims) return "obvh_build_atrbvh: OBVH_BUILD_COLLAPSE needs collapsed and primitives";
+        // with the transform's depth-first ranks at hand, the gather reads rank runs
+        const bool ranked = (flags & OBVH_BUILD_OBBS) != 0;
         OBVH_TRY(collapse::enqueue(nodes, parents, collapsed, counts, prims, costs, ci, ct, n, n - 1, ws + L.col_ws, s,
-                                   nullptr));
+                                   nullptr, ranked ? obbtree::dfs_first(ws + L.obb_ws, n) : nullptr,
+                                   ranked ? obbtree::dfs_prims(ws + L.obb_ws, n) : nullptr));
     }
     return kr_success;
 }

@@ -143,6 +143,54 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(const kr_bvh_node* nod
     cw[8] = (cw[8] & 0xffff0000u) | static_cast<uint32_t>(pos);
 }
 
+// The same, from depth-first ranks: right-first depth-first order, which
+// bvh_node_collapse walks, visits a subtree's leaves in the reverse of their
+// left-first ranks, so a collapsed node's primitives are its rank run read
+// backwards (repeats skipped).
+__global__ void __launch_bounds__(kThreads) gather_ranked_kernel(const uint32_t* sizes, const uint32_t* offsets,
+                                                                 const uint32_t* dfs_first, const uint32_t* dfs_prims,
+                                                                 uint32_t n, uint32_t nn, kr_bvh_node* collapsed,
+                                                                 uint32_t* counts, uint32_t* primitives,
+                                                                 uint32_t* err) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nn) return;
+    const uint32_t cnt = sizes[c];
+    if (cnt == 0) return;
+    if (cnt > kMaxLeafSize || c >= n - 1) {  // a collapse root with more than one primitive is internal
+        atomicOr(err, kErrBadInput);
+        return;
+    }
+    const uint32_t f = dfs_first[c], off = offsets[c];
+    if (f + cnt > n) {
+        atomicOr(err, kErrBadInput);
+        return;
+    }
+    uint32_t out[kMaxLeafSize];
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t t = 0; t < kMaxLeafSize; ++t) {
+        if (t < cnt) {
+            const uint32_t prim = dfs_prims[f + cnt - 1 - t];
+            bool uniq = true;
+#pragma unroll
+            for (uint32_t q = 0; q < kMaxLeafSize; ++q) uniq = uniq && !(q < pos && out[q] == prim);
+            if (uniq) {
+#pragma unroll
+                for (uint32_t q = 0; q < kMaxLeafSize; ++q)
+                    if (q == pos) out[q] = prim;
+                ++pos;
+            }
+        }
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < kMaxLeafSize; ++q)
+        if (q < pos) primitives[off + q] = out[q];
+    counts[c] = pos;
+    uint32_t* cw = reinterpret_cast<uint32_t*>(collapsed + c);
+    cw[6] = off;
+    cw[8] = (cw[8] & 0xffff0000u) | pos;
+}
+
 // ---------------------------------------------------------------------------
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
@@ -162,7 +210,8 @@ Layout layout(uint32_t n) {
 
 kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, kr_bvh_node* collapsed, uint32_t* counts,
                  uint32_t* primitives, float* costs, float ci, float ct, uint32_t n, uint32_t internal,
-                 void* workspace, cudaStream_t s, cudaEvent_t mid_event) {
+                 void* workspace, cudaStream_t s, cudaEvent_t mid_event, const uint32_t* dfs_first,
+                 const uint32_t* dfs_prims) {
     if (n == 0) return kr_success;
     if (!nodes || !parents || !collapsed || !counts || !primitives || !costs || !workspace)
         return "kr_cuda_bvh_collapse: null pointer argument";
@@ -192,7 +241,11 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, kr_bvh_node*
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     OBVH_TRY(exclusive_scan_u32(sizes, offsets, nn, &ctl->total, ws + L.scan, s));
-    {
+    if (dfs_first && dfs_prims && n > 1) {
+        ProfScope prof_scope_("gather_ranked_kernel", s);
+        gather_ranked_kernel<<<gn, kThreads, 0, s>>>(sizes, offsets, dfs_first, dfs_prims, n, nn, collapsed, counts,
+                                                     primitives, &ctl->error);
+    } else {
         ProfScope prof_scope_("gather_kernel", s);
         gather_kernel<<<gn, kThreads, 0, s>>>(nodes, sizes, offsets, nn, collapsed, counts, primitives, &ctl->error);
     }

@@ -18,9 +18,13 @@ Layout layout(uint32_t n);
 
 // Enqueues the collapse; the workspace's first 256 bytes must be zero.
 // mid_event (nullable) is recorded between the mark and gather phases.
+// dfs_first / dfs_prims (both or neither): the depth-first ranks of the same
+// tree (obbtree::dfs_first / dfs_prims); with them a collapsed node's
+// primitives are its rank run read backwards instead of a subtree walk.
 kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, kr_bvh_node* collapsed, uint32_t* counts,
                  uint32_t* primitives, float* costs, float ci, float ct, uint32_t n, uint32_t internal,
-                 void* workspace, cudaStream_t s, cudaEvent_t mid_event);
+                 void* workspace, cudaStream_t s, cudaEvent_t mid_event, const uint32_t* dfs_first = nullptr,
+                 const uint32_t* dfs_prims = nullptr);
 
 }  // namespace collapse
 }  // namespace obvh

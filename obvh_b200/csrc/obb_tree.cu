@@ -135,7 +135,8 @@ __global__ void __launch_bounds__(kThreads) summary_up_kernel(const kr_bvh_node*
 __global__ void __launch_bounds__(kThreads) dfs_rank_kernel(const kr_bvh_node* nodes, const uint32_t* parents,
                                                             const uint32_t* counts, const kr_vec3* verts,
                                                             const kr_uvec4* faces, uint32_t n, uint32_t internal,
-                                                            uint32_t* first, float* tris, uint32_t* err) {
+                                                            uint32_t* first, float* tris, uint32_t* rank_prims,
+                                                            uint32_t* err) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n || *err) return;  // an earlier pass found a malformed tree
     const uint32_t leaf = internal + j;
@@ -156,6 +157,7 @@ __global__ void __launch_bounds__(kThreads) dfs_rank_kernel(const kr_bvh_node* n
         atomicOr(err, kErrBadInput);
         return;
     }
+    rank_prims[rank] = __ldg(reinterpret_cast<const uint32_t*>(nodes + leaf) + 6);
     const uint4 face = leaf_face(nodes, faces, leaf);
     const f3 a = load_vertex(verts, face.x), b = load_vertex(verts, face.y), c = load_vertex(verts, face.z);
     float* t = tris + 9 * static_cast<size_t>(rank);
@@ -541,6 +543,7 @@ Layout layout(uint32_t n) {
     L.summary = o;  o += align256(112 * ni);
     L.first = o;    o += align256(4 * ni);
     L.tris = o;     o += align256(36ull * (n > 0 ? n : 1));
+    L.rank_prims = o; o += align256(4ull * (n > 0 ? n : 1));
     L.cand = o;     o += align256(sizeof(Cand) * ni);
     L.nunits = o;   o += align256(4 * ni);
     L.ustart = o;   o += align256(4 * ni);
@@ -581,6 +584,7 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec
     {
         ProfScope prof_scope_("dfs_rank_kernel", s);
         dfs_rank_kernel<<<gl, kThreads, 0, s>>>(nodes, parents, counts, verts, faces, n, internal, first, tris,
+                                                reinterpret_cast<uint32_t*>(ws + L.rank_prims),
                                                 &ctl->error);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
@@ -598,6 +602,13 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec
     fb.err = &ctl->error;
     fb.total_units = &ctl->total_units;
     return enqueue_frames(fb, internal, obbs, xfs, s);
+}
+
+const uint32_t* dfs_first(const void* workspace, uint32_t n) {
+    return reinterpret_cast<const uint32_t*>(static_cast<const char*>(workspace) + layout(n).first);
+}
+const uint32_t* dfs_prims(const void* workspace, uint32_t n) {
+    return reinterpret_cast<const uint32_t*>(static_cast<const char*>(workspace) + layout(n).rank_prims);
 }
 
 size_t cand_bytes(uint32_t internal) { return sizeof(Cand) * (internal > 0 ? internal : 1); }

@@ -13,9 +13,15 @@ namespace obbtree {
 
 // Byte offsets inside a transform workspace for n primitives.
 struct Layout {
-    size_t ctl, visits, counts, summary, first, tris, cand, nunits, ustart, keys, scan, total;
+    size_t ctl, visits, counts, summary, first, tris, rank_prims, cand, nunits, ustart, keys, scan, total;
 };
 Layout layout(uint32_t n);
+
+// After a transform enqueued on `workspace` (n primitives) has run: each
+// internal node's first leaf in depth-first order (left child first), and
+// the primitive of the leaf at each depth-first rank.
+const uint32_t* dfs_first(const void* workspace, uint32_t n);
+const uint32_t* dfs_prims(const void* workspace, uint32_t n);
 
 // Enqueues the transform; the workspace's first 256 bytes must be zero.
 kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec3* verts, const kr_uvec4* faces,
