@@ -625,9 +625,11 @@ kr_error check_args(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uin
     return kr_success;
 }
 
+// refit false: the nodes are emitted with zero internal bounds, and counts
+// and costs are left to the caller's own bottom-up pass.
 kr_error enqueue_tree(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32_t tau, uint32_t iterations,
                       float ci, float ct, kr_bvh_node* nodes, uint32_t* parents, uint32_t* counts, float* costs,
-                      kr_aabb3* scene_out, void* workspace, cudaStream_t s) {
+                      kr_aabb3* scene_out, void* workspace, cudaStream_t s, bool refit = true) {
     OBVH_TRY(check_args(verts, faces, n, tau, workspace));
     if (!nodes || !parents || !counts || !costs) return "obvh_atrbvh: null pointer argument";
     char* ws = static_cast<char*>(workspace);
@@ -692,7 +694,7 @@ kr_error enqueue_tree(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, u
         emit_kernel<<<(2 * n - 1 + kThreads - 1) / kThreads, kThreads, 0, s>>>(t, n, nodes, parents);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
-    OBVH_TRY(lbvh::enqueue_refit(nodes, parents, counts, costs, counters, n, err, s));
+    if (refit) OBVH_TRY(lbvh::enqueue_refit(nodes, parents, counts, costs, counters, n, err, s));
     if (scene_out) OBVH_TRY_CUDA(cudaMemcpyAsync(scene_out, scene, sizeof(kr_aabb3), cudaMemcpyDeviceToDevice, s));
     return kr_success;
 }
@@ -701,21 +703,30 @@ kr_error enqueue_full(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, u
                       uint32_t iterations, float ci, float ct, kr_bvh_node* nodes, uint32_t* parents,
                       uint32_t* counts, float* costs, kr_aabb3* scene_out, kr_obb3* obbs, kr_mat4* xfs,
                       kr_bvh_node* collapsed, uint32_t* prims, void* workspace, cudaStream_t s) {
+    const bool want_obbs = (flags & OBVH_BUILD_OBBS) != 0, want_collapse = (flags & OBVH_BUILD_COLLAPSE) != 0;
+    if (want_obbs && (!obbs || !xfs)) return "obvh_build_atrbvh: OBVH_BUILD_OBBS needs obbs and transforms";
+    if (want_collapse && (!collapsed || !prims))
+        return "obvh_build_atrbvh: OBVH_BUILD_COLLAPSE needs collapsed and primitives";
+    // With a transform or a collapse to follow, the refit, the subtree
+    // summaries and the collapse marks are one walk (obbtree::enqueue_walk).
+    const bool walk = want_obbs || want_collapse;
     OBVH_TRY(enqueue_tree(verts, faces, n, tau, iterations, ci, ct, nodes, parents, counts, costs, scene_out,
-                          workspace, s));
+                          workspace, s, !walk));
+    if (!walk) return kr_success;
     char* ws = static_cast<char*>(workspace);
     const Layout L = layout(n);
-    if (flags & OBVH_BUILD_OBBS) {
-        if (!obbs || !xfs) return "obvh_build_atrbvh: OBVH_BUILD_OBBS needs obbs and transforms";
-        OBVH_TRY(obbtree::enqueue(nodes, parents, verts, faces, obbs, xfs, n, n - 1, ws + L.obb_ws, s));
-    }
-    if (flags & OBVH_BUILD_COLLAPSE) {
-        if (!collapsed || !prims) return "obvh_build_atrbvh: OBVH_BUILD_COLLAPSE needs collapsed and primitives";
+    uint8_t* cflags = want_collapse ? collapse::flags_of(ws + L.col_ws, n) : nullptr;
+    if (want_collapse) OBVH_TRY_CUDA(cudaMemsetAsync(cflags, 0, 2ull * n - 1, s));
+    OBVH_TRY(obbtree::enqueue_walk(nodes, parents, verts, faces, n, counts, costs, obbs, xfs,
+                                   want_obbs ? ws + L.obb_ws : nullptr, want_collapse ? collapsed : nullptr, cflags, ci,
+                                   ct, collapse::visits_of(ws + L.col_ws, n), &reinterpret_cast<Ctl*>(ws + L.ctl)->error,
+                                   s));
+    if (want_obbs) OBVH_TRY(obbtree::enqueue_ranks_frames(nodes, parents, counts, verts, faces, obbs, xfs, n, ws + L.obb_ws, s));
+    if (want_collapse) {
         // with the transform's depth-first ranks at hand, the gather reads rank runs
-        const bool ranked = (flags & OBVH_BUILD_OBBS) != 0;
-        OBVH_TRY(collapse::enqueue(nodes, parents, collapsed, counts, prims, costs, ci, ct, n, n - 1, ws + L.col_ws, s,
-                                   nullptr, ranked ? obbtree::dfs_first(ws + L.obb_ws, n) : nullptr,
-                                   ranked ? obbtree::dfs_prims(ws + L.obb_ws, n) : nullptr));
+        OBVH_TRY(collapse::enqueue_gather(nodes, parents, collapsed, counts, prims, n, ws + L.col_ws, s,
+                                          want_obbs ? obbtree::dfs_first(ws + L.obb_ws, n) : nullptr,
+                                          want_obbs ? obbtree::dfs_prims(ws + L.obb_ws, n) : nullptr));
     }
     return kr_success;
 }

@@ -221,8 +221,6 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, kr_bvh_node*
     const uint32_t nn = n + internal;
     Ctl* ctl = reinterpret_cast<Ctl*>(ws + L.ctl);
     uint8_t* flags = reinterpret_cast<uint8_t*>(ws + L.flags);
-    uint32_t* sizes = reinterpret_cast<uint32_t*>(ws + L.sizes);
-    uint32_t* offsets = reinterpret_cast<uint32_t*>(ws + L.offsets);
     OBVH_TRY_CUDA(cudaMemcpyAsync(collapsed, nodes, sizeof(kr_bvh_node) * nn, cudaMemcpyDeviceToDevice, s));
     OBVH_TRY_CUDA(cudaMemsetAsync(flags, 0, nn, s));
     OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.visits, 0, 4ull * nn, s));
@@ -234,6 +232,25 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, kr_bvh_node*
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     if (mid_event) OBVH_TRY_CUDA(cudaEventRecord(mid_event, s));
+    return enqueue_gather(nodes, parents, collapsed, counts, primitives, n, workspace, s, dfs_first, dfs_prims);
+}
+
+uint8_t* flags_of(void* workspace, uint32_t n) { return static_cast<uint8_t*>(workspace) + layout(n).flags; }
+uint32_t* visits_of(void* workspace, uint32_t n) {
+    return reinterpret_cast<uint32_t*>(static_cast<char*>(workspace) + layout(n).visits);
+}
+
+kr_error enqueue_gather(const kr_bvh_node* nodes, const uint32_t* parents, kr_bvh_node* collapsed, uint32_t* counts,
+                        uint32_t* primitives, uint32_t n, void* workspace, cudaStream_t s, const uint32_t* dfs_first,
+                        const uint32_t* dfs_prims) {
+    if (n == 0) return kr_success;
+    char* ws = static_cast<char*>(workspace);
+    const Layout L = layout(n);
+    const uint32_t nn = 2 * n - 1;
+    Ctl* ctl = reinterpret_cast<Ctl*>(ws + L.ctl);
+    uint8_t* flags = reinterpret_cast<uint8_t*>(ws + L.flags);
+    uint32_t* sizes = reinterpret_cast<uint32_t*>(ws + L.sizes);
+    uint32_t* offsets = reinterpret_cast<uint32_t*>(ws + L.offsets);
     const unsigned gn = (nn + kThreads - 1) / kThreads;
     {
         ProfScope prof_scope_("roots_kernel", s);

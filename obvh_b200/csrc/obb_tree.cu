@@ -45,6 +45,7 @@ using namespace tree;
 
 constexpr int kThreads = 256;
 constexpr uint32_t kThreadMax = 32;  // leaves handled by one thread per node
+constexpr uint32_t kCollapseLeafMax = 8;  // MAX_LEAF_SIZE (transforms.cu:65)
 constexpr uint32_t kUnit = 1024;    // leaves per warp unit
 constexpr uint32_t kUnitRun = 4;   // consecutive units per warp visit
 constexpr int kTileShift = 10;      // tiled extents: 1,024 leaves per tile
@@ -127,6 +128,196 @@ __global__ void __launch_bounds__(kThreads) summary_up_kernel(const kr_bvh_node*
         child = p;
         p = grand;
     }
+}
+
+// ---------------------------------------------------------------------------
+// One leaf-to-root walk doing, on any binary tree, what the LBVH refit
+// (lbvh.cu:399-457), summary_up above and the collapse marking
+// (transforms.cu:65-136) do in three: internal bounds (kr_aabb_expand of the
+// children), counts, SAH costs (the collapse's rule when collapsing, the
+// LBVH's otherwise), collapse marks and collapsed records, the 7-direction
+// summaries and the leaf boxes.  The arriving thread carries its own child's
+// values and reads only the sibling's.
+struct WalkArgs {
+    kr_bvh_node* nodes;       // children and leaf boxes in; internal bounds out
+    kr_bvh_node* collapsed;   // null: no collapse; else every record, with marks
+    const uint32_t* parents;
+    const kr_vec3* verts;
+    const uint4* faces;
+    uint32_t n;
+    uint32_t* counts;
+    float* costs;
+    uint8_t* flags;           // null with collapsed
+    float ci, ct;
+    uint4* summary;           // null: no summaries or leaf boxes
+    kr_obb3* obbs;
+    kr_mat4* xfs;
+    uint32_t* visits;
+    uint32_t* err;
+};
+
+__device__ __forceinline__ void mark_hidden(kr_bvh_node* collapsed, uint32_t i) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(collapsed + i) + 8;
+    __stcg(w, (__ldcg(w) & 0xffff0000u) | 0xffffu);
+}
+
+__global__ void __launch_bounds__(kThreads) walk_kernel(WalkArgs a) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= a.n) return;
+    const uint32_t internal = a.n - 1;
+    const uint32_t leaf = internal + j;
+    const bool collapse = a.collapsed != nullptr;
+    uint32_t rec[9];
+    {
+        const uint32_t* lw = reinterpret_cast<const uint32_t*>(a.nodes + leaf);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) rec[k] = __ldg(lw + k);
+    }
+    float olo[3], ohi[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        olo[k] = __uint_as_float(rec[k]);
+        ohi[k] = __uint_as_float(rec[3 + k]);
+    }
+    // leaf cost: ct * area in the collapse (transforms.cu:97), 1 * area in the LBVH (lbvh.cu:427)
+    float ocost = (collapse ? a.ct : 1.0f) * box_area(olo, ohi);
+    uint32_t ocount = 1;
+    __stcg(a.costs + leaf, ocost);
+    __stcg(a.counts + leaf, 1u);
+    if (collapse) {
+        uint32_t* cw = reinterpret_cast<uint32_t*>(a.collapsed + leaf);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) __stcg(cw + k, rec[k]);
+    }
+    Summary own;
+    if (a.summary) {
+        const uint4 face = __ldg(a.faces + rec[6]);
+        leaf_box(load_vertex(a.verts, face.x), load_vertex(a.verts, face.y), load_vertex(a.verts, face.z),
+                 a.obbs + leaf, a.xfs + leaf);
+        leaf_summary(a.verts, face, own);
+    }
+    uint32_t child = leaf;
+    uint32_t p = a.parents[leaf];
+    for (uint32_t steps = 0; p != kNoParent; ++steps) {
+        if (steps > internal || p >= internal) {
+            atomicOr(a.err, kErrCycle);
+            return;
+        }
+        // written before this kernel: read ahead of the arrival
+        const uint32_t* pw = reinterpret_cast<const uint32_t*>(a.nodes + p);
+        const uint32_t L = __ldg(pw + 6), R = __ldg(pw + 7), w8 = __ldg(pw + 8);
+        const uint32_t grand = __ldg(a.parents + p);
+        if (arrive(a.visits + p) == 0) return;
+        const bool from_left = (L == child);
+        const uint32_t other = from_left ? R : L;
+        if ((L != child && R != child) || other >= internal + a.n) {
+            atomicOr(a.err, kErrBadInput);
+            return;
+        }
+        float slo[3], shi[3];
+        {
+            const uint32_t* sw = reinterpret_cast<const uint32_t*>(a.nodes + other);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                slo[k] = __uint_as_float(__ldcg(sw + k));
+                shi[k] = __uint_as_float(__ldcg(sw + 3 + k));
+            }
+        }
+        const uint32_t scount = __ldcg(a.counts + other);
+        const float scost = __ldcg(a.costs + other);
+        const float* llo = from_left ? olo : slo;
+        const float* lhi = from_left ? ohi : shi;
+        const float* rlo = from_left ? slo : olo;
+        const float* rhi = from_left ? shi : ohi;
+        float lo[3], hi[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {  // kr_aabb_expand(left, right)
+            lo[k] = kmin(kmin(llo[k], rlo[k]), rhi[k]);
+            hi[k] = kmax(kmax(lhi[k], rlo[k]), rhi[k]);
+        }
+        {
+            uint32_t* w = reinterpret_cast<uint32_t*>(a.nodes + p);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                __stcg(w + k, __float_as_uint(lo[k]));
+                __stcg(w + 3 + k, __float_as_uint(hi[k]));
+            }
+            if (collapse) {
+                uint32_t* cw = reinterpret_cast<uint32_t*>(a.collapsed + p);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    __stcg(cw + k, __float_as_uint(lo[k]));
+                    __stcg(cw + 3 + k, __float_as_uint(hi[k]));
+                }
+                __stcg(cw + 6, L);
+                __stcg(cw + 7, R);
+                __stcg(cw + 8, w8);
+            }
+        }
+        const uint32_t count = ocount + scount;
+        __stcg(a.counts + p, count);
+        const float area = box_area(lo, hi);
+        const float cl = from_left ? ocost : scost, cr = from_left ? scost : ocost;
+        float cost;
+        if (collapse) {
+            // bvh_mark_collapse_kernel (transforms.cu:111-133)
+            const float node_cost = a.ci * area + cl + cr;
+            const float leaf_cost = a.ct * area * static_cast<float>(count);
+            if (leaf_cost < node_cost && count <= kCollapseLeafMax) {
+                cost = leaf_cost;
+                a.flags[p] = 1;
+                a.flags[L] = 1;
+                a.flags[R] = 1;
+                mark_hidden(a.collapsed, L);
+                mark_hidden(a.collapsed, R);
+            } else {
+                cost = node_cost;
+            }
+        } else {
+            cost = 1.2f * area + cr + cl;  // calculate_aabbs_kernel (lbvh.cu:452)
+        }
+        __stcg(a.costs + p, cost);
+        if (a.summary) {
+            Summary o;
+            if (other >= internal) leaf_summary(a.verts, __ldg(a.faces + __ldg(reinterpret_cast<const uint32_t*>(a.nodes + other) + 6)), o);
+            else load_summary(a.summary + 7 * static_cast<size_t>(other), o);
+            if (from_left) {
+                merge_right(own, o);
+            } else {
+                merge_right(o, own);
+                own = o;
+            }
+            store_summary(a.summary + 7 * static_cast<size_t>(p), own);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { olo[k] = lo[k]; ohi[k] = hi[k]; }
+        ocount = count;
+        ocost = cost;
+        child = p;
+        p = grand;
+    }
+}
+
+kr_error enqueue_walk(kr_bvh_node* nodes, const uint32_t* parents, const kr_vec3* verts, const kr_uvec4* faces,
+                      uint32_t n, uint32_t* counts, float* costs, kr_obb3* obbs, kr_mat4* xfs, void* obb_workspace,
+                      kr_bvh_node* collapsed, uint8_t* flags, float ci, float ct, uint32_t* visits, uint32_t* err,
+                      cudaStream_t s) {
+    if (n == 0) return kr_success;
+    if (!nodes || !parents || !verts || !faces || !counts || !costs || !visits || !err)
+        return "enqueue_walk: null pointer argument";
+    if (obb_workspace && (!obbs || !xfs)) return "enqueue_walk: summaries need the leaf boxes' outputs";
+    if ((collapsed == nullptr) != (flags == nullptr)) return "enqueue_walk: collapsed records and marks go together";
+    WalkArgs a{nodes, collapsed, parents, verts, reinterpret_cast<const uint4*>(faces), n, counts, costs, flags, ci, ct,
+               obb_workspace ? reinterpret_cast<uint4*>(static_cast<char*>(obb_workspace) + layout(n).summary)
+                             : nullptr,
+               obbs, xfs, visits, err};
+    if (n > 1) OBVH_TRY_CUDA(cudaMemsetAsync(visits, 0, 4ull * (n - 1), s));
+    {
+        ProfScope prof_scope_("walk_kernel", s);
+        walk_kernel<<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(a);
+    }
+    OBVH_TRY_CUDA(cudaGetLastError());
+    return kr_success;
 }
 
 // DFS rank of every leaf (left subtree first); the leaf's triangle goes to
@@ -565,12 +756,6 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec
     Ctl* ctl = reinterpret_cast<Ctl*>(ws + L.ctl);
     uint32_t* counts = reinterpret_cast<uint32_t*>(ws + L.counts);
     uint4* summary = reinterpret_cast<uint4*>(ws + L.summary);
-    uint32_t* first = reinterpret_cast<uint32_t*>(ws + L.first);
-    float* tris = reinterpret_cast<float*>(ws + L.tris);
-    Cand* cand = reinterpret_cast<Cand*>(ws + L.cand);
-    uint32_t* nunits = reinterpret_cast<uint32_t*>(ws + L.nunits);
-    uint32_t* ustart = reinterpret_cast<uint32_t*>(ws + L.ustart);
-    uint32_t* keys = reinterpret_cast<uint32_t*>(ws + L.keys);
     const unsigned gl = (n + kThreads - 1) / kThreads;
 
     if (internal > 0) OBVH_TRY_CUDA(cudaMemsetAsync(ws + L.visits, 0, 4ull * internal, s));
@@ -580,7 +765,25 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec
                                                   reinterpret_cast<uint32_t*>(ws + L.visits), obbs, xfs, &ctl->error);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
-    if (internal == 0) return kr_success;
+    return enqueue_ranks_frames(nodes, parents, counts, verts, faces, obbs, xfs, n, workspace, s);
+}
+
+kr_error enqueue_ranks_frames(const kr_bvh_node* nodes, const uint32_t* parents, const uint32_t* counts,
+                              const kr_vec3* verts, const kr_uvec4* faces, kr_obb3* obbs, kr_mat4* xfs, uint32_t n,
+                              void* workspace, cudaStream_t s) {
+    const uint32_t internal = n - 1;
+    if (n < 2) return kr_success;
+    char* ws = static_cast<char*>(workspace);
+    const Layout L = layout(n);
+    Ctl* ctl = reinterpret_cast<Ctl*>(ws + L.ctl);
+    uint4* summary = reinterpret_cast<uint4*>(ws + L.summary);
+    uint32_t* first = reinterpret_cast<uint32_t*>(ws + L.first);
+    float* tris = reinterpret_cast<float*>(ws + L.tris);
+    Cand* cand = reinterpret_cast<Cand*>(ws + L.cand);
+    uint32_t* nunits = reinterpret_cast<uint32_t*>(ws + L.nunits);
+    uint32_t* ustart = reinterpret_cast<uint32_t*>(ws + L.ustart);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(ws + L.keys);
+    const unsigned gl = (n + kThreads - 1) / kThreads;
     {
         ProfScope prof_scope_("dfs_rank_kernel", s);
         dfs_rank_kernel<<<gl, kThreads, 0, s>>>(nodes, parents, counts, verts, faces, n, internal, first, tris,

@@ -28,6 +28,22 @@ kr_error enqueue(const kr_bvh_node* nodes, const uint32_t* parents, const kr_vec
                  kr_obb3* obbs, kr_mat4* xfs, uint32_t n, uint32_t internal, void* workspace, cudaStream_t s);
 uint32_t* error_word(void* workspace);
 
+// The transform's stages after the summaries (depth-first ranks, frames,
+// extents, boxes) for counts computed elsewhere.
+kr_error enqueue_ranks_frames(const kr_bvh_node* nodes, const uint32_t* parents, const uint32_t* counts,
+                              const kr_vec3* verts, const kr_uvec4* faces, kr_obb3* obbs, kr_mat4* xfs, uint32_t n,
+                              void* workspace, cudaStream_t s);
+
+// One leaf-to-root walk over a binary tree whose nodes hold the children and
+// the leaf boxes: internal bounds, counts and costs; with obb_workspace the
+// subtree summaries there and the leaf boxes in obbs/xfs; with collapsed and
+// flags every collapsed record and the collapse marks (costs then follow the
+// collapse's rule with ci/ct, else the LBVH's).  visits: n - 1 counters.
+kr_error enqueue_walk(kr_bvh_node* nodes, const uint32_t* parents, const kr_vec3* verts, const kr_uvec4* faces,
+                      uint32_t n, uint32_t* counts, float* costs, kr_obb3* obbs, kr_mat4* xfs, void* obb_workspace,
+                      kr_bvh_node* collapsed, uint8_t* flags, float ci, float ct, uint32_t* visits, uint32_t* err,
+                      cudaStream_t s);
+
 // The stages after the subtree summaries: candidate frames, extents and the
 // final boxes of the internal nodes [0, internal).  points[id] (packed xyz)
 // resolves the summaries' vertex ids; tris holds each subtree's triangles

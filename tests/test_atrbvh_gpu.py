@@ -98,6 +98,33 @@ def test_full_commit_matches_the_three_steps(builder):
     assert np.array_equal(o["primitives"].cpu().numpy().view(np.uint32)[:used], prims[:used])
 
 
+@pytest.mark.parametrize("flags", [1, 2])
+@pytest.mark.parametrize("n", [2, 3, 700, 30_000])
+def test_commit_parts_match_the_steps(builder, flags, n):
+    """The OBB transform alone (LBVH costs) and the collapse alone (its
+    primitive lists gathered by walking subtrees) against the oracle's steps."""
+    v, f = workloads.triangle_soup(n, seed=900 + n)
+    o, slots = _run(builder, v, f, flags=flags, tau=7)
+    r = ref.atrbvh_build(v, f, 7, 2)
+    _check_tree(o, r, n)
+    if flags == 1:
+        assert np.array_equal(o["counts"].cpu().numpy().view(np.uint32), r["counts"])
+        assert same_bits(o["costs"].cpu().numpy(), r["costs"])
+        obbs, xfs, _ = ref.obb_tree(r["nodes"], r["parents"], v, f)
+        assert same_bits(o["obbs"].cpu().numpy(), obbs)
+        assert same_bits(o["transforms"].cpu().numpy(), xfs)
+    else:
+        col, cnt, prims, cst, used = ref.collapse(r["nodes"], r["parents"], r["counts"], r["costs"], 1.2, 1.0)
+        c = bvh.nodes_numpy(o["collapsed"])
+        assert np.array_equal(c["left"], col["left"])
+        assert np.array_equal(c["n_prims"], col["n_prims"])
+        assert same_bits(c["b"], col["b"])
+        assert np.array_equal(o["counts"].cpu().numpy().view(np.uint32), cnt)
+        assert same_bits(o["costs"].cpu().numpy(), cst)
+        assert slots == used
+        assert np.array_equal(o["primitives"].cpu().numpy().view(np.uint32)[:used], prims[:used])
+
+
 def test_knot_full_size_properties(builder):
     """The 917,504-triangle torus knot: a valid tree whose SAH is below the
     LBVH's, and every triangle inside its leaf box and every ancestor's."""
