@@ -18,7 +18,10 @@
 //                    union area, and keeps the result if its SAH is lower
 //                    (AgglomerativeTreelet.cu:405-570, Treelet.cuh:55-129)
 //   emit_kernel      SoA tree -> kr_bvh_node + parents (atrbvh.cu:95-123),
-//                    then the LBVH refit for bounds, counts and costs.
+//                    then the LBVH refit for bounds, counts and costs, or,
+//                    for a full commit, one walk that also does the
+//                    transform's summaries and the collapse's marks
+//                    (obbtree::enqueue_walk).
 //
 // The reference runs its treelet kernel with __syncthreads() inside
 // warp-divergent loops; every shared array it touches there is per warp, so

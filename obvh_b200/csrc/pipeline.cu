@@ -10,10 +10,12 @@
 //     depth-first rank pass of the stand-alone transform is not needed;
 //   - the leaf pass writes the leaves, their triangles in that order and the
 //     leaves' own boxes (triangle frames) in one go;
-//   - one bottom-up pass computes the bounds, primitive counts, the SAH costs
-//     and collapse decisions, and the 7-direction subtree summaries that the
-//     reference computes in three separate leaf-to-root walks
-//     (lbvh.cu:399-457, transforms.cu:287-411, transforms.cu:65-136);
+//   - one bottom-up pass (two kernels: the nodes inside each CTA's leaves,
+//     from shared memory; then the few crossing CTA edges) computes the
+//     bounds, the SAH costs and collapse decisions, and the 7-direction
+//     subtree summaries that the reference computes in three separate
+//     leaf-to-root walks (lbvh.cu:399-457, transforms.cu:287-411,
+//     transforms.cu:65-136); primitive counts are the key-range sizes;
 //   - a collapse root's primitive list (right child first, transforms.cu:18-63)
 //     is its leaf range read backwards, so no tree walk is needed to gather it.
 #include <cuda_runtime.h>
