@@ -222,6 +222,22 @@ def timed_steps(a, dist, step_fn, sampler, stream):
     return dist.max(start.elapsed_time(stop)), prof, clocks
 
 
+def kernel_table(prof, steps, bytes_per_launch, peak):
+    """Per kernel: launches and device time per step, and, where its
+    algorithmic bytes are known, the HBM throughput they imply over its
+    launch time and that as a fraction of the measured peak."""
+    out = {}
+    for k, (launches, total_ms) in prof.items():
+        e = {"launches": launches, "ms_per_step": round(total_ms / steps, 5)}
+        algo = bytes_per_launch.get(k)
+        if algo and launches and total_ms > 0:
+            gbs = algo / (total_ms / launches / 1e3) / 1e9
+            e["algorithmic_gbs"] = round(gbs, 1)
+            e["frac"] = round(gbs / peak, 4)
+        out[k] = e
+    return out
+
+
 def roofline(prof, bytes_per_launch, peak, peak_kind, traffic_file=None):
     """The roofline object of the kernel with the largest device time."""
     name, (launches, total_ms) = max(prof.items(), key=lambda kv: kv[1][1])
@@ -275,6 +291,9 @@ def tree_bytes_per_launch(n):
         "treelet_kernel": 48 * nn * 2 + 8 * nn * 2,
         "emit_kernel": 48 * nn + 36 * nn + 4 * nn,
         "roots_kernel": 14 * nn,
+        # ATRBVH commit walk: leaf records, faces and vertices in; bounds, collapsed records, counts, costs,
+        # summaries, leaf boxes + transforms and marks out
+        "walk_kernel": 36 * n + 52 * n + 24 * ni + 36 * nn + 8 * nn + 112 * ni + 124 * n + nn,
         "gather_kernel": 8 * nn,
         "gather_ranked_kernel": 8 * nn,
         "scan_tile_sums": 4 * nn,
@@ -342,7 +361,7 @@ def bench_tree_ours(a, dist, atrbvh=False):
     ms_step = total_ms / a.steps
     value = dist.world * nn * a.steps / (total_ms / 1e3) / 1e6
     peak, peak_kind = peaks()
-    kern = {k: {"launches": v[0], "ms_per_step": round(v[1] / a.steps, 5)} for k, v in prof.items()}
+    kern = kernel_table(prof, a.steps, tree_bytes_per_launch(n), peak)
     roof = roofline(prof, tree_bytes_per_launch(n), peak, peak_kind,
                     os.path.join(ROOT, "profiles", f"{wname}_traffic.json"))
     launches = sum(v[0] for v in prof.values())
@@ -569,8 +588,8 @@ def bench_dito_ours(a, dist):
         return {"profile": "dito", "points": n, "ms_per_step": total_ms / a.steps, "kernels": prof}
     peak, peak_kind = peaks()
     value = dist.world * n * a.steps / (total_ms / 1e3) / 1e6
-    roof = roofline(prof, {"dito_extremal_pass": 12 * n, "dito_extent_pass": 12 * n}, peak, peak_kind,
-                    os.path.join(ROOT, "profiles", "dito_traffic.json"))
+    dito_bytes = {"dito_extremal_pass": 12 * n, "dito_extent_pass": 12 * n}
+    roof = roofline(prof, dito_bytes, peak, peak_kind, os.path.join(ROOT, "profiles", "dito_traffic.json"))
 
     host = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
     host.copy_(sets[0])
@@ -590,7 +609,7 @@ def bench_dito_ours(a, dist):
         "config": {"workload": "dito_plain_fit", "points_per_gpu": n, "point_bytes": 12,
                    "l2": "two 1.2 GB point sets alternated between steps (> 126 MB L2), no flush",
                    "parallelism": f"replicas{dist.world}", "path": path},
-        "kernels": {k: {"launches": v[0], "ms_per_step": round(v[1] / a.steps, 5)} for k, v in prof.items()},
+        "kernels": kernel_table(prof, a.steps, dito_bytes, peak),
         "gpu_launches": sum(v[0] for v in prof.values()), "roofline": roof,
         "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mpoints/s", "h2d_bytes_per_step": 12 * n,
                 "d2h_bytes_per_step": 316, "api": "obvh_points_obb (kr_cuda_points_obb with errors), pinned host"},
@@ -664,7 +683,8 @@ def bench_batch_ours(a, dist):
     peak, peak_kind = peaks()
     value = dist.world * total * a.steps / (total_ms / 1e3) / 1e6
     # every set (at most 3 MB) fits in L2 between its two passes: 12 B/point compulsory
-    roof = roofline(prof, {"dito_batch_kernel": 12 * total}, peak, peak_kind,
+    batch_bytes = {"dito_batch_kernel": 12 * total}
+    roof = roofline(prof, batch_bytes, peak, peak_kind,
                     os.path.join(ROOT, "profiles", "dito_batch_traffic.json"))
 
     # plain per-call path on the same device-resident buffer: one fit per set
@@ -712,7 +732,7 @@ def bench_batch_ours(a, dist):
                    "l2": f"{12 * total / 1e9:.2f} GB of points per step (> 126 MB L2), no flush",
                    "launch": "one graph: memset + one persistent kernel", "tuning": tuning,
                    "autotuned_ms": tuned_ms, "parallelism": f"replicas{dist.world}"},
-        "kernels": {k: {"launches": v[0], "ms_per_step": round(v[1] / a.steps, 5)} for k, v in prof.items()},
+        "kernels": kernel_table(prof, a.steps, batch_bytes, peak),
         "gpu_launches": sum(v[0] for v in prof.values()), "roofline": roof,
         "per_call": {"value": round(pc_value, 3), "unit": "Mpoints/s", "ms_per_batch": round(pc_ms, 3),
                      "api": "obvh_dito_fit_async per set (2 kernels per set), same device buffer",
