@@ -519,7 +519,8 @@ __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, floa
             if (lane == 0) atomicOr(err, kErrCycle);
             break;
         }
-        __threadfence();
+        // (the arrival's release orders this lane's writes; the lanes that
+        // rewrote a treelet fenced theirs before the warp synchronised)
         int32_t count = 0;
         if (cur >= 0) {
             if (cur >= internal) {
