@@ -213,8 +213,11 @@ __global__ void __launch_bounds__(kThreads) boxes_up_kernel(const kr_vec3* verts
             atomicOr(err, kErrCycle);
             return;
         }
+        // p's children and parent are final before this kernel: read them
+        // ahead of the arrival
+        const int32_t L = __ldg(&t[p].left), R = __ldg(&t[p].right);
+        const int32_t grand = __ldg(&t[p].parent);
         if (tree::arrive(visits + p) == 0) return;
-        const int32_t L = __ldcg(&t[p].left), R = __ldcg(&t[p].right);
         const int32_t sib = L == child ? R : L;
         if (sib < 0 || sib >= static_cast<int32_t>(2 * n - 1)) {
             atomicOr(err, kErrCycle);
@@ -229,7 +232,7 @@ __global__ void __launch_bounds__(kThreads) boxes_up_kernel(const kr_vec3* verts
         }
         store_box(t, p, lo, hi);
         child = p;
-        p = __ldcg(&t[p].parent);
+        p = grand;
     }
 }
 
