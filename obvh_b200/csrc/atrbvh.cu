@@ -526,18 +526,25 @@ __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, floa
         // rewrote a treelet fenced theirs before the warp synchronised)
         int32_t count = 0;
         if (cur >= 0) {
+            // cur's children and area change only in cur's own treelet (or an
+            // ancestor's), later: read them ahead of the arrival
+            int32_t L = -1, R = -1;
+            float area = 0.f;
+            if (cur < internal) {
+                L = __ldcg(&t[cur].left);
+                R = __ldcg(&t[cur].right);
+                area = __ldcg(&t[cur].area);
+            }
             if (cur >= internal) {
                 atomicOr(err, kErrCycle);
                 cur = -1;
             } else if (tree::arrive(counters + cur) == 0) {
                 cur = -1;  // the first child to arrive stops; the second carries on
             } else {
-                const int32_t L = __ldcg(&t[cur].left), R = __ldcg(&t[cur].right);
                 if (L < 0 || L >= 2 * n - 1 || R < 0 || R >= 2 * n - 1) {
                     atomicOr(err, kErrCycle);
                     cur = -1;
                 } else {
-                    const float area = __ldcg(&t[cur].area);
                     count = __ldcg(tris + L) + __ldcg(tris + R);
                     __stcg(tris + cur, count);
                     __stcg(sah_arr + cur, ci * area + __ldcg(sah_arr + L) + __ldcg(sah_arr + R));
