@@ -25,6 +25,7 @@
 //                per 1,024 consecutive leaves stages their triangles in shared
 //                memory once and serves every node over them from there.
 //   finalize     the nodes of more than one unit or tile.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -372,6 +373,8 @@ struct ChainArgs {
     uint32_t* chains;
     uint32_t* chain_counts;
     uint32_t* err;
+    uint32_t* final_list;     // tiles: the nodes finalize_list_kernel finishes
+    uint32_t* final_count;
 };
 
 // The ancestors of tile tau's first leaf (side 0) and last leaf (side 1) whose
@@ -448,6 +451,14 @@ __global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* sum
         uint32_t* k = keys + 6 * static_cast<size_t>(a);
         k[0] = f2key(c.lo.x); k[1] = f2key(c.lo.y); k[2] = f2key(c.lo.z);
         k[3] = f2key(c.hi.x); k[4] = f2key(c.hi.y); k[5] = f2key(c.hi.z);
+    }
+    if (chain.parents && units != 0) {  // listed for finalize_list_kernel, one atomic per warp
+        namespace cg = cooperative_groups;
+        const cg::coalesced_group g = cg::coalesced_threads();
+        uint32_t base = 0;
+        if (g.thread_rank() == 0) base = atomicAdd(chain.final_count, g.size());
+        base = g.shfl(base, 0);
+        chain.final_list[base + g.thread_rank()] = a;
     }
 }
 
@@ -708,6 +719,22 @@ __global__ void __launch_bounds__(kThreads) extents_tile_kernel(const Cand* cand
     }
 }
 
+// The listed nodes (those finished through the keys), one thread each.
+__global__ void __launch_bounds__(kThreads) finalize_list_kernel(const Cand* cand, const uint32_t* list,
+                                                                 const uint32_t* count, const uint32_t* keys,
+                                                                 uint32_t internal, kr_obb3* obbs, kr_mat4* xfs,
+                                                                 const uint32_t* err) {
+    if (*err) return;
+    const uint32_t total = min(*count, internal);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const uint32_t a = list[i];
+        if (a >= internal) continue;
+        const uint32_t* k = keys + 6 * static_cast<size_t>(a);
+        finalize_node(load_cand(cand, a), mk3(key2f(k[0]), key2f(k[1]), key2f(k[2])),
+                      mk3(key2f(k[3]), key2f(k[4]), key2f(k[5])), obbs + a, xfs + a);
+    }
+}
+
 // Nodes handled in warp units: the box from the extents in the keys (one unit:
 // written by it; several: the atomic min/max over the units).
 __global__ void __launch_bounds__(kThreads) finalize_multi_kernel(const Cand* cand, const uint32_t* nunits,
@@ -826,7 +853,7 @@ kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs,
     const bool tiled = b.chains != nullptr;
     const uint32_t ntiles = (n + kTile - 1) >> kTileShift;
     ChainArgs chain{tiled ? b.parents : nullptr, b.first, n, tiled ? (2 * ntiles + kThreads - 1) / kThreads : 0u,
-                    b.chains, b.chain_counts, b.err};
+                    b.chains, b.chain_counts, b.err, b.ustart, b.total_units};
     if (tiled && !b.parents) return "enqueue_frames: tiled extents need the parents";
     {
         // the chain walks go first, so that they overlap the candidate search
@@ -843,8 +870,11 @@ kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs,
         }
         OBVH_TRY_CUDA(cudaGetLastError());
         {
-            ProfScope prof_scope_("finalize_multi_kernel", s);
-            finalize_multi_kernel<<<gi, kThreads, 0, s>>>(cand, b.nunits, b.keys, internal, obbs, xfs, b.err);
+            // the list is a few percent of the nodes; its length is on the device
+            const unsigned cap = 2u * static_cast<unsigned>(device_info().sm_count);
+            ProfScope prof_scope_("finalize_list_kernel", s);
+            finalize_list_kernel<<<gi < cap ? gi : cap, kThreads, 0, s>>>(cand, b.ustart, b.total_units, b.keys,
+                                                                           internal, obbs, xfs, b.err);
         }
         OBVH_TRY_CUDA(cudaGetLastError());
         return kr_success;

@@ -56,7 +56,7 @@ struct FrameBuffers {
     const float* tris;         // 9 floats per leaf, depth-first
     void* cand;                // cand_bytes(internal)
     uint32_t* nunits;          // internal entries each
-    uint32_t* ustart;
+    uint32_t* ustart;          // (tiles: the nodes finished through the keys, total_units of them)
     uint32_t* keys;            // 6 per internal node
     void* scan;                // scan_temp_bytes(internal)
     uint32_t* err;
