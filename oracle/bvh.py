@@ -39,6 +39,7 @@ def _bind():
         "oracle_lbvh_build": (None, [_f32, _u32, c.c_uint32, _node, _u32, _u32, _u32, _f32, _f32, _f32]),
         "oracle_leaf_obb": (None, [_f32, _f32, _f32]),
         "oracle_obb_tree": (c.c_int, [_node, _u32, _f32, _u32, c.c_uint32, c.c_uint32, _f32, _f32, _f32]),
+        "oracle_obb_summaries": (c.c_int, [_node, _f32, _u32, c.c_uint32, c.c_uint32, _f32, _f32, _f32]),
         "oracle_collapse": (c.c_int, [_node, _u32, _node, _u32, _u32, _f32, c.c_float, c.c_float, c.c_uint32,
                                       c.c_uint32]),
         "oracle_aabb_refit": (c.c_int, [_node, c.c_uint32, _u32, _f32]),
@@ -128,6 +129,22 @@ def obb_tree(nodes, parents, verts, faces):
     if rc != 0:
         raise ValueError("malformed tree")
     return obbs, xfs, axes[:ni]
+
+
+def obb_summaries(nodes, verts, faces):
+    """The subtree summaries in the reference's arrays: (min_proj [nodes x 7],
+    max_proj [nodes x 7], minmax pairs [nodes x 7 x 6])."""
+    l = _bind()
+    v, f, _ = _mesh(verts, faces)
+    nn = nodes.shape[0]
+    n = (nn + 1) // 2
+    mn = np.zeros((nn, 7), np.float32)
+    mx = np.zeros((nn, 7), np.float32)
+    pairs = np.zeros((nn, 7, 6), np.float32)
+    if l.oracle_obb_summaries(np.ascontiguousarray(nodes), v, f, n, n - 1, mn.reshape(-1), mx.reshape(-1),
+                              pairs.reshape(-1)) != 0:
+        raise ValueError("malformed tree")
+    return mn, mx, pairs
 
 
 def collapse(nodes, parents, counts, costs, ci=1.2, ct=1.0):
@@ -233,3 +250,84 @@ def ref_atrbvh():
         f.restype = res
         f.argtypes = args
     return r
+
+
+# ---- the reference's own GPU tree kernels (oracle/_ref/libref_tree_gpu*.so) --
+# Built for sm_100a from lbvh.cu / transforms.cu by oracle/Makefile; the calls
+# below need a GPU.  variant "nofma": compiled with --fmad=false, the
+# arithmetic of the restatement; "fmad": nvcc's default contraction, the
+# reference as its own build compiles it.
+_REF_GPU = {"nofma": "libref_tree_gpu.so", "fmad": "libref_tree_gpu_fmad.so"}
+_ref_gpu = {}
+
+
+def ref_gpu_available(variant: str = "nofma") -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", _REF_GPU[variant]))
+
+
+def ref_gpu(variant: str = "nofma"):
+    if variant not in _ref_gpu:
+        p = os.path.join(HERE, "_ref", _REF_GPU[variant])
+        if not os.path.exists(p):
+            raise FileNotFoundError(p)
+        l = ctypes.CDLL(p)
+        c = ctypes
+        l.refgpu_lbvh.restype = c.c_int
+        l.refgpu_lbvh.argtypes = [_f32, c.c_uint32, _u32, c.c_uint32, _f32, _node, _u32, _u32, _u32, _f32]
+        l.refgpu_obb_from_summaries.restype = c.c_int
+        l.refgpu_obb_from_summaries.argtypes = [_node, _u32, _u32, _f32, c.c_uint32, _u32, c.c_uint32, _f32, _f32,
+                                                _f32, _f32, _f32]
+        l.refgpu_collapse.restype = c.c_int
+        l.refgpu_collapse.argtypes = [_node, _u32, _u32, _f32, c.c_float, c.c_float, c.c_uint32, _node, _u32]
+        _ref_gpu[variant] = l
+    return _ref_gpu[variant]
+
+
+def refgpu_lbvh(verts, faces, variant: str = "nofma"):
+    """The reference's LBVH kernels (codes, stable sort, Karras tree, bottom-up
+    boxes, counts, costs) on the oracle's centroid box: dict as lbvh_build."""
+    l = ref_gpu(variant)
+    v, f, n = _mesh(verts, faces)
+    _, centroid = scene_bounds(verts, faces)
+    nn = 2 * n - 1
+    out = {"nodes": np.zeros(nn, NODE), "parents": np.zeros(nn, np.uint32), "codes": np.zeros(n, np.uint32),
+           "counts": np.zeros(nn, np.uint32), "costs": np.zeros(nn, np.float32)}
+    rc = l.refgpu_lbvh(v, v.shape[0] // 3, f, n, centroid, out["nodes"], out["parents"], out["codes"], out["counts"],
+                       out["costs"])
+    if rc != 0:
+        raise RuntimeError(f"refgpu_lbvh: CUDA error {rc}")
+    return out
+
+
+def refgpu_obb_tree(nodes, parents, counts, verts, faces, variant: str = "nofma"):
+    """The reference's candidate, refit and finalize kernels on the oracle's
+    subtree summaries: (obbs [nodes x 15], transforms [nodes x 16])."""
+    l = ref_gpu(variant)
+    v, f, n = _mesh(verts, faces)
+    mn, mx, pairs = obb_summaries(nodes, verts, faces)
+    nn = 2 * n - 1
+    obbs = np.zeros((nn, 15), np.float32)
+    xfs = np.zeros((nn, 16), np.float32)
+    rc = l.refgpu_obb_from_summaries(np.ascontiguousarray(nodes), np.ascontiguousarray(parents, np.uint32),
+                                     np.ascontiguousarray(counts, np.uint32), v, v.shape[0] // 3, f, n,
+                                     mn.reshape(-1), mx.reshape(-1), pairs.reshape(-1), obbs.reshape(-1),
+                                     xfs.reshape(-1))
+    if rc != 0:
+        raise RuntimeError(f"refgpu_obb_from_summaries: CUDA error {rc}")
+    return obbs, xfs
+
+
+def refgpu_collapse(nodes, parents, counts, costs, ci=1.2, ct=1.0, variant: str = "nofma"):
+    """kr_cuda_bvh_collapse: (collapsed nodes, counts, primitives, costs)."""
+    l = ref_gpu(variant)
+    nn = nodes.shape[0]
+    n = (nn + 1) // 2
+    out = np.zeros(nn, NODE)
+    cnt = np.ascontiguousarray(counts, np.uint32).copy()
+    cst = np.ascontiguousarray(costs, np.float32).copy()
+    prims = np.zeros(n, np.uint32)
+    rc = l.refgpu_collapse(np.ascontiguousarray(nodes), np.ascontiguousarray(parents, np.uint32), cnt, cst, ci, ct, n,
+                           out, prims)
+    if rc != 0:
+        raise RuntimeError(f"refgpu_collapse: CUDA error {rc}")
+    return out, cnt, prims, cst

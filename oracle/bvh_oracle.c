@@ -18,13 +18,16 @@
  *   - collapsed-leaf primitive lists are laid out by an exclusive scan over
  *     collapse roots in node-index order (transforms.cu:188,199 use
  *     atomicAdd); the list contents and order are the reference's.
- * Floating point is restated uncontracted (compile with -ffp-contract=off):
- * the reference built with --fmad=false.
+ * Floating point is restated uncontracted (compile with -ffp-contract=off),
+ * the arithmetic of the reference's kernels built with --fmad=false.
  *
- * Parity unpinned by the reference for the tree path: it has no tests or
- * golden data, and its GPU kernels cannot run here.  The pieces that exist
- * as host-callable reference code (Morton encoding, kr_minverse4, kr_mmul4,
- * kr_aabb_surface_area3) are pinned against it by tests/test_oracle_bvh.py.
+ * Pinned against the reference itself: tests/test_ref_gpu_pin.py runs the
+ * reference's own lbvh.cu / transforms.cu kernels (oracle/_ref, built by
+ * oracle/Makefile) on the GPU and requires every output of this restatement
+ * bit for bit from the --fmad=false build; its subtree-summary pass, which
+ * is not run, is fed from oracle_obb_summaries.  The host-callable pieces
+ * (Morton encoding, kr_minverse4, kr_mmul4, kr_aabb_surface_area3) are also
+ * pinned on the CPU by tests/test_oracle_bvh.py.
  */
 #include <math.h>
 #include <stdint.h>
@@ -518,29 +521,73 @@ void oracle_leaf_obb(const float* tri9, float obb[15], float xf[16]) {
     write_box(obb, xf, a0, a1, a2, lo, hi);
 }
 
+/* The subtree summaries of every node (calculate_obbs_kernel_shared,
+ * transforms.cu:287-411): leaves from their triangle, internal nodes in post
+ * order, the left child's summary merged with the right one's.  Returns the
+ * post order's length, n_internal for a well-formed tree. */
+static int64_t summaries(const obvh_oracle_node* nodes, const float* verts, const uint32_t* faces4,
+                         uint32_t n_leaves, uint32_t n_internal, summary* sm) {
+    for (uint32_t j = 0; j < n_leaves; j++) {
+        uint32_t f = nodes[n_internal + j].left;
+        v3 a = vtx(verts, faces4[4 * f]), b = vtx(verts, faces4[4 * f + 1]), c = vtx(verts, faces4[4 * f + 2]);
+        leaf_summary(a, b, c, &sm[n_internal + j]);
+    }
+    uint32_t* po = malloc(sizeof(uint32_t) * (n_internal + 1));
+    int64_t m = post_order(nodes, n_internal, po);
+    if (m == (int64_t)n_internal) {
+        for (int64_t k = 0; k < m; k++) {
+            uint32_t v = po[k];
+            sm[v] = sm[nodes[v].left];
+            merge_summary(&sm[v], &sm[nodes[v].right]);
+        }
+    }
+    free(po);
+    return m;
+}
+
+/* The summaries in the reference's arrays: per node 7 minimum and 7 maximum
+ * projections, and 7 (min point, max point) pairs of 6 floats (kr_minmax_pair).
+ * Returns 0, or -1 for a malformed tree. */
+int oracle_obb_summaries(const obvh_oracle_node* nodes, const float* verts, const uint32_t* faces4,
+                         uint32_t n_leaves, uint32_t n_internal, float* min_proj, float* max_proj,
+                         float* pairs) {
+    const uint32_t nn = n_leaves + n_internal;
+    summary* sm = malloc(sizeof(summary) * nn);
+    if (summaries(nodes, verts, faces4, n_leaves, n_internal, sm) != (int64_t)n_internal) {
+        free(sm);
+        return -1;
+    }
+    for (uint32_t v = 0; v < nn; v++) {
+        memcpy(min_proj + 7 * v, sm[v].lo, 28);
+        memcpy(max_proj + 7 * v, sm[v].hi, 28);
+        for (int k = 0; k < 7; k++) {
+            float* p = pairs + 42 * (size_t)v + 6 * k;
+            p[0] = sm[v].plo[k].x; p[1] = sm[v].plo[k].y; p[2] = sm[v].plo[k].z;
+            p[3] = sm[v].phi[k].x; p[4] = sm[v].phi[k].y; p[5] = sm[v].phi[k].z;
+        }
+    }
+    free(sm);
+    return 0;
+}
+
 int oracle_obb_tree(const obvh_oracle_node* nodes, const uint32_t* parents, const float* verts,
                     const uint32_t* faces4, uint32_t n_leaves, uint32_t n_internal, float* obbs, float* xfs,
                     float* axes_out) {
-    (void)parents;
     const uint32_t nn = n_leaves + n_internal;
     summary* sm = malloc(sizeof(summary) * nn);
     float* mn = malloc(sizeof(float) * 7 * nn);
     float* mx = malloc(sizeof(float) * 7 * nn);
+    if (summaries(nodes, verts, faces4, n_leaves, n_internal, sm) != (int64_t)n_internal) {
+        free(sm); free(mn); free(mx);
+        return -1;
+    }
     for (uint32_t j = 0; j < n_leaves; j++) {
-        const obvh_oracle_node* lf = &nodes[n_internal + j];
-        uint32_t f = lf->left;
+        uint32_t f = nodes[n_internal + j].left;
         v3 a = vtx(verts, faces4[4 * f]), b = vtx(verts, faces4[4 * f + 1]), c = vtx(verts, faces4[4 * f + 2]);
-        leaf_summary(a, b, c, &sm[n_internal + j]);
         float tri9[9] = { a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z };
         oracle_leaf_obb(tri9, obbs + 15 * (n_internal + j), xfs + 16 * (n_internal + j));
     }
-    uint32_t* po = malloc(sizeof(uint32_t) * (n_internal + 1));
-    int64_t m = post_order(nodes, n_internal, po);
-    if (m != (int64_t)n_internal) { free(po); free(sm); free(mn); free(mx); return -1; }
-    for (int64_t k = 0; k < m; k++) {
-        uint32_t v = po[k];
-        sm[v] = sm[nodes[v].left];
-        merge_summary(&sm[v], &sm[nodes[v].right]);
+    for (uint32_t v = 0; v < n_internal; v++) {
         memcpy(mn + 7 * v, sm[v].lo, 28);
         memcpy(mx + 7 * v, sm[v].hi, 28);
     }
@@ -587,7 +634,6 @@ int oracle_obb_tree(const obvh_oracle_node* nodes, const uint32_t* parents, cons
     }
     if (axes_out) memcpy(axes_out, ax, sizeof(float) * 9 * n_internal);
     free(ax);
-    free(po);
     free(sm);
     free(mn);
     free(mx);

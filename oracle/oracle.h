@@ -50,6 +50,9 @@ void oracle_lbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, o
                        float scene[6], float centroid[6]);
 int oracle_aabb_refit(obvh_oracle_node* nodes, uint32_t n, uint32_t* counts, float* costs);
 void oracle_leaf_obb(const float* tri9, float obb[15], float xf[16]);
+int oracle_obb_summaries(const obvh_oracle_node* nodes, const float* verts, const uint32_t* faces4,
+                         uint32_t n_leaves, uint32_t n_internal, float* min_proj, float* max_proj,
+                         float* pairs);
 int oracle_obb_tree(const obvh_oracle_node* nodes, const uint32_t* parents, const float* verts,
                     const uint32_t* faces4, uint32_t n_leaves, uint32_t n_internal, float* obbs, float* xfs,
                     float* axes_out);

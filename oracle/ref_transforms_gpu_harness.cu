@@ -1,0 +1,128 @@
+/*
+ * ref_transforms_gpu_harness.cu - TEST INFRASTRUCTURE ONLY.  The reference's
+ * OBB-tree transform and node collapse (src/ads/common/cuda/transforms.cu,
+ * included from the reference tree by oracle/Makefile into oracle/_ref), with
+ * extern "C" entry points over host arrays for tests/test_ref_gpu_pin.py,
+ * which runs them on the GPU to pin the oracle's restatement to the
+ * reference's own kernels.  The product never links it.
+ *
+ * What runs, with the launch shapes of kr_cuda_bvh_obb_tree
+ * (transforms.cu:966-1059): calculate_candidate_obb_kernel,
+ * refit_obbs_kernel_new and finalize_obbs_kernel; and kr_cuda_bvh_collapse
+ * itself (transforms.cu:1061-1125).  All of them are one thread per node or
+ * leaf, with leaf-to-root walks and compare-and-swap loops that end.
+ *
+ * What does not run: calculate_obbs_kernel_shared (transforms.cu:287-411).
+ * Its threads return early before a __syncthreads() (:311-316) and leave the
+ * walk loop that holds the next __syncthreads() at different trips
+ * (:345-410), a barrier the CUDA programming model leaves undefined.  Its
+ * output, the 7-slab subtree summaries, comes from the oracle
+ * (oracle_obb_summaries) instead, in the same arrays.
+ */
+#include "ads/common/cuda/transforms.cu"
+
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+static_assert(sizeof(kr_bvh_node) == 36, "kr_bvh_node layout");
+static_assert(sizeof(kr_obb3) == 60, "kr_obb3 layout");
+static_assert(sizeof(kr_mat4) == 64, "kr_mat4 layout");
+static_assert(sizeof(kr_minmax_pair) == 24, "kr_minmax_pair layout");
+
+namespace {
+
+// Device buffers of one call, freed on return; the first CUDA error is kept.
+struct Arena {
+    std::vector<void*> ptrs;
+    cudaError_t err = cudaSuccess;
+    void note(cudaError_t e) {
+        if (err == cudaSuccess && e != cudaSuccess) err = e;
+    }
+    void* zeroed(size_t bytes) {
+        void* p = nullptr;
+        note(cudaMalloc(&p, bytes ? bytes : 4));
+        if (p) {
+            ptrs.push_back(p);
+            note(cudaMemset(p, 0, bytes ? bytes : 4));
+        }
+        return p;
+    }
+    void* copy(const void* h, size_t bytes) {
+        void* p = zeroed(bytes);
+        if (p && bytes) note(cudaMemcpy(p, h, bytes, cudaMemcpyHostToDevice));
+        return p;
+    }
+    void back(void* h, const void* d, size_t bytes) {
+        if (err == cudaSuccess && bytes) note(cudaMemcpy(h, d, bytes, cudaMemcpyDeviceToHost));
+    }
+    ~Arena() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+// The transform's candidate, refit and finalize stages on a tree whose
+// summaries are given.  nodes: 2n - 1 kr_bvh_node; parents, counts: 2n - 1;
+// faces4: n x 4; min_proj, max_proj: (2n - 1) x 7; pairs: (2n - 1) x 7 x 6.
+// Writes obbs (2n - 1) x 15 and xfs (2n - 1) x 16.  Returns 0 or the CUDA
+// error code; -1 when n < 2.
+extern "C" int refgpu_obb_from_summaries(const void* nodes, const uint32_t* parents, const uint32_t* counts,
+                                         const float* verts, uint32_t n_verts, const uint32_t* faces4, uint32_t n,
+                                         const float* min_proj, const float* max_proj, const float* pairs,
+                                         float* obbs, float* xfs) {
+    if (n < 2) return -1;
+    const u32 ni = n - 1, nn = 2 * n - 1;
+    Arena a;
+    auto* d_nodes = static_cast<kr_bvh_node*>(a.copy(nodes, sizeof(kr_bvh_node) * nn));
+    auto* d_parents = static_cast<u32*>(a.copy(parents, 4ull * nn));
+    auto* d_counts = static_cast<u32*>(a.copy(counts, 4ull * nn));
+    auto* d_verts = static_cast<kr_vec3*>(a.copy(verts, 12ull * n_verts));
+    auto* d_faces = static_cast<kr_uvec4*>(a.copy(faces4, 16ull * n));
+    auto* d_min = static_cast<kr_scalar*>(a.copy(min_proj, 28ull * nn));
+    auto* d_max = static_cast<kr_scalar*>(a.copy(max_proj, 28ull * nn));
+    auto* d_pairs = static_cast<kr_minmax_pair*>(a.copy(pairs, 168ull * nn));
+    auto* d_obbs = static_cast<kr_obb3*>(a.zeroed(sizeof(kr_obb3) * nn));
+    auto* d_xfs = static_cast<kr_mat4*>(a.zeroed(sizeof(kr_mat4) * nn));
+    auto* d_visit = static_cast<b32*>(a.zeroed(4ull * ni));
+    if (a.err != cudaSuccess) return static_cast<int>(a.err);
+
+    calculate_candidate_obb_kernel<<<(ni + 31) / 32, 32>>>(d_obbs, d_min, d_max, d_pairs, n, ni);
+    a.note(cudaGetLastError());
+    refit_obbs_kernel_new<<<(n + 127) / 128, 128>>>(d_nodes, d_verts, d_faces, d_obbs, d_xfs, d_parents, d_counts,
+                                                    nullptr, d_visit, d_min, d_max, n, ni);
+    a.note(cudaGetLastError());
+    finalize_obbs_kernel<<<(ni + 511) / 512, 512>>>(d_nodes, d_min, d_max, d_obbs, d_xfs, n, ni);
+    a.note(cudaGetLastError());
+    a.note(cudaDeviceSynchronize());
+    a.back(obbs, d_obbs, sizeof(kr_obb3) * nn);
+    a.back(xfs, d_xfs, sizeof(kr_mat4) * nn);
+    return static_cast<int>(a.err);
+}
+
+// kr_cuda_bvh_collapse on a tree with its counts and costs.  counts and costs
+// (2n - 1) are updated in place as the reference updates them; collapsed
+// receives 2n - 1 nodes and prims n primitive ids.  Returns 0 or the CUDA
+// error code; -1 when n < 2.
+extern "C" int refgpu_collapse(const void* nodes, const uint32_t* parents, uint32_t* counts, float* costs, float ci,
+                               float ct, uint32_t n, void* collapsed, uint32_t* prims) {
+    if (n < 2) return -1;
+    const u32 ni = n - 1, nn = 2 * n - 1;
+    Arena a;
+    auto* d_nodes = static_cast<kr_bvh_node*>(a.copy(nodes, sizeof(kr_bvh_node) * nn));
+    auto* d_parents = static_cast<u32*>(a.copy(parents, 4ull * nn));
+    auto* d_counts = static_cast<u32*>(a.copy(counts, 4ull * nn));
+    auto* d_costs = static_cast<kr_scalar*>(a.copy(costs, 4ull * nn));
+    auto* d_collapsed = static_cast<kr_bvh_node*>(a.zeroed(sizeof(kr_bvh_node) * nn));
+    auto* d_prims = static_cast<u32*>(a.zeroed(4ull * n));
+    if (a.err != cudaSuccess) return static_cast<int>(a.err);
+    kr_cuda_bvh_collapse(d_nodes, d_parents, d_collapsed, d_counts, d_prims, d_costs, ci, ct, n, ni, nullptr);
+    a.note(cudaGetLastError());
+    a.note(cudaDeviceSynchronize());
+    a.back(collapsed, d_collapsed, sizeof(kr_bvh_node) * nn);
+    a.back(counts, d_counts, 4ull * nn);
+    a.back(costs, d_costs, 4ull * nn);
+    a.back(prims, d_prims, 4ull * n);
+    return static_cast<int>(a.err);
+}

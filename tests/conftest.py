@@ -17,6 +17,27 @@ def pytest_configure(config):
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
+def deep_or_tied_mesh(layout: str):
+    """Trees far from balanced, as (vertices, faces): centroids on a geometric
+    sequence along the diagonal ("geometric": a chain of key bits, so leaf
+    ranges cross CTA and tile edges high up), or 37 centroids shared by 811
+    triangles each ("duplicates": keys tied, split by index)."""
+    rng = np.random.default_rng(7)
+    if layout == "geometric":
+        k = rng.integers(0, 10, size=30_000)
+        c = (0.5 ** k)[:, None] * np.ones((1, 3)) * 0.999 + rng.uniform(0, 1e-4, size=(30_000, 1))
+    else:
+        c = np.repeat(rng.uniform(0, 1, size=(37, 3)), 811, axis=0)
+    n = c.shape[0]
+    tri = np.array([[0, 0, 0], [1e-3, 0, 0], [0, 1e-3, 0]], np.float64)
+    v = (c[:, None, :] + tri[None]).reshape(-1, 3).astype(np.float32)
+    f = np.zeros((n, 4), np.uint32)
+    f[:, 0] = np.arange(0, 3 * n, 3)
+    f[:, 1] = f[:, 0] + 1
+    f[:, 2] = f[:, 0] + 2
+    return v, f
+
+
 def golden_dito():
     d = np.load(os.path.join(GOLDEN, "dito_golden.npz"))
     for i, name in enumerate(d["names"]):

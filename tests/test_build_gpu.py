@@ -3,7 +3,7 @@ collapse in one chain) against the oracle running the three steps in turn."""
 import numpy as np
 import pytest
 
-from conftest import same_bits
+from conftest import deep_or_tied_mesh, same_bits
 from oracle import bvh as ref
 from obvh_b200 import bvh, workloads
 
@@ -94,22 +94,7 @@ def test_fused_build_partial_flags(builder, flags):
 
 @pytest.mark.parametrize("layout", ["geometric", "duplicates"])
 def test_fused_build_deep_and_tied_trees(builder, layout):
-    """Trees far from balanced: centroids on a geometric sequence along the
-    diagonal (a chain of key bits, so leaf ranges cross CTA and tile edges
-    high up), or many triangles sharing each centroid (keys tied, split by
-    index)."""
-    rng = np.random.default_rng(7)
-    if layout == "geometric":
-        k = rng.integers(0, 10, size=30_000)
-        c = (0.5 ** k)[:, None] * np.ones((1, 3)) * 0.999 + rng.uniform(0, 1e-4, size=(30_000, 1))
-    else:
-        c = np.repeat(rng.uniform(0, 1, size=(37, 3)), 811, axis=0)
-    n = c.shape[0]
-    tri = np.array([[0, 0, 0], [1e-3, 0, 0], [0, 1e-3, 0]], np.float64)
-    v = (c[:, None, :] + tri[None]).reshape(-1, 3).astype(np.float32)
-    f = np.zeros((n, 4), np.uint32)
-    f[:, 0] = np.arange(0, 3 * n, 3)
-    f[:, 1] = f[:, 0] + 1
-    f[:, 2] = f[:, 0] + 2
+    """Trees far from balanced (conftest.deep_or_tied_mesh)."""
+    v, f = deep_or_tied_mesh(layout)
     o, slots = _run(builder, v, f, 3)
-    _check(o, slots, _expect(v, f), n, 3)
+    _check(o, slots, _expect(v, f), f.shape[0], 3)
