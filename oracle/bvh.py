@@ -331,3 +331,53 @@ def refgpu_collapse(nodes, parents, counts, costs, ci=1.2, ct=1.0, variant: str 
     if rc != 0:
         raise RuntimeError(f"refgpu_collapse: CUDA error {rc}")
     return out, cnt, prims, cst
+
+
+def refgpu_lbvh63_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_lbvh63_gpu.so"))
+
+
+_ref63 = None
+
+
+def refgpu_lbvh63(verts, faces):
+    """The reference's ATRBVH seed build on the GPU (LBVH.cu / CubWrapper.cu):
+    (sorted 63-bit codes, their triangle order, (left, right, parent, data))."""
+    global _ref63
+    if _ref63 is None:
+        l = ctypes.CDLL(os.path.join(HERE, "_ref", "libref_lbvh63_gpu.so"))
+        l.refgpu_lbvh63.restype = ctypes.c_int
+        l.refgpu_lbvh63.argtypes = [_f32, ctypes.c_uint32, _f32, _u64, _u32, _i32, _i32, _i32, _i32]
+        _ref63 = l
+    tri = triangles9(verts, faces)
+    n = tri.shape[0]
+    codes = np.zeros(n, np.uint64)
+    order = np.zeros(n, np.uint32)
+    arrs = [np.zeros(2 * n - 1, np.int32) for _ in range(4)]
+    rc = _ref63.refgpu_lbvh63(tri.reshape(-1), n, scene_box9(tri), codes, order, *arrs)
+    if rc != 0:
+        raise RuntimeError(f"refgpu_lbvh63: CUDA error {rc}")
+    return codes, order, tuple(arrs)
+
+
+def triangles9(verts, faces):
+    """The triangles as an n x 9 float32 soup."""
+    v = np.asarray(verts, np.float32).reshape(-1, 3)
+    f = np.asarray(faces, np.uint32).reshape(-1, np.asarray(faces).shape[-1])[:, :3]
+    return np.ascontiguousarray(v[f].reshape(-1, 9))
+
+
+def scene_box9(tri9):
+    """Union of the triangle boxes (min xyz, max xyz), atrbvh.cu:282-298."""
+    p = tri9.reshape(-1, 3)
+    return np.ascontiguousarray(np.concatenate([p.min(axis=0), p.max(axis=0)]), np.float32)
+
+
+def lbvh63_seed(verts, faces):
+    """The oracle's seed build: (sorted codes, order, (left, right, parent, data))."""
+    tri = triangles9(verts, faces)
+    box = scene_box9(tri)
+    keys = np.array([morton63(t, box) for t in tri], np.uint64)
+    order = np.argsort(keys, kind="stable").astype(np.uint32)
+    sorted_keys = keys[order]
+    return sorted_keys, order, karras63(sorted_keys, order)

@@ -13,6 +13,10 @@ in the reference's own arrays.
 * "nofma" is the reference built with --fmad=false, the arithmetic the
   restatement and the CUDA path use.  Every output must equal the oracle's bit
   for bit (zero signs aside), and the CUDA path's, checked directly here.
+* The ATRBVH seed build (oracle/_ref/libref_lbvh63_gpu.so: LBVH.cu and
+  CubWrapper.cu through their own host wrappers) must equal the oracle's
+  63-bit codes, order and Karras tree exactly.  Its node boxes and the treelet
+  optimiser are not run (barriers in divergent loops).
 * "fmad" is the reference as its own build compiles it: nvcc's default
   contraction of multiplies and adds.  Codes, order, topology, counts, boxes
   and collapse decisions must still be identical and costs within 1e-6
@@ -157,3 +161,34 @@ def test_reference_as_shipped(case):
     share, p999 = _frame_agreement(obbs, gb, n - 1)
     assert share >= 0.98, share
     assert p999 <= 1e-5, p999
+
+
+def _lattice():
+    g = np.stack(np.meshgrid(np.arange(12), np.arange(12), np.arange(12), indexing="ij"), -1).reshape(-1, 3)
+    c = np.repeat(g, 2, axis=0).astype(np.float32) * 0.5
+    tri = np.array([[0, 0, 0], [0.2, 0, 0], [0, 0.2, 0]], np.float32)
+    v = (c[:, None, :] + tri[None]).reshape(-1, 3)
+    n = c.shape[0]
+    f = np.zeros((n, 4), np.uint32)
+    f[:, 0] = np.arange(0, 3 * n, 3)
+    f[:, 1] = f[:, 0] + 1
+    f[:, 2] = f[:, 0] + 2
+    return v, f
+
+
+@pytest.mark.skipif(not ref.refgpu_lbvh63_available(), reason="oracle/_ref ATRBVH seed library not built")
+@pytest.mark.parametrize("case", [("soup", 2), ("soup", 3), ("soup", 1000), ("soup", 65_537), ("knot917k", 0),
+                                  ("lattice", 0), ("duplicates", 0)], ids=lambda c: f"{c[0]}{c[1] or ''}")
+def test_atrbvh_seed_kernels_equal_the_oracle(case):
+    if case[0] == "knot917k":
+        v, f = workloads.torus_knot_mesh()
+    elif case[0] == "lattice":
+        v, f = _lattice()
+    else:
+        v, f = _mesh(case)
+    codes, order, tree = ref.refgpu_lbvh63(v, f)
+    ocodes, oorder, otree = ref.lbvh63_seed(v, f)
+    assert np.array_equal(codes, ocodes)
+    assert np.array_equal(order, oorder)
+    for mine, theirs in zip(otree, tree):
+        assert np.array_equal(mine, theirs)
