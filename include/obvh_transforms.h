@@ -86,6 +86,52 @@ OBVH_EXPORT kr_error obvh_bvh_collapse_async(const kr_bvh_node* d_nodes, const k
                                              kr_u32 leaf_count, kr_u32 internal_count, void* d_workspace,
                                              void* stream);
 
+/*
+ * Traversal packing (transforms.cuh:26-38, transforms.cu:1252-1364).  Device
+ * pointers, node_count = 2n - 1 nodes, synchronous.  Each node's 64-byte
+ * record gets, for an internal node, both children's boxes and their indices
+ * (bitwise-negated for a child with primitives); for a node with primitives,
+ * its own box, its first primitive and one past its last.  The OBB form also
+ * copies both children's transforms into the pair of each internal node
+ * ((node_count - 1) / 2 pairs), writes the node's axis to metadata.z and skips
+ * hidden nodes (nPrimitives == 0xFFFF).  Fields the reference leaves alone
+ * (rbounds of a leaf, metadata.w, skipped records, pairs of leaf-type nodes)
+ * keep the caller's contents.  Replace kr_cuda_bvh_persistent and
+ * kr_cuda_obvh_persistent.
+ */
+OBVH_EXPORT kr_error kr_cuda_bvh_persistent(const kr_bvh_node* nodes, kr_bvh_node_packed* packed_nodes,
+                                            kr_u32 node_count);
+OBVH_EXPORT kr_error kr_cuda_obvh_persistent(const kr_bvh_node* nodes, const kr_mat4* transforms,
+                                             kr_bvh_node_packed* packed_nodes,
+                                             kr_bvh_transformation_pair* packed_transforms, kr_u32 node_count);
+/*
+ * SoA OBVH from packed records and pairs (kr_cuda_soa_obvh, transforms.cuh:
+ * 72-77, transforms.cu:1366-1449): left_T / right_T are the 4x3 parts of each
+ * internal node's pair, metadata each node's record metadata.  Allocates the
+ * three arrays and the struct on the device and stores the struct's device
+ * address in *soa_bvh (the reference's kr_SoA_OBVH*& is the same pointer
+ * argument at the C ABI).  Built on the device; the reference copies through
+ * the host.  Synchronous.  Free with obvh_soa_obvh_free.
+ */
+OBVH_EXPORT kr_error kr_cuda_soa_obvh(const kr_bvh_node_packed* packed_bvh,
+                                      const kr_bvh_transformation_pair* packed_transforms, kr_SoA_OBVH** soa_bvh,
+                                      kr_u32 internal_count, kr_u32 node_count);
+/* Frees what kr_cuda_soa_obvh allocated (NULL is a no-op).  No counterpart in
+ * the reference, which never frees it. */
+OBVH_EXPORT kr_error obvh_soa_obvh_free(kr_SoA_OBVH* soa_bvh);
+/*
+ * kr_cuda_obvh_persistent and kr_cuda_soa_obvh fused into one pass on
+ * `stream`, into caller arrays, without synchronising: d_transforms == NULL
+ * gives the AABB form (kr_cuda_bvh_persistent); d_left_t, d_right_t and
+ * d_metadata (all or none, internal_count / node_count entries) add the SoA
+ * arrays.  All arrays 16-byte aligned.  d_error (nullable) gets bit 0 set for
+ * a child index or an internal node outside the tree; such nodes are skipped.
+ * No counterpart in the reference.
+ */
+OBVH_EXPORT kr_error obvh_obvh_pack_async(const kr_bvh_node* d_nodes, const kr_mat4* d_transforms,
+                                          kr_bvh_node_packed* d_packed, kr_bvh_transformation_pair* d_pairs,
+                                          kr_mat43* d_left_t, kr_mat43* d_right_t, kr_ivec4* d_metadata,
+                                          kr_u32 node_count, kr_u32 internal_count, kr_u32* d_error, void* stream);
 /* Reads the device error word of the last transform made with a workspace
  * (synchronises `stream`): 0 ok, 4 parent walk longer than the tree. */
 OBVH_EXPORT kr_error obvh_obb_tree_error(const void* d_workspace, void* stream, kr_u32* device_error);

@@ -97,6 +97,11 @@ typedef struct {
 
 typedef struct { kr_mat4 l; kr_mat4 r; } kr_bvh_transformation_pair;
 
+/* SoA OBVH for traversal (ads.h:166-170): per internal node the two
+ * children's transforms as 4x3 matrices, per node the packed metadata
+ * (left, right, axis, w).  Device pointers. */
+typedef struct { kr_mat43* left_T; kr_mat43* right_T; kr_ivec4* metadata; } kr_SoA_OBVH;
+
 typedef struct { const char* key; const char* value; } kr_descriptor;
 typedef struct { kr_descriptor* descriptors; kr_size descriptor_count; } kr_descriptor_container;
 

@@ -51,6 +51,11 @@ def _declare(lib: ctypes.CDLL) -> None:
         "obvh_dito_fit_async": (err, [vp, c.c_uint64, c.c_uint32, vp, vp, vp]),
         "obvh_dito_fit_pass_async": (err, [vp, c.c_uint64, c.c_uint32, vp, vp, vp, c.c_int]),
         "obvh_points_obb_noalloc": (err, [vp, c.c_uint64, c.c_uint32, vp, vp]),
+        "kr_cuda_bvh_persistent": (err, [vp, vp, c.c_uint32]),
+        "kr_cuda_obvh_persistent": (err, [vp, vp, vp, vp, c.c_uint32]),
+        "kr_cuda_soa_obvh": (err, [vp, vp, c.POINTER(c.c_void_p), c.c_uint32, c.c_uint32]),
+        "obvh_soa_obvh_free": (err, [vp]),
+        "obvh_obvh_pack_async": (err, [vp, vp, vp, vp, vp, vp, vp, c.c_uint32, c.c_uint32, vp, vp]),
         "kr_cuda_bbox_calculate": (err, [vp, vp, c.c_uint32, vp]),
         "kr_cuda_centroid_bbox_calculate": (err, [vp, vp, c.c_uint32, vp]),
         "obvh_lbvh_workspace_bytes": (c.c_uint64, [c.c_uint32]),

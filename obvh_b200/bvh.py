@@ -279,3 +279,88 @@ class AtrbvhBuilder(ObvhBuilder):
         _native.check(self.lib.obvh_atrbvh_status(_ptr(self.ws), n, _stream(self.torch, stream), ctypes.byref(err),
                                                   ctypes.byref(slots)))
         return err.value, slots.value
+
+
+# ---- traversal packing (include/obvh_transforms.h) -------------------------
+PACKED = np.dtype([("lb", "<f4", (6,)), ("rb", "<f4", (6,)), ("meta", "<i4", (4,))])
+assert PACKED.itemsize == 64
+
+
+def persistent(nodes, node_count: int, transforms=None, packed=None, pairs=None):
+    """kr_cuda_bvh_persistent (transforms=None) or kr_cuda_obvh_persistent on
+    device tensors; packed / pairs are updated in place (zeroed when not given).
+    Returns dict(packed, pairs)."""
+    import torch
+    lib = _native.lib()
+    dev = nodes.device
+    ni = (node_count - 1) // 2
+    if packed is None:
+        packed = torch.zeros(node_count * 64, dtype=torch.uint8, device=dev)
+    if transforms is None:
+        _native.check(lib.kr_cuda_bvh_persistent(_ptr(nodes), _ptr(packed), node_count))
+        return {"packed": packed, "pairs": None}
+    if pairs is None:
+        pairs = torch.zeros(max(ni, 1) * 32, dtype=torch.float32, device=dev)
+    _native.check(lib.kr_cuda_obvh_persistent(_ptr(nodes), _ptr(transforms), _ptr(packed), _ptr(pairs), node_count))
+    return {"packed": packed, "pairs": pairs}
+
+
+def _cudart():
+    import ctypes.util
+    for name in ("libcudart.so", "libcudart.so.12", ctypes.util.find_library("cudart") or ""):
+        try:
+            return ctypes.CDLL(name)
+        except OSError:
+            continue
+    raise _native.ObvhError("the CUDA runtime library is needed to read a kr_SoA_OBVH back")
+
+
+def soa_obvh(packed, pairs, internal_count: int, node_count: int):
+    """kr_cuda_soa_obvh: the library allocates the SoA arrays on the device; this
+    reads them back (numpy left_T [ni x 12], right_T [ni x 12], metadata
+    [nodes x 4]) and frees them with obvh_soa_obvh_free."""
+    lib = _native.lib()
+    d_soa = ctypes.c_void_p(0)
+    _native.check(lib.kr_cuda_soa_obvh(_ptr(packed), _ptr(pairs), ctypes.byref(d_soa), internal_count, node_count))
+    rt = _cudart()
+    rt.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    try:
+        ptrs = (ctypes.c_void_p * 3)()
+        if rt.cudaMemcpy(ctypes.cast(ptrs, ctypes.c_void_p), d_soa, 24, 2) != 0:
+            raise _native.ObvhError("reading the kr_SoA_OBVH struct back failed")
+        out = {"left_T": np.zeros((internal_count, 12), np.float32),
+               "right_T": np.zeros((internal_count, 12), np.float32),
+               "metadata": np.zeros((node_count, 4), np.int32)}
+        for k, key in enumerate(("left_T", "right_T", "metadata")):
+            a = out[key]
+            if a.nbytes and rt.cudaMemcpy(a.ctypes.data_as(ctypes.c_void_p), ptrs[k], a.nbytes, 2) != 0:
+                raise _native.ObvhError("reading the SoA arrays back failed")
+        return out
+    finally:
+        _native.check(lib.obvh_soa_obvh_free(d_soa))
+
+
+def obvh_pack(nodes, node_count: int, internal_count: int, transforms=None, packed=None, pairs=None, soa=True,
+              stream=None):
+    """obvh_obvh_pack_async: packed records, pairs and (soa=True) the SoA
+    arrays in one pass on `stream`.  Returns dict(packed, pairs, left_T,
+    right_T, metadata, error) of device tensors (error: int32 [1])."""
+    import torch
+    lib = _native.lib()
+    dev = nodes.device
+    if packed is None:
+        packed = torch.zeros(node_count * 64, dtype=torch.uint8, device=dev)
+    out = {"packed": packed, "pairs": None, "left_T": None, "right_T": None, "metadata": None,
+           "error": torch.zeros(1, dtype=torch.int32, device=dev)}
+    if transforms is not None:
+        out["pairs"] = pairs if pairs is not None else torch.zeros(max(internal_count, 1) * 32, dtype=torch.float32,
+                                                                   device=dev)
+        if soa:
+            out["left_T"] = torch.empty(max(internal_count, 1) * 12, dtype=torch.float32, device=dev)
+            out["right_T"] = torch.empty(max(internal_count, 1) * 12, dtype=torch.float32, device=dev)
+            out["metadata"] = torch.empty(max(node_count, 1) * 4, dtype=torch.int32, device=dev)
+    _native.check(lib.obvh_obvh_pack_async(_ptr(nodes), _ptr(transforms), _ptr(packed), _ptr(out["pairs"]),
+                                           _ptr(out["left_T"]), _ptr(out["right_T"]), _ptr(out["metadata"]),
+                                           node_count, internal_count, _ptr(out["error"]),
+                                           _stream(torch, stream)))
+    return out

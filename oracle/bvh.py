@@ -40,6 +40,8 @@ def _bind():
         "oracle_leaf_obb": (None, [_f32, _f32, _f32]),
         "oracle_obb_tree": (c.c_int, [_node, _u32, _f32, _u32, c.c_uint32, c.c_uint32, _f32, _f32, _f32]),
         "oracle_obb_summaries": (c.c_int, [_node, _f32, _u32, c.c_uint32, c.c_uint32, _f32, _f32, _f32]),
+        "oracle_pack": (None, [_node, c.c_void_p, c.c_uint32, c.c_int, c.c_void_p, c.c_void_p]),
+        "oracle_soa_obvh": (None, [c.c_void_p, c.c_void_p, c.c_uint32, c.c_uint32, _f32, _f32, _i32]),
         "oracle_collapse": (c.c_int, [_node, _u32, _node, _u32, _u32, _f32, c.c_float, c.c_float, c.c_uint32,
                                       c.c_uint32]),
         "oracle_aabb_refit": (c.c_int, [_node, c.c_uint32, _u32, _f32]),
@@ -277,6 +279,8 @@ def ref_gpu(variant: str = "nofma"):
         l.refgpu_obb_from_summaries.restype = c.c_int
         l.refgpu_obb_from_summaries.argtypes = [_node, _u32, _u32, _f32, c.c_uint32, _u32, c.c_uint32, _f32, _f32,
                                                 _f32, _f32, _f32]
+        l.refgpu_pack.restype = c.c_int
+        l.refgpu_pack.argtypes = [_node, c.c_void_p, c.c_uint32, c.c_void_p, c.c_void_p, _f32, _f32, _i32]
         l.refgpu_collapse.restype = c.c_int
         l.refgpu_collapse.argtypes = [_node, _u32, _u32, _f32, c.c_float, c.c_float, c.c_uint32, _node, _u32]
         _ref_gpu[variant] = l
@@ -381,3 +385,62 @@ def lbvh63_seed(verts, faces):
     order = np.argsort(keys, kind="stable").astype(np.uint32)
     sorted_keys = keys[order]
     return sorted_keys, order, karras63(sorted_keys, order)
+
+
+# ---- traversal packing (pack_oracle.c) ---------------------------------------
+PACKED = np.dtype([("lb", "<f4", (6,)), ("rb", "<f4", (6,)), ("meta", "<i4", (4,))])
+assert PACKED.itemsize == 64
+
+
+def pack(nodes, transforms=None, packed=None, pairs=None):
+    """bvh_persistent_prepare (transforms None) or obvh_persistent_prepare over
+    every node, updating copies of packed [nodes] (PACKED) and pairs
+    [internal x 32] (zeros when not given): (packed, pairs)."""
+    l = _bind()
+    nodes = np.ascontiguousarray(nodes)
+    nn = nodes.shape[0]
+    ni = (nn - 1) // 2
+    pk = np.zeros(nn, PACKED) if packed is None else np.array(packed, PACKED, copy=True)
+    pr = np.zeros((max(ni, 1), 32), np.float32) if pairs is None else np.array(pairs, np.float32, copy=True)
+    xf = None if transforms is None else np.ascontiguousarray(transforms, np.float32)
+    l.oracle_pack(nodes, None if xf is None else xf.ctypes.data, nn, 0 if xf is None else 1, pk.ctypes.data,
+                  pr.ctypes.data)
+    return pk, pr
+
+
+def soa_obvh(packed, pairs, internal_count):
+    """kr_cuda_soa_obvh's arrays: (left_T [ni x 12], right_T [ni x 12], metadata [nodes x 4])."""
+    l = _bind()
+    pk = np.ascontiguousarray(packed, PACKED)
+    pr = np.ascontiguousarray(pairs, np.float32)
+    nn = pk.shape[0]
+    lt = np.zeros((max(internal_count, 1), 12), np.float32)
+    rt = np.zeros((max(internal_count, 1), 12), np.float32)
+    meta = np.zeros((nn, 4), np.int32)
+    l.oracle_soa_obvh(pk.ctypes.data, pr.ctypes.data, internal_count, nn, lt.reshape(-1), rt.reshape(-1),
+                      meta.reshape(-1))
+    return lt[:internal_count], rt[:internal_count], meta
+
+
+def refgpu_pack(nodes, transforms=None, packed=None, pairs=None, variant: str = "nofma"):
+    """The reference's kr_cuda_bvh_persistent (transforms None) or
+    kr_cuda_obvh_persistent + kr_cuda_soa_obvh on the GPU, from the given
+    initial buffers (zeros when not given): (packed, pairs, left_T, right_T,
+    metadata); the SoA parts are None for the AABB form."""
+    l = ref_gpu(variant)
+    nodes = np.ascontiguousarray(nodes)
+    nn = nodes.shape[0]
+    ni = (nn - 1) // 2
+    pk = np.zeros(nn, PACKED) if packed is None else np.array(packed, PACKED, copy=True)
+    pr = np.zeros((max(ni, 1), 32), np.float32) if pairs is None else np.array(pairs, np.float32, copy=True)
+    lt = np.zeros((max(ni, 1), 12), np.float32)
+    rt = np.zeros((max(ni, 1), 12), np.float32)
+    meta = np.zeros((nn, 4), np.int32)
+    xf = None if transforms is None else np.ascontiguousarray(transforms, np.float32)
+    rc = l.refgpu_pack(nodes, None if xf is None else xf.ctypes.data, nn, pk.ctypes.data, pr.ctypes.data,
+                       lt.reshape(-1), rt.reshape(-1), meta.reshape(-1))
+    if rc != 0:
+        raise RuntimeError(f"refgpu_pack: CUDA error {rc}")
+    if xf is None:
+        return pk, None, None, None, None
+    return pk, pr, lt[:ni], rt[:ni], meta

@@ -60,6 +60,12 @@ int oracle_collapse(const obvh_oracle_node* nodes, const uint32_t* parents, obvh
                     uint32_t* counts, uint32_t* prims, float* costs, float ci, float ct, uint32_t n_leaves,
                     uint32_t n_internal);
 
+/* traversal packing (pack_oracle.c) */
+void oracle_pack(const obvh_oracle_node* nodes, const float* transforms, uint32_t node_count, int with_obbs,
+                 void* packed_io, float* pairs_io);
+void oracle_soa_obvh(const void* packed_in, const float* pairs, uint32_t internal_count, uint32_t node_count,
+                     float* left_t, float* right_t, int32_t* metadata);
+
 /* ATRBVH path (atrbvh_oracle.c) */
 uint64_t oracle_morton63(const float tri9[9], const float scene[6]);
 uint64_t oracle_morton63_unit(float x, float y, float z);  /* a point already in the unit cube */

@@ -126,3 +126,50 @@ extern "C" int refgpu_collapse(const void* nodes, const uint32_t* parents, uint3
     a.back(prims, d_prims, 4ull * n);
     return static_cast<int>(a.err);
 }
+
+// The reference's traversal packing on a tree: kr_cuda_bvh_persistent when
+// transforms is NULL, else kr_cuda_obvh_persistent then kr_cuda_soa_obvh
+// (transforms.cu:1281-1449).  packed_io (node_count x 64 bytes) and pairs_io
+// ((node_count - 1) / 2 x 32 floats) are the buffers' initial contents and
+// receive the results; left_t, right_t (internal x 12 floats) and metadata
+// (node_count x 4) receive the SoA arrays, which are freed here (the
+// reference never frees them).  Returns 0 or the CUDA error code.
+extern "C" int refgpu_pack(const void* nodes, const float* transforms, uint32_t node_count, void* packed_io,
+                           float* pairs_io, float* left_t, float* right_t, int32_t* metadata) {
+    if (node_count == 0) return -1;
+    const u32 ni = (node_count - 1) / 2;
+    Arena a;
+    auto* d_nodes = static_cast<kr_bvh_node*>(a.copy(nodes, sizeof(kr_bvh_node) * node_count));
+    auto* d_packed = static_cast<kr_bvh_node_packed*>(a.copy(packed_io, sizeof(kr_bvh_node_packed) * node_count));
+    if (a.err != cudaSuccess) return static_cast<int>(a.err);
+    if (!transforms) {
+        kr_cuda_bvh_persistent(d_nodes, d_packed, node_count);
+        a.note(cudaGetLastError());
+        a.note(cudaDeviceSynchronize());
+        a.back(packed_io, d_packed, sizeof(kr_bvh_node_packed) * node_count);
+        return static_cast<int>(a.err);
+    }
+    auto* d_xfs = static_cast<kr_mat4*>(a.copy(transforms, sizeof(kr_mat4) * node_count));
+    auto* d_pairs = static_cast<kr_bvh_transformation_pair*>(
+        a.copy(pairs_io, sizeof(kr_bvh_transformation_pair) * (ni ? ni : 1)));
+    if (a.err != cudaSuccess) return static_cast<int>(a.err);
+    kr_cuda_obvh_persistent(d_nodes, d_xfs, d_packed, d_pairs, node_count);
+    a.note(cudaGetLastError());
+    kr_SoA_OBVH* d_soa = nullptr;
+    kr_cuda_soa_obvh(d_packed, d_pairs, d_soa, ni, node_count);
+    a.note(cudaGetLastError());
+    a.note(cudaDeviceSynchronize());
+    kr_SoA_OBVH h;
+    memset(&h, 0, sizeof h);
+    if (d_soa) a.note(cudaMemcpy(&h, d_soa, sizeof h, cudaMemcpyDeviceToHost));
+    a.back(left_t, h.left_T, sizeof(mat43) * ni);
+    a.back(right_t, h.right_T, sizeof(mat43) * ni);
+    a.back(metadata, h.metadata, sizeof(ivec4) * node_count);
+    cudaFree(h.left_T);
+    cudaFree(h.right_T);
+    cudaFree(h.metadata);
+    cudaFree(d_soa);
+    a.back(packed_io, d_packed, sizeof(kr_bvh_node_packed) * node_count);
+    a.back(pairs_io, d_pairs, sizeof(kr_bvh_transformation_pair) * ni);
+    return static_cast<int>(a.err);
+}
