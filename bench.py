@@ -54,7 +54,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["lbvh_obb_tree", "atrbvh_obb_tree", "dito", "dito_batch", "serve"],
+    ap.add_argument("--workload", choices=["lbvh_obb_tree", "atrbvh_obb_tree", "dito", "dito_batch", "serve",
+                                           "obvh_pack"],
                     default="lbvh_obb_tree")
     ap.add_argument("--treelet", type=int, default=7, help="atrbvh_obb_tree: treelet size")
     ap.add_argument("--requests", type=int, default=300, help="serve: requests in the stream")
@@ -592,6 +593,164 @@ def bench_tree_reference(a, dist):
 
 
 # ---------------------------------------------------------------------------
+def pack_bytes(nodes):
+    """Algorithmic bytes of one fused packing pass (pack_kernel) over a tree:
+    every node read (36 B) and its metadata word read and written (16 + 16 B);
+    an internal node also reads both children's boxes and counts (2 x 28 B)
+    and transforms (2 x 64 B) and writes its record (60 B), its pair (128 B)
+    and two 4x3 rows (96 B); a node with primitives writes 36 B of its record;
+    an internal-index node without a new pair reads the pair (128 B) for its
+    SoA rows (96 B)."""
+    import numpy as np
+    npr = nodes["n_prims"].astype(np.int64)
+    nn = npr.shape[0]
+    ni = (nn - 1) // 2
+    internal = npr == 0
+    leafy = (npr != 0) & (npr != 0xFFFF)
+    no_pair = ~internal & (np.arange(nn) < ni)
+    return int(68 * nn + internal.sum() * (56 + 128 + 60 + 128 + 96) + leafy.sum() * 36 + no_pair.sum() * (128 + 96))
+
+
+def _pack_tree(n, seed, dev):
+    """The collapsed tree and OBB transforms of an n-triangle fused build (device)."""
+    import torch
+    from obvh_b200 import bvh, workloads
+    v, f = workloads.triangle_soup(n, seed=seed)
+    b = bvh.ObvhBuilder(dev)
+    o = b.build(bvh.Mesh(v, f, device=dev), flags=3)
+    torch.cuda.synchronize()
+    if b.status(n)[0]:
+        raise RuntimeError("build failed")
+    return o["collapsed"].clone(), o["transforms"].clone()
+
+
+def bench_pack_ours(a, dist):
+    """Traversal packing of the collapsed OBB tree of the 2M-triangle soup:
+    packed records, child-transform pairs and SoA OBVH arrays in one pass."""
+    import ctypes as c
+    import torch
+    from obvh_b200 import _native, bvh
+    n = a.tris
+    dev = torch.device("cuda", torch.cuda.current_device())
+    nodes, xfs = _pack_tree(n, 1 + dist.rank, dev)
+    nn, ni = 2 * n - 1, n - 1
+    out = {"packed": torch.zeros(nn * 64, dtype=torch.uint8, device=dev),
+           "pairs": torch.zeros(ni * 32, dtype=torch.float32, device=dev),
+           "left_T": torch.zeros(ni * 12, dtype=torch.float32, device=dev),
+           "right_T": torch.zeros(ni * 12, dtype=torch.float32, device=dev),
+           "metadata": torch.zeros(nn * 4, dtype=torch.int32, device=dev),
+           "error": torch.zeros(1, dtype=torch.int32, device=dev)}
+    lib = _native.lib()
+    stream = torch.cuda.current_stream(dev)
+    ptr = {k: c.c_void_p(t.data_ptr()) for k, t in out.items()}
+    s_ptr = c.c_void_p(stream.cuda_stream)
+
+    def step(j):
+        _native.check(lib.obvh_obvh_pack_async(c.c_void_p(nodes.data_ptr()), c.c_void_p(xfs.data_ptr()),
+                                               ptr["packed"], ptr["pairs"], ptr["left_T"], ptr["right_T"],
+                                               ptr["metadata"], nn, ni, ptr["error"], s_ptr))
+
+    sampler = ClockSampler(dev.index, enabled=not a.profile)
+    total_ms, prof, clocks = timed_steps(a, dist, step, sampler, stream)
+    if int(out["error"].item()):
+        raise RuntimeError("packing reported a malformed tree")
+    if a.profile:
+        return {"profile": "obvh_pack", "triangles": n, "ms_per_step": total_ms / a.steps, "kernels": prof}
+    nodes_np = bvh.nodes_numpy(nodes)
+    algo = {"pack_kernel": pack_bytes(nodes_np)}
+    peak, peak_kind = peaks()
+    value = dist.world * nn * a.steps / (total_ms / 1e3) / 1e6
+    roof = roofline(prof, algo, peak, peak_kind, os.path.join(ROOT, "profiles", "obvh_pack_traffic.json"))
+
+    # end to end through the reference-facing calls: the tree and transforms
+    # copied from pinned host memory, kr_cuda_obvh_persistent, then
+    # kr_cuda_soa_obvh with its arrays read back to the host
+    h_nodes = torch.empty(nodes.shape, dtype=nodes.dtype, pin_memory=True)
+    h_xfs = torch.empty(xfs.shape, dtype=xfs.dtype, pin_memory=True)
+    h_nodes.copy_(nodes)
+    h_xfs.copy_(xfs)
+    d_nodes, d_xfs = torch.empty_like(nodes), torch.empty_like(xfs)
+
+    def e2e_step():
+        d_nodes.copy_(h_nodes, non_blocking=True)
+        d_xfs.copy_(h_xfs, non_blocking=True)
+        torch.cuda.synchronize()
+        o = bvh.persistent(d_nodes, nn, d_xfs, out["packed"], out["pairs"])
+        bvh.soa_obvh(o["packed"], o["pairs"], ni, nn)
+
+    e2e_step()
+    e2e_steps = max(3, min(a.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    e2e_min = -dist.max(-(nn * e2e_steps / e2e_s / 1e6))
+    line = {
+        "metric": "OBVH traversal packing throughput (Mnodes/s)", "value": round(value, 3), "unit": "Mnodes/s",
+        "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(total_ms / a.steps, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: collapsed LBVH OBB tree of the 2M thin-triangle soup (same generator as lbvh_obb_tree)",
+        "config": {"workload": "obvh_pack_collapsed_tree", "triangles_per_gpu": n, "nodes_per_gpu": nn,
+                   "l2": "inputs 400 MB and outputs 768 MB per pass (> 126 MB L2), no flush",
+                   "parallelism": f"replicas{dist.world}"},
+        "kernels": kernel_table(prof, a.steps, algo, peak),
+        "gpu_launches": sum(v[0] for v in prof.values()), "roofline": roof,
+        "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mnodes/s",
+                "h2d_bytes_per_step": nn * (36 + 64), "d2h_bytes_per_step": ni * 96 + nn * 16,
+                "api": "kr_cuda_obvh_persistent + kr_cuda_soa_obvh, tree from pinned host memory, SoA read back"},
+        "clocks": clocks,
+    }
+    if dist.rank == 0 and dist.world == 1:
+        from oracle import bvh as ref
+        xf_np = xfs.cpu().numpy().reshape(-1, 16)
+        reps, t0 = 0, time.perf_counter()
+        while True:
+            pk, pr = ref.pack(nodes_np, xf_np)
+            ref.soa_obvh(pk, pr, ni)
+            reps += 1
+            dt = time.perf_counter() - t0
+            if dt > 8.0 or reps >= 10:
+                break
+        line["cpu_baseline"] = {"value": round(nn * reps / dt / 1e6, 3), "unit": "Mnodes/s", "cores": 1,
+                                "kind": "port",
+                                "sample": f"{reps} packings of the same {nn}-node tree ({dt:.1f} s), oracle C "
+                                          "restatement"}
+    return line
+
+
+def bench_pack_reference(a, dist):
+    """The CPU restatement of the packing (oracle port) on this host's cores,
+    on the collapsed tree of a 200K-triangle sample: every host thread packs
+    its own copy each step (the reference packs on the GPU and converts to SoA
+    through a single-threaded host loop)."""
+    from oracle import bvh as ref
+    from obvh_b200 import workloads
+    n = min(a.tris, 200_000)
+    v, f = workloads.triangle_soup(n, seed=1)
+    r = ref.lbvh_build(v, f)
+    _, xfs, _ = ref.obb_tree(r["nodes"], r["parents"], v, f)
+    col, _, _, _, _ = ref.collapse(r["nodes"], r["parents"], r["counts"], r["costs"])
+    threads = host_threads()
+    nn = 2 * n - 1
+
+    def work():
+        pk, pr = ref.pack(col, xfs)
+        ref.soa_obvh(pk, pr, n - 1)
+
+    times = parallel_steps(a, work, threads)
+    value = threads * nn * len(times) / sum(times) / 1e6
+    return {"metric": "OBVH traversal packing throughput (Mnodes/s)", "impl": "reference",
+            "value": round(value, 4), "unit": "Mnodes/s", "n_gpus": dist.world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (same generator as the ours arm)",
+            "config": {"workload": "obvh_pack_collapsed_tree", "triangles_per_gpu": a.tris, "sample_triangles": n},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mnodes/s", "cores": threads, "kind": "port",
+                             "sample": f"{threads} concurrent packings of a {n}-triangle collapsed tree per step "
+                                       "(oracle C restatement, one host thread each)"},
+            "e2e": {"value": round(value, 4), "unit": "Mnodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# ---------------------------------------------------------------------------
 def bench_dito_ours(a, dist):
     import torch
     from obvh_b200 import DitoFitter, points_obb, workloads
@@ -981,13 +1140,16 @@ def main():
             print(json.dumps(ref(a, dist)), flush=True)
         elif a.workload == "atrbvh_obb_tree":
             print(json.dumps(bench_atrbvh_reference(a, dist)), flush=True)
+        elif a.workload == "obvh_pack":
+            print(json.dumps(bench_pack_reference(a, dist)), flush=True)
         else:
             print(json.dumps(bench_tree_reference(a, dist)), flush=True)
         return
     dist.init()
     try:
         run = {"lbvh_obb_tree": bench_tree_ours, "atrbvh_obb_tree": lambda a, d: bench_tree_ours(a, d, atrbvh=True),
-               "dito": bench_dito_ours, "dito_batch": bench_batch_ours, "serve": bench_serve_ours}
+               "dito": bench_dito_ours, "dito_batch": bench_batch_ours, "serve": bench_serve_ours,
+               "obvh_pack": bench_pack_ours}
         line = run[a.workload](a, dist)
         if dist.rank == 0:
             print(json.dumps(line), flush=True)

@@ -11,7 +11,7 @@
 //                            boxes and transforms are read once and written
 //                            to the packed node, the pair and the SoA rows.
 //
-// One thread per node.  The outputs are updated in place, field by field as
+// Four lanes per node.  The outputs are updated in place, field by field as
 // the reference writes them: a hidden node (nPrimitives == 0xFFFF) is skipped
 // by the OBB form, a leaf-type node leaves its rbounds and the pair untouched,
 // metadata.w is never written and metadata.z only by the OBB form.  The SoA
@@ -33,34 +33,6 @@ constexpr int kThreads = 256;
 constexpr uint32_t kHidden = 0xFFFFu;
 constexpr uint32_t kErrIndex = 1u;  // a child index or an internal node out of range
 
-struct NodeRec {
-    float b[6];
-    uint32_t left, right;
-    uint32_t np, axis;
-};
-
-// kr_bvh_node is 36 bytes with 4-byte alignment: nine word loads.
-__device__ __forceinline__ NodeRec load_node(const kr_bvh_node* nodes, uint32_t i) {
-    const uint32_t* p = reinterpret_cast<const uint32_t*>(nodes + i);
-    NodeRec r;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) r.b[k] = __uint_as_float(__ldg(p + k));
-    r.left = __ldg(p + 6);
-    r.right = __ldg(p + 7);
-    const uint32_t w = __ldg(p + 8);
-    r.np = w & 0xFFFFu;
-    r.axis = (w >> 16) & 0xFFu;
-    return r;
-}
-
-// The box and primitive count of a child (its first 6 words and word 8).
-__device__ __forceinline__ void load_child(const kr_bvh_node* nodes, uint32_t i, float b[6], uint32_t& np) {
-    const uint32_t* p = reinterpret_cast<const uint32_t*>(nodes + i);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) b[k] = __uint_as_float(__ldg(p + k));
-    np = __ldg(p + 8) & 0xFFFFu;
-}
-
 // The first three rows of each column of a column-major 4x4 (kr_m43from4,
 // vecmath.h:895-901), stored as three 16-byte words.
 __device__ __forceinline__ void store_m43(kr_mat43* dst, const float4 c[4]) {
@@ -70,82 +42,120 @@ __device__ __forceinline__ void store_m43(kr_mat43* dst, const float4 c[4]) {
     d[2] = make_float4(c[2].z, c[3].x, c[3].y, c[3].z);
 }
 
-__device__ __forceinline__ void load_mat(const kr_mat4* m, float4 c[4]) {
-    const float4* s = reinterpret_cast<const float4*>(m);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) c[k] = __ldg(s + k);
-}
-
 // kObb: the OBB form (obvh_persistent_prepare), else the AABB form
 // (bvh_persistent_prepare).  kSoa (OBB form only): also the SoA OBVH rows.
+//
+// Four lanes (a quad) per node, eight nodes per warp iteration, so that every
+// access is a coalesced piece of a contiguous record: lane q loads words q
+// and q + 4 of the node, of each child (boxes and counts), column q of each
+// child's transform, and stores chunk q of the 64-byte record, column q of
+// both halves of the 128-byte pair and row-word q of the 48-byte SoA rows.
+// The chunks are assembled through a per-quad shared-memory stage.
+constexpr int kQuads = kThreads / 4;
+constexpr int kStage = 48;  // words per quad: 14 box/count words, 32 column words
+
 template <bool kObb, bool kSoa>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 8)
 pack_kernel(const kr_bvh_node* __restrict__ nodes, const kr_mat4* __restrict__ xfs, kr_bvh_node_packed* packed,
             kr_bvh_transformation_pair* pairs, kr_mat43* left_t, kr_mat43* right_t, kr_ivec4* meta_out,
             uint32_t node_count, uint32_t internal_count, uint32_t* err) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < node_count; i += gridDim.x * blockDim.x) {
-        const NodeRec nd = load_node(nodes, i);
-        char* rec = reinterpret_cast<char*>(packed + i);
-        int2 lr = make_int2(0, 0);
-        bool wrote_pair = false;
-        float4 lc[4], rc[4];
-        if (kObb && nd.np == kHidden) {
-            // skipped: the record and the pair keep their contents
-        } else if (nd.np == 0) {
-            if (nd.left >= node_count || nd.right >= node_count || (kObb && i >= internal_count)) {
-                if (err) atomicOr(err, kErrIndex);
-                continue;
-            }
-            float lb[6], rb[6];
-            uint32_t lnp, rnp;
-            load_child(nodes, nd.left, lb, lnp);
-            load_child(nodes, nd.right, rb, rnp);
-            float4* q = reinterpret_cast<float4*>(rec);
-            q[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
-            q[1] = make_float4(lb[4], lb[5], rb[0], rb[1]);
-            q[2] = make_float4(rb[2], rb[3], rb[4], rb[5]);
-            lr = make_int2(lnp > 0 ? ~static_cast<int>(nd.left) : static_cast<int>(nd.left),
-                           rnp > 0 ? ~static_cast<int>(nd.right) : static_cast<int>(nd.right));
-            if (kObb) {
-                load_mat(xfs + nd.left, lc);
-                load_mat(xfs + nd.right, rc);
-                float4* pq = reinterpret_cast<float4*>(pairs + i);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    pq[k] = lc[k];
-                    pq[4 + k] = rc[k];
-                }
-                wrote_pair = true;
-            }
-        } else {
-            float4* q = reinterpret_cast<float4*>(rec);
-            q[0] = make_float4(nd.b[0], nd.b[1], nd.b[2], nd.b[3]);
-            *reinterpret_cast<float2*>(rec + 16) = make_float2(nd.b[4], nd.b[5]);
-            lr = make_int2(static_cast<int>(nd.left), static_cast<int>(nd.left + nd.np));
+    __shared__ __align__(16) uint32_t stage[kQuads * kStage];
+    const uint32_t lane = threadIdx.x & 31, q = lane & 3;
+    uint32_t* st = stage + (threadIdx.x >> 2) * kStage;
+    float* cols = reinterpret_cast<float*>(st + 16);
+    const uint32_t warps = gridDim.x * (kThreads / 32);
+    for (uint32_t base = (blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)) * 8; base < node_count;
+         base += warps * 8) {
+        const uint32_t i = base + (lane >> 2);
+        const bool valid = i < node_count;
+        // the node: lane q holds words q and q + 4, word 8 goes to the whole quad
+        const uint32_t* rec = reinterpret_cast<const uint32_t*>(nodes + (valid ? i : 0));
+        const uint32_t wa = valid ? __ldg(rec + q) : 0u, wb = valid ? __ldg(rec + q + 4) : 0u;
+        const uint32_t w8 = __shfl_sync(0xffffffffu, valid && q == 0 ? __ldg(rec + 8) : 0u, lane & ~3u);
+        const uint32_t left = __shfl_sync(0xffffffffu, wb, (lane & ~3u) + 2);   // word 6
+        const uint32_t right = __shfl_sync(0xffffffffu, wb, (lane & ~3u) + 3);  // word 7
+        const uint32_t np = w8 & 0xFFFFu, axis = (w8 >> 16) & 0xFFu;
+        const bool hidden = kObb && np == kHidden;
+        bool inner = valid && !hidden && np == 0;
+        if (inner && (left >= node_count || right >= node_count || (kObb && i >= internal_count))) {
+            if (err && q == 0) atomicOr(err, kErrIndex);
+            inner = false;
         }
-        const bool skipped = kObb && nd.np == kHidden;
-        if (!skipped) {
-            *reinterpret_cast<int2*>(rec + 48) = lr;
-            if (kObb) *reinterpret_cast<int*>(rec + 56) = static_cast<int>(nd.axis);
+        const bool leafy = valid && !hidden && np != 0;
+        // stage words 0..5: first box (left child's, or the node's own for a
+        // leaf-type node), 6..11: right child's box, 12/13: children's counts
+        if (inner) {
+            const uint32_t* L = reinterpret_cast<const uint32_t*>(nodes + left);
+            const uint32_t* R = reinterpret_cast<const uint32_t*>(nodes + right);
+            st[q] = __ldg(L + q);
+            st[6 + q] = __ldg(R + q);
+            if (q < 2) {
+                st[4 + q] = __ldg(L + 4 + q);
+                st[10 + q] = __ldg(R + 4 + q);
+            } else {
+                st[10 + q] = __ldg((q == 2 ? L : R) + 8);  // words 12, 13
+            }
+        } else if (leafy) {
+            st[q] = wa;
+            if (q < 2) st[4 + q] = wb;
+        }
+        // columns: the children's transforms, or the pair as it stands (a
+        // node without a new pair still gives its SoA rows from it)
+        const bool soa_row = kSoa && valid && i < internal_count;
+        float4 lc = make_float4(0.f, 0.f, 0.f, 0.f), rc = lc;
+        if (kObb && inner) {
+            lc = __ldg(reinterpret_cast<const float4*>(xfs + left) + q);
+            rc = __ldg(reinterpret_cast<const float4*>(xfs + right) + q);
+        } else if (soa_row) {
+            lc = reinterpret_cast<const float4*>(pairs + i)[q];
+            rc = reinterpret_cast<const float4*>(pairs + i)[4 + q];
         }
         if (kSoa) {
-            // metadata as it now stands: x, y (and z) as written, w as found
-            const int4 old = *reinterpret_cast<const int4*>(rec + 48);
-            meta_out[i] = skipped ? kr_ivec4{{old.x, old.y, old.z, old.w}}
-                                  : kr_ivec4{{lr.x, lr.y, static_cast<int>(nd.axis), old.w}};
-            if (i < internal_count) {
-                if (!wrote_pair) {
-                    const float4* pq = reinterpret_cast<const float4*>(pairs + i);
+            reinterpret_cast<float4*>(cols)[q] = lc;
+            reinterpret_cast<float4*>(cols)[4 + q] = rc;
+        }
+        __syncwarp();
+        char* out = reinterpret_cast<char*>(packed + (valid ? i : 0));
+        int2 lr = make_int2(0, 0);
+        if (inner) {
+            lr = make_int2((st[12] & 0xFFFFu) ? ~static_cast<int>(left) : static_cast<int>(left),
+                           (st[13] & 0xFFFFu) ? ~static_cast<int>(right) : static_cast<int>(right));
+            if (q < 3) reinterpret_cast<uint4*>(out)[q] = reinterpret_cast<const uint4*>(st)[q];
+            if (kObb) {
+                float4* pq = reinterpret_cast<float4*>(pairs + i);
+                pq[q] = lc;
+                pq[4 + q] = rc;
+            }
+        } else if (leafy) {
+            lr = make_int2(static_cast<int>(left), static_cast<int>(left + np));
+            if (q == 0) reinterpret_cast<uint4*>(out)[0] = reinterpret_cast<const uint4*>(st)[0];
+            if (q == 1) *reinterpret_cast<uint2*>(out + 16) = make_uint2(st[4], st[5]);
+        }
+        if (q == 3 && (inner || leafy)) {
+            *reinterpret_cast<int2*>(out + 48) = lr;
+            if (kObb) *reinterpret_cast<int*>(out + 56) = static_cast<int>(axis);
+        }
+        if (kSoa && valid) {
+            if (q == 3) {
+                // metadata as it now stands: x, y, z as written, w as found
+                const int4 old = *reinterpret_cast<const int4*>(out + 48);
+                meta_out[i] = (inner || leafy) ? kr_ivec4{{lr.x, lr.y, static_cast<int>(axis), old.w}}
+                                               : kr_ivec4{{old.x, old.y, old.z, old.w}};
+            } else if (soa_row) {
+                // row-word q of each 4x3 (kr_m43from4): words 4q..4q+3 of
+                // (c0.xyz, c1.xyz, c2.xyz, c3.xyz)
+                float l4[4], r4[4];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        lc[k] = pq[k];
-                        rc[k] = pq[4 + k];
-                    }
+                for (int k = 0; k < 4; ++k) {
+                    const uint32_t j = 4 * q + k;
+                    l4[k] = cols[4 * (j / 3) + j % 3];
+                    r4[k] = cols[16 + 4 * (j / 3) + j % 3];
                 }
-                store_m43(left_t + i, lc);
-                store_m43(right_t + i, rc);
+                reinterpret_cast<float4*>(left_t + i)[q] = make_float4(l4[0], l4[1], l4[2], l4[3]);
+                reinterpret_cast<float4*>(right_t + i)[q] = make_float4(r4[0], r4[1], r4[2], r4[3]);
             }
         }
+        __syncwarp();
     }
 }
 
@@ -176,6 +186,14 @@ inline unsigned grid_for(uint32_t n) {
     return want < cap ? (want ? want : 1u) : cap;
 }
 
+// pack_kernel: one quad per node, eight nodes per warp; enough warps for
+// every node (up to 64 blocks per SM of grid-stride work).
+inline unsigned pack_grid(uint32_t n) {
+    const unsigned want = (n + 8u * (kThreads / 32) - 1) / (8u * (kThreads / 32));
+    const unsigned cap = static_cast<unsigned>(device_info().sm_count) * 64u;
+    return want < cap ? (want ? want : 1u) : cap;
+}
+
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 // internal_count of a binary tree with node_count = 2n - 1 nodes
@@ -190,7 +208,7 @@ kr_error enqueue_pack(const kr_bvh_node* nodes, const kr_mat4* xfs, kr_bvh_node_
     if (!aligned16(packed) || (obb && (!aligned16(pairs) || !aligned16(xfs))) ||
         (soa && (!aligned16(left_t) || !aligned16(right_t) || !aligned16(meta))))
         return "obvh pack: packed records, pairs, transforms and SoA arrays must be 16-byte aligned";
-    const unsigned g = grid_for(node_count);
+    const unsigned g = pack_grid(node_count);
     ProfScope prof_scope_("pack_kernel", s);
     if (!obb)
         pack_kernel<false, false><<<g, kThreads, 0, s>>>(nodes, nullptr, packed, nullptr, nullptr, nullptr, nullptr,
