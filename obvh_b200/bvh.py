@@ -315,10 +315,12 @@ def _cudart():
     raise _native.ObvhError("the CUDA runtime library is needed to read a kr_SoA_OBVH back")
 
 
-def soa_obvh(packed, pairs, internal_count: int, node_count: int):
+def soa_obvh(packed, pairs, internal_count: int, node_count: int, out=None):
     """kr_cuda_soa_obvh: the library allocates the SoA arrays on the device; this
-    reads them back (numpy left_T [ni x 12], right_T [ni x 12], metadata
-    [nodes x 4]) and frees them with obvh_soa_obvh_free."""
+    reads them back and frees them with obvh_soa_obvh_free.  Returns numpy
+    left_T [ni x 12], right_T [ni x 12], metadata [nodes x 4]; with `out`
+    (dict of host tensors or arrays of those sizes, e.g. pinned) the arrays
+    are copied into it instead."""
     lib = _native.lib()
     d_soa = ctypes.c_void_p(0)
     _native.check(lib.kr_cuda_soa_obvh(_ptr(packed), _ptr(pairs), ctypes.byref(d_soa), internal_count, node_count))
@@ -328,12 +330,15 @@ def soa_obvh(packed, pairs, internal_count: int, node_count: int):
         ptrs = (ctypes.c_void_p * 3)()
         if rt.cudaMemcpy(ctypes.cast(ptrs, ctypes.c_void_p), d_soa, 24, 2) != 0:
             raise _native.ObvhError("reading the kr_SoA_OBVH struct back failed")
-        out = {"left_T": np.zeros((internal_count, 12), np.float32),
-               "right_T": np.zeros((internal_count, 12), np.float32),
-               "metadata": np.zeros((node_count, 4), np.int32)}
+        if out is None:
+            out = {"left_T": np.zeros((internal_count, 12), np.float32),
+                   "right_T": np.zeros((internal_count, 12), np.float32),
+                   "metadata": np.zeros((node_count, 4), np.int32)}
+        sizes = {"left_T": 48 * internal_count, "right_T": 48 * internal_count, "metadata": 16 * node_count}
         for k, key in enumerate(("left_T", "right_T", "metadata")):
             a = out[key]
-            if a.nbytes and rt.cudaMemcpy(a.ctypes.data_as(ctypes.c_void_p), ptrs[k], a.nbytes, 2) != 0:
+            dst = a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+            if sizes[key] and rt.cudaMemcpy(ctypes.c_void_p(dst), ptrs[k], sizes[key], 2) != 0:
                 raise _native.ObvhError("reading the SoA arrays back failed")
         return out
     finally:
