@@ -132,6 +132,36 @@ OBVH_EXPORT kr_error obvh_obvh_pack_async(const kr_bvh_node* d_nodes, const kr_m
                                           kr_bvh_node_packed* d_packed, kr_bvh_transformation_pair* d_pairs,
                                           kr_mat43* d_left_t, kr_mat43* d_right_t, kr_ivec4* d_metadata,
                                           kr_u32 node_count, kr_u32 internal_count, kr_u32* d_error, void* stream);
+/*
+ * Closest-hit ray traversal of a SoA OBVH (kr_cuda_soa_obvh_intersect,
+ * intersectors.cuh:81-91, intersectors.cu:1452-1473, kernel :801-974).
+ * bvh: the device struct kr_cuda_soa_obvh returns; vertices/faces the mesh;
+ * primitives the collapse's primitive list (leaves of more than one
+ * primitive); rays/isects ray_count device records.  Each ray follows the
+ * reference's own sequence of node and triangle tests, so the hits are the
+ * reference's.  block_size, grid_size and warp_counter are accepted and not
+ * used (the reference ignores the first two; its ray counter is not needed).
+ * Indices are trusted, as in the reference.  Synchronous.
+ */
+OBVH_EXPORT kr_error kr_cuda_soa_obvh_intersect(const kr_SoA_OBVH* bvh, const kr_vec3* vertices,
+                                                const kr_uvec4* faces, const kr_u32* primitives, const kr_ray* rays,
+                                                kr_intersection* isects, kr_u32 ray_count, kr_u32 block_size,
+                                                kr_u32 grid_size, kr_u32* warp_counter);
+/*
+ * The same traversal on the SoA arrays themselves (as obvh_obvh_pack_async
+ * writes them), on `stream`, without synchronising.  Every index is checked
+ * against the sizes given: a ray that meets one out of range, or a stack
+ * deeper than 64 entries, keeps its miss record and sets bit 0 (index) or
+ * bit 1 (stack) of *d_error.  d_primitives may be NULL when every leaf holds
+ * one primitive.  No counterpart in the reference.
+ */
+OBVH_EXPORT kr_error obvh_soa_obvh_intersect_async(const kr_mat43* d_left_t, const kr_mat43* d_right_t,
+                                                   const kr_ivec4* d_metadata, kr_u32 internal_count,
+                                                   kr_u32 node_count, const kr_vec3* d_vertices,
+                                                   const kr_uvec4* d_faces, kr_u32 face_count,
+                                                   const kr_u32* d_primitives, kr_u32 primitive_slots,
+                                                   const kr_ray* d_rays, kr_intersection* d_isects,
+                                                   kr_u32 ray_count, kr_u32* d_error, void* stream);
 /* Reads the device error word of the last transform made with a workspace
  * (synchronises `stream`): 0 ok, 4 parent walk longer than the tree. */
 OBVH_EXPORT kr_error obvh_obb_tree_error(const void* d_workspace, void* stream, kr_u32* device_error);

@@ -49,6 +49,7 @@ typedef const void* kr_error;
 
 typedef union { kr_scalar v[3]; struct { kr_scalar x, y, z; }; } kr_vec3;
 typedef union { kr_scalar v[4]; struct { kr_scalar x, y, z, w; }; } kr_vec4;
+typedef union { kr_scalar v[2]; struct { kr_scalar x, y; }; } kr_vec2;
 typedef union { kr_u32 v[4]; struct { kr_u32 x, y, z, w; }; } kr_uvec4;
 typedef union { kr_i32 v[4]; struct { kr_i32 x, y, z, w; }; } kr_ivec4;
 typedef union {
@@ -96,6 +97,11 @@ typedef struct {
 } kr_bvh_node_packed;
 
 typedef struct { kr_mat4 l; kr_mat4 r; } kr_bvh_transformation_pair;
+
+/* A ray and its closest hit (ads.h:64-76).  A miss keeps primitive =
+ * 0xFFFFFFFF, barys (0.5, 0.5) and geom_normal = the ray direction. */
+typedef struct { kr_vec3 origin; kr_scalar tmin; kr_vec3 direction; kr_scalar tmax; } kr_ray;
+typedef struct { kr_vec3 geom_normal; kr_vec2 barys; kr_u32 primitive; kr_u32 instance; } kr_intersection;
 
 /* SoA OBVH for traversal (ads.h:166-170): per internal node the two
  * children's transforms as 4x3 matrices, per node the packed metadata
@@ -218,6 +224,8 @@ OBVH_STATIC_ASSERT(offsetof(kr_bvh_node, right) == 28, "kr_bvh_node.right");
 OBVH_STATIC_ASSERT(offsetof(kr_bvh_node, nPrimitives) == 32, "kr_bvh_node.nPrimitives");
 OBVH_STATIC_ASSERT(offsetof(kr_bvh_node, axis) == 34, "kr_bvh_node.axis");
 OBVH_STATIC_ASSERT(sizeof(kr_bvh_node_packed) == 64, "kr_bvh_node_packed layout");
+OBVH_STATIC_ASSERT(sizeof(kr_ray) == 32, "kr_ray layout");
+OBVH_STATIC_ASSERT(sizeof(kr_intersection) == 28, "kr_intersection layout");
 OBVH_STATIC_ASSERT(offsetof(kr_scene, objects) == 304, "kr_scene.objects");
 OBVH_STATIC_ASSERT(offsetof(kr_scene, benchmark_file) == 416, "kr_scene.benchmark_file");
 OBVH_STATIC_ASSERT(sizeof(kr_object) == 80, "kr_object layout");

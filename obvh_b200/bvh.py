@@ -369,3 +369,24 @@ def obvh_pack(nodes, node_count: int, internal_count: int, transforms=None, pack
                                            node_count, internal_count, _ptr(out["error"]),
                                            _stream(torch, stream)))
     return out
+
+
+# ---- SoA OBVH ray traversal ---------------------------------------------------
+def soa_obvh_intersect(soa: dict, mesh: "Mesh", primitives, rays, node_count: int, internal_count: int,
+                       isects=None, stream=None):
+    """obvh_soa_obvh_intersect_async: closest hits of `rays` (a device uint8
+    tensor of kr_ray records) against the SoA arrays of obvh_pack (soa:
+    left_T, right_T, metadata).  Returns (isects uint8 tensor of 28-byte
+    records, error int32 [1])."""
+    import torch
+    lib = _native.lib()
+    n = rays.numel() // 32
+    if isects is None:
+        isects = torch.empty(max(n, 1) * 28, dtype=torch.uint8, device=rays.device)
+    err = torch.zeros(1, dtype=torch.int32, device=rays.device)
+    slots = 0 if primitives is None else primitives.numel()
+    _native.check(lib.obvh_soa_obvh_intersect_async(
+        _ptr(soa["left_T"]), _ptr(soa["right_T"]), _ptr(soa["metadata"]), internal_count, node_count,
+        _ptr(mesh.verts), _ptr(mesh.faces), mesh.n_faces, _ptr(primitives), slots, _ptr(rays), _ptr(isects), n,
+        _ptr(err), _stream(torch, stream)))
+    return isects, err

@@ -235,3 +235,25 @@ def gaussian_cloud_torch(n: int, rng: np.random.Generator, device="cuda", sigma_
     x = torch.randn((n, 3), generator=g, device=device, dtype=torch.float64) * torch.tensor(sig, device=device)
     y = x @ torch.tensor(rot.T, device=device) + torch.tensor(off, device=device)
     return y.to(torch.float32).contiguous()
+
+
+RAY = np.dtype([("origin", "<f4", (3,)), ("tmin", "<f4"), ("direction", "<f4", (3,)), ("tmax", "<f4")])
+ISECT = np.dtype([("normal", "<f4", (3,)), ("barys", "<f4", (2,)), ("primitive", "<u4"), ("instance", "<u4")])
+
+
+def probe_rays(n: int, lo, hi, seed: int = 5, tmax: float = 1e30) -> np.ndarray:
+    """n rays (kr_ray records) into the box [lo, hi]: origins uniform on the
+    sphere of twice the box's half-diagonal around its centre, directions
+    (unnormalised) towards uniform points inside the box, tmin 0."""
+    rng = np.random.default_rng(seed)
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    c = 0.5 * (lo + hi)
+    radius = float(np.linalg.norm(hi - lo))
+    o = c + radius * unit_vectors(rng, n)
+    target = lo + rng.uniform(0.0, 1.0, size=(n, 3)) * (hi - lo)
+    r = np.zeros(n, RAY)
+    r["origin"] = o.astype(np.float32)
+    r["direction"] = (target - o).astype(np.float32)
+    r["tmax"] = np.float32(tmax)
+    return r

@@ -42,6 +42,9 @@ def _bind():
         "oracle_obb_summaries": (c.c_int, [_node, _f32, _u32, c.c_uint32, c.c_uint32, _f32, _f32, _f32]),
         "oracle_pack": (None, [_node, c.c_void_p, c.c_uint32, c.c_int, c.c_void_p, c.c_void_p]),
         "oracle_soa_obvh": (None, [c.c_void_p, c.c_void_p, c.c_uint32, c.c_uint32, _f32, _f32, _i32]),
+        "oracle_soa_obvh_intersect": (c.c_int64, [c.c_void_p, c.c_void_p, c.c_void_p, c.c_uint32, c.c_uint32,
+                                                  c.c_void_p, c.c_void_p, c.c_uint32, c.c_void_p, c.c_uint32,
+                                                  c.c_void_p, c.c_uint64, c.c_uint64, c.c_void_p]),
         "oracle_collapse": (c.c_int, [_node, _u32, _node, _u32, _u32, _f32, c.c_float, c.c_float, c.c_uint32,
                                       c.c_uint32]),
         "oracle_aabb_refit": (c.c_int, [_node, c.c_uint32, _u32, _f32]),
@@ -444,3 +447,56 @@ def refgpu_pack(nodes, transforms=None, packed=None, pairs=None, variant: str = 
     if xf is None:
         return pk, None, None, None, None
     return pk, pr, lt[:ni], rt[:ni], meta
+
+
+# ---- SoA OBVH ray traversal (trace_oracle.c) ----------------------------------
+ISECT = np.dtype([("normal", "<f4", (3,)), ("barys", "<f4", (2,)), ("primitive", "<u4"), ("instance", "<u4")])
+
+
+def soa_obvh_intersect(left_t, right_t, metadata, verts, faces, prims, rays, threads: int = 1):
+    """Closest hits of kr_ray records (8 floats each) against a SoA OBVH:
+    ISECT records.  Raises if any ray meets an index outside the arrays."""
+    from concurrent.futures import ThreadPoolExecutor
+    l = _bind()
+    lt = np.ascontiguousarray(left_t, np.float32)
+    rt = np.ascontiguousarray(right_t, np.float32)
+    meta = np.ascontiguousarray(metadata, np.int32).reshape(-1, 4)
+    v, f, nf = _mesh(verts, faces)
+    pr = None if prims is None else np.ascontiguousarray(prims, np.uint32)
+    ry = np.ascontiguousarray(rays).view(np.uint8)
+    n = ry.nbytes // 32
+    out = np.zeros(n, ISECT)
+    ni = lt.reshape(-1, 12).shape[0]
+    args = (lt.ctypes.data, rt.ctypes.data, meta.ctypes.data, ni, meta.shape[0], v.ctypes.data, f.ctypes.data, nf,
+            None if pr is None else pr.ctypes.data, 0 if pr is None else pr.size, ry.ctypes.data)
+    bounds = np.linspace(0, n, max(1, threads) + 1).astype(np.int64)
+    with ThreadPoolExecutor(max_workers=max(1, threads)) as pool:
+        bad = sum(pool.map(lambda k: l.oracle_soa_obvh_intersect(*args, int(bounds[k]), int(bounds[k + 1]),
+                                                                  out.ctypes.data), range(len(bounds) - 1)))
+    if bad:
+        raise ValueError(f"{bad} rays met an index outside the arrays")
+    return out
+
+
+def refgpu_soa_obvh_intersect(left_t, right_t, metadata, verts, faces, prims, rays, variant: str = "nofma"):
+    """The reference's kr_cuda_soa_obvh_intersect on the GPU: ISECT records."""
+    l = ref_gpu(variant)
+    c = ctypes
+    f_ = l.refgpu_soa_obvh_intersect
+    f_.restype = c.c_int
+    f_.argtypes = [c.c_void_p] * 3 + [c.c_uint32] * 2 + [c.c_void_p, c.c_uint32, c.c_void_p, c.c_uint32,
+                                                         c.c_void_p, c.c_uint32, c.c_void_p, c.c_uint32, c.c_void_p]
+    lt = np.ascontiguousarray(left_t, np.float32)
+    rt = np.ascontiguousarray(right_t, np.float32)
+    meta = np.ascontiguousarray(metadata, np.int32).reshape(-1, 4)
+    v, f, nf = _mesh(verts, faces)
+    pr = None if prims is None else np.ascontiguousarray(prims, np.uint32)
+    ry = np.ascontiguousarray(rays).view(np.uint8)
+    n = ry.nbytes // 32
+    out = np.zeros(n, ISECT)
+    rc = f_(lt.ctypes.data, rt.ctypes.data, meta.ctypes.data, lt.reshape(-1, 12).shape[0], meta.shape[0],
+            v.ctypes.data, v.size // 3, f.ctypes.data, nf, None if pr is None else pr.ctypes.data,
+            0 if pr is None else pr.size, ry.ctypes.data, n, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"refgpu_soa_obvh_intersect: CUDA error {rc}")
+    return out

@@ -66,6 +66,13 @@ void oracle_pack(const obvh_oracle_node* nodes, const float* transforms, uint32_
 void oracle_soa_obvh(const void* packed_in, const float* pairs, uint32_t internal_count, uint32_t node_count,
                      float* left_t, float* right_t, int32_t* metadata);
 
+/* SoA OBVH ray traversal (trace_oracle.c): rays 8 floats each, isects 7 words */
+int64_t oracle_soa_obvh_intersect(const float* left_t, const float* right_t, const int32_t* metadata,
+                                  uint32_t internal_count, uint32_t node_count, const float* verts,
+                                  const uint32_t* faces4, uint32_t face_count, const uint32_t* prims,
+                                  uint32_t prim_slots, const float* rays, uint64_t first, uint64_t last,
+                                  uint32_t* isects);
+
 /* ATRBVH path (atrbvh_oracle.c) */
 uint64_t oracle_morton63(const float tri9[9], const float scene[6]);
 uint64_t oracle_morton63_unit(float x, float y, float z);  /* a point already in the unit cube */

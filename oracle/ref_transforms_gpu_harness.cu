@@ -173,3 +173,39 @@ extern "C" int refgpu_pack(const void* nodes, const float* transforms, uint32_t 
     a.back(pairs_io, d_pairs, sizeof(kr_bvh_transformation_pair) * ni);
     return static_cast<int>(a.err);
 }
+
+#include "ads/common/cuda/intersectors.cuh"
+
+// The reference's SoA OBVH traversal (kr_cuda_soa_obvh_intersect,
+// intersectors.cu:1452-1473, kernel :801-974) on SoA arrays given from the
+// host: left_t / right_t internal_count x 12 floats, metadata node_count x 4,
+// faces4 face_count x 4, primitives prim_slots (nullable), rays ray_count x 8
+// floats; isects receives ray_count x 7 words.  Its warp counter is zeroed
+// first, as the reference's callers do (lbvh.cu:49).  Returns 0 or the CUDA
+// error code.
+extern "C" int refgpu_soa_obvh_intersect(const float* left_t, const float* right_t, const int32_t* metadata,
+                                         uint32_t internal_count, uint32_t node_count, const float* verts,
+                                         uint32_t n_verts, const uint32_t* faces4, uint32_t face_count,
+                                         const uint32_t* prims, uint32_t prim_slots, const float* rays,
+                                         uint32_t ray_count, void* isects) {
+    static_assert(sizeof(kr_ray) == 32 && sizeof(kr_intersection) == 28, "ray layouts");
+    if (internal_count == 0 || ray_count == 0) return -1;
+    Arena a;
+    kr_SoA_OBVH h;
+    h.left_T = static_cast<mat43*>(a.copy(left_t, sizeof(mat43) * internal_count));
+    h.right_T = static_cast<mat43*>(a.copy(right_t, sizeof(mat43) * internal_count));
+    h.metadata = static_cast<ivec4*>(a.copy(metadata, sizeof(ivec4) * node_count));
+    auto* d_soa = static_cast<kr_SoA_OBVH*>(a.copy(&h, sizeof h));
+    auto* d_verts = static_cast<kr_vec3*>(a.copy(verts, 12ull * n_verts));
+    auto* d_faces = static_cast<kr_uvec4*>(a.copy(faces4, 16ull * face_count));
+    auto* d_prims = prims ? static_cast<u32*>(a.copy(prims, 4ull * prim_slots)) : nullptr;
+    auto* d_rays = static_cast<kr_ray*>(a.copy(rays, sizeof(kr_ray) * ray_count));
+    auto* d_isects = static_cast<kr_intersection*>(a.zeroed(sizeof(kr_intersection) * ray_count));
+    auto* d_counter = static_cast<u32*>(a.zeroed(4));
+    if (a.err != cudaSuccess) return static_cast<int>(a.err);
+    kr_cuda_soa_obvh_intersect(d_soa, d_verts, d_faces, d_prims, d_rays, d_isects, ray_count, 128, 0, d_counter);
+    a.note(cudaGetLastError());
+    a.note(cudaDeviceSynchronize());
+    a.back(isects, d_isects, sizeof(kr_intersection) * ray_count);
+    return static_cast<int>(a.err);
+}
