@@ -55,7 +55,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["lbvh_obb_tree", "atrbvh_obb_tree", "dito", "dito_batch", "serve",
-                                           "obvh_pack"],
+                                           "obvh_pack", "obvh_trace"],
                     default="lbvh_obb_tree")
     ap.add_argument("--treelet", type=int, default=7, help="atrbvh_obb_tree: treelet size")
     ap.add_argument("--requests", type=int, default=300, help="serve: requests in the stream")
@@ -63,6 +63,7 @@ def parse_args():
     ap.add_argument("--no-autotune", action="store_true", help="dito_batch: default knobs")
     ap.add_argument("--points", type=int, default=100_000_000, help="dito: points per fit")
     ap.add_argument("--tris", type=int, default=2_000_000, help="lbvh_obb_tree: triangles per build")
+    ap.add_argument("--rays", type=int, default=4_000_000, help="obvh_trace: rays per pass")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + timed steps, no clock soak, e2e or CPU legs (for ncu captures)")
     return ap.parse_args()
@@ -755,6 +756,168 @@ def bench_pack_reference(a, dist):
 
 
 # ---------------------------------------------------------------------------
+def trace_bytes_per_ray(counts, hit_fraction):
+    """Bytes a traversal touches per ray (read once each, cached or not): the
+    ray (32 B) and its record (28 B), per internal node its metadata and two
+    4x3 rows (16 + 96 B), per leaf its metadata (16 B), per triangle tested
+    its face and vertices (16 + 36 B), per primitive-list entry 4 B, and per
+    hit the hit triangle again for the normal (52 B)."""
+    return (60 + 112 * counts["internal_visits"] + 16 * counts["leaf_visits"] + 52 * counts["triangle_tests"]
+            + 4 * counts["list_reads"] + 52 * hit_fraction)
+
+
+def _trace_scene(n, dev):
+    """The collapsed OBB tree of the n-triangle soup packed as a SoA OBVH (device)."""
+    import torch
+    from obvh_b200 import bvh, workloads
+    v, f = workloads.triangle_soup(n, seed=1)
+    mesh = bvh.Mesh(v, f, device=dev)
+    b = bvh.ObvhBuilder(dev)
+    o = b.build(mesh, flags=3)
+    torch.cuda.synchronize()
+    if b.status(n)[0]:
+        raise RuntimeError("build failed")
+    s = bvh.obvh_pack(o["collapsed"], 2 * n - 1, n - 1, o["transforms"])
+    torch.cuda.synchronize()
+    return v, f, mesh, s, o["primitives"]
+
+
+def bench_trace_ours(a, dist):
+    """Closest-hit traversal of a.rays probe rays through the SoA OBVH of the
+    collapsed 2M-triangle soup tree."""
+    import ctypes as c
+    import numpy as np
+    import torch
+    from obvh_b200 import _native, bvh, workloads
+    n = a.tris
+    dev = torch.device("cuda", torch.cuda.current_device())
+    v, f, mesh, soa, prims = _trace_scene(n, dev)
+    nn, ni = 2 * n - 1, n - 1
+    ray_sets = [workloads.probe_rays(a.rays, [0, 0, 0], [1, 1, 1], seed=21 + 2 * dist.rank + j) for j in range(2)]
+    d_rays = [torch.from_numpy(r.view(np.uint8).copy()).to(dev) for r in ray_sets]
+    isects = torch.empty(28 * a.rays, dtype=torch.uint8, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    lib = _native.lib()
+    stream = torch.cuda.current_stream(dev)
+    P = lambda t: c.c_void_p(t.data_ptr())  # noqa: E731
+
+    def step(j):
+        _native.check(lib.obvh_soa_obvh_intersect_async(P(soa["left_T"]), P(soa["right_T"]), P(soa["metadata"]), ni,
+                                                        nn, P(mesh.verts), P(mesh.faces), n, P(prims), prims.numel(),
+                                                        P(d_rays[j & 1]), P(isects), a.rays, P(err),
+                                                        c.c_void_p(stream.cuda_stream)))
+
+    sampler = ClockSampler(dev.index, enabled=not a.profile)
+    total_ms, prof, clocks = timed_steps(a, dist, step, sampler, stream)
+    if int(err.item()):
+        raise RuntimeError("traversal reported a bad index")
+    if a.profile:
+        return {"profile": "obvh_trace", "rays": a.rays, "ms_per_step": total_ms / a.steps, "kernels": prof}
+    hits = np.frombuffer(isects.cpu().numpy().tobytes(), dtype=workloads.ISECT)
+    hit_fraction = float((hits["primitive"] != 0xFFFFFFFF).mean())
+    peak, peak_kind = peaks()
+    value = dist.world * a.rays * a.steps / (total_ms / 1e3) / 1e6
+
+    # work per ray from the oracle's counters on a sample of the same rays
+    from oracle import bvh as ref
+    lt = soa["left_T"].cpu().numpy().reshape(-1, 12)[:ni]
+    rt = soa["right_T"].cpu().numpy().reshape(-1, 12)[:ni]
+    meta = soa["metadata"].cpu().numpy().reshape(-1, 4)
+    pr = prims.cpu().numpy().view(np.uint32)
+    counts = ref.soa_obvh_traversal_counts(lt, rt, meta, v, f, pr, ray_sets[0][:20_000])
+    per_ray = trace_bytes_per_ray(counts, hit_fraction)
+    algo = {"trace_kernel": int(per_ray * a.rays)}
+    roof = roofline(prof, algo, peak, peak_kind, os.path.join(ROOT, "profiles", "obvh_trace_traffic.json"))
+
+    # end to end through kr_cuda_soa_obvh_intersect: the scene resident, the
+    # rays copied from pinned host memory and the records read back each step
+    d_soa = c.c_void_p(0)
+    _native.check(lib.kr_cuda_soa_obvh(P(soa["packed"]), P(soa["pairs"]), c.byref(d_soa), ni, nn))
+    h_rays = torch.empty(32 * a.rays, dtype=torch.uint8, pin_memory=True)
+    h_rays.copy_(d_rays[0])
+    h_isects = torch.empty(28 * a.rays, dtype=torch.uint8, pin_memory=True)
+    counter = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def e2e_step():
+        d_rays[1].copy_(h_rays, non_blocking=True)
+        torch.cuda.synchronize()
+        _native.check(lib.kr_cuda_soa_obvh_intersect(d_soa, P(mesh.verts), P(mesh.faces), P(prims), P(d_rays[1]),
+                                                     P(isects), a.rays, 128, 0, P(counter)))
+        h_isects.copy_(isects)
+
+    try:
+        e2e_step()
+        e2e_steps = max(3, min(a.steps, 10))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        e2e_s = time.perf_counter() - t0
+    finally:
+        _native.check(lib.obvh_soa_obvh_free(d_soa))
+    e2e_min = -dist.max(-(a.rays * e2e_steps / e2e_s / 1e6))
+    line = {
+        "metric": "OBVH closest-hit traversal throughput (Mrays/s)", "value": round(value, 3), "unit": "Mrays/s",
+        "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(total_ms / a.steps, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: probe rays from a sphere around [0,1]^3 towards uniform points in it, through the "
+                "collapsed OBB tree of the 2M thin-triangle soup",
+        "config": {"workload": "obvh_trace_collapsed_tree", "triangles": n, "rays_per_gpu": a.rays,
+                   "hit_fraction": round(hit_fraction, 4), "work_per_ray": {k: round(x, 2) for k, x in counts.items()},
+                   "l2": "two ray sets of 128 MB alternated; the tree's SoA (256 MB) and mesh (104 MB) exceed L2",
+                   "parallelism": f"replicas{dist.world}"},
+        "kernels": kernel_table(prof, a.steps, algo, peak),
+        "gpu_launches": sum(x[0] for x in prof.values()), "roofline": roof,
+        "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 32 * a.rays,
+                "d2h_bytes_per_step": 28 * a.rays,
+                "api": "kr_cuda_soa_obvh_intersect, rays from pinned host memory, records read back to pinned memory"},
+        "clocks": clocks,
+    }
+    if dist.rank == 0 and dist.world == 1:
+        sample = ray_sets[0][:200_000]
+        t0 = time.perf_counter()
+        ref.soa_obvh_intersect(lt, rt, meta, v, f, pr, sample, threads=1)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(len(sample) / dt / 1e6, 4), "unit": "Mrays/s", "cores": 1,
+                                "kind": "port",
+                                "sample": f"{len(sample)} of the rays ({dt:.1f} s), oracle C restatement"}
+    return line
+
+
+def bench_trace_reference(a, dist):
+    """The CPU restatement of the traversal (oracle port) on this host's cores:
+    each step every host thread traces its slice of a 400K-ray sample through
+    the collapsed OBB tree of the 2M-triangle soup (built once, by the oracle)."""
+    import numpy as np
+    from oracle import bvh as ref
+    from obvh_b200 import workloads
+    n = a.tris
+    v, f = workloads.triangle_soup(n, seed=1)
+    r = ref.lbvh_build(v, f)
+    _, xfs, _ = ref.obb_tree(r["nodes"], r["parents"], v, f)
+    col, _, prims, _, _ = ref.collapse(r["nodes"], r["parents"], r["counts"], r["costs"])
+    pk, pr = ref.pack(col, xfs)
+    lt, rt, meta = ref.soa_obvh(pk, pr, n - 1)
+    rays = workloads.probe_rays(min(a.rays, 400_000), [0, 0, 0], [1, 1, 1], seed=21)
+    threads = host_threads()
+    times = []
+    for j in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
+        ref.soa_obvh_intersect(lt, rt, meta, v, f, prims, rays, threads=threads)
+        if j >= a.warmup:
+            times.append(time.perf_counter() - t0)
+    value = len(rays) * len(times) / sum(times) / 1e6
+    return {"metric": "OBVH closest-hit traversal throughput (Mrays/s)", "impl": "reference",
+            "value": round(value, 4), "unit": "Mrays/s", "n_gpus": dist.world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (same generator as the ours arm)",
+            "config": {"workload": "obvh_trace_collapsed_tree", "triangles": n, "sample_rays": len(rays)},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": threads, "kind": "port",
+                             "sample": f"{len(rays)} rays per step over {threads} host threads (oracle C "
+                                       "restatement)"},
+            "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# ---------------------------------------------------------------------------
 def bench_dito_ours(a, dist):
     import torch
     from obvh_b200 import DitoFitter, points_obb, workloads
@@ -1146,6 +1309,8 @@ def main():
             print(json.dumps(bench_atrbvh_reference(a, dist)), flush=True)
         elif a.workload == "obvh_pack":
             print(json.dumps(bench_pack_reference(a, dist)), flush=True)
+        elif a.workload == "obvh_trace":
+            print(json.dumps(bench_trace_reference(a, dist)), flush=True)
         else:
             print(json.dumps(bench_tree_reference(a, dist)), flush=True)
         return
@@ -1153,7 +1318,7 @@ def main():
     try:
         run = {"lbvh_obb_tree": bench_tree_ours, "atrbvh_obb_tree": lambda a, d: bench_tree_ours(a, d, atrbvh=True),
                "dito": bench_dito_ours, "dito_batch": bench_batch_ours, "serve": bench_serve_ours,
-               "obvh_pack": bench_pack_ours}
+               "obvh_pack": bench_pack_ours, "obvh_trace": bench_trace_ours}
         line = run[a.workload](a, dist)
         if dist.rank == 0:
             print(json.dumps(line), flush=True)

@@ -9,9 +9,10 @@
 // intersected after the next node is popped; triangles are tested in the
 // leaf's order and a hit replaces the closest one only if strictly nearer.
 // The reference's warp ballots only decide when a warp leaves its loops, so
-// they are not needed here: one thread per ray, node records read as 16-byte
-// words through the read-only path, the 64-entry stack in registers/local
-// memory as in the reference.  Indices are checked: a node, leaf, primitive
+// the scheduling is free: persistent warps hand each lane a new ray as soon
+// as its ray is done (below), node records are read as 16-byte words through
+// the read-only path, and the 64-entry stack lives in local memory as in the
+// reference.  Indices are checked: a node, leaf, primitive
 // slot or face outside its array, or a stack deeper than 64, stops that ray
 // with its miss record and sets the error word.
 #include <cuda_runtime.h>
@@ -74,132 +75,193 @@ __device__ __forceinline__ V3 vertex(const kr_vec3* v, uint32_t i) {
     return v3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
 }
 
+// Per-ray traversal state: everything one ray carries between steps.
+struct RayState {
+    V3 o, d;
+    float hit_t, b1, b2;
+    uint32_t hit, fail;
+    int32_t inode, leaf;
+    int sp;
+};
+
+// The reference's record for a finished ray: the miss record, or the hit
+// triangle's unit normal, barycentrics and index.
+__device__ __forceinline__ void finish(const RayState& st, const kr_vec3* verts, const kr_uvec4* faces,
+                                       kr_intersection* out, uint32_t* err) {
+    uint32_t hit = st.hit;
+    if (st.fail) {
+        atomicOr(err, st.fail);
+        hit = 0xFFFFFFFFu;
+    }
+    kr_intersection rec;
+    if (hit == 0xFFFFFFFFu) {
+        rec.geom_normal = kr_vec3{{st.d.x, st.d.y, st.d.z}};
+        rec.barys = kr_vec2{{0.5f, 0.5f}};
+    } else {
+        const uint4 f = __ldg(reinterpret_cast<const uint4*>(faces + hit));
+        const V3 va = vertex(verts, f.x), vb = vertex(verts, f.y), vc = vertex(verts, f.z);
+        const V3 n = cross(sub(vb, va), sub(vc, va));
+        const float len = sqrtf(dot(n, n));
+        rec.geom_normal = kr_vec3{{n.x / len, n.y / len, n.z / len}};
+        rec.barys = kr_vec2{{st.b1, st.b2}};
+    }
+    rec.primitive = hit;
+    rec.instance = 0;
+    *out = rec;
+}
+
+// Persistent warps: warp w owns rays [w * per, (w + 1) * per) and hands a
+// lane the next of them as soon as that lane's ray is finished, at the top of
+// every outer step (one descent to a leaf plus the leaves found, the body of
+// the reference's outer loop), so lanes do not wait for the warp's slowest
+// ray.  A ray's own steps are those of the reference, in the same order.
 __global__ void __launch_bounds__(kThreads)
 trace_kernel(const kr_mat43* __restrict__ left_t, const kr_mat43* __restrict__ right_t,
              const kr_ivec4* __restrict__ meta, uint32_t internal_count, uint32_t node_count,
              const kr_vec3* __restrict__ verts, const kr_uvec4* __restrict__ faces, uint32_t face_count,
              const kr_u32* __restrict__ prims, uint32_t prim_slots, const kr_ray* __restrict__ rays,
-             kr_intersection* isects, uint32_t ray_count, uint32_t* err) {
-    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < ray_count; r += gridDim.x * blockDim.x) {
-        const float4* rp = reinterpret_cast<const float4*>(rays + r);
-        const float4 ra = __ldg(rp), rb = __ldg(rp + 1);
-        const V3 o = v3(ra.x, ra.y, ra.z), d = v3(rb.x, rb.y, rb.z);
-        float hit_t = rb.w;
-        uint32_t hit = 0xFFFFFFFFu;
-        float b1 = 0.0f, b2 = 0.0f;
-        uint32_t fail = 0;
-        int32_t stack[kStack];
-        int sp = 0;
-        stack[0] = kSentinel;
-        int32_t inode = 0, leaf = 0;
-        while (inode != kSentinel && !fail) {
-            bool searching = true;
-            while (searching && inode >= 0 && inode != kSentinel) {
-                if (static_cast<uint32_t>(inode) >= internal_count) {
-                    fail = kErrIndex;
+             kr_intersection* isects, uint32_t ray_count, uint32_t per_warp, uint32_t* err) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t first = warp * per_warp;
+    const uint64_t last = first + per_warp;
+    const uint32_t end = last < ray_count ? static_cast<uint32_t>(last) : ray_count;
+    uint32_t next = first < ray_count ? static_cast<uint32_t>(first) : ray_count;  // next unassigned ray
+    int32_t stack[kStack];
+    RayState st;
+    uint32_t r = 0;
+    bool busy = false;
+    for (;;) {
+        // hand the warp's next rays to the idle lanes, in lane order
+        const uint32_t idle = __ballot_sync(0xffffffffu, !busy);
+        if (!busy) {
+            const uint32_t k = next + __popc(idle & ((1u << lane) - 1u));
+            if (k < end) {
+                r = k;
+                busy = true;
+                const float4* rp = reinterpret_cast<const float4*>(rays + r);
+                const float4 ra = __ldg(rp), rb = __ldg(rp + 1);
+                st.o = v3(ra.x, ra.y, ra.z);
+                st.d = v3(rb.x, rb.y, rb.z);
+                st.hit_t = rb.w;
+                st.hit = 0xFFFFFFFFu;
+                st.b1 = st.b2 = 0.0f;
+                st.fail = 0;
+                st.inode = 0;
+                st.leaf = 0;
+                st.sp = 0;
+                stack[0] = kSentinel;
+            }
+        }
+        next = min(end, next + __popc(idle));
+        if (!__any_sync(0xffffffffu, busy)) break;
+        if (!busy) continue;
+        const V3 o = st.o, d = st.d;
+        // descend until a leaf is found (the reference's inner loop)
+        bool searching = true;
+        while (searching && st.inode >= 0 && st.inode != kSentinel) {
+            if (static_cast<uint32_t>(st.inode) >= internal_count) {
+                st.fail = kErrIndex;
+                break;
+            }
+            const int4 m = __ldg(reinterpret_cast<const int4*>(meta + st.inode));
+            const float2 li = unit_box(load_m43(left_t + st.inode), d, o);
+            const float2 ri = unit_box(load_m43(right_t + st.inode), d, o);
+            const bool tl = (li.y >= li.x) && (li.y >= 0.0f) && (li.x <= st.hit_t);
+            const bool tr = (ri.y >= ri.x) && (ri.y >= 0.0f) && (ri.x <= st.hit_t);
+            int32_t inode = m.x;
+            int32_t rnode = m.y;
+            if (tl != tr) {
+                if (tr) inode = rnode;
+            } else if (!tl) {
+                inode = stack[st.sp--];
+            } else {
+                if (ri.x < li.x) {
+                    const int32_t t = inode;
+                    inode = rnode;
+                    rnode = t;
+                }
+                if (st.sp + 1 >= kStack) {
+                    st.fail = kErrStack;
                     break;
                 }
-                const int4 m = __ldg(reinterpret_cast<const int4*>(meta + inode));
-                const float2 li = unit_box(load_m43(left_t + inode), d, o);
-                const float2 ri = unit_box(load_m43(right_t + inode), d, o);
-                const bool tl = (li.y >= li.x) && (li.y >= 0.0f) && (li.x <= hit_t);
-                const bool tr = (ri.y >= ri.x) && (ri.y >= 0.0f) && (ri.x <= hit_t);
-                inode = m.x;
-                int32_t rnode = m.y;
-                if (tl != tr) {
-                    if (tr) inode = rnode;
-                } else if (!tl) {
-                    inode = stack[sp--];
+                stack[++st.sp] = rnode;
+            }
+            if (inode < 0 && st.leaf >= 0) {
+                searching = false;
+                st.leaf = inode;
+                inode = st.sp >= 0 ? stack[st.sp--] : kSentinel;
+            }
+            st.inode = inode;
+        }
+        // the leaves found (the reference's leaf loop)
+        while (!st.fail && st.leaf < 0) {
+            const uint32_t li = static_cast<uint32_t>(~st.leaf);
+            if (li >= node_count) {
+                st.fail = kErrIndex;
+                break;
+            }
+            const int4 m = __ldg(reinterpret_cast<const int4*>(meta + li));
+            const int32_t num = m.y - m.x;
+            for (int32_t beg = m.x; beg < m.y; ++beg) {
+                uint32_t pid;
+                if (num == 1) {
+                    pid = static_cast<uint32_t>(beg);
                 } else {
-                    if (ri.x < li.x) {
-                        const int32_t t = inode;
-                        inode = rnode;
-                        rnode = t;
-                    }
-                    if (sp + 1 >= kStack) {
-                        fail = kErrStack;
+                    if (beg < 0 || static_cast<uint32_t>(beg) >= prim_slots) {
+                        st.fail = kErrIndex;
                         break;
                     }
-                    stack[++sp] = rnode;
+                    pid = __ldg(prims + beg);
                 }
-                if (inode < 0 && leaf >= 0) {
-                    searching = false;
-                    leaf = inode;
-                    inode = sp >= 0 ? stack[sp--] : kSentinel;
-                }
-            }
-            while (!fail && leaf < 0) {
-                const uint32_t li = static_cast<uint32_t>(~leaf);
-                if (li >= node_count) {
-                    fail = kErrIndex;
+                if (pid >= face_count) {
+                    st.fail = kErrIndex;
                     break;
                 }
-                const int4 m = __ldg(reinterpret_cast<const int4*>(meta + li));
-                const int32_t num = m.y - m.x;
-                for (int32_t beg = m.x; beg < m.y; ++beg) {
-                    uint32_t pid;
-                    if (num == 1) {
-                        pid = static_cast<uint32_t>(beg);
-                    } else {
-                        if (beg < 0 || static_cast<uint32_t>(beg) >= prim_slots) {
-                            fail = kErrIndex;
-                            break;
-                        }
-                        pid = __ldg(prims + beg);
-                    }
-                    if (pid >= face_count) {
-                        fail = kErrIndex;
-                        break;
-                    }
-                    const uint4 f = __ldg(reinterpret_cast<const uint4*>(faces + pid));
-                    const V3 p1 = vertex(verts, f.x), p2 = vertex(verts, f.y), p3 = vertex(verts, f.z);
-                    // kr_ray_triangle_intersect
-                    const V3 e1 = sub(p2, p1), e2 = sub(p3, p1);
-                    const V3 s1 = cross(d, e2);
-                    const float invd = 1.0f / dot(s1, e1);
-                    const V3 dd = sub(o, p1);
-                    const float c1 = dot(dd, s1) * invd;
-                    const V3 s2 = cross(dd, e1);
-                    const float c2 = dot(d, s2) * invd;
-                    const float t = dot(e2, s2) * invd;
-                    const bool miss = c1 < 0.0f || c1 > 1.0f || c2 < 0.0f || c1 + c2 > 1.0f || t < 0.0f || t > hit_t;
-                    if (!miss && t < hit_t) {
-                        hit_t = t;
-                        hit = pid;
-                        b1 = c1;
-                        b2 = c2;
-                    }
+                const uint4 f = __ldg(reinterpret_cast<const uint4*>(faces + pid));
+                const V3 p1 = vertex(verts, f.x), p2 = vertex(verts, f.y), p3 = vertex(verts, f.z);
+                // kr_ray_triangle_intersect
+                const V3 e1 = sub(p2, p1), e2 = sub(p3, p1);
+                const V3 s1 = cross(d, e2);
+                const float invd = 1.0f / dot(s1, e1);
+                const V3 dd = sub(o, p1);
+                const float c1 = dot(dd, s1) * invd;
+                const V3 s2 = cross(dd, e1);
+                const float c2 = dot(d, s2) * invd;
+                const float t = dot(e2, s2) * invd;
+                const bool miss = c1 < 0.0f || c1 > 1.0f || c2 < 0.0f || c1 + c2 > 1.0f || t < 0.0f || t > st.hit_t;
+                if (!miss && t < st.hit_t) {
+                    st.hit_t = t;
+                    st.hit = pid;
+                    st.b1 = c1;
+                    st.b2 = c2;
                 }
-                if (fail) break;
-                leaf = inode;
-                if (inode < 0) inode = sp >= 0 ? stack[sp--] : kSentinel;
             }
+            if (st.fail) break;
+            st.leaf = st.inode;
+            if (st.inode < 0) st.inode = st.sp >= 0 ? stack[st.sp--] : kSentinel;
         }
-        kr_intersection out;
-        if (fail) {
-            atomicOr(err, fail);
-            hit = 0xFFFFFFFFu;
+        if (st.fail || st.inode == kSentinel) {
+            finish(st, verts, faces, isects + r, err);
+            busy = false;
         }
-        if (hit == 0xFFFFFFFFu) {
-            out.geom_normal = kr_vec3{{d.x, d.y, d.z}};
-            out.barys = kr_vec2{{0.5f, 0.5f}};
-        } else {
-            const uint4 f = __ldg(reinterpret_cast<const uint4*>(faces + hit));
-            const V3 va = vertex(verts, f.x), vb = vertex(verts, f.y), vc = vertex(verts, f.z);
-            const V3 n = cross(sub(vb, va), sub(vc, va));
-            const float len = sqrtf(dot(n, n));
-            out.geom_normal = kr_vec3{{n.x / len, n.y / len, n.z / len}};
-            out.barys = kr_vec2{{b1, b2}};
-        }
-        out.primitive = hit;
-        out.instance = 0;
-        isects[r] = out;
     }
 }
 
+// Persistent grid: every block resident at once (the occupancy of
+// trace_kernel, looked up once per device), and no more blocks than rays
+// need.
 inline unsigned grid_for(uint32_t n) {
+    static int per_sm[64] = {0};
+    const DeviceInfo& dev = device_info();
+    int& k = per_sm[dev.device & 63];
+    if (k == 0 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, trace_kernel, kThreads, 0) != cudaSuccess) {
+        (void)cudaGetLastError();
+        k = 8;
+    }
+    if (k < 1) k = 1;
     const unsigned want = (n + kThreads - 1) / kThreads;
-    const unsigned cap = static_cast<unsigned>(device_info().sm_count) * 64u;
+    const unsigned cap = static_cast<unsigned>(dev.sm_count) * static_cast<unsigned>(k);
     return want < cap ? (want ? want : 1u) : cap;
 }
 
@@ -215,10 +277,12 @@ kr_error enqueue(const kr_mat43* left_t, const kr_mat43* right_t, const kr_ivec4
     if (internal_count == 0) return "obvh trace: the tree has no internal node (one primitive) to traverse";
     if (!aligned16(left_t) || !aligned16(right_t) || !aligned16(meta) || !aligned16(faces) || !aligned16(rays))
         return "obvh trace: SoA arrays, faces and rays must be 16-byte aligned";
+    const unsigned g = grid_for(ray_count);
+    const uint64_t warps = static_cast<uint64_t>(g) * (kThreads / 32);
+    const uint32_t per_warp = static_cast<uint32_t>((ray_count + warps - 1) / warps);
     ProfScope prof_scope_("trace_kernel", s);
-    trace_kernel<<<grid_for(ray_count), kThreads, 0, s>>>(left_t, right_t, meta, internal_count, node_count, verts,
-                                                          faces, face_count, prims, prim_slots, rays, isects,
-                                                          ray_count, err);
+    trace_kernel<<<g, kThreads, 0, s>>>(left_t, right_t, meta, internal_count, node_count, verts, faces, face_count,
+                                        prims, prim_slots, rays, isects, ray_count, per_warp, err);
     OBVH_TRY_CUDA(cudaGetLastError());
     return kr_success;
 }

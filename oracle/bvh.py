@@ -45,6 +45,10 @@ def _bind():
         "oracle_soa_obvh_intersect": (c.c_int64, [c.c_void_p, c.c_void_p, c.c_void_p, c.c_uint32, c.c_uint32,
                                                   c.c_void_p, c.c_void_p, c.c_uint32, c.c_void_p, c.c_uint32,
                                                   c.c_void_p, c.c_uint64, c.c_uint64, c.c_void_p]),
+        "oracle_soa_obvh_intersect_counts": (c.c_int64, [c.c_void_p, c.c_void_p, c.c_void_p, c.c_uint32,
+                                                         c.c_uint32, c.c_void_p, c.c_void_p, c.c_uint32, c.c_void_p,
+                                                         c.c_uint32, c.c_void_p, c.c_uint64, c.c_uint64, c.c_void_p,
+                                                         c.c_void_p]),
         "oracle_collapse": (c.c_int, [_node, _u32, _node, _u32, _u32, _f32, c.c_float, c.c_float, c.c_uint32,
                                       c.c_uint32]),
         "oracle_aabb_refit": (c.c_int, [_node, c.c_uint32, _u32, _f32]),
@@ -500,3 +504,51 @@ def refgpu_soa_obvh_intersect(left_t, right_t, metadata, verts, faces, prims, ra
     if rc != 0:
         raise RuntimeError(f"refgpu_soa_obvh_intersect: CUDA error {rc}")
     return out
+
+
+def soa_obvh_traversal_counts(left_t, right_t, metadata, verts, faces, prims, rays):
+    """Per-ray means of the traversal's work on these rays: dict of internal
+    nodes visited, leaves visited, triangles tested, primitive-list reads."""
+    l = _bind()
+    lt = np.ascontiguousarray(left_t, np.float32)
+    rt = np.ascontiguousarray(right_t, np.float32)
+    meta = np.ascontiguousarray(metadata, np.int32).reshape(-1, 4)
+    v, f, nf = _mesh(verts, faces)
+    pr = None if prims is None else np.ascontiguousarray(prims, np.uint32)
+    ry = np.ascontiguousarray(rays).view(np.uint8)
+    n = ry.nbytes // 32
+    out = np.zeros(n, ISECT)
+    counts = np.zeros(4, np.int64)
+    bad = l.oracle_soa_obvh_intersect_counts(lt.ctypes.data, rt.ctypes.data, meta.ctypes.data, lt.reshape(-1, 12).shape[0],
+                                             meta.shape[0], v.ctypes.data, f.ctypes.data, nf,
+                                             None if pr is None else pr.ctypes.data, 0 if pr is None else pr.size,
+                                             ry.ctypes.data, 0, n, out.ctypes.data, counts.ctypes.data)
+    if bad:
+        raise ValueError(f"{bad} rays met an index outside the arrays")
+    return {"internal_visits": counts[0] / n, "leaf_visits": counts[1] / n, "triangle_tests": counts[2] / n,
+            "list_reads": counts[3] / n}
+
+
+def refgpu_soa_obvh_intersect_ms(left_t, right_t, metadata, verts, faces, prims, rays, reps=5, variant="nofma"):
+    """Mean device time (ms) of one launch of the reference's traversal kernel
+    on device-resident data."""
+    l = ref_gpu(variant)
+    c = ctypes
+    f_ = l.refgpu_soa_obvh_intersect_timed
+    f_.restype = c.c_int
+    f_.argtypes = [c.c_void_p] * 3 + [c.c_uint32] * 2 + [c.c_void_p, c.c_uint32, c.c_void_p, c.c_uint32,
+                                                         c.c_void_p, c.c_uint32, c.c_void_p, c.c_uint32, c.c_uint32,
+                                                         c.POINTER(c.c_float)]
+    lt = np.ascontiguousarray(left_t, np.float32)
+    rt = np.ascontiguousarray(right_t, np.float32)
+    meta = np.ascontiguousarray(metadata, np.int32).reshape(-1, 4)
+    v, f, nf = _mesh(verts, faces)
+    pr = None if prims is None else np.ascontiguousarray(prims, np.uint32)
+    ry = np.ascontiguousarray(rays).view(np.uint8)
+    ms = c.c_float(0.0)
+    rc = f_(lt.ctypes.data, rt.ctypes.data, meta.ctypes.data, lt.reshape(-1, 12).shape[0], meta.shape[0],
+            v.ctypes.data, v.size // 3, f.ctypes.data, nf, None if pr is None else pr.ctypes.data,
+            0 if pr is None else pr.size, ry.ctypes.data, ry.nbytes // 32, reps, c.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"refgpu_soa_obvh_intersect_timed: CUDA error {rc}")
+    return ms.value

@@ -72,6 +72,11 @@ int64_t oracle_soa_obvh_intersect(const float* left_t, const float* right_t, con
                                   const uint32_t* faces4, uint32_t face_count, const uint32_t* prims,
                                   uint32_t prim_slots, const float* rays, uint64_t first, uint64_t last,
                                   uint32_t* isects);
+int64_t oracle_soa_obvh_intersect_counts(const float* left_t, const float* right_t, const int32_t* metadata,
+                                         uint32_t internal_count, uint32_t node_count, const float* verts,
+                                         const uint32_t* faces4, uint32_t face_count, const uint32_t* prims,
+                                         uint32_t prim_slots, const float* rays, uint64_t first, uint64_t last,
+                                         uint32_t* isects, int64_t* counts);
 
 /* ATRBVH path (atrbvh_oracle.c) */
 uint64_t oracle_morton63(const float tri9[9], const float scene[6]);

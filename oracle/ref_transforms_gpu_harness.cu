@@ -209,3 +209,50 @@ extern "C" int refgpu_soa_obvh_intersect(const float* left_t, const float* right
     a.back(isects, d_isects, sizeof(kr_intersection) * ray_count);
     return static_cast<int>(a.err);
 }
+
+// The reference's traversal timed on device-resident data: the same inputs as
+// refgpu_soa_obvh_intersect, `reps` launches of kr_cuda_soa_obvh_intersect
+// (its ray counter zeroed before each, as its callers do) between CUDA
+// events; *ms receives the mean time of one launch.  Returns 0 or the CUDA
+// error code.
+extern "C" int refgpu_soa_obvh_intersect_timed(const float* left_t, const float* right_t, const int32_t* metadata,
+                                               uint32_t internal_count, uint32_t node_count, const float* verts,
+                                               uint32_t n_verts, const uint32_t* faces4, uint32_t face_count,
+                                               const uint32_t* prims, uint32_t prim_slots, const float* rays,
+                                               uint32_t ray_count, uint32_t reps, float* ms) {
+    if (internal_count == 0 || ray_count == 0 || reps == 0) return -1;
+    Arena a;
+    kr_SoA_OBVH h;
+    h.left_T = static_cast<mat43*>(a.copy(left_t, sizeof(mat43) * internal_count));
+    h.right_T = static_cast<mat43*>(a.copy(right_t, sizeof(mat43) * internal_count));
+    h.metadata = static_cast<ivec4*>(a.copy(metadata, sizeof(ivec4) * node_count));
+    auto* d_soa = static_cast<kr_SoA_OBVH*>(a.copy(&h, sizeof h));
+    auto* d_verts = static_cast<kr_vec3*>(a.copy(verts, 12ull * n_verts));
+    auto* d_faces = static_cast<kr_uvec4*>(a.copy(faces4, 16ull * face_count));
+    auto* d_prims = prims ? static_cast<u32*>(a.copy(prims, 4ull * prim_slots)) : nullptr;
+    auto* d_rays = static_cast<kr_ray*>(a.copy(rays, sizeof(kr_ray) * ray_count));
+    auto* d_isects = static_cast<kr_intersection*>(a.zeroed(sizeof(kr_intersection) * ray_count));
+    auto* d_counter = static_cast<u32*>(a.zeroed(4));
+    if (a.err != cudaSuccess) return static_cast<int>(a.err);
+    cudaEvent_t e0, e1;
+    a.note(cudaEventCreate(&e0));
+    a.note(cudaEventCreate(&e1));
+    cudaMemset(d_counter, 0, 4);
+    kr_cuda_soa_obvh_intersect(d_soa, d_verts, d_faces, d_prims, d_rays, d_isects, ray_count, 128, 0, d_counter);
+    a.note(cudaDeviceSynchronize());
+    float total = 0.f;
+    for (uint32_t k = 0; k < reps && a.err == cudaSuccess; ++k) {
+        a.note(cudaMemset(d_counter, 0, 4));
+        a.note(cudaEventRecord(e0));
+        kr_cuda_soa_obvh_intersect(d_soa, d_verts, d_faces, d_prims, d_rays, d_isects, ray_count, 128, 0, d_counter);
+        a.note(cudaEventRecord(e1));
+        a.note(cudaEventSynchronize(e1));
+        float t = 0.f;
+        a.note(cudaEventElapsedTime(&t, e0, e1));
+        total += t;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = total / reps;
+    return static_cast<int>(a.err);
+}

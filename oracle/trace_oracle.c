@@ -75,7 +75,7 @@ static t3 vtx(const float* v, uint32_t i) { return mk3(v[3 * i], v[3 * i + 1], v
  * arrays or a stack deeper than the reference's 64 entries. */
 static int trace_one(const float* lt, const float* rt, const int32_t* meta, uint32_t internal_count,
                      uint32_t node_count, const float* verts, const uint32_t* faces4, uint32_t face_count,
-                     const uint32_t* prims, uint32_t prim_slots, const float* ray, uint32_t* out) {
+                     const uint32_t* prims, uint32_t prim_slots, const float* ray, uint32_t* out, int64_t* counts) {
     int32_t stack[STACK];
     int sp = 0;
     stack[0] = SENTINEL;
@@ -93,6 +93,7 @@ static int trace_one(const float* lt, const float* rt, const int32_t* meta, uint
         int searching = 1;
         while (searching && inode >= 0 && inode != SENTINEL) {
             if ((uint32_t)inode >= internal_count) return -1;
+            if (counts) counts[0]++;
             const int32_t* m = meta + 4 * (size_t)inode;
             const float* L = lt + 12 * (size_t)inode;
             const float* R = rt + 12 * (size_t)inode;
@@ -125,6 +126,11 @@ static int trace_one(const float* lt, const float* rt, const int32_t* meta, uint
             if (li >= node_count) return -1;
             const int32_t* m = meta + 4 * (size_t)li;
             int32_t beg = m[0], end = m[1], num = end - beg;
+            if (counts) {
+                counts[1]++;
+                counts[2] += num > 0 ? num : 0;
+                counts[3] += num > 1 ? num : 0;
+            }
             for (; beg < end; ++beg) {
                 uint32_t pid;
                 if (num == 1) pid = (uint32_t)beg;
@@ -170,7 +176,22 @@ int64_t oracle_soa_obvh_intersect(const float* left_t, const float* right_t, con
     int64_t bad = 0;
     for (uint64_t r = first; r < last; r++)
         if (trace_one(left_t, right_t, metadata, internal_count, node_count, verts, faces4, face_count, prims,
-                      prim_slots, rays + 8 * r, isects + 7 * r))
+                      prim_slots, rays + 8 * r, isects + 7 * r, NULL))
+            bad++;
+    return bad;
+}
+
+/* The same traversal, counting into counts[4]: internal nodes visited, leaves
+ * visited, triangles tested, and primitive-list entries read. */
+int64_t oracle_soa_obvh_intersect_counts(const float* left_t, const float* right_t, const int32_t* metadata,
+                                         uint32_t internal_count, uint32_t node_count, const float* verts,
+                                         const uint32_t* faces4, uint32_t face_count, const uint32_t* prims,
+                                         uint32_t prim_slots, const float* rays, uint64_t first, uint64_t last,
+                                         uint32_t* isects, int64_t* counts) {
+    int64_t bad = 0;
+    for (uint64_t r = first; r < last; r++)
+        if (trace_one(left_t, right_t, metadata, internal_count, node_count, verts, faces4, face_count, prims,
+                      prim_slots, rays + 8 * r, isects + 7 * r, counts))
             bad++;
     return bad;
 }

@@ -136,3 +136,30 @@ def test_bad_index_is_reported():
     _, err = bvh.soa_obvh_intersect(s, mesh, prims, _dev_rays(rays), nn, ni)
     torch.cuda.synchronize()
     assert int(err.item()) & 1
+
+
+@pytest.mark.skipif(not ref.ref_gpu_available("nofma"), reason="oracle/_ref reference GPU libraries not built")
+def test_traversal_speed_against_the_reference_kernel(capsys):
+    """Both kernels on the same device-resident SoA OBVH and 1M rays (CUDA
+    events, mean of 5 launches after one warm-up): the traversal is at least
+    as fast as the reference's own kernel built as it ships."""
+    import torch
+    v, f, mesh, s, prims, nn, ni = _scene("soup", 2_000_000, True, seed=1)
+    rays = _rays(1_000_000, seed=21)
+    d_rays = _dev_rays(rays)
+    bvh.soa_obvh_intersect(s, mesh, prims, d_rays, nn, ni)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        out, err = bvh.soa_obvh_intersect(s, mesh, prims, d_rays, nn, ni)
+    e1.record()
+    torch.cuda.synchronize()
+    ours = e0.elapsed_time(e1) / 5
+    lt, rt, meta = _soa_numpy(s, ni)
+    p = prims.cpu().numpy().view(np.uint32)
+    theirs = {var: ref.refgpu_soa_obvh_intersect_ms(lt, rt, meta, v, f, p, rays, 5, var) for var in ("nofma", "fmad")}
+    with capsys.disabled():
+        print(f"\ntraversal of 1M rays, 2M-triangle collapsed tree: ours {ours:.3f} ms, reference kernel "
+              f"{theirs['fmad']:.3f} ms as shipped, {theirs['nofma']:.3f} ms uncontracted")
+    assert ours <= theirs["fmad"] * 1.05
