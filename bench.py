@@ -469,6 +469,11 @@ def bench_tree_ours(a, dist, atrbvh=False):
                            "api": "the same calls with each step's copy, build and read-back waited for in turn"}},
         "clocks": clocks,
     }
+    # tree quality of the last build (SAH over the root's area, on the device)
+    q = [bvh.bvh_sah(out["nodes"], out["parents"], o).cpu().tolist()[1] for o in (None, out["obbs"])]
+    q.append(bvh.bvh_sah(out["collapsed"], out["parents"], out["obbs"]).cpu().tolist()[1])
+    line["tree_quality"] = {"sah_aabb": round(q[0], 4), "sah_obb": round(q[1], 4), "sah_obb_collapsed": round(q[2], 4),
+                            "ci": 1.2, "ct": 1.0, "api": "obvh_bvh_sah_async (kr_bvh_sah's cost, on the device)"}
     if dist.rank == 0 and dist.world == 1:
         line["cpu_baseline"] = cpu_atrbvh_baseline(a.treelet) if atrbvh else cpu_tree_baseline()
     return line

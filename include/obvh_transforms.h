@@ -162,6 +162,28 @@ OBVH_EXPORT kr_error obvh_soa_obvh_intersect_async(const kr_mat43* d_left_t, con
                                                    const kr_u32* d_primitives, kr_u32 primitive_slots,
                                                    const kr_ray* d_rays, kr_intersection* d_isects,
                                                    kr_u32 ray_count, kr_u32* d_error, void* stream);
+/*
+ * SAH cost of a tree over its root's area (kr_bvh_sah,
+ * src/ads/common/transforms.h:38, transforms.cpp:250-303).  Host arrays, as
+ * in the reference: nodes from root_idx, obbs nullable (then AABB areas);
+ * the sum runs depth first, right child first, in float, so the result is
+ * the reference's bit for bit.  outputFile (nullable) gets "%f," appended.
+ */
+OBVH_EXPORT kr_scalar kr_bvh_sah(const kr_bvh_node* nodes, kr_i32 root_idx, kr_scalar ci, kr_scalar ct,
+                                 const kr_obb3* obbs, const char* outputFile);
+/* Workspace bytes of obvh_bvh_sah_async. */
+OBVH_EXPORT kr_size obvh_bvh_sah_workspace_bytes(kr_u32 node_count);
+/*
+ * The same cost on the device for a tree rooted at node 0 (d_parents names
+ * each node's parent, 0xFFFFFFFF for the root): the same float terms, summed
+ * in double in a fixed order.  d_result[0] = the SAH sum, d_result[1] = the
+ * sum over the root's area.  d_obbs nullable.  On `stream`, without
+ * synchronising.  No counterpart in the reference (which computes it on the
+ * host after copying the tree back).
+ */
+OBVH_EXPORT kr_error obvh_bvh_sah_async(const kr_bvh_node* d_nodes, const kr_u32* d_parents, const kr_obb3* d_obbs,
+                                        kr_u32 node_count, kr_scalar ci, kr_scalar ct, double* d_result,
+                                        void* d_workspace, void* stream);
 /* Reads the device error word of the last transform made with a workspace
  * (synchronises `stream`): 0 ok, 4 parent walk longer than the tree. */
 OBVH_EXPORT kr_error obvh_obb_tree_error(const void* d_workspace, void* stream, kr_u32* device_error);

@@ -59,6 +59,9 @@ def _declare(lib: ctypes.CDLL) -> None:
         "kr_cuda_soa_obvh_intersect": (err, [vp, vp, vp, vp, vp, vp, c.c_uint32, c.c_uint32, c.c_uint32, vp]),
         "obvh_soa_obvh_intersect_async": (err, [vp, vp, vp, c.c_uint32, c.c_uint32, vp, vp, c.c_uint32, vp,
                                                 c.c_uint32, vp, vp, c.c_uint32, vp, vp]),
+        "kr_bvh_sah": (c.c_float, [vp, c.c_int32, c.c_float, c.c_float, vp, c.c_char_p]),
+        "obvh_bvh_sah_workspace_bytes": (c.c_uint64, [c.c_uint32]),
+        "obvh_bvh_sah_async": (err, [vp, vp, vp, c.c_uint32, c.c_float, c.c_float, vp, vp, vp]),
         "kr_cuda_bbox_calculate": (err, [vp, vp, c.c_uint32, vp]),
         "kr_cuda_centroid_bbox_calculate": (err, [vp, vp, c.c_uint32, vp]),
         "obvh_lbvh_workspace_bytes": (c.c_uint64, [c.c_uint32]),

@@ -390,3 +390,26 @@ def soa_obvh_intersect(soa: dict, mesh: "Mesh", primitives, rays, node_count: in
         _ptr(mesh.verts), _ptr(mesh.faces), mesh.n_faces, _ptr(primitives), slots, _ptr(rays), _ptr(isects), n,
         _ptr(err), _stream(torch, stream)))
     return isects, err
+
+
+# ---- SAH cost ----------------------------------------------------------------
+def bvh_sah_host(nodes: np.ndarray, ci: float = 1.2, ct: float = 1.0, obbs: np.ndarray = None,
+                 root: int = 0) -> float:
+    """kr_bvh_sah on host arrays (NODE records, obbs [nodes x 15] or None)."""
+    lib = _native.lib()
+    n = np.ascontiguousarray(nodes)
+    o = None if obbs is None else np.ascontiguousarray(obbs, np.float32)
+    return float(lib.kr_bvh_sah(n.ctypes.data, root, ci, ct, None if o is None else o.ctypes.data, None))
+
+
+def bvh_sah(nodes, parents, obbs=None, ci: float = 1.2, ct: float = 1.0, stream=None):
+    """obvh_bvh_sah_async on device tensors: (SAH sum, SAH / root area), as
+    a device float64 tensor [2]."""
+    import torch
+    lib = _native.lib()
+    nn = parents.numel()
+    ws = torch.empty(int(lib.obvh_bvh_sah_workspace_bytes(nn)), dtype=torch.uint8, device=parents.device)
+    out = torch.empty(2, dtype=torch.float64, device=parents.device)
+    _native.check(lib.obvh_bvh_sah_async(_ptr(nodes), _ptr(parents), _ptr(obbs), nn, ci, ct, _ptr(out), _ptr(ws),
+                                         _stream(torch, stream)))
+    return out

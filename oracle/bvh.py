@@ -552,3 +552,46 @@ def refgpu_soa_obvh_intersect_ms(left_t, right_t, metadata, verts, faces, prims,
     if rc != 0:
         raise RuntimeError(f"refgpu_soa_obvh_intersect_timed: CUDA error {rc}")
     return ms.value
+
+
+# ---- SAH cost ------------------------------------------------------------------
+def ref_bvh_sah(nodes, ci=1.2, ct=1.0, obbs=None, root=0):
+    """The reference's own kr_bvh_sah (host code in oracle/_ref/libref_tree_gpu.so)."""
+    l = ref_gpu("nofma")
+    f_ = l.kr_bvh_sah
+    f_.restype = ctypes.c_float
+    f_.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_char_p]
+    n = np.ascontiguousarray(nodes)
+    o = None if obbs is None else np.ascontiguousarray(obbs, np.float32)
+    return float(f_(n.ctypes.data, root, ci, ct, None if o is None else o.ctypes.data, None))
+
+
+def sah_terms(nodes, parents, obbs=None, ci=1.2, ct=1.0):
+    """Per-node float32 terms of the SAH cost (0 for nodes a traversal cannot
+    reach from root 0) and the root's area; their exact sum is the cost."""
+    npr = nodes["n_prims"].astype(np.int64)
+    nn = npr.shape[0]
+    par = np.asarray(parents, np.int64).copy()
+    par[par == 0xFFFFFFFF] = -1
+    reached = np.ones(nn, bool)
+    cur = par.copy()
+    while (cur >= 0).any():
+        live = cur >= 0
+        reached[live] &= npr[cur[live]] == 0
+        cur[live] = par[cur[live]]
+    b = nodes["b"].astype(np.float32)
+    d = (b[:, 3:] - b[:, :3]).astype(np.float32)
+    aabb = np.float32(2) * (d[:, 0] * d[:, 1] + d[:, 0] * d[:, 2] + d[:, 1] * d[:, 2])
+    if obbs is not None:
+        e = (np.float32(2) * np.asarray(obbs, np.float32)[:, 12:15]).astype(np.float32)
+        area = np.float32(2) * (e[:, 0] * e[:, 1] + e[:, 0] * e[:, 2] + e[:, 1] * e[:, 2])
+    else:
+        area = aabb
+    ci, ct = np.float32(ci), np.float32(ct)
+    npf = npr.astype(np.float32)
+    term = np.where(npr == 0, ci * area, (ct * npf) * np.where(npr == 1, aabb, area)).astype(np.float32)
+    if npr[0] != 0:
+        term[0] = (ct * area[0]) * npf[0]
+    term[npr == 0xFFFF] = 0
+    term[~reached] = 0
+    return term, float(area[0])
