@@ -18,14 +18,24 @@
  *                           LBVH (30-bit Morton) or ATRBVH (treelet size 9,
  *                           2 iterations), the OBB tree when use_obbs, the
  *                           collapse when collapse (lbvh.cu:1646-1764,
- *                           atrbvh.cu:258-530); like the reference, each object
- *                           replaces the previous one's tree
+ *                           atrbvh.cu:258-530), and with use_persistent_kernel
+ *                           the traversal packing of the (collapsed) tree, plus
+ *                           the SoA OBVH when use_obbs (lbvh.cu:1516-1545);
+ *                           like the reference, each object replaces the
+ *                           previous one's tree
  *   NAME                 -> "LBVH GPU" / "ATRBVH"
  *   PREFERRED_QUERY_TYPE -> KR_QUERY_TYPE_CUDA
  *   GET_BLAS             -> const obvh_ads_blas* (extension: the device-resident
  *                           result; the reference returns nothing here)
  *   DESTROY              -> frees the context (a no-op in the reference)
- *   INTERSECTION_QUERY   -> an error: ray traversal is not part of this library
+ *   INTERSECTION_QUERY   -> kr_intersection_query* of CUDA kind: closest hits
+ *                           through the SoA OBVH when use_obbs and
+ *                           use_persistent_kernel (lbvh.cu:45-110, the
+ *                           reference's kr_cuda_soa_obvh_intersect); nothing,
+ *                           as in the reference, when neither is set; an error
+ *                           for the traversal forms not built here (AABB,
+ *                           non-persistent OBVH, intersect_bounds)
+ *   OCCLUSION_QUERY      -> an error: not built
  *   others               -> kr_success, as in the reference
  * Errors are static strings; NULL is success.
  */
@@ -62,6 +72,12 @@ typedef struct obvh_ads_blas {
     kr_scalar ci, ct;
     kr_b32 collapse, use_obbs, save_construction_information, intersect_bounds, use_persistent_kernel;
     kr_i32 intersect_bounds_level;
+    /* traversal packing (use_persistent_kernel = y) */
+    kr_bvh_node_packed* bvh_packed;              /* node_count records */
+    kr_bvh_transformation_pair* transformations; /* internal_count pairs (use_obbs) */
+    kr_mat43* soa_left_T;                        /* SoA OBVH (use_obbs) */
+    kr_mat43* soa_right_T;
+    kr_ivec4* soa_metadata;
 } obvh_ads_blas;
 
 /* The whole action switch of one plugin kind (OBVH_ADS_LBVH / OBVH_ADS_ATRBVH). */

@@ -184,6 +184,15 @@ typedef enum {
     KR_QUERY_TYPE_CUDA_MANAGED, KR_QUERY_TYPE_MAX
 } kr_query_type;
 
+/* An intersection query (ads.h:92-114): rays and records of ray_count rays;
+ * device pointers for the CUDA kinds. */
+typedef struct { const kr_ray* rays; kr_intersection* isects; kr_size ray_count; } kr_intersection_query_cpu;
+typedef struct { const kr_ray* rays; kr_intersection* isects; kr_size ray_count; } kr_intersection_query_cuda;
+typedef struct {
+    kr_query_type type;
+    union { kr_intersection_query_cpu cpu; kr_intersection_query_cuda cuda; kr_intersection_query_cuda cuda_managed; };
+} kr_intersection_query;
+
 typedef struct kr_ads kr_ads;
 typedef kr_error (*kr_ads_callback)(kr_ads*, kr_handle, kr_ads_action);
 struct kr_ads {

@@ -3,9 +3,10 @@
 // src/ads/lbvh_gpu/module.c:6-41 and src/ads/atrbvh_gpu/module.c:6-41).
 //
 // A context keeps one device-resident build: the committed mesh, the tree,
-// its OBBs and the collapsed copy, in grow-only buffers, plus one build
-// workspace.  COMMIT runs the whole chain on a private stream and waits for
-// it, as the reference's commit returns with its tree built.
+// its OBBs, the collapsed copy and the traversal packing, in grow-only
+// buffers, plus one build workspace.  COMMIT runs the whole chain on a
+// private stream and waits for it, as the reference's commit returns with its
+// tree built; INTERSECTION_QUERY traces on the same stream and waits.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -16,6 +17,7 @@
 #include "obvh_atrbvh.h"
 #include "obvh_build.h"
 #include "obvh_plugin.h"
+#include "obvh_transforms.h"
 #include "runtime.h"
 
 namespace obvh {
@@ -30,11 +32,12 @@ struct Context {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DeviceBuffer verts, faces, nodes, collapsed, parents, counts, costs, obbs, xfs, prims, bounds, ws;
+    DeviceBuffer packed, pairs, soa_l, soa_r, soa_m, err;  // traversal packing, and an error word
     uint32_t ws_faces = 0;
 
     ~Context() {
         for (DeviceBuffer* b : {&verts, &faces, &nodes, &collapsed, &parents, &counts, &costs, &obbs, &xfs, &prims,
-                                &bounds, &ws})
+                                &bounds, &ws, &packed, &pairs, &soa_l, &soa_r, &soa_m, &err})
             b->release();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -60,6 +63,84 @@ kr_error init(Context* c, const kr_descriptor_container* settings) {
         else if (equals(d.key, "intersect_bounds")) s.intersect_bounds = equals(d.value, "y");
         else if (equals(d.key, "use_persistent_kernel")) s.use_persistent_kernel = equals(d.value, "y");
     }
+    return kr_success;
+}
+
+// The traversal packing of the committed tree (lbvh_cuda_blas_prepare_persistent,
+// lbvh.cu:1516-1545): the collapsed tree when there is one, records and, with
+// OBBs, the pairs and the SoA OBVH, into zeroed buffers as the reference's
+// fresh allocations are.
+kr_error pack(Context* c, size_t nn, uint32_t n) {
+    obvh_ads_blas& b = c->blas;
+    b.bvh_packed = nullptr;
+    b.transformations = nullptr;
+    b.soa_left_T = b.soa_right_T = nullptr;
+    b.soa_metadata = nullptr;
+    if (!b.use_persistent_kernel) return kr_success;
+    cudaStream_t s = c->stream;
+    const size_t ni = n > 1 ? n - 1 : 1;
+    OBVH_TRY(c->packed.reserve(nn * sizeof(kr_bvh_node_packed)));
+    OBVH_TRY(c->err.reserve(256));
+    OBVH_TRY_CUDA(cudaMemsetAsync(c->packed.ptr, 0, nn * sizeof(kr_bvh_node_packed), s));
+    OBVH_TRY_CUDA(cudaMemsetAsync(c->err.ptr, 0, 4, s));
+    kr_bvh_transformation_pair* pairs = nullptr;
+    kr_mat43 *lt = nullptr, *rt = nullptr;
+    kr_ivec4* meta = nullptr;
+    if (b.use_obbs) {
+        OBVH_TRY(c->pairs.reserve(ni * sizeof(kr_bvh_transformation_pair)));
+        OBVH_TRY(c->soa_l.reserve(ni * sizeof(kr_mat43)));
+        OBVH_TRY(c->soa_r.reserve(ni * sizeof(kr_mat43)));
+        OBVH_TRY(c->soa_m.reserve(nn * sizeof(kr_ivec4)));
+        OBVH_TRY_CUDA(cudaMemsetAsync(c->pairs.ptr, 0, ni * sizeof(kr_bvh_transformation_pair), s));
+        pairs = static_cast<kr_bvh_transformation_pair*>(c->pairs.ptr);
+        lt = static_cast<kr_mat43*>(c->soa_l.ptr);
+        rt = static_cast<kr_mat43*>(c->soa_r.ptr);
+        meta = static_cast<kr_ivec4*>(c->soa_m.ptr);
+    }
+    const kr_bvh_node* tree = b.collapse ? b.collapsed : b.nodes;
+    kr_u32* d_err = static_cast<kr_u32*>(c->err.ptr);
+    OBVH_TRY(obvh_obvh_pack_async(tree, b.use_obbs ? b.transforms : nullptr,
+                                  static_cast<kr_bvh_node_packed*>(c->packed.ptr), pairs, lt, rt, meta,
+                                  static_cast<kr_u32>(nn), n - 1, d_err, s));
+    kr_u32 err = 0;
+    OBVH_TRY_CUDA(cudaMemcpyAsync(&err, d_err, 4, cudaMemcpyDeviceToHost, s));
+    OBVH_TRY_CUDA(cudaStreamSynchronize(s));
+    if (err) return "obvh_ads COMMIT: the packing met a child index outside the tree";
+    b.bvh_packed = static_cast<kr_bvh_node_packed*>(c->packed.ptr);
+    b.transformations = pairs;
+    b.soa_left_T = lt;
+    b.soa_right_T = rt;
+    b.soa_metadata = meta;
+    return kr_success;
+}
+
+// INTERSECTION_QUERY (lbvh_cuda_query_intersection, lbvh.cu:45-110).
+kr_error query(Context* c, const kr_intersection_query* q) {
+    if (!q) return "obvh_ads INTERSECTION_QUERY: null query";
+    if (q->type != KR_QUERY_TYPE_CUDA && q->type != KR_QUERY_TYPE_CUDA_MANAGED)
+        return "obvh_ads INTERSECTION_QUERY: only CUDA queries (rays and records in device memory)";
+    const obvh_ads_blas& b = c->blas;
+    if (b.commits == 0) return "obvh_ads INTERSECTION_QUERY: nothing committed";
+    if (b.intersect_bounds) return "obvh_ads INTERSECTION_QUERY: the intersect_bounds traversal is not built";
+    if (!b.use_persistent_kernel) {
+        if (!b.use_obbs) return kr_success;  // the reference does nothing here either (lbvh.cu:111-115)
+        return "obvh_ads INTERSECTION_QUERY: the non-persistent OBVH traversal is not built "
+               "(use_persistent_kernel = y selects the SoA OBVH traversal)";
+    }
+    if (!b.use_obbs) return "obvh_ads INTERSECTION_QUERY: the AABB-BVH traversal is not built";
+    if (q->cuda.ray_count > 0xFFFFFFFFull) return "obvh_ads INTERSECTION_QUERY: more than 2^32 - 1 rays";
+    if (q->cuda.ray_count == 0) return kr_success;
+    cudaStream_t s = c->stream;
+    kr_u32* d_err = static_cast<kr_u32*>(c->err.ptr);
+    OBVH_TRY_CUDA(cudaMemsetAsync(d_err, 0, 4, s));
+    OBVH_TRY(obvh_soa_obvh_intersect_async(b.soa_left_T, b.soa_right_T, b.soa_metadata, b.internal_count,
+                                           b.node_count, b.vertices, b.faces, b.primitive_count, b.primitives,
+                                           b.collapse ? b.primitive_count : 0, q->cuda.rays, q->cuda.isects,
+                                           static_cast<kr_u32>(q->cuda.ray_count), d_err, s));
+    kr_u32 err = 0;
+    OBVH_TRY_CUDA(cudaMemcpyAsync(&err, d_err, 4, cudaMemcpyDeviceToHost, s));
+    OBVH_TRY_CUDA(cudaStreamSynchronize(s));
+    if (err) return "obvh_ads INTERSECTION_QUERY: a ray met an index outside the tree or a stack past 64 entries";
     return kr_success;
 }
 
@@ -149,7 +230,7 @@ kr_error build_object(Context* c, const kr_object* object) {
     b.primitive_slots = b.collapse ? slots : 0;
     b.build_ms = ms;
     b.commits += 1;
-    return kr_success;
+    return pack(c, nn, n);
 }
 
 kr_error commit(Context* c, const kr_scene* scene) {
@@ -230,9 +311,15 @@ extern "C" kr_error obvh_ads_action(kr_u32 kind, kr_ads* ads, kr_handle descript
                 ads->context = nullptr;
             }
             return kr_success;
-        case KR_ADS_ACTION_INTERSECTION_QUERY:
+        case KR_ADS_ACTION_INTERSECTION_QUERY: {
+            if (!c) return "obvh_ads INTERSECTION_QUERY: no context (CREATE first)";
+            std::lock_guard<std::mutex> lock(c->mutex);
+            kr_error e = obvh::ads::query(c, static_cast<const kr_intersection_query*>(descriptor));
+            if (e) obvh::set_last_error(e);
+            return e;
+        }
         case KR_ADS_ACTION_OCCLUSION_QUERY:
-            return "obvh_ads: ray queries are not implemented (this library builds the trees only)";
+            return "obvh_ads: occlusion queries are not built";
         default:
             return kr_success;
     }

@@ -78,12 +78,25 @@ class Blas(ctypes.Structure):
                [("aabb", ctypes.c_float * 6), ("build_ms", ctypes.c_float), ("commits", ctypes.c_uint32),
                 ("ci", ctypes.c_float), ("ct", ctypes.c_float)] + \
                [(n, ctypes.c_int32) for n in ("collapse", "use_obbs", "save_construction_information",
-                                              "intersect_bounds", "use_persistent_kernel", "intersect_bounds_level")]
+                                              "intersect_bounds", "use_persistent_kernel", "intersect_bounds_level")] + \
+               [(n, ctypes.c_void_p) for n in ("bvh_packed", "transformations", "soa_left_T", "soa_right_T",
+                                               "soa_metadata")]
 
 
 assert ctypes.sizeof(Scene) == 424 and Scene.objects.offset == 304 and Scene.benchmark_file.offset == 416
 assert ctypes.sizeof(Object) == 80 and ctypes.sizeof(Mesh) == 48
-assert ctypes.sizeof(Blas) == 160
+assert ctypes.sizeof(Blas) == 200
+
+KR_QUERY_TYPE_CUDA = 2
+
+
+class IntersectionQuery(ctypes.Structure):
+    """kr_intersection_query of CUDA kind (include/obvh_types.h)."""
+    _fields_ = [("type", ctypes.c_int32), ("rays", ctypes.c_void_p), ("isects", ctypes.c_void_p),
+                ("ray_count", ctypes.c_uint64)]
+
+
+assert ctypes.sizeof(IntersectionQuery) == 32 and IntersectionQuery.rays.offset == 8
 
 _CALLBACK = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.POINTER(Ads), ctypes.c_void_p, ctypes.c_int)
 
@@ -149,6 +162,13 @@ class Intersector:
 
     def preferred_query_type(self) -> int:
         return int(self.call("PREFERRED_QUERY_TYPE") or 0)
+
+    def intersect(self, d_rays: int, d_isects: int, ray_count: int):
+        """INTERSECTION_QUERY of CUDA kind over device rays and records."""
+        q = IntersectionQuery()
+        q.type = KR_QUERY_TYPE_CUDA
+        q.rays, q.isects, q.ray_count = d_rays, d_isects, ray_count
+        self.check("INTERSECTION_QUERY", ctypes.cast(ctypes.pointer(q), ctypes.c_void_p))
 
     def blas(self) -> Blas:
         p = self.call("GET_BLAS")

@@ -45,7 +45,8 @@ def test_empty_scene_and_queries_are_errors(ads):
     _, a = ads
     with pytest.raises(_native.ObvhError, match="no intersectable primitives"):
         a.commit(plugin.MeshScene([(np.zeros((0, 3), np.float32), np.zeros((0, 4), np.uint32))]))
-    assert a.call("INTERSECTION_QUERY")  # not part of this library: an error string, never a silent success
+    assert a.call("INTERSECTION_QUERY")  # a null query: an error string, never a silent success
+    assert a.call("OCCLUSION_QUERY")  # not built: an error string
     assert a.call("SETTINGS_UPDATE") is None and a.call("CSV_EXPORT") is None
 
 

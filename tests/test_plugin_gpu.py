@@ -70,3 +70,55 @@ def test_recommit_and_flags_off():
     assert np.array_equal(_d2h(b.nodes, ref.NODE, 2 * 9_000 - 1)["left"], r["nodes"]["left"])
     assert same_bits(_d2h(b.costs, np.float32, 2 * 9_000 - 1), r["costs"])
     a.destroy()
+
+
+@pytest.mark.parametrize("kind", ["lbvh_gpu", "atrbvh_gpu"])
+def test_intersection_query_matches_the_oracle(kind):
+    """COMMIT with use_obbs, collapse and use_persistent_kernel packs the tree;
+    INTERSECTION_QUERY then gives the oracle's closest hits (the reference's
+    traversal restated) through the oracle's own build, pack and SoA OBVH."""
+    import torch
+    v, f = workloads.triangle_soup(20_000, seed=31)
+    n = f.shape[0]
+    a = plugin.Intersector(kind)
+    a.init(collapse="y", use_obbs="y", use_persistent_kernel="y", ci="1.2", ct="1.0")
+    a.commit(plugin.MeshScene([(v, f)]))
+    b = a.blas()
+    assert b.bvh_packed and b.soa_left_T and b.soa_metadata
+    rays = workloads.probe_rays(30_000, [0, 0, 0], [1, 1, 1], seed=4)
+    d_rays = torch.from_numpy(rays.view(np.uint8).copy()).cuda()
+    d_isects = torch.zeros(28 * len(rays), dtype=torch.uint8, device="cuda")
+    a.intersect(d_rays.data_ptr(), d_isects.data_ptr(), len(rays))
+    got = d_isects.cpu().numpy().view(ref.ISECT)
+    r = ref.lbvh_build(v, f) if kind == "lbvh_gpu" else ref.atrbvh_build(v, f, 9, 2)
+    _, xfs, _ = ref.obb_tree(r["nodes"], r["parents"], v, f)
+    col, _, prims, _, _ = ref.collapse(r["nodes"], r["parents"], r["counts"], r["costs"])
+    pk, pr = ref.pack(col, xfs)
+    lt, rt, meta = ref.soa_obvh(pk, pr, n - 1)
+    want = ref.soa_obvh_intersect(lt, rt, meta, v, f, prims, rays, threads=8)
+    assert got.tobytes() == want.tobytes()
+    assert (got["primitive"] != 0xFFFFFFFF).sum() > 0
+    a.destroy()
+
+
+def test_query_forms_not_built_are_errors():
+    """The traversal forms the reference has but this library does not build
+    answer with an error; with neither use_obbs nor use_persistent_kernel the
+    query does nothing, as the reference's does."""
+    import torch
+    v, f = workloads.triangle_soup(1000, seed=2)
+    rays = workloads.probe_rays(100, [0, 0, 0], [1, 1, 1], seed=1)
+    d_rays = torch.from_numpy(rays.view(np.uint8).copy()).cuda()
+    d_isects = torch.zeros(28 * len(rays), dtype=torch.uint8, device="cuda")
+    for settings, ok in (({"use_obbs": "y"}, False), ({"use_persistent_kernel": "y"}, False),
+                         ({"use_obbs": "y", "use_persistent_kernel": "y", "intersect_bounds": "y"}, False), ({}, True)):
+        a = plugin.Intersector("lbvh_gpu")
+        a.init(**settings)
+        a.commit(plugin.MeshScene([(v, f)]))
+        if ok:
+            a.intersect(d_rays.data_ptr(), d_isects.data_ptr(), len(rays))
+            assert int(d_isects.sum().item()) == 0
+        else:
+            with pytest.raises(plugin._native.ObvhError, match="not built"):
+                a.intersect(d_rays.data_ptr(), d_isects.data_ptr(), len(rays))
+        a.destroy()
