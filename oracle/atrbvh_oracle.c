@@ -3,13 +3,16 @@
  * reference's ATRBVH builder (src/ads/atrbvh_gpu), used by tests/ to check the
  * GPU path.  The product never links or calls it.
  *
- * Parity status: the reference's ATRBVH kernels cannot be run as a checker
- * (their __syncthreads() sit inside warp-divergent loops, see
+ * Parity status: the seed tree (63-bit codes, stable sort, Karras tree) is
+ * pinned against the reference's own LBVH.cu / CubWrapper.cu kernels run on
+ * the GPU (oracle/ref_lbvh63_gpu_harness.cu, tests/test_ref_gpu_pin.py).  The
+ * treelet optimisation's kernels cannot be run as a checker (their
+ * __syncthreads() sit inside warp-divergent loops, see
  * AgglomerativeTreelet.cu:451-510, and the reference has no tests or golden
- * trees), so this restatement is pinned only piecewise: the 63-bit Morton
- * expansion, the surface-area formulas, the lower-triangular index maps and the
- * agglomerative schedule against the reference's own host-callable code
- * (oracle/ref_atrbvh_harness.cpp).  The whole-tree result is "parity unpinned".
+ * trees), so that part is pinned only piecewise: the surface-area formulas,
+ * the lower-triangular index maps and the agglomerative schedule against the
+ * reference's own host-callable code (oracle/ref_atrbvh_harness.cpp).  The
+ * optimised tree as a whole is "parity unpinned".
  *
  * What it follows, formula for formula:
  *   scene box and Morton-63 codes   atrbvh.cu:258-300, LBVH.cu:10-36,72-93,
