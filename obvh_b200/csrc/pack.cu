@@ -64,14 +64,25 @@ pack_kernel(const kr_bvh_node* __restrict__ nodes, const kr_mat4* __restrict__ x
     uint32_t* st = stage + (threadIdx.x >> 2) * kStage;
     float* cols = reinterpret_cast<float*>(st + 16);
     const uint32_t warps = gridDim.x * (kThreads / 32);
-    for (uint32_t base = (blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)) * 8; base < node_count;
-         base += warps * 8) {
+    // the node words of the next iteration are loaded while this one's
+    // children and transforms are on their way
+    auto node_words = [&](uint32_t b, uint32_t& wa, uint32_t& wb, uint32_t& w8) {
+        const uint32_t i = b + (lane >> 2);
+        const bool ok = i < node_count;
+        const uint32_t* rec = reinterpret_cast<const uint32_t*>(nodes + (ok ? i : 0));
+        wa = ok ? __ldg(rec + q) : 0u;
+        wb = ok ? __ldg(rec + q + 4) : 0u;
+        w8 = ok && q == 0 ? __ldg(rec + 8) : 0u;
+    };
+    uint32_t base = (blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)) * 8;
+    uint32_t na = 0, nb = 0, n8 = 0;
+    if (base < node_count) node_words(base, na, nb, n8);
+    for (; base < node_count; base += warps * 8) {
         const uint32_t i = base + (lane >> 2);
         const bool valid = i < node_count;
-        // the node: lane q holds words q and q + 4, word 8 goes to the whole quad
-        const uint32_t* rec = reinterpret_cast<const uint32_t*>(nodes + (valid ? i : 0));
-        const uint32_t wa = valid ? __ldg(rec + q) : 0u, wb = valid ? __ldg(rec + q + 4) : 0u;
-        const uint32_t w8 = __shfl_sync(0xffffffffu, valid && q == 0 ? __ldg(rec + 8) : 0u, lane & ~3u);
+        const uint32_t wa = na, wb = nb;
+        const uint32_t w8 = __shfl_sync(0xffffffffu, n8, lane & ~3u);
+        if (base + warps * 8 < node_count) node_words(base + warps * 8, na, nb, n8);
         const uint32_t left = __shfl_sync(0xffffffffu, wb, (lane & ~3u) + 2);   // word 6
         const uint32_t right = __shfl_sync(0xffffffffu, wb, (lane & ~3u) + 3);  // word 7
         const uint32_t np = w8 & 0xFFFFu, axis = (w8 >> 16) & 0xFFu;
