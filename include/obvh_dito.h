@@ -81,7 +81,12 @@ OBVH_EXPORT kr_error obvh_dito_fit_pass_async(const kr_vec3* d_points, kr_size c
  * addresses (once per device); make that first call before any stream
  * capture.  All calls on a device share the arrays: calls whose GPU work
  * overlapped would race, so the library serialises calls with a lock and
- * never returns with work in flight.
+ * never returns with work in flight.  `stream` must belong to the current
+ * device (another device's stream is rejected with an error).  The device
+ * addresses looked up by the first call are kept for the life of the
+ * process: they do not survive a cudaDeviceReset of that device.  Errors
+ * name their cause: a device wait that timed out, or points with no finite
+ * projection (non-finite input).
  */
 OBVH_EXPORT kr_error obvh_points_obb_noalloc(const kr_vec3* points, kr_size count, kr_u32 flags,
                                              kr_obb3* obb, void* stream);

@@ -416,6 +416,18 @@ HostContext& host_context() {
     return *c;
 }
 
+kr_error describe_device_error(uint32_t word, bool noalloc) {
+    if (word == 0) return kr_success;
+    // a timeout is reported first: it can leave any other word half-written
+    if (word & kErrWaitTimeout)
+        return noalloc ? "obvh_points_obb_noalloc: a device wait timed out"
+                       : "obvh_points_obb: a device wait timed out";
+    if (word & kErrBadInput)
+        return noalloc ? "obvh_points_obb_noalloc: invalid input (no finite projection: non-finite points)"
+                       : "obvh_points_obb: invalid input (no finite projection: non-finite points)";
+    return noalloc ? "obvh_points_obb_noalloc: device error" : "obvh_points_obb: device error";
+}
+
 kr_error fit_host(const kr_vec3* points, uint64_t count, uint32_t flags, kr_obb3* obb, float* elapsed) {
     if (!obb || (count > 0 && !points)) return "obvh_points_obb: null pointer argument";
     HostContext& hc = host_context();
@@ -433,9 +445,10 @@ kr_error fit_host(const kr_vec3* points, uint64_t count, uint32_t flags, kr_obb3
     OBVH_TRY_CUDA(cudaStreamSynchronize(hc.stream));
     const Ctl* ctl = static_cast<const Ctl*>(hc.result.ptr);
     if (ctl->error) {
+        const kr_error e = describe_device_error(ctl->error, false);
         cudaMemsetAsync(ws, 0, sizeof(Ctl), hc.stream);
         cudaStreamSynchronize(hc.stream);
-        return "obvh_points_obb: device wait timed out";
+        return e;
     }
     std::memcpy(obb, static_cast<const char*>(hc.result.ptr) + kOffObb, sizeof(kr_obb3));
     if (elapsed) {

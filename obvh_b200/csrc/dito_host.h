@@ -17,5 +17,10 @@ namespace dito {
 kr_error enqueue(const kr_vec3* d_points, uint64_t count, uint32_t flags, kr_obb3* d_obb, void* ws,
                  cudaStream_t stream, int passes = 3);
 
+// The kr_error for a fit whose control block ended with device error word
+// `word` (kErr* bits), or kr_success for 0.  `noalloc` picks the message
+// prefix of obvh_points_obb_noalloc instead of obvh_points_obb.
+kr_error describe_device_error(uint32_t word, bool noalloc);
+
 }  // namespace dito
 }  // namespace obvh

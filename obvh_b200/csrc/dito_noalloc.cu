@@ -49,6 +49,8 @@ DeviceSlot g_slots[kMaxDevices];
 
 // Once per device, with that device current: the device addresses of the
 // arrays.  This is the only set-up; it runs inside the first call on a device.
+// The addresses are cached for the life of the process, so they do not
+// survive a cudaDeviceReset of that device.
 kr_error setup(DeviceSlot& slot) {
     if (slot.ready) return kr_success;
     void* ws = nullptr;
@@ -68,6 +70,11 @@ kr_error fit_noalloc(const kr_vec3* points, kr_size count, kr_u32 flags, kr_obb3
     int dev = 0;
     OBVH_TRY_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return "obvh_points_obb_noalloc: device index out of range";
+    // The arrays' addresses belong to the current device: a stream of another
+    // device would be handed addresses it cannot use.
+    int stream_dev = dev;
+    OBVH_TRY_CUDA(cudaStreamGetDevice(stream, &stream_dev));
+    if (stream_dev != dev) return "obvh_points_obb_noalloc: the stream belongs to another device than the current one";
 
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     DeviceSlot& slot = g_slots[dev];
@@ -89,7 +96,8 @@ kr_error fit_noalloc(const kr_vec3* points, kr_size count, kr_u32 flags, kr_obb3
     OBVH_TRY_CUDA(cudaMemcpyAsync(&result, slot.workspace, sizeof(Ctl) + sizeof(kr_obb3), cudaMemcpyDeviceToHost,
                                   stream));
     OBVH_TRY_CUDA(cudaStreamSynchronize(stream));
-    if (result.ctl.error) return "obvh_points_obb_noalloc: device wait timed out or invalid input";
+    // the next call clears the control block before it launches anything
+    OBVH_TRY(describe_device_error(result.ctl.error, true));
     std::memcpy(obb, &result.box, sizeof(kr_obb3));
     return kr_success;
 }

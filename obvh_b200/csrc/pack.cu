@@ -67,22 +67,26 @@ pack_kernel(const kr_bvh_node* __restrict__ nodes, const kr_mat4* __restrict__ x
     // the node words of the next iteration are loaded while this one's
     // children and transforms are on their way
     auto node_words = [&](uint32_t b, uint32_t& wa, uint32_t& wb, uint32_t& w8) {
-        const uint32_t i = b + (lane >> 2);
+        const uint64_t i = static_cast<uint64_t>(b) + (lane >> 2);
         const bool ok = i < node_count;
         const uint32_t* rec = reinterpret_cast<const uint32_t*>(nodes + (ok ? i : 0));
         wa = ok ? __ldg(rec + q) : 0u;
         wb = ok ? __ldg(rec + q + 4) : 0u;
         w8 = ok && q == 0 ? __ldg(rec + 8) : 0u;
     };
-    uint32_t base = (blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)) * 8;
+    // the warp's first node and the stride in 64 bits, so that neither the
+    // loop step nor the look-ahead can wrap below node_count
+    const uint64_t stride = static_cast<uint64_t>(warps) * 8u;
+    uint64_t base = (static_cast<uint64_t>(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5)) * 8u;
     uint32_t na = 0, nb = 0, n8 = 0;
-    if (base < node_count) node_words(base, na, nb, n8);
-    for (; base < node_count; base += warps * 8) {
-        const uint32_t i = base + (lane >> 2);
-        const bool valid = i < node_count;
+    if (base < node_count) node_words(static_cast<uint32_t>(base), na, nb, n8);
+    for (; base < node_count; base += stride) {
+        const uint64_t i64 = base + (lane >> 2);
+        const bool valid = i64 < node_count;
+        const uint32_t i = static_cast<uint32_t>(valid ? i64 : 0);
         const uint32_t wa = na, wb = nb;
         const uint32_t w8 = __shfl_sync(0xffffffffu, n8, lane & ~3u);
-        if (base + warps * 8 < node_count) node_words(base + warps * 8, na, nb, n8);
+        if (base + stride < node_count) node_words(static_cast<uint32_t>(base + stride), na, nb, n8);
         const uint32_t left = __shfl_sync(0xffffffffu, wb, (lane & ~3u) + 2);   // word 6
         const uint32_t right = __shfl_sync(0xffffffffu, wb, (lane & ~3u) + 3);  // word 7
         const uint32_t np = w8 & 0xFFFFu, axis = (w8 >> 16) & 0xFFu;

@@ -28,10 +28,14 @@ _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 
 
-def build(force: bool = False) -> None:
-    """Compile liboracle.so (and _ref when the reference tree exists)."""
-    if force or not os.path.exists(_LIB) or _stale():
-        subprocess.run(["make", "-s", "-C", HERE], check=True)
+def build(force: bool = False, ref_tree: str | None = None) -> None:
+    """Compile liboracle.so, and _ref from the reference source tree
+    ``ref_tree`` (or the ``REF`` environment variable) when one is given."""
+    cmd = ["make", "-s", "-C", HERE]
+    if ref_tree:
+        cmd.append(f"REF={ref_tree}")
+    if force or ref_tree or not os.path.exists(_LIB) or _stale():
+        subprocess.run(cmd, check=True)
 
 
 def _stale() -> bool:

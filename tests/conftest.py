@@ -17,6 +17,22 @@ def pytest_configure(config):
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
+def lattice_mesh(k: int = 12):
+    """Two equal small triangles on every point of a k^3 lattice, as
+    (vertices, faces): ties in the sort, the Karras split, the treelet leaf to
+    expand and the pair to merge."""
+    g = np.stack(np.meshgrid(np.arange(k), np.arange(k), np.arange(k), indexing="ij"), -1).reshape(-1, 3)
+    c = np.repeat(g, 2, axis=0).astype(np.float32) * 0.5
+    tri = np.array([[0, 0, 0], [0.2, 0, 0], [0, 0.2, 0]], np.float32)
+    v = (c[:, None, :] + tri[None]).reshape(-1, 3)
+    n = c.shape[0]
+    f = np.zeros((n, 4), np.uint32)
+    f[:, 0] = np.arange(0, 3 * n, 3)
+    f[:, 1] = f[:, 0] + 1
+    f[:, 2] = f[:, 0] + 2
+    return v, f
+
+
 def deep_or_tied_mesh(layout: str):
     """Trees far from balanced, as (vertices, faces): centroids on a geometric
     sequence along the diagonal ("geometric": a chain of key bits, so leaf
@@ -85,3 +101,35 @@ def contained(points, obb, rel: float = 1e-6) -> bool:
     p = np.asarray(points, np.float64).reshape(-1, 3)
     tol = rel * (1.0 + np.abs(p).max(axis=1))
     return bool(np.all(obb_overshoot(p, obb) <= tol))
+
+
+def uncontained_leaves(v, f4, leaf_prims, parents, obbs, rel: float = 1e-6) -> int:
+    """FP64 containment of every leaf's triangle in its leaf box and in every
+    ancestor's box, for all leaves at once: the number of (leaf, box) pairs
+    in which some vertex lies outside by more than rel * (1 + |p|).
+
+    `leaf_prims[j]` is leaf j's triangle (node n-1+j); the walk moves all
+    leaves one level up per step, so it takes depth steps of array work."""
+    n = (len(parents) + 1) // 2
+    tri = np.asarray(v, np.float64)[np.asarray(f4)[np.asarray(leaf_prims, np.int64), :3]]  # (n, 3, 3)
+    tol = rel * (1.0 + np.abs(tri).max(axis=2))                                              # (n, 3)
+    node = np.arange(n - 1, 2 * n - 1, dtype=np.int64)
+    active = np.arange(n, dtype=np.int64)
+    obbs = np.asarray(obbs, np.float64)
+    bad = 0
+    for _ in range(2 * n):
+        if active.size == 0:
+            break
+        o = obbs[node[active]]
+        mid, axes, ext = o[:, 0:3], o[:, 3:12].reshape(-1, 3, 3), o[:, 12:15]
+        la = np.linalg.norm(axes, axis=2)                                  # (k, 3)
+        c = np.einsum("kpj,kaj->kpa", tri[active] - mid[:, None, :], axes) / (la * la)[:, None, :]
+        over = ((np.abs(c) - ext[:, None, :]) * la[:, None, :]).max(axis=2)  # (k, 3 vertices)
+        bad += int(np.count_nonzero((~(over <= tol[active])).any(axis=1)))
+        up = np.asarray(parents, np.uint32)[node[active]]
+        keep = up != 0xFFFFFFFF
+        active = active[keep]
+        node[active] = up[keep].astype(np.int64)
+    else:
+        raise AssertionError("parent walk longer than the tree")
+    return bad

@@ -4,7 +4,7 @@ kr_cuda_bvh_obb_tree and kr_cuda_bvh_collapse."""
 import numpy as np
 import pytest
 
-from conftest import contained, same_bits
+from conftest import contained, same_bits, uncontained_leaves
 from oracle import bvh as ref
 from obvh_b200 import bvh, workloads
 
@@ -38,8 +38,10 @@ def _check_obbs(mesh, tree, v, f, sample_leaves=None):
     # every vertex lies in its leaf's box and in every ancestor's box
     n = (len(parents) + 1) // 2
     f4 = bvh.as_faces4(f)
-    leaves = range(n) if sample_leaves is None else np.random.default_rng(0).choice(n, sample_leaves, replace=False)
-    for j in leaves:
+    if sample_leaves is None:
+        assert uncontained_leaves(v, f4, nodes["left"][n - 1:], parents, got_o) == 0
+        return got_o
+    for j in np.random.default_rng(0).choice(n, sample_leaves, replace=False):
         tri = v[f4[nodes["left"][n - 1 + j], :3]]
         node = n - 1 + j
         while node != 0xFFFFFFFF:
@@ -52,20 +54,21 @@ def _check_obbs(mesh, tree, v, f, sample_leaves=None):
 def test_obb_tree_soup(builder, n):
     v, f = workloads.triangle_soup(n, seed=100 + n)
     mesh, tree = _lbvh(builder, v, f)
-    _check_obbs(mesh, tree, v, f, sample_leaves=None if n <= 5000 else 2000)
+    _check_obbs(mesh, tree, v, f)
 
 
 def test_obb_tree_full_size(builder):
-    """The 2M-triangle LBVH + OBB-tree workload."""
+    """The 2M-triangle LBVH + OBB-tree workload: every vertex of every leaf
+    inside its leaf's box and every ancestor's box (FP64)."""
     v, f = workloads.triangle_soup(2_000_000, seed=1)
     mesh, tree = _lbvh(builder, v, f)
-    _check_obbs(mesh, tree, v, f, sample_leaves=500)
+    _check_obbs(mesh, tree, v, f)
 
 
 def test_obb_tree_mesh(builder):
     v, f = workloads.torus_knot_mesh(segments=256, around=112)
     mesh, tree = _lbvh(builder, v, f)
-    _check_obbs(mesh, tree, v, f, sample_leaves=2000)
+    _check_obbs(mesh, tree, v, f)
 
 
 def _random_tree(n, rng):
