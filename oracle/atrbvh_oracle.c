@@ -6,13 +6,15 @@
  * Parity status: the seed tree (63-bit codes, stable sort, Karras tree) is
  * pinned against the reference's own LBVH.cu / CubWrapper.cu kernels run on
  * the GPU (oracle/ref_lbvh63_gpu_harness.cu, tests/test_ref_gpu_pin.py).  The
- * treelet optimisation's kernels cannot be run as a checker (their
- * __syncthreads() sit inside warp-divergent loops, see
- * AgglomerativeTreelet.cu:451-510, and the reference has no tests or golden
- * trees), so that part is pinned only piecewise: the surface-area formulas,
- * the lower-triangular index maps and the agglomerative schedule against the
- * reference's own host-callable code (oracle/ref_atrbvh_harness.cpp).  The
- * optimised tree as a whole is "parity unpinned".
+ * treelet optimisation is pinned against the reference's own treelet kernel
+ * (AgglomerativeTreelet.cu, Treelet.cuh) run as host code by a lockstep warp
+ * emulation (oracle/ref_treelet_emu.cpp, tests/test_ref_treelet_pin.py): the
+ * optimised SoA trees are identical bit for bit.  The kernel itself cannot be
+ * run on the GPU as a checker: as launched by the reference, its
+ * __syncthreads() sit in loops whose trip counts differ between the warps of
+ * a block (AgglomerativeTreelet.cu:451-510).  The surface-area formulas, the
+ * lower-triangular index maps and the agglomerative schedule are also checked
+ * against the reference's own host-callable code (oracle/ref_atrbvh_harness.cpp).
  *
  * What it follows, formula for formula:
  *   scene box and Morton-63 codes   atrbvh.cu:258-300, LBVH.cu:10-36,72-93,
@@ -378,10 +380,46 @@ static int optimize_pass(opt_ctx* c, int32_t gamma, float ct, int32_t* tris, int
     return visited == internal ? 0 : -1;
 }
 
-int oracle_atrbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, int treelet_size, int iterations,
-                        float ci, float ct, obvh_oracle_node* nodes, uint32_t* parents, uint32_t* counts,
-                        float* costs, uint64_t* codes_sorted, float* sah_out) {
-    if (n < 2 || treelet_size < 3 || treelet_size > 32) return -1;
+/* ------------------------------------------------------ SoA tree stages */
+
+/* The reference's SoABVHTree fields (SoABVHTree.h:19-44) as flat arrays:
+ * int32 parent/left/right/data per node, float4 box min/max (w unused),
+ * float area. */
+static void soa_load(tnode* t, uint32_t nn, const int32_t* parent, const int32_t* left, const int32_t* right,
+                     const int32_t* data, const float* lo4, const float* hi4, const float* area) {
+    for (uint32_t i = 0; i < nn; i++) {
+        t[i].parent = parent[i];
+        t[i].left = left[i];
+        t[i].right = right[i];
+        t[i].data = data[i];
+        for (int k = 0; k < 3; k++) {
+            t[i].lo[k] = lo4[4 * (size_t)i + k];
+            t[i].hi[k] = hi4[4 * (size_t)i + k];
+        }
+        t[i].area = area[i];
+    }
+}
+
+static void soa_store(const tnode* t, uint32_t nn, int32_t* parent, int32_t* left, int32_t* right, int32_t* data,
+                      float* lo4, float* hi4, float* area) {
+    for (uint32_t i = 0; i < nn; i++) {
+        parent[i] = t[i].parent;
+        left[i] = t[i].left;
+        right[i] = t[i].right;
+        data[i] = t[i].data;
+        for (int k = 0; k < 3; k++) {
+            lo4[4 * (size_t)i + k] = t[i].lo[k];
+            hi4[4 * (size_t)i + k] = t[i].hi[k];
+        }
+        lo4[4 * (size_t)i + 3] = 0.0f;
+        hi4[4 * (size_t)i + 3] = 0.0f;
+        area[i] = t[i].area;
+    }
+}
+
+/* Seed tree of the ATRBVH build: scene box, Morton-63 codes, stable sort,
+ * Karras tree, leaf and node boxes (atrbvh.cu:258-300, LBVH.cu). */
+static int seed_tree(const float* verts, const uint32_t* faces4, uint32_t n, tnode* t, uint64_t* codes_sorted) {
     const uint32_t internal = n - 1, nn = 2 * n - 1;
     /* scene box: union of the triangle boxes (atrbvh.cu:282-298) */
     float scene[6] = { FLT_MAX_ORACLE, FLT_MAX_ORACLE, FLT_MAX_ORACLE,
@@ -405,11 +443,11 @@ int oracle_atrbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, 
     for (uint32_t i = 0; i < n; i++) sorted[i] = keys[order[i]];
     if (codes_sorted) memcpy(codes_sorted, sorted, sizeof(uint64_t) * n);
 
-    tnode* t = calloc(nn, sizeof(tnode));
     int32_t *L = malloc(sizeof(int32_t) * nn), *R = malloc(sizeof(int32_t) * nn), *P = malloc(sizeof(int32_t) * nn),
             *D = malloc(sizeof(int32_t) * nn);
     oracle_karras63(sorted, order, n, L, R, P, D);
     for (uint32_t i = 0; i < nn; i++) {
+        memset(&t[i], 0, sizeof(t[i]));
         t[i].left = i < internal ? L[i] : -1;
         t[i].right = i < internal ? R[i] : -1;
         t[i].parent = P[i];
@@ -427,40 +465,63 @@ int oracle_atrbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, 
         lf->area = box_area(lf->lo, lf->hi);
     }
     int32_t* stack = malloc(sizeof(int32_t) * (2 * (size_t)n + 2));
-    int32_t* tris = malloc(sizeof(int32_t) * nn);
     int rc = 0;
-    {
-        int64_t sp = 0, seen = 0;
-        stack[sp++] = 0;
-        while (sp > 0 && rc == 0) {
-            int32_t v = stack[--sp];
-            if (v < 0) {
-                v = ~v;
-                for (int k = 0; k < 3; k++) {
-                    t[v].lo[k] = dmin(t[t[v].left].lo[k], t[t[v].right].lo[k]);
-                    t[v].hi[k] = dmax(t[t[v].left].hi[k], t[t[v].right].hi[k]);
-                }
-                t[v].area = box_area(t[v].lo, t[v].hi);
-                seen++;
-                continue;
+    int64_t sp = 0, seen = 0;
+    stack[sp++] = 0;
+    while (sp > 0 && rc == 0) {
+        int32_t v = stack[--sp];
+        if (v < 0) {
+            v = ~v;
+            for (int k = 0; k < 3; k++) {
+                t[v].lo[k] = dmin(t[t[v].left].lo[k], t[t[v].right].lo[k]);
+                t[v].hi[k] = dmax(t[t[v].left].hi[k], t[t[v].right].hi[k]);
             }
-            if (seen + sp > 2 * (int64_t)n) rc = -1;
-            stack[sp++] = ~v;
-            if (t[v].right < (int32_t)internal) stack[sp++] = t[v].right;
-            if (t[v].left < (int32_t)internal) stack[sp++] = t[v].left;
+            t[v].area = box_area(t[v].lo, t[v].hi);
+            seen++;
+            continue;
         }
+        if (seen + sp > 2 * (int64_t)n) rc = -1;
+        stack[sp++] = ~v;
+        if (t[v].right < (int32_t)internal) stack[sp++] = t[v].right;
+        if (t[v].left < (int32_t)internal) stack[sp++] = t[v].left;
     }
+    free(tri);
+    free(keys);
+    free(sorted);
+    free(order);
+    free(L);
+    free(R);
+    free(P);
+    free(D);
+    free(stack);
+    return rc;
+}
 
+/* The treelet optimisation loop (AgglomerativeTreeletOptimizer.cpp:73-98):
+ * gamma = treelet size, doubled after each iteration. */
+static int optimize_tree(tnode* t, uint32_t n, int treelet_size, int iterations, float ci, float ct, float* sah_out) {
+    const uint32_t nn = 2 * n - 1;
+    int32_t* stack = malloc(sizeof(int32_t) * (2 * (size_t)n + 2));
+    int32_t* tris = malloc(sizeof(int32_t) * nn);
     float* nodes_sah = malloc(sizeof(float) * nn);
     opt_ctx c = { t, (int32_t)n, treelet_size, ci, nodes_sah };
     int32_t gamma = treelet_size;
+    int rc = 0;
     for (int it = 0; it < iterations && rc == 0; it++) {
         rc = optimize_pass(&c, gamma, ct, tris, stack);
         if (sah_out) sah_out[it] = nodes_sah[0];
         gamma *= 2;
     }
+    free(stack);
+    free(tris);
+    free(nodes_sah);
+    return rc;
+}
 
-    /* copyTree_kernel + calculate_aabbs_kernel (atrbvh.cu:95-183) */
+/* copyTree_kernel + calculate_aabbs_kernel (atrbvh.cu:95-183) */
+static int emit_tree(const tnode* t, uint32_t n, obvh_oracle_node* nodes, uint32_t* parents, uint32_t* counts,
+                     float* costs) {
+    const uint32_t nn = 2 * n - 1;
     for (uint32_t i = 0; i < nn; i++) {
         obvh_oracle_node* nd = &nodes[i];
         memset(nd, 0, sizeof(*nd));
@@ -477,18 +538,53 @@ int oracle_atrbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, 
             nd->left = (uint32_t)t[i].data;
         }
     }
-    if (rc == 0) rc = oracle_aabb_refit(nodes, n, counts, costs);
-    free(tri);
-    free(keys);
-    free(sorted);
-    free(order);
+    return oracle_aabb_refit(nodes, n, counts, costs);
+}
+
+int oracle_atrbvh_seed(const float* verts, const uint32_t* faces4, uint32_t n, int32_t* parent, int32_t* left,
+                       int32_t* right, int32_t* data, float* lo4, float* hi4, float* area, uint64_t* codes_sorted) {
+    if (n < 2) return -1;
+    const uint32_t nn = 2 * n - 1;
+    tnode* t = calloc(nn, sizeof(tnode));
+    const int rc = seed_tree(verts, faces4, n, t, codes_sorted);
+    soa_store(t, nn, parent, left, right, data, lo4, hi4, area);
     free(t);
-    free(L);
-    free(R);
-    free(P);
-    free(D);
-    free(stack);
-    free(tris);
-    free(nodes_sah);
+    return rc;
+}
+
+int oracle_atrbvh_optimize(uint32_t n, int treelet_size, int iterations, float ci, float ct, int32_t* parent,
+                           int32_t* left, int32_t* right, int32_t* data, float* lo4, float* hi4, float* area,
+                           float* sah_out) {
+    if (n < 2 || treelet_size < 3 || treelet_size > 32) return -1;
+    const uint32_t nn = 2 * n - 1;
+    tnode* t = calloc(nn, sizeof(tnode));
+    soa_load(t, nn, parent, left, right, data, lo4, hi4, area);
+    const int rc = optimize_tree(t, n, treelet_size, iterations, ci, ct, sah_out);
+    soa_store(t, nn, parent, left, right, data, lo4, hi4, area);
+    free(t);
+    return rc;
+}
+
+int oracle_atrbvh_emit(uint32_t n, const int32_t* parent, const int32_t* left, const int32_t* right,
+                       const int32_t* data, const float* lo4, const float* hi4, const float* area,
+                       obvh_oracle_node* nodes, uint32_t* parents, uint32_t* counts, float* costs) {
+    if (n < 2) return -1;
+    const uint32_t nn = 2 * n - 1;
+    tnode* t = calloc(nn, sizeof(tnode));
+    soa_load(t, nn, parent, left, right, data, lo4, hi4, area);
+    const int rc = emit_tree(t, n, nodes, parents, counts, costs);
+    free(t);
+    return rc;
+}
+
+int oracle_atrbvh_build(const float* verts, const uint32_t* faces4, uint32_t n, int treelet_size, int iterations,
+                        float ci, float ct, obvh_oracle_node* nodes, uint32_t* parents, uint32_t* counts,
+                        float* costs, uint64_t* codes_sorted, float* sah_out) {
+    if (n < 2 || treelet_size < 3 || treelet_size > 32) return -1;
+    tnode* t = calloc(2 * (size_t)n - 1, sizeof(tnode));
+    int rc = seed_tree(verts, faces4, n, t, codes_sorted);
+    if (rc == 0) rc = optimize_tree(t, n, treelet_size, iterations, ci, ct, sah_out);
+    if (rc == 0) rc = emit_tree(t, n, nodes, parents, counts, costs);
+    free(t);
     return rc;
 }

@@ -62,6 +62,11 @@ def _bind():
         "oracle_karras63": (None, [_u64, _u32, c.c_uint32, _i32, _i32, _i32, _i32]),
         "oracle_atrbvh_build": (c.c_int, [_f32, _u32, c.c_uint32, c.c_int, c.c_int, c.c_float, c.c_float, _node,
                                           _u32, _u32, _f32, _u64, _f32]),
+        "oracle_atrbvh_seed": (c.c_int, [_f32, _u32, c.c_uint32, _i32, _i32, _i32, _i32, _f32, _f32, _f32, _u64]),
+        "oracle_atrbvh_optimize": (c.c_int, [c.c_uint32, c.c_int, c.c_int, c.c_float, c.c_float, _i32, _i32, _i32,
+                                             _i32, _f32, _f32, _f32, _f32]),
+        "oracle_atrbvh_emit": (c.c_int, [c.c_uint32, _i32, _i32, _i32, _i32, _f32, _f32, _f32, _node, _u32, _u32,
+                                         _f32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(l, name)
@@ -239,6 +244,87 @@ def atrbvh_build(verts, faces, treelet_size=9, iterations=2, ci=1.2, ct=1.0):
     return out
 
 
+SOA_FIELDS = ("parent", "left", "right", "data", "lo", "hi", "area")
+
+
+def atrbvh_seed(verts, faces):
+    """The ATRBVH seed tree (LBVH-63 with node boxes) in the reference's SoA
+    layout (SoABVHTree.h:19-44): dict of int32 parent/left/right/data,
+    float32 (nodes, 4) lo/hi boxes and float32 area, plus the sorted codes."""
+    l = _bind()
+    v, f, n = _mesh(verts, faces)
+    nn = 2 * n - 1
+    t = {k: np.zeros(nn, np.int32) for k in ("parent", "left", "right", "data")}
+    t.update(lo=np.zeros((nn, 4), np.float32), hi=np.zeros((nn, 4), np.float32), area=np.zeros(nn, np.float32))
+    codes = np.zeros(n, np.uint64)
+    if l.oracle_atrbvh_seed(v, f, n, t["parent"], t["left"], t["right"], t["data"], t["lo"], t["hi"], t["area"],
+                            codes) != 0:
+        raise ValueError("oracle_atrbvh_seed failed")
+    t["codes"] = codes
+    return t
+
+
+def soa_copy(tree):
+    return {k: np.array(tree[k], copy=True) for k in SOA_FIELDS}
+
+
+def atrbvh_optimize(tree, treelet_size=7, iterations=2, ci=1.2, ct=1.0):
+    """The restatement's treelet optimisation of an SoA tree (a copy is
+    returned) and the root SAH after each iteration."""
+    l = _bind()
+    t = soa_copy(tree)
+    n = (len(t["parent"]) + 1) // 2
+    sah = np.zeros(max(iterations, 1), np.float32)
+    if l.oracle_atrbvh_optimize(n, treelet_size, iterations, ci, ct, t["parent"], t["left"], t["right"], t["data"],
+                                t["lo"], t["hi"], t["area"], sah) != 0:
+        raise ValueError("oracle_atrbvh_optimize failed")
+    return t, sah
+
+
+def atrbvh_emit(tree):
+    """copyTree + refit of an SoA tree: dict of kr_bvh_node records, parents,
+    counts, costs (atrbvh.cu:95-183)."""
+    l = _bind()
+    n = (len(tree["parent"]) + 1) // 2
+    nn = 2 * n - 1
+    out = {"nodes": np.zeros(nn, NODE), "parents": np.zeros(nn, np.uint32), "counts": np.zeros(nn, np.uint32),
+           "costs": np.zeros(nn, np.float32)}
+    t = soa_copy(tree)
+    if l.oracle_atrbvh_emit(n, t["parent"], t["left"], t["right"], t["data"], t["lo"], t["hi"], t["area"],
+                            out["nodes"], out["parents"], out["counts"], out["costs"]) != 0:
+        raise ValueError("oracle_atrbvh_emit failed")
+    return out
+
+
+_ref_treelet = None
+
+
+def ref_treelet_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_treelet_emu.so"))
+
+
+def ref_treelet_optimize(tree, treelet_size=7, iterations=2, ci=1.2, ct=1.0):
+    """The reference's own treelet kernel (AgglomerativeTreelet.cu), run as
+    host code by the lockstep warp emulation in ref_treelet_emu.cpp, on a copy
+    of an SoA tree; returns the optimised copy."""
+    global _ref_treelet
+    if _ref_treelet is None:
+        r = ctypes.CDLL(os.path.join(HERE, "_ref", "libref_treelet_emu.so"))
+        r.ref_treelet_optimize.restype = ctypes.c_int
+        r.ref_treelet_optimize.argtypes = [ctypes.c_uint, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                           ctypes.c_float, _i32, _i32, _i32, _i32, _f32, _f32, _f32,
+                                           ctypes.POINTER(ctypes.c_char_p)]
+        _ref_treelet = r
+    t = soa_copy(tree)
+    n = (len(t["parent"]) + 1) // 2
+    err = ctypes.c_char_p()
+    rc = _ref_treelet.ref_treelet_optimize(n, treelet_size, iterations, ci, ct, t["parent"], t["left"], t["right"],
+                                           t["data"], t["lo"], t["hi"], t["area"], ctypes.byref(err))
+    if rc != 0:
+        raise ValueError((err.value or b"ref_treelet_optimize failed").decode())
+    return t
+
+
 def ref_atrbvh():
     """The reference's host-callable ATRBVH helpers (oracle/_ref/libref_atrbvh.so), or None."""
     path = os.path.join(HERE, "_ref", "libref_atrbvh.so")
@@ -290,6 +376,11 @@ def ref_gpu(variant: str = "nofma"):
         l.refgpu_pack.argtypes = [_node, c.c_void_p, c.c_uint32, c.c_void_p, c.c_void_p, _f32, _f32, _i32]
         l.refgpu_collapse.restype = c.c_int
         l.refgpu_collapse.argtypes = [_node, _u32, _u32, _f32, c.c_float, c.c_float, c.c_uint32, _node, _u32]
+        l.refgpu_lbvh_ms.restype = c.c_int
+        l.refgpu_lbvh_ms.argtypes = [_f32, c.c_uint32, _u32, c.c_uint32, _f32, c.c_int, _f32]
+        l.refgpu_transform_ms.restype = c.c_int
+        l.refgpu_transform_ms.argtypes = [_node, _u32, _u32, _f32, _f32, c.c_uint32, _u32, c.c_uint32, _f32, _f32,
+                                          _f32, c.c_float, c.c_float, c.c_int, _f32]
         _ref_gpu[variant] = l
     return _ref_gpu[variant]
 
@@ -342,6 +433,31 @@ def refgpu_collapse(nodes, parents, counts, costs, ci=1.2, ct=1.0, variant: str 
     if rc != 0:
         raise RuntimeError(f"refgpu_collapse: CUDA error {rc}")
     return out, cnt, prims, cst
+
+
+def refgpu_tree_ms(verts, faces, reps=5, variant: str = "fmad", ci=1.2, ct=1.0):
+    """Mean device time (ms) of each of the reference's tree kernels on
+    device-resident data: dict of morton, sort, tree, aabb (lbvh.cu's commit
+    steps), candidate, refit, finalize (kr_cuda_bvh_obb_tree's stages) and
+    collapse (kr_cuda_bvh_collapse's mark and gather kernels).  The subtree
+    summaries and the centroid box the reference's skipped kernels would
+    make come from the oracle and are not timed."""
+    l = ref_gpu(variant)
+    v, f, n = _mesh(verts, faces)
+    _, centroid = scene_bounds(verts, faces)
+    a = np.zeros(4, np.float32)
+    rc = l.refgpu_lbvh_ms(v, v.shape[0] // 3, f, n, centroid, reps, a)
+    if rc != 0:
+        raise RuntimeError(f"refgpu_lbvh_ms: CUDA error {rc}")
+    t = refgpu_lbvh(verts, faces, variant)
+    mn, mx, pairs = obb_summaries(t["nodes"], verts, faces)
+    b = np.zeros(4, np.float32)
+    rc = l.refgpu_transform_ms(t["nodes"], t["parents"], t["counts"], t["costs"], v, v.shape[0] // 3, f, n,
+                               mn.reshape(-1), mx.reshape(-1), pairs.reshape(-1), ci, ct, reps, b)
+    if rc != 0:
+        raise RuntimeError(f"refgpu_transform_ms: CUDA error {rc}")
+    keys = ("morton", "sort", "tree", "aabb", "candidate", "refit", "finalize", "collapse")
+    return dict(zip(keys, [float(x) for x in np.concatenate([a, b])]))
 
 
 def refgpu_lbvh63_available() -> bool:

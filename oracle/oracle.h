@@ -89,6 +89,18 @@ void oracle_stable_order64(const uint64_t* keys, uint32_t n, uint32_t* order);
 /* SoA tree of the 63-bit Karras build: left/right/parent/data per node (-1 = none). */
 void oracle_karras63(const uint64_t* sorted, const uint32_t* order, uint32_t n, int32_t* left, int32_t* right,
                      int32_t* parent, int32_t* data);
+/* The three stages of oracle_atrbvh_build over the reference's SoA tree
+ * fields (SoABVHTree.h:19-44): int32 parent/left/right/data, float4 box
+ * min/max, float area per node.  seed: LBVH-63 tree with boxes; optimize:
+ * the treelet optimisation in place; emit: copy to kr_bvh_node + refit. */
+int oracle_atrbvh_seed(const float* verts, const uint32_t* faces4, uint32_t n, int32_t* parent, int32_t* left,
+                       int32_t* right, int32_t* data, float* lo4, float* hi4, float* area, uint64_t* codes_sorted);
+int oracle_atrbvh_optimize(uint32_t n, int treelet_size, int iterations, float ci, float ct, int32_t* parent,
+                           int32_t* left, int32_t* right, int32_t* data, float* lo4, float* hi4, float* area,
+                           float* sah_out);
+int oracle_atrbvh_emit(uint32_t n, const int32_t* parent, const int32_t* left, const int32_t* right,
+                       const int32_t* data, const float* lo4, const float* hi4, const float* area,
+                       obvh_oracle_node* nodes, uint32_t* parents, uint32_t* counts, float* costs);
 /* LBVH-63 + agglomerative treelet optimisation + copy to kr_bvh_node + refit.
  * codes_sorted (nullable) receives the sorted Morton codes, sah_out (nullable)
  * the root's treelet-optimiser SAH after each iteration.  Returns 0 or -1. */

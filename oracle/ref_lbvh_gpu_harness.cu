@@ -108,3 +108,66 @@ extern "C" int refgpu_lbvh(const float* verts, uint32_t n_verts, const uint32_t*
     a.back(costs, d_costs, 4ull * nn);
     return static_cast<int>(a.err);
 }
+
+// Device time of each step of refgpu_lbvh, on device-resident inputs, as the
+// mean over `reps` builds after one untimed build: ms[0] mortons_kernel,
+// ms[1] thrust::stable_sort_by_key (with the temporary storage thrust
+// allocates on every call, as the reference's commit runs it), ms[2]
+// radix_tree_build_kernel, ms[3] calculate_aabbs_kernel.  CUDA events on the
+// default stream.  Returns 0 or the CUDA error code; -1 for bad arguments.
+extern "C" int refgpu_lbvh_ms(const float* verts, uint32_t n_verts, const uint32_t* faces4, uint32_t n,
+                              const float* centroid_box, int reps, float* ms) {
+    if (n < 2 || reps < 1) return -1;
+    const u32 ni = n - 1, nn = 2 * n - 1;
+    Arena a;
+    auto* d_verts = static_cast<kr_vec3*>(a.copy(verts, 12ull * n_verts));
+    auto* d_faces = static_cast<kr_uvec4*>(a.copy(faces4, 16ull * n));
+    kr_object_cu object;
+    memset(&object, 0, sizeof object);
+    object.type = KR_OBJECT_MESH;
+    object.as_mesh.vertices = d_verts;
+    object.as_mesh.attr_count = n_verts;
+    object.as_mesh.faces = d_faces;
+    object.as_mesh.face_count = n;
+    auto* d_object = static_cast<kr_object_cu*>(a.copy(&object, sizeof object));
+    aabb3 boxes[2];
+    boxes[0] = kr_aabb_empty3();
+    boxes[1].min = {centroid_box[0], centroid_box[1], centroid_box[2]};
+    boxes[1].max = {centroid_box[3], centroid_box[4], centroid_box[5]};
+    auto* d_boxes = static_cast<aabb3*>(a.copy(boxes, sizeof boxes));
+    auto* d_mortons = static_cast<kr_morton*>(a.zeroed(sizeof(kr_morton) * n));
+    auto* d_bvh = static_cast<kr_bvh_node*>(a.zeroed(sizeof(kr_bvh_node) * nn));
+    auto* d_parents = static_cast<u32*>(a.zeroed(4ull * nn));
+    auto* d_counts = static_cast<u32*>(a.zeroed(4ull * nn));
+    auto* d_costs = static_cast<kr_scalar*>(a.zeroed(4ull * nn));
+    auto* d_visit = static_cast<b32*>(a.zeroed(4ull * ni));
+    if (a.err != cudaSuccess) return static_cast<int>(a.err);
+    cudaEvent_t ev[5];
+    for (auto& e : ev) a.note(cudaEventCreate(&e));
+    double sum[4] = {0, 0, 0, 0};
+    for (int r = 0; r <= reps && a.err == cudaSuccess; ++r) {
+        a.note(cudaMemset(d_visit, 0, 4ull * ni));
+        a.note(cudaEventRecord(ev[0]));
+        mortons_kernel<<<(n + 255) / 256, 256>>>(d_object, d_mortons, d_bvh + ni, d_boxes);
+        a.note(cudaEventRecord(ev[1]));
+        thrust::stable_sort_by_key(thrust::device_ptr<kr_morton>(d_mortons),
+                                   thrust::device_ptr<kr_morton>(d_mortons + n),
+                                   thrust::device_ptr<kr_bvh_node>(d_bvh + ni));
+        a.note(cudaEventRecord(ev[2]));
+        radix_tree_build_kernel<<<(ni + 255) / 256, 256>>>(d_object, d_bvh, d_mortons, d_parents);
+        a.note(cudaEventRecord(ev[3]));
+        calculate_aabbs_kernel<<<(n + 511) / 512, 512>>>(d_object, d_bvh, d_parents, d_counts, d_costs, d_visit);
+        a.note(cudaEventRecord(ev[4]));
+        a.note(cudaGetLastError());
+        a.note(cudaEventSynchronize(ev[4]));
+        if (r == 0) continue;  // warm-up
+        for (int k = 0; k < 4; ++k) {
+            float t = 0.0f;
+            a.note(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+            sum[k] += t;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 4; ++k) ms[k] = static_cast<float>(sum[k] / reps);
+    return static_cast<int>(a.err);
+}

@@ -127,6 +127,78 @@ extern "C" int refgpu_collapse(const void* nodes, const uint32_t* parents, uint3
     return static_cast<int>(a.err);
 }
 
+// Device time of the transform's stages and of the collapse, on
+// device-resident inputs, as the mean over `reps` runs after one untimed run:
+// ms[0] calculate_candidate_obb_kernel, ms[1] refit_obbs_kernel_new, ms[2]
+// finalize_obbs_kernel (CUDA events around each launch, with the launch
+// shapes of kr_cuda_bvh_obb_tree), ms[3] the mark and gather kernels of
+// kr_cuda_bvh_collapse (the kernel times the reference itself reports in its
+// metrics).  Each run starts from the given summaries, counts and costs.
+// Arguments as refgpu_obb_from_summaries and refgpu_collapse.  Returns 0 or
+// the CUDA error code; -1 for bad arguments.
+extern "C" int refgpu_transform_ms(const void* nodes, const uint32_t* parents, const uint32_t* counts,
+                                   const float* costs, const float* verts, uint32_t n_verts, const uint32_t* faces4,
+                                   uint32_t n, const float* min_proj, const float* max_proj, const float* pairs,
+                                   float ci, float ct, int reps, float* ms) {
+    if (n < 2 || reps < 1) return -1;
+    const u32 ni = n - 1, nn = 2 * n - 1;
+    Arena a;
+    auto* d_nodes = static_cast<kr_bvh_node*>(a.copy(nodes, sizeof(kr_bvh_node) * nn));
+    auto* d_parents = static_cast<u32*>(a.copy(parents, 4ull * nn));
+    auto* d_counts0 = static_cast<u32*>(a.copy(counts, 4ull * nn));
+    auto* d_costs0 = static_cast<kr_scalar*>(a.copy(costs, 4ull * nn));
+    auto* d_counts = static_cast<u32*>(a.zeroed(4ull * nn));
+    auto* d_costs = static_cast<kr_scalar*>(a.zeroed(4ull * nn));
+    auto* d_verts = static_cast<kr_vec3*>(a.copy(verts, 12ull * n_verts));
+    auto* d_faces = static_cast<kr_uvec4*>(a.copy(faces4, 16ull * n));
+    auto* d_min0 = static_cast<kr_scalar*>(a.copy(min_proj, 28ull * nn));
+    auto* d_max0 = static_cast<kr_scalar*>(a.copy(max_proj, 28ull * nn));
+    auto* d_min = static_cast<kr_scalar*>(a.zeroed(28ull * nn));
+    auto* d_max = static_cast<kr_scalar*>(a.zeroed(28ull * nn));
+    auto* d_pairs = static_cast<kr_minmax_pair*>(a.copy(pairs, 168ull * nn));
+    auto* d_obbs = static_cast<kr_obb3*>(a.zeroed(sizeof(kr_obb3) * nn));
+    auto* d_xfs = static_cast<kr_mat4*>(a.zeroed(sizeof(kr_mat4) * nn));
+    auto* d_visit = static_cast<b32*>(a.zeroed(4ull * ni));
+    auto* d_collapsed = static_cast<kr_bvh_node*>(a.zeroed(sizeof(kr_bvh_node) * nn));
+    auto* d_prims = static_cast<u32*>(a.zeroed(4ull * n));
+    if (a.err != cudaSuccess) return static_cast<int>(a.err);
+    cudaEvent_t ev[4];
+    for (auto& e : ev) a.note(cudaEventCreate(&e));
+    double sum[4] = {0, 0, 0, 0};
+    for (int r = 0; r <= reps && a.err == cudaSuccess; ++r) {
+        a.note(cudaMemcpy(d_min, d_min0, 28ull * nn, cudaMemcpyDeviceToDevice));
+        a.note(cudaMemcpy(d_max, d_max0, 28ull * nn, cudaMemcpyDeviceToDevice));
+        a.note(cudaMemcpy(d_counts, d_counts0, 4ull * nn, cudaMemcpyDeviceToDevice));
+        a.note(cudaMemcpy(d_costs, d_costs0, 4ull * nn, cudaMemcpyDeviceToDevice));
+        a.note(cudaMemset(d_visit, 0, 4ull * ni));
+        a.note(cudaEventRecord(ev[0]));
+        calculate_candidate_obb_kernel<<<(ni + 31) / 32, 32>>>(d_obbs, d_min, d_max, d_pairs, n, ni);
+        a.note(cudaEventRecord(ev[1]));
+        refit_obbs_kernel_new<<<(n + 127) / 128, 128>>>(d_nodes, d_verts, d_faces, d_obbs, d_xfs, d_parents,
+                                                        d_counts, nullptr, d_visit, d_min, d_max, n, ni);
+        a.note(cudaEventRecord(ev[2]));
+        finalize_obbs_kernel<<<(ni + 511) / 512, 512>>>(d_nodes, d_min, d_max, d_obbs, d_xfs, n, ni);
+        a.note(cudaEventRecord(ev[3]));
+        a.note(cudaGetLastError());
+        a.note(cudaEventSynchronize(ev[3]));
+        kr_ads_collapse_metrics metrics;
+        memset(&metrics, 0, sizeof metrics);
+        kr_cuda_bvh_collapse(d_nodes, d_parents, d_collapsed, d_counts, d_prims, d_costs, ci, ct, n, ni, &metrics);
+        a.note(cudaGetLastError());
+        a.note(cudaDeviceSynchronize());
+        if (r == 0) continue;  // warm-up
+        for (int k = 0; k < 3; ++k) {
+            float t = 0.0f;
+            a.note(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+            sum[k] += t;
+        }
+        sum[3] += metrics.collapse_mark_time + metrics.collapse_time;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 4; ++k) ms[k] = static_cast<float>(sum[k] / reps);
+    return static_cast<int>(a.err);
+}
+
 // The reference's traversal packing on a tree: kr_cuda_bvh_persistent when
 // transforms is NULL, else kr_cuda_obvh_persistent then kr_cuda_soa_obvh
 // (transforms.cu:1281-1449).  packed_io (node_count x 64 bytes) and pairs_io

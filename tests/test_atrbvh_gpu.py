@@ -9,7 +9,7 @@ guarantees at the torus-knot size of the benchmark.
 import numpy as np
 import pytest
 
-from conftest import contained, same_bits
+from conftest import contained, lattice_mesh, same_bits
 from oracle import bvh as ref
 from obvh_b200 import bvh, workloads
 
@@ -65,17 +65,33 @@ def test_tree_other_settings(builder, iters, tau, ci, ct):
 def test_lattice_ties(builder):
     # many equal centroids and equal areas: ties in the sort, the Karras
     # split, the leaf to expand and the pair to merge
-    g = np.stack(np.meshgrid(np.arange(12), np.arange(12), np.arange(12), indexing="ij"), -1).reshape(-1, 3)
-    c = np.repeat(g, 2, axis=0).astype(np.float32) * 0.5
-    tri = np.array([[0, 0, 0], [0.2, 0, 0], [0, 0.2, 0]], np.float32)
-    v = (c[:, None, :] + tri[None]).reshape(-1, 3)
-    n = c.shape[0]
-    f = np.zeros((n, 4), np.uint32)
-    f[:, 0] = np.arange(0, 3 * n, 3)
-    f[:, 1] = f[:, 0] + 1
-    f[:, 2] = f[:, 0] + 2
+    v, f = lattice_mesh(12)
     o, _ = _run(builder, v, f, flags=0, tau=7)
-    _check_tree(o, ref.atrbvh_build(v, f, 7, 2), n)
+    _check_tree(o, ref.atrbvh_build(v, f, 7, 2), f.shape[0])
+
+
+def _pin_mesh(kind):
+    if kind == "soup":
+        return workloads.triangle_soup(20_000, seed=1500)
+    if kind == "lattice":
+        return lattice_mesh(12)
+    return workloads.torus_knot_mesh(128, 56, seed=2)
+
+
+@pytest.mark.skipif(not ref.ref_treelet_available(), reason="oracle/_ref/libref_treelet_emu.so not built")
+@pytest.mark.parametrize("kind", ["soup", "lattice", "knot"])
+@pytest.mark.parametrize("tau", [7, 9])
+def test_tree_matches_the_reference_treelet_kernel(builder, kind, tau):
+    """The GPU tree against the reference's own treelet kernel
+    (AgglomerativeTreelet.cu, run as host code by oracle/ref_treelet_emu.cpp)
+    applied to the seed tree, then copied and refit (atrbvh.cu:95-183)."""
+    v, f = _pin_mesh(kind)
+    n = f.shape[0]
+    r = ref.atrbvh_emit(ref.ref_treelet_optimize(ref.atrbvh_seed(v, f), tau, 2))
+    o, _ = _run(builder, v, f, flags=0, tau=tau)
+    _check_tree(o, r, n)
+    assert np.array_equal(o["counts"].cpu().numpy().view(np.uint32), r["counts"])
+    assert same_bits(o["costs"].cpu().numpy(), r["costs"])
 
 
 def test_full_commit_matches_the_three_steps(builder):

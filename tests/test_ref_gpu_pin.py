@@ -15,14 +15,18 @@ in the reference's own arrays.
   for bit (zero signs aside), and the CUDA path's, checked directly here.
 * The ATRBVH seed build (oracle/_ref/libref_lbvh63_gpu.so: LBVH.cu and
   CubWrapper.cu through their own host wrappers) must equal the oracle's
-  63-bit codes, order and Karras tree exactly.  Its node boxes and the treelet
-  optimiser are not run (barriers in divergent loops).
+  63-bit codes, order and Karras tree exactly.  Its node-box kernel and the
+  treelet kernel are not run on the GPU (barriers in divergent loops); the
+  treelet kernel runs as host code instead (tests/test_ref_treelet_pin.py,
+  tests/test_atrbvh_gpu.py).
 * "fmad" is the reference as its own build compiles it: nvcc's default
   contraction of multiplies and adds.  Codes, order, topology, counts, boxes
   and collapse decisions must still be identical and costs within 1e-6
   relative.  OBBs: contraction moves near-ties in the candidate score, so a
   small share of internal nodes picks another frame; the rest agree in their
-  axes to about 1e-6.
+  axes to about 1e-6 and in surface area to rounding (a few 1e-5).
+* Speed: each phase of the reference's kernels, timed on the device against
+  the fused chain here on the same 2M-triangle soup.
 """
 import numpy as np
 import pytest
@@ -192,3 +196,98 @@ def test_atrbvh_seed_kernels_equal_the_oracle(case):
     assert np.array_equal(order, oorder)
     for mine, theirs in zip(otree, tree):
         assert np.array_equal(mine, theirs)
+
+
+def _obb_surface_area(obbs):
+    """FP64 surface area of each box: half-extents times the axis lengths
+    (a leaf's third axis is the unnormalised normal)."""
+    o = np.asarray(obbs, np.float64)
+    e = o[:, 12:15] * np.linalg.norm(o[:, 3:12].reshape(-1, 3, 3), axis=2)
+    return 8.0 * (e[:, 0] * e[:, 1] + e[:, 0] * e[:, 2] + e[:, 1] * e[:, 2])
+
+
+def _ms(fn, reps=5):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def test_tree_speed_against_the_reference_kernels(capsys):
+    """Device time of each phase on the 2M-triangle soup, device-resident
+    inputs: the reference's kernels (built as shipped and uncontracted) against
+    the fused chain here, timed through its flags (LBVH only; + OBB tree;
+    + collapse).  The reference's summary and scene-box kernels are not run,
+    so its totals leave them out; the chain here includes its equivalents."""
+    import torch
+    v, f = workloads.triangle_soup(2_000_000, seed=1)
+    theirs = {var: ref.refgpu_tree_ms(v, f, 5, var) for var in ("fmad", "nofma")}
+    builder = bvh.ObvhBuilder()
+    mesh = bvh.Mesh(v, f)
+    out = builder.outputs(f.shape[0])
+    t = {flags: _ms(lambda: builder.build(mesh, flags=flags, out=out)) for flags in (0, 1, 3)}
+    assert builder.status(f.shape[0])[0] == 0
+    ours = {"lbvh": t[0], "obb tree": t[1] - t[0], "collapse": t[3] - t[1], "total": t[3]}
+    groups = {"lbvh": ("morton", "sort", "tree", "aabb"), "obb tree": ("candidate", "refit", "finalize"),
+              "collapse": ("collapse",)}
+    with capsys.disabled():
+        print("\nphase      reference as shipped (uncontracted)   this build    [2M-triangle soup, ms]")
+        for k, v_ in theirs["fmad"].items():
+            print(f"  {k:10s} {v_:9.3f} ({theirs['nofma'][k]:7.3f})")
+        for g, keys in groups.items():
+            r = sum(theirs["fmad"][k] for k in keys)
+            print(f"{g:10s}   {r:9.3f} ({sum(theirs['nofma'][k] for k in keys):7.3f})              {ours[g]:8.3f}")
+        total = sum(theirs["fmad"].values())
+        print(f"{'total':10s}   {total:9.3f} ({sum(theirs['nofma'].values()):7.3f})              {ours['total']:8.3f}")
+    assert ours["total"] < total
+
+
+@pytest.mark.parametrize("case", [("soup", 300_000), ("knot", 0)], ids=lambda c: f"{c[0]}{c[1] or ''}")
+def test_surface_area_against_the_reference_as_shipped(case, capsys):
+    """OBB surface areas (FP64, extents times axis lengths) of the CUDA path
+    against the reference built as it ships (with contraction), node by node,
+    split into the nodes whose candidate frame agrees and those where
+    contraction moved a near-tie to another frame.  The CUDA path equals the
+    reference built without contraction bit for bit (the tests above), so
+    these figures are the reference's own spread between its two builds:
+    rounding of fused multiply-adds, largest at leaves, whose third axis is
+    the unnormalised normal.  Prints the counts outside 1e-5 relative."""
+    import torch
+    v, f = _mesh(case)
+    n = f.shape[0]
+    builder = bvh.ObvhBuilder()
+    o = builder.build(bvh.Mesh(v, f), flags=1)
+    torch.cuda.synchronize()
+    assert builder.status(n)[0] == 0
+    mine = o["obbs"].cpu().numpy()
+    g = ref.refgpu_lbvh(v, f, "fmad")
+    theirs, _ = ref.refgpu_obb_tree(g["nodes"], g["parents"], g["counts"], v, f, "fmad")
+    sa_m, sa_t = _obb_surface_area(mine), _obb_surface_area(theirs)
+    rel = np.abs(sa_m - sa_t) / np.maximum(sa_t, 1e-300)
+    a = mine[:, 3:12].astype(np.float64).reshape(-1, 3, 3)
+    b = theirs[:, 3:12].astype(np.float64).reshape(-1, 3, 3)
+    d = (np.linalg.norm(a - b, axis=2) / np.maximum(np.linalg.norm(b, axis=2), 1e-30)).max(axis=1)
+    same = d <= 1e-3
+    internal = np.arange(2 * n - 1) < n - 1
+    rows = {}
+    for name, m in (("internal, same frame", internal & same), ("internal, other frame", internal & ~same),
+                    ("leaves, same frame", ~internal & same), ("leaves, other frame", ~internal & ~same)):
+        k = int(m.sum())
+        rows[name] = (k, int((rel[m] > 1e-5).sum()), float(np.quantile(rel[m], 0.999)) if k else 0.0,
+                      float(rel[m].max()) if k else 0.0)
+    with capsys.disabled():
+        print(f"\nOBB surface area vs the reference as shipped, {case[0]} {n} triangles "
+              "(nodes, > 1e-5 rel, p99.9 rel, max rel):")
+        for name, r in rows.items():
+            print(f"  {name:22s} {r[0]:8d} {r[1]:8d} {r[2]:.2e} {r[3]:.2e}")
+    # same frame: rounding-level differences only; another frame: a small share
+    assert rows["internal, same frame"][3] <= 2e-4
+    assert rows["leaves, same frame"][3] <= 2e-3
+    assert rows["internal, other frame"][0] <= 0.02 * (n - 1)
+    assert rows["leaves, other frame"][0] <= 1e-3 * n
