@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--rays", type=int, default=4_000_000, help="obvh_trace: rays per pass")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + timed steps, no clock soak, e2e or CPU legs (for ncu captures)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="lbvh_obb_tree at 1 GPU: leave out the DiTO-100M, batch and serve sub-objects")
     return ap.parse_args()
 
 
@@ -1297,6 +1299,37 @@ def bench_serve_ours(a, dist):
     }
 
 
+def extra_workloads(a, dist, line):
+    """The default line at 1 GPU also carries the other measured workloads
+    (the 100M-point DiTO fit, the 4,096-set batch, the served mix), each with
+    its own CUDA-event timing, clocks, roofline, per-call comparison and e2e,
+    so that every target is timed in the same run.  About a minute extra."""
+    import copy
+    import gc
+    import torch
+    subs = {"dito_100M": ("dito", 20, 5, bench_dito_ours), "dito_batch": ("dito_batch", 10, 3, bench_batch_ours),
+            "serve": ("serve", 1, 1, bench_serve_ours)}
+    for key, (workload, steps, warmup, fn) in subs.items():
+        b = copy.copy(a)
+        b.workload, b.steps, b.warmup = workload, steps, warmup
+        if workload == "serve":
+            b.requests = 200
+        t0 = time.perf_counter()
+        sub = fn(b, dist)
+        sub.pop("kernels", None)
+        sub["wall_s"] = round(time.perf_counter() - t0, 1)
+        line[key] = sub
+        gc.collect()
+        torch.cuda.empty_cache()
+    d = line["dito_100M"]
+    # the whole fit against 24 B/point (two compulsory passes over 12-byte points)
+    fit_gbs = 24 * d["config"]["points_per_gpu"] / (d["ms_per_step"] / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    d["fit_roofline"] = {"bound": "hbm", "achieved": round(fit_gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(fit_gbs / peak, 4), "bytes_per_point": 24,
+                         "note": f"both passes, one fit per step, peak {peak_kind}"}
+
+
 def main():
     a = parse_args()
     dist = Dist()
@@ -1325,6 +1358,8 @@ def main():
                "dito": bench_dito_ours, "dito_batch": bench_batch_ours, "serve": bench_serve_ours,
                "obvh_pack": bench_pack_ours, "obvh_trace": bench_trace_ours}
         line = run[a.workload](a, dist)
+        if a.workload == "lbvh_obb_tree" and dist.world == 1 and not (a.profile or a.no_extras):
+            extra_workloads(a, dist, line)
         if dist.rank == 0:
             print(json.dumps(line), flush=True)
     finally:
