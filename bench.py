@@ -55,11 +55,12 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["lbvh_obb_tree", "atrbvh_obb_tree", "dito", "dito_batch", "serve",
-                                           "obvh_pack", "obvh_trace"],
+                                           "obvh_pack", "obvh_trace", "mesh_batch"],
                     default="lbvh_obb_tree")
     ap.add_argument("--treelet", type=int, default=7, help="atrbvh_obb_tree: treelet size")
     ap.add_argument("--requests", type=int, default=300, help="serve: requests in the stream")
     ap.add_argument("--sets", type=int, default=4096, help="dito_batch: point sets per batch")
+    ap.add_argument("--meshes", type=int, default=2048, help="mesh_batch: meshes per batch")
     ap.add_argument("--no-autotune", action="store_true", help="dito_batch: default knobs")
     ap.add_argument("--points", type=int, default=100_000_000, help="dito: points per fit")
     ap.add_argument("--tris", type=int, default=2_000_000, help="lbvh_obb_tree: triangles per build")
@@ -1145,6 +1146,186 @@ def bench_batch_reference(a, dist):
             "e2e": {"value": round(value, 3), "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def _mesh_batch_inputs(n_meshes, seed, dev):
+    """Thin-triangle soups (the configs[1] generator) of log-uniform sizes
+    64..16,384 triangles, packed: (verts, faces int32 [F, 4], vertex and face
+    CSR offsets as numpy uint64)."""
+    import numpy as np
+    import torch
+    from obvh_b200 import workloads
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(64), np.log(16384), size=n_meshes)).astype(np.int64)
+    vs, fs = [], []
+    for k, n in enumerate(sizes):
+        v, f = workloads.triangle_soup_torch(int(n), seed=seed * 100003 + k, device=dev)
+        vs.append(v)
+        fs.append(f)
+    vo = np.concatenate([[0], np.cumsum([v.shape[0] for v in vs])]).astype(np.uint64)
+    fo = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    return torch.cat(vs).contiguous(), torch.cat(fs).contiguous(), vo, fo
+
+
+def bench_mesh_batch_ours(a, dist):
+    import numpy as np
+    import torch
+    from obvh_b200 import _native, bvh
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    verts, faces, vo, fo = _mesh_batch_inputs(a.meshes, 5 + dist.rank, dev)
+    sizes = np.diff(fo).astype(np.int64)
+    nodes = int(np.sum(2 * sizes - 1))
+    batch = bvh.BuildBatch(vo, fo, flags=bvh.BUILD_OBBS | bvh.BUILD_COLLAPSE, device=dev)
+    out = batch.outputs()
+    stream = torch.cuda.current_stream(dev)
+    batch.capture(verts, faces, out)
+    sampler = ClockSampler(dev.index, enabled=not a.profile)
+    total_ms, prof, clocks = timed_steps(a, dist, lambda j: batch.launch(stream), sampler, stream)
+    err, slots = batch.status(stream)
+    if err:
+        raise RuntimeError(f"device error word {err}")
+    if a.profile:
+        return {"profile": "mesh_batch", "meshes": a.meshes, "ms_per_step": total_ms / a.steps, "kernels": prof}
+    peak, peak_kind = peaks()
+    ms_step = total_ms / a.steps
+    value = dist.world * nodes / (ms_step / 1e3) / 1e6
+    # the whole-build bytes of the tree workload, per mesh: 164 B per node + 52 B per triangle
+    batch_bytes = {"mesh_batch_graph": int(np.sum(164 * (2 * sizes - 1) + 52 * sizes))}
+    roof = roofline(prof, batch_bytes, peak, peak_kind)
+
+    # plain per-call path: obvh_build_async per mesh on the same device buffers,
+    # enqueued back to back on one stream (no waits between meshes)
+    lib = _native.lib()
+    nmax = int(sizes.max())
+    ws = torch.empty(int(lib.obvh_build_workspace_bytes(nmax)), dtype=torch.uint8, device=dev)
+    S = ctypes.c_void_p(stream.cuda_stream)
+    _native.check(lib.obvh_build_workspace_init(ctypes.c_void_p(ws.data_ptr()), nmax, S))
+    P = {k: t.data_ptr() for k, t in out.items()}
+    vb, fb = verts.data_ptr(), faces.data_ptr()
+    calls = []
+    for m in range(a.meshes):
+        nb, f0, n = batch.node_offset(m), int(fo[m]), int(sizes[m])
+        calls.append([ctypes.c_void_p(vb + 12 * int(vo[m])), ctypes.c_void_p(fb + 16 * f0), n, 3,
+                      ctypes.c_float(1.2), ctypes.c_float(1.0),
+                      ctypes.c_void_p(P["nodes"] + 36 * nb), ctypes.c_void_p(P["parents"] + 4 * nb),
+                      ctypes.c_void_p(P["counts"] + 4 * nb), ctypes.c_void_p(P["costs"] + 4 * nb),
+                      ctypes.c_void_p(P["bounds"] + 48 * m), ctypes.c_void_p(P["obbs"] + 60 * nb),
+                      ctypes.c_void_p(P["transforms"] + 64 * nb), ctypes.c_void_p(P["collapsed"] + 36 * nb),
+                      ctypes.c_void_p(P["primitives"] + 4 * f0), ctypes.c_void_p(ws.data_ptr()), S])
+
+    def per_call():
+        for c in calls:
+            e = lib.obvh_build_async(*c)
+            if e:
+                _native.check(e)
+    per_call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    per_call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    pc_ms = e0.elapsed_time(e1)
+    pc_value = -dist.max(-(nodes / (pc_ms / 1e3) / 1e6)) * dist.world
+
+    # end to end: the packed meshes from pinned host memory every step, the
+    # graph, the per-mesh slot counts read back
+    hv = torch.empty_like(verts, device="cpu").pin_memory()
+    hf = torch.empty_like(faces, device="cpu").pin_memory()
+    hv.copy_(verts)
+    hf.copy_(faces)
+    e2e_steps = max(3, min(a.steps, 10))
+
+    def e2e_step():
+        verts.copy_(hv, non_blocking=True)
+        faces.copy_(hf, non_blocking=True)
+        batch.launch(stream)
+        batch.status(stream)
+    e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    e2e_min = -dist.max(-(nodes * e2e_steps / e2e_s / 1e6))
+    info = batch.info()
+    line = {
+        "metric": "Batched LBVH + OBB-tree + collapse builds (Mnodes/s)", "value": round(value, 3),
+        "unit": "Mnodes/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": round(ms_step, 5), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: thin random triangle soups (configs[1] generator), sizes log-U[64,16384], seeded",
+        "config": {"workload": "mesh_batch", "meshes_per_gpu": a.meshes, "triangles_per_gpu": int(sizes.sum()),
+                   "nodes_per_gpu": nodes, "launch": "one graph: memset + one persistent kernel, one mesh per CTA",
+                   "plan": info, "l2": f"{(12 * int(vo[-1]) + 16 * int(fo[-1])) / 1e6:.0f} MB of meshes in, "
+                                       "~1.5 GB written per step, no flush",
+                   "parallelism": f"replicas{dist.world}"},
+        "kernels": kernel_table(prof, a.steps, batch_bytes, peak),
+        "gpu_launches": sum(v[0] for v in prof.values()), "roofline": roof,
+        "per_call": {"value": round(pc_value, 3), "unit": "Mnodes/s", "ms_per_batch": round(pc_ms, 3),
+                     "api": "obvh_build_async per mesh (the whole-GPU chain), back to back on one stream",
+                     "speedup": round(value / pc_value, 2)},
+        "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mnodes/s",
+                "h2d_bytes_per_step": int(verts.numel() * 4 + faces.numel() * 4),
+                "d2h_bytes_per_step": 4 * (a.meshes + 1), "api": "obvh_build_batch_launch, pinned host meshes"},
+        "clocks": clocks,
+    }
+    if dist.rank == 0 and dist.world == 1:
+        line["cpu_baseline"] = cpu_mesh_batch_baseline(verts, faces, vo, fo)
+    return line
+
+
+def cpu_mesh_batch_baseline(verts, faces, vo, fo, budget_s=8.0):
+    """The oracle port of the same builds on one host core, over the batch's
+    first meshes until the time budget is spent."""
+    from oracle import bvh as ref
+    hv, hf = verts.cpu().numpy(), faces.cpu().numpy().view("uint32")
+    done_nodes, m, t0 = 0, 0, time.perf_counter()
+    while m < len(fo) - 1 and time.perf_counter() - t0 < budget_s:
+        v = hv[int(vo[m]):int(vo[m + 1])]
+        f = hf[int(fo[m]):int(fo[m + 1])]
+        r = ref.lbvh_build(v, f)
+        ref.obb_tree(r["nodes"], r["parents"], v, f)
+        ref.collapse(r["nodes"], r["parents"], r["counts"], r["costs"])
+        done_nodes += 2 * f.shape[0] - 1
+        m += 1
+    dt = time.perf_counter() - t0
+    return {"value": round(done_nodes / dt / 1e6, 4), "unit": "Mnodes/s", "cores": 1, "kind": "port",
+            "sample": f"the first {m} meshes of the batch ({dt:.1f} s), oracle C restatement"}
+
+
+def bench_mesh_batch_reference(a, dist):
+    """The oracle port of the batch's builds on this host's cores: each step,
+    every host thread builds one sample of the batch's meshes (the first 64,
+    about a tenth of a second of work per thread)."""
+    import numpy as np
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    verts, faces, vo, fo = _mesh_batch_inputs(a.meshes, 5, dev)
+    hv, hf = verts.cpu().numpy(), faces.cpu().numpy().view(np.uint32)
+    sample = min(64, len(fo) - 1)
+    nodes = int(sum(2 * (int(fo[m + 1]) - int(fo[m])) - 1 for m in range(sample)))
+    from oracle import bvh as ref
+
+    def work():
+        for m in range(sample):
+            v = hv[int(vo[m]):int(vo[m + 1])]
+            f = hf[int(fo[m]):int(fo[m + 1])]
+            r = ref.lbvh_build(v, f)
+            ref.obb_tree(r["nodes"], r["parents"], v, f)
+            ref.collapse(r["nodes"], r["parents"], r["counts"], r["costs"])
+    threads = host_threads()
+    times = parallel_steps(a, work, threads)
+    value = threads * nodes * len(times) / sum(times) / 1e6
+    return {"metric": "Batched LBVH + OBB-tree + collapse builds (Mnodes/s)", "impl": "reference",
+            "value": round(value, 4), "unit": "Mnodes/s", "n_gpus": dist.world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (same generator as the ours arm)",
+            "config": {"workload": "mesh_batch", "meshes_per_gpu": a.meshes, "sample_meshes": sample},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mnodes/s", "cores": threads, "kind": "port",
+                             "sample": f"{threads} threads each building the batch's first {sample} meshes per "
+                                       "step, oracle C restatement"},
+            "e2e": {"value": round(value, 4), "unit": "Mnodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def _serve_requests(n_req, seed, dev):
     """The served mix: 70% DiTO fits of Gaussian clouds (1k..4M points,
     log-uniform), 30% LBVH + OBB-tree + collapse builds of thin-triangle
@@ -1349,6 +1530,8 @@ def main():
             print(json.dumps(bench_pack_reference(a, dist)), flush=True)
         elif a.workload == "obvh_trace":
             print(json.dumps(bench_trace_reference(a, dist)), flush=True)
+        elif a.workload == "mesh_batch":
+            print(json.dumps(bench_mesh_batch_reference(a, dist)), flush=True)
         else:
             print(json.dumps(bench_tree_reference(a, dist)), flush=True)
         return
@@ -1356,7 +1539,7 @@ def main():
     try:
         run = {"lbvh_obb_tree": bench_tree_ours, "atrbvh_obb_tree": lambda a, d: bench_tree_ours(a, d, atrbvh=True),
                "dito": bench_dito_ours, "dito_batch": bench_batch_ours, "serve": bench_serve_ours,
-               "obvh_pack": bench_pack_ours, "obvh_trace": bench_trace_ours}
+               "obvh_pack": bench_pack_ours, "obvh_trace": bench_trace_ours, "mesh_batch": bench_mesh_batch_ours}
         line = run[a.workload](a, dist)
         if a.workload == "lbvh_obb_tree" and dist.world == 1 and not (a.profile or a.no_extras):
             extra_workloads(a, dist, line)

@@ -133,6 +133,33 @@ OBVH_EXPORT kr_error obvh_obvh_pack_async(const kr_bvh_node* d_nodes, const kr_m
                                           kr_mat43* d_left_t, kr_mat43* d_right_t, kr_ivec4* d_metadata,
                                           kr_u32 node_count, kr_u32 internal_count, kr_u32* d_error, void* stream);
 /*
+ * Compressed SoA OBVH from packed records and pairs
+ * (kr_cuda_soa_compressed_obvh, transforms.cuh:79-84, transforms.cu:
+ * 1452-1535): per internal node lbounds/rbounds = (pair column 1,
+ * 1 / pair column 2) of each child's 4x4, metadata = the record metadata
+ * with z (left) and w (right) shifted left a byte at a time through the
+ * bytes -trunc(127 c0.x), -trunc(127 c0.y), -trunc(127 c0.z), trunc(127 c0.w)
+ * of that child's column 0, exactly as the reference's host loop does.
+ * Allocates the three arrays and the struct on the device and stores the
+ * struct's device address in *soa_bvh.  Built on the device; the reference
+ * copies through the host.  Synchronous.  Free with
+ * obvh_soa_obvh_compressed_free.
+ */
+OBVH_EXPORT kr_error kr_cuda_soa_compressed_obvh(const kr_bvh_node_packed* packed_bvh,
+                                                 const kr_bvh_transformation_pair* packed_transforms,
+                                                 kr_SoA_OBVH_Compressed** soa_bvh, kr_u32 internal_count,
+                                                 kr_u32 node_count);
+/* Frees what kr_cuda_soa_compressed_obvh allocated (NULL is a no-op).  No
+ * counterpart in the reference. */
+OBVH_EXPORT kr_error obvh_soa_obvh_compressed_free(kr_SoA_OBVH_Compressed* soa_bvh);
+/* kr_cuda_soa_compressed_obvh into caller arrays (internal_count boxes each,
+ * node_count metadata, 16-byte aligned metadata) on `stream`, without
+ * synchronising.  No counterpart in the reference. */
+OBVH_EXPORT kr_error obvh_soa_compressed_obvh_async(const kr_bvh_node_packed* d_packed,
+                                                    const kr_bvh_transformation_pair* d_pairs,
+                                                    kr_aabb3* d_lbounds, kr_aabb3* d_rbounds, kr_ivec4* d_metadata,
+                                                    kr_u32 internal_count, kr_u32 node_count, void* stream);
+/*
  * Closest-hit ray traversal of a SoA OBVH (kr_cuda_soa_obvh_intersect,
  * intersectors.cuh:81-91, intersectors.cu:1452-1473, kernel :801-974).
  * bvh: the device struct kr_cuda_soa_obvh returns; vertices/faces the mesh;
@@ -162,6 +189,32 @@ OBVH_EXPORT kr_error obvh_soa_obvh_intersect_async(const kr_mat43* d_left_t, con
                                                    const kr_u32* d_primitives, kr_u32 primitive_slots,
                                                    const kr_ray* d_rays, kr_intersection* d_isects,
                                                    kr_u32 ray_count, kr_u32* d_error, void* stream);
+/*
+ * Closest-hit ray traversal of a compressed SoA OBVH
+ * (kr_cuda_obvh_compressed_persistent_intersect, intersectors.cuh:69-79,
+ * intersectors.cu:1146-1172, kernel :975-1144): at an internal node each
+ * child's ray is (rotate(d), rotate(o - min)) times max, rotated about the
+ * dequantised axis by the dequantised angle (Rodrigues' formula with cosf and
+ * sinf, kr_vrotate_angle_axis3), against the unit cube.  Otherwise as
+ * kr_cuda_soa_obvh_intersect: the reference's own sequence per ray, so the
+ * hits are the reference's.  Synchronous.
+ */
+OBVH_EXPORT kr_error kr_cuda_obvh_compressed_persistent_intersect(const kr_SoA_OBVH_Compressed* bvh,
+                                                                  const kr_vec3* vertices, const kr_uvec4* faces,
+                                                                  const kr_u32* primitives, const kr_ray* rays,
+                                                                  kr_intersection* isects, kr_u32 ray_count,
+                                                                  kr_u32 block_size, kr_u32 grid_size,
+                                                                  kr_u32* warp_counter);
+/* The compressed traversal on the arrays themselves, indices checked, on
+ * `stream`, without synchronising (as obvh_soa_obvh_intersect_async).  No
+ * counterpart in the reference. */
+OBVH_EXPORT kr_error obvh_soa_compressed_obvh_intersect_async(const kr_aabb3* d_lbounds, const kr_aabb3* d_rbounds,
+                                                              const kr_ivec4* d_metadata, kr_u32 internal_count,
+                                                              kr_u32 node_count, const kr_vec3* d_vertices,
+                                                              const kr_uvec4* d_faces, kr_u32 face_count,
+                                                              const kr_u32* d_primitives, kr_u32 primitive_slots,
+                                                              const kr_ray* d_rays, kr_intersection* d_isects,
+                                                              kr_u32 ray_count, kr_u32* d_error, void* stream);
 /*
  * SAH cost of a tree over its root's area (kr_bvh_sah,
  * src/ads/common/transforms.h:38, transforms.cpp:250-303).  Host arrays, as

@@ -108,6 +108,12 @@ typedef struct { kr_vec3 geom_normal; kr_vec2 barys; kr_u32 primitive; kr_u32 in
  * (left, right, axis, w).  Device pointers. */
 typedef struct { kr_mat43* left_T; kr_mat43* right_T; kr_ivec4* metadata; } kr_SoA_OBVH;
 
+/* Compressed SoA OBVH (ads.h:172-176): per internal node each child's box
+ * as a translation (min) and an inverse scale (max), its rotation as a
+ * quantised axis and angle in metadata.z (left) and .w (right), one byte
+ * each for x, y, z, angle.  Device pointers. */
+typedef struct { kr_aabb3* lbounds; kr_aabb3* rbounds; kr_ivec4* metadata; } kr_SoA_OBVH_Compressed;
+
 typedef struct { const char* key; const char* value; } kr_descriptor;
 typedef struct { kr_descriptor* descriptors; kr_size descriptor_count; } kr_descriptor_container;
 

@@ -104,6 +104,19 @@ def _declare(lib: ctypes.CDLL) -> None:
         "obvh_points_obb_batch": (err, [vp, vp, c.c_uint64, c.c_uint32, vp, c.POINTER(c.c_float)]),
         "obvh_dito_workspace_report": (err, [vp, vp, c.POINTER(c.c_uint32), c.POINTER(c.c_float),
                                              c.POINTER(c.c_uint32)]),
+        "kr_cuda_soa_compressed_obvh": (err, [vp, vp, c.POINTER(c.c_void_p), c.c_uint32, c.c_uint32]),
+        "obvh_soa_obvh_compressed_free": (err, [vp]),
+        "obvh_soa_compressed_obvh_async": (err, [vp] * 5 + [c.c_uint32, c.c_uint32, vp]),
+        "kr_cuda_obvh_compressed_persistent_intersect": (err, [vp] * 6 + [c.c_uint32] * 3 + [vp]),
+        "obvh_soa_compressed_obvh_intersect_async": (err, [vp, vp, vp, c.c_uint32, c.c_uint32, vp, vp, c.c_uint32,
+                                                           vp, c.c_uint32, vp, vp, c.c_uint32, vp, vp]),
+        "obvh_build_batch_create": (err, [vp, vp, c.c_uint64, c.c_uint32, c.c_uint32, c.POINTER(vp)]),
+        "obvh_build_batch_destroy": (err, [vp]),
+        "obvh_build_batch_enqueue": (err, [vp, vp, vp, c.c_float, c.c_float] + [vp] * 10),
+        "obvh_build_batch_capture": (err, [vp, vp, vp, c.c_float, c.c_float] + [vp] * 9),
+        "obvh_build_batch_launch": (err, [vp, vp]),
+        "obvh_build_batch_status": (err, [vp, vp, c.POINTER(c.c_uint32), vp]),
+        "obvh_build_batch_info": (err, [vp] + [c.POINTER(c.c_uint32)] * 3),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

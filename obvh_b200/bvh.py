@@ -392,6 +392,68 @@ def soa_obvh_intersect(soa: dict, mesh: "Mesh", primitives, rays, node_count: in
     return isects, err
 
 
+# ---- compressed SoA OBVH --------------------------------------------------------
+def soa_compressed_obvh(packed, pairs, internal_count: int, node_count: int, out=None, stream=None):
+    """obvh_soa_compressed_obvh_async: the compressed SoA arrays (lbounds,
+    rbounds: float32 [ni, 6], metadata: int32 [nodes, 4]) of packed records
+    and pairs (device tensors), on `stream`."""
+    import torch
+    lib = _native.lib()
+    dev = packed.device
+    if out is None:
+        out = {"lbounds": torch.empty((max(internal_count, 1), 6), dtype=torch.float32, device=dev),
+               "rbounds": torch.empty((max(internal_count, 1), 6), dtype=torch.float32, device=dev),
+               "metadata": torch.empty((max(node_count, 1), 4), dtype=torch.int32, device=dev)}
+    _native.check(lib.obvh_soa_compressed_obvh_async(_ptr(packed), _ptr(pairs), _ptr(out["lbounds"]),
+                                                     _ptr(out["rbounds"]), _ptr(out["metadata"]), internal_count,
+                                                     node_count, _stream(torch, stream)))
+    return out
+
+
+def soa_compressed_obvh_sync(packed, pairs, internal_count: int, node_count: int):
+    """kr_cuda_soa_compressed_obvh (the reference-signature, allocating form):
+    numpy lbounds [ni, 6], rbounds [ni, 6], metadata [nodes, 4], read back and
+    freed with obvh_soa_obvh_compressed_free."""
+    lib = _native.lib()
+    d_soa = ctypes.c_void_p(0)
+    _native.check(lib.kr_cuda_soa_compressed_obvh(_ptr(packed), _ptr(pairs), ctypes.byref(d_soa), internal_count,
+                                                  node_count))
+    rt = _cudart()
+    rt.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    try:
+        ptrs = (ctypes.c_void_p * 3)()
+        if rt.cudaMemcpy(ctypes.cast(ptrs, ctypes.c_void_p), d_soa, 24, 2) != 0:
+            raise _native.ObvhError("reading the kr_SoA_OBVH_Compressed struct back failed")
+        out = {"lbounds": np.zeros((internal_count, 6), np.float32), "rbounds": np.zeros((internal_count, 6), np.float32),
+               "metadata": np.zeros((node_count, 4), np.int32)}
+        for k, key in enumerate(("lbounds", "rbounds", "metadata")):
+            if out[key].nbytes and rt.cudaMemcpy(ctypes.c_void_p(out[key].ctypes.data), ptrs[k], out[key].nbytes,
+                                                 2) != 0:
+                raise _native.ObvhError("reading the compressed SoA arrays back failed")
+        return out
+    finally:
+        _native.check(lib.obvh_soa_obvh_compressed_free(d_soa))
+
+
+def soa_compressed_obvh_intersect(soa: dict, mesh: "Mesh", primitives, rays, node_count: int, internal_count: int,
+                                  isects=None, stream=None):
+    """obvh_soa_compressed_obvh_intersect_async: closest hits of `rays`
+    against the compressed arrays (soa: lbounds, rbounds, metadata).  Returns
+    (isects uint8 tensor of 28-byte records, error int32 [1])."""
+    import torch
+    lib = _native.lib()
+    n = rays.numel() // 32
+    if isects is None:
+        isects = torch.empty(max(n, 1) * 28, dtype=torch.uint8, device=rays.device)
+    err = torch.zeros(1, dtype=torch.int32, device=rays.device)
+    slots = 0 if primitives is None else primitives.numel()
+    _native.check(lib.obvh_soa_compressed_obvh_intersect_async(
+        _ptr(soa["lbounds"]), _ptr(soa["rbounds"]), _ptr(soa["metadata"]), internal_count, node_count,
+        _ptr(mesh.verts), _ptr(mesh.faces), mesh.n_faces, _ptr(primitives), slots, _ptr(rays), _ptr(isects), n,
+        _ptr(err), _stream(torch, stream)))
+    return isects, err
+
+
 # ---- SAH cost ----------------------------------------------------------------
 def bvh_sah_host(nodes: np.ndarray, ci: float = 1.2, ct: float = 1.0, obbs: np.ndarray = None,
                  root: int = 0) -> float:
@@ -413,3 +475,82 @@ def bvh_sah(nodes, parents, obbs=None, ci: float = 1.2, ct: float = 1.0, stream=
     _native.check(lib.obvh_bvh_sah_async(_ptr(nodes), _ptr(parents), _ptr(obbs), nn, ci, ct, _ptr(out), _ptr(ws),
                                          _stream(torch, stream)))
     return out
+
+
+class BuildBatch:
+    """obvh_build_batch_*: LBVH + OBB tree + collapse builds of many meshes
+    in one launch sequence (include/obvh_build_batch.h).  `vertex_offsets`
+    and `face_offsets` are CSR arrays (meshes + 1 values); faces index their
+    own mesh's vertices.  Outputs: node arrays of 2F - M entries (mesh m at
+    2 face_offsets[m] - m), primitives of F entries (mesh m at
+    face_offsets[m]), bounds 2 boxes per mesh."""
+
+    def __init__(self, vertex_offsets, face_offsets, flags=BUILD_OBBS | BUILD_COLLAPSE, cta_max_faces=0,
+                 device="cuda"):
+        import torch
+        self.torch = torch
+        self.device = torch.device(device)
+        self.lib = _native.lib()
+        self.voff = np.ascontiguousarray(vertex_offsets, dtype=np.uint64)
+        self.foff = np.ascontiguousarray(face_offsets, dtype=np.uint64)
+        self.meshes = self.foff.shape[0] - 1
+        self.flags = flags
+        h = ctypes.c_void_p()
+        _native.check(self.lib.obvh_build_batch_create(self.voff.ctypes.data, self.foff.ctypes.data, self.meshes,
+                                                       flags, cta_max_faces, ctypes.byref(h)))
+        self.handle = h
+        self.faces = int(self.foff[-1])
+        self.nodes = 2 * self.faces - self.meshes
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            self.lib.obvh_build_batch_destroy(h)
+            self.handle = None
+
+    def node_offset(self, m: int) -> int:
+        return 2 * int(self.foff[m]) - m
+
+    def outputs(self):
+        t, d, nn, f = self.torch, self.device, self.nodes, self.faces
+        o = {"nodes": t.empty(nn * NODE_BYTES, dtype=t.uint8, device=d), "parents": t.empty(nn, dtype=t.int32, device=d),
+             "counts": t.empty(nn, dtype=t.int32, device=d), "costs": t.empty(nn, dtype=t.float32, device=d),
+             "bounds": t.empty((self.meshes, 12), dtype=t.float32, device=d)}
+        if self.flags & BUILD_OBBS:
+            o["obbs"] = t.empty((nn, 15), dtype=t.float32, device=d)
+            o["transforms"] = t.empty((nn, 16), dtype=t.float32, device=d)
+        if self.flags & BUILD_COLLAPSE:
+            o["collapsed"] = t.empty(nn * NODE_BYTES, dtype=t.uint8, device=d)
+            o["primitives"] = t.zeros(f, dtype=t.int32, device=d)
+        return o
+
+    def _args(self, verts, faces, o, ci, ct):
+        return [_ptr(verts), _ptr(faces), ci, ct, _ptr(o["nodes"]), _ptr(o["parents"]), _ptr(o["counts"]),
+                _ptr(o["costs"]), _ptr(o.get("bounds")), _ptr(o.get("obbs")), _ptr(o.get("transforms")),
+                _ptr(o.get("collapsed")), _ptr(o.get("primitives"))]
+
+    def enqueue(self, verts, faces, out=None, ci=1.2, ct=1.0, stream=None):
+        """verts: float32 [V, 3], faces: int32/uint32 [F, 4] device tensors."""
+        o = out if out is not None else self.outputs()
+        _native.check(self.lib.obvh_build_batch_enqueue(self.handle, *self._args(verts, faces, o, ci, ct),
+                                                        _stream(self.torch, stream)))
+        return o
+
+    def capture(self, verts, faces, out, ci=1.2, ct=1.0):
+        _native.check(self.lib.obvh_build_batch_capture(self.handle, *self._args(verts, faces, out, ci, ct)))
+
+    def launch(self, stream=None):
+        _native.check(self.lib.obvh_build_batch_launch(self.handle, _stream(self.torch, stream)))
+
+    def status(self, stream=None):
+        """(device error word, per-mesh primitive slots)."""
+        err = ctypes.c_uint32(0)
+        slots = np.zeros(self.meshes, np.uint32)
+        _native.check(self.lib.obvh_build_batch_status(self.handle, _stream(self.torch, stream), ctypes.byref(err),
+                                                       slots.ctypes.data))
+        return err.value, slots
+
+    def info(self):
+        a, b, g = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _native.check(self.lib.obvh_build_batch_info(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(g)))
+        return {"cta_meshes": a.value, "chain_meshes": b.value, "grid": g.value}

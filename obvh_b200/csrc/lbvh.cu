@@ -21,6 +21,7 @@
 #include <unordered_map>
 
 #include "device_common.cuh"
+#include "lbvh_device.cuh"
 #include "lbvh_host.h"
 #include "obvh_lbvh.h"
 #include "obvh_transforms.h"
@@ -48,16 +49,6 @@ struct Ctl {
 };
 
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void tri_box(const kr_vec3* verts, uint4 f, f3& lo, f3& hi) {
-    const f3 a = tree::load_vertex(verts, f.x), b = tree::load_vertex(verts, f.y), c = tree::load_vertex(verts, f.z);
-    lo = a;  // kr_aabb_create3(va, va), then expand by vb, vc
-    hi = a;
-    lo = tree::vmin3(lo, b);
-    hi = tree::vmax3(hi, b);
-    lo = tree::vmin3(lo, c);
-    hi = tree::vmax3(hi, c);
-}
-
 __device__ __forceinline__ float warp_red(float v, bool is_min) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -133,37 +124,11 @@ __global__ void __launch_bounds__(kThreads) tri_bounds_kernel(const kr_vec3* ver
 }
 
 // 30-bit Morton code of the triangle centroid (mortons_kernel); value = index.
-__device__ __forceinline__ uint32_t stretch3(uint32_t x) {
-    x &= 0x3ffu;
-    x = (x | (x << 16)) & 0x30000ffu;
-    x = (x | (x << 8)) & 0x300f00fu;
-    x = (x | (x << 4)) & 0x30c30c3u;
-    x = (x | (x << 2)) & 0x9249249u;
-    return x;
-}
-
-__device__ __forceinline__ uint32_t morton30(f3 c) {  // kr_v32morton3
-    const float q[3] = {c.x, c.y, c.z};
-    uint32_t code = 0;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) code |= stretch3(static_cast<uint32_t>(kmin(kmax(q[k] * 1024.0f, 0.0f), 1023.0f)))
-                                       << (2 - k);
-    return code;
-}
-
 __global__ void __launch_bounds__(kThreads) morton_kernel(const float* tri_boxes, uint32_t n, const kr_aabb3* boxes,
                                                           uint32_t* keys, uint32_t* vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float* cb = reinterpret_cast<const float*>(boxes + 1);  // centroid box
-    const f3 cmin = mk3(cb[0], cb[1], cb[2]);
-    const f3 ext = sub3(mk3(cb[3], cb[4], cb[5]), cmin);
-    const f3 neg = mk3(-cmin.x, -cmin.y, -cmin.z);
-    const float* b = tri_boxes + 6 * static_cast<size_t>(i);
-    const f3 lo = add3(mk3(b[0], b[1], b[2]), neg), hi = add3(mk3(b[3], b[4], b[5]), neg);  // kr_aabb_offset3
-    f3 c = tree::mulv(add3(lo, hi), 0.5f);
-    c = mk3(ext.x != 0 ? c.x / ext.x : 0.f, ext.y != 0 ? c.y / ext.y : 0.f, ext.z != 0 ? c.z / ext.z : 0.f);  // kr_vdiv3s
-    keys[i] = morton30(c);
+    keys[i] = morton_code(tri_boxes + 6 * static_cast<size_t>(i), reinterpret_cast<const float*>(boxes + 1));
     vals[i] = i;
 }
 
@@ -182,52 +147,14 @@ __global__ void __launch_bounds__(kThreads) leaves_kernel(const float* tri_boxes
     w[8] = 1;  // nPrimitives = 1, axis = 0
 }
 
-__device__ __forceinline__ int delta(const uint32_t* codes, int i, int j, uint32_t n) {
-    if (j > static_cast<int>(n) - 1 || j < 0) return -1;
-    const uint32_t a = codes[i], b = codes[j];
-    if (a == b) return 32 + __clz(static_cast<uint32_t>(i) ^ static_cast<uint32_t>(j));
-    return __clz(a ^ b);
-}
-
-__device__ __forceinline__ int halve_up(int x) { return x == 1 ? 0 : ((x % 2) == 1 ? x / 2 + 1 : x / 2); }
-
 // first (nullable) receives each internal node's first leaf in depth-first
 // order: the lower end of its key range; span (nullable) the number of leaves
 // in the range, which is the node's primitive count (one primitive per leaf).
 __global__ void __launch_bounds__(kThreads) karras_kernel(const uint32_t* codes, uint32_t n, kr_bvh_node* nodes,
                                                           uint32_t* parents, uint32_t* first, uint32_t* span) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t internal = n - 1;
-    if (i >= static_cast<int>(internal)) return;
-    const int da = delta(codes, i, i + 1, n), db = delta(codes, i, i - 1, n);
-    const int d = (da - db > 0) - (da - db < 0);
-    const int dmin = delta(codes, i, i - d, n);
-    int lmax = 2;
-    while (delta(codes, i, i + lmax * d, n) > dmin) lmax *= 2;
-    int l = 0;
-    for (int t = lmax / 2; t >= 1; t /= 2)
-        if (delta(codes, i, i + (l + t) * d, n) > dmin) l += t;
-    const int j = i + l * d;
-    const int dnode = delta(codes, i, j, n);
-    int s = 0;
-    for (int t = halve_up(l); t >= 1; t = halve_up(t))
-        if (delta(codes, i, i + (s + t) * d, n) > dnode) s += t;
-    const int split = i + s * d + (d < 0 ? d : 0);
-    const int lo = i < j ? i : j, hi = i < j ? j : i;
-    const uint32_t left = static_cast<uint32_t>(split) + (lo == split ? internal : 0u);
-    const uint32_t right = static_cast<uint32_t>(split) + 1u + (hi == split + 1 ? internal : 0u);
-    parents[left] = static_cast<uint32_t>(i);
-    parents[right] = static_cast<uint32_t>(i);
-    uint32_t* w = reinterpret_cast<uint32_t*>(nodes + i);
-    const uint32_t big = __float_as_uint(3.402823466e+38f), nbig = __float_as_uint(-3.402823466e+38f);
-    w[0] = w[1] = w[2] = big;  // kr_aabb_empty3
-    w[3] = w[4] = w[5] = nbig;
-    w[6] = left;
-    w[7] = right;
-    w[8] = 0;  // nPrimitives 0, axis 0
-    if (first) first[i] = static_cast<uint32_t>(lo);
-    if (span) span[i] = static_cast<uint32_t>(hi - lo + 1);
-    if (i == 0) parents[0] = tree::kNoParent;
+    if (i >= static_cast<int>(n - 1)) return;
+    karras_node(codes, n, i, nodes, parents, first, span);
 }
 
 // Bottom-up bounds, counts and costs; the second thread to reach a node

@@ -33,6 +33,7 @@
 #include <unordered_map>
 
 #include "device_common.cuh"
+#include "obb_device.cuh"
 #include "obb_tree_host.h"
 #include "obvh_transforms.h"
 #include "runtime.h"
@@ -62,16 +63,6 @@ struct Ctl {
     uint32_t total_units;
     uint32_t pad[62];
 };
-
-// Per internal node after the candidate search (96 bytes):
-// axes b0 b1 b2, initial OBB extents lo/hi, AABB lo/hi.
-struct Cand {
-    float ax[9];
-    float olo[3], ohi[3];
-    float alo[3], ahi[3];
-    float pad[3];
-};
-static_assert(sizeof(Cand) == 96, "Cand is 96 bytes");
 
 __device__ __forceinline__ uint32_t count_of(const uint32_t* counts, uint32_t node, uint32_t internal) {
     return node >= internal ? 1u : __ldcg(counts + node);
@@ -424,7 +415,21 @@ __global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* sum
         P[2 * k] = load_vertex(verts, s.ilo[k]);
         P[2 * k + 1] = load_vertex(verts, s.ihi[k]);
     }
-    const Candidate c = node_candidate(P, s);
+    int at = 0;
+    float far = len2_3(sub3(P[1], P[0]));
+#pragma unroll
+    for (int k = 1; k < 7; ++k) {
+        const float d = len2_3(sub3(P[2 * k + 1], P[2 * k]));
+        if (d > far) { far = d; at = k; }
+    }
+    f3 p0 = P[0], p1 = P[1];
+#pragma unroll
+    for (int k = 1; k < 7; ++k)
+        if (at == k) { p0 = P[2 * k]; p1 = P[2 * k + 1]; }
+    PointsK<14> Q;
+#pragma unroll
+    for (int k = 0; k < 14; ++k) Q.p[k] = P[k];
+    const Candidate c = node_candidate<14>(Q, p0, p1, s.lo, s.hi);
     Cand out;
     out.ax[0] = c.b0.x; out.ax[1] = c.b0.y; out.ax[2] = c.b0.z;
     out.ax[3] = c.b1.x; out.ax[4] = c.b1.y; out.ax[5] = c.b1.z;
@@ -459,66 +464,6 @@ __global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* sum
         if (g.thread_rank() == 0) base = atomicAdd(chain.final_count, g.size());
         base = g.shfl(base, 0);
         chain.final_list[base + g.thread_rank()] = a;
-    }
-}
-
-// The box of an internal node from its final extents (finalize_obbs_kernel).
-// The OBB if its half area is strictly smaller than the AABB's, else the AABB
-// (arguments selected first, so that a warp whose lanes differ makes one call).
-__device__ __forceinline__ void finalize_node(const Cand& c, f3 lo, f3 hi, kr_obb3* obb, kr_mat4* xf) {
-    const float aq = half_area3(mk3(c.ahi[0] - c.alo[0], c.ahi[1] - c.alo[1], c.ahi[2] - c.alo[2]));
-    const float oq = half_area3(sub3(hi, lo));
-    const bool o = oq < aq;
-    write_box(obb, xf, o ? mk3(c.ax[0], c.ax[1], c.ax[2]) : mk3(1, 0, 0),
-              o ? mk3(c.ax[3], c.ax[4], c.ax[5]) : mk3(0, 1, 0), o ? mk3(c.ax[6], c.ax[7], c.ax[8]) : mk3(0, 0, 1),
-              o ? lo : mk3(c.alo[0], c.alo[1], c.alo[2]), o ? hi : mk3(c.ahi[0], c.ahi[1], c.ahi[2]));
-}
-
-__device__ __forceinline__ Cand load_cand(const Cand* cand, uint32_t a) {
-    Cand c;
-    float4* d = reinterpret_cast<float4*>(&c);
-    const float4* s = reinterpret_cast<const float4*>(cand + a);
-#pragma unroll
-    for (int q = 0; q < 6; ++q) d[q] = __ldg(s + q);
-    return c;
-}
-
-// projections of one triangle (9 floats) on the three axes, into lo/hi
-// (three-input min/max over the three vertices).
-struct Axes {
-    f3 b0, b1, b2;
-};
-__device__ __forceinline__ Axes make_axes(f3 b0, f3 b1, f3 b2) { return Axes{b0, b1, b2}; }
-__device__ __forceinline__ void project_tri(const float* t, const Axes& ax, float lo[3], float hi[3]) {
-    float q[3][3];
-#pragma unroll
-    for (int v = 0; v < 3; ++v) {
-        const f3 p = mk3(__ldg(t + 3 * v), __ldg(t + 3 * v + 1), __ldg(t + 3 * v + 2));
-        q[0][v] = dot3(p, ax.b0);
-        q[1][v] = dot3(p, ax.b1);
-        q[2][v] = dot3(p, ax.b2);
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        lo[k] = fminf(min3f(lo[k], q[k][0], q[k][1]), q[k][2]);
-        hi[k] = fmaxf(max3f(hi[k], q[k][0], q[k][1]), q[k][2]);
-    }
-}
-
-// project_tri for a triangle in shared memory
-__device__ __forceinline__ void project_tri_s(const float* t, const Axes& ax, float lo[3], float hi[3]) {
-    float q[3][3];
-#pragma unroll
-    for (int v = 0; v < 3; ++v) {
-        const f3 p = mk3(t[3 * v], t[3 * v + 1], t[3 * v + 2]);
-        q[0][v] = dot3(p, ax.b0);
-        q[1][v] = dot3(p, ax.b1);
-        q[2][v] = dot3(p, ax.b2);
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        lo[k] = fminf(min3f(lo[k], q[k][0], q[k][1]), q[k][2]);
-        hi[k] = fmaxf(max3f(hi[k], q[k][0], q[k][1]), q[k][2]);
     }
 }
 
@@ -852,14 +797,15 @@ kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs,
     const uint32_t n = internal + 1;
     const bool tiled = b.chains != nullptr;
     const uint32_t ntiles = (n + kTile - 1) >> kTileShift;
-    ChainArgs chain{tiled ? b.parents : nullptr, b.first, n, tiled ? (2 * ntiles + kThreads - 1) / kThreads : 0u,
+    ChainArgs chain{tiled ? b.parents : nullptr, b.first, n,
+                    tiled ? (2 * ntiles + kThreads - 1) / kThreads : 0u,
                     b.chains, b.chain_counts, b.err, b.ustart, b.total_units};
     if (tiled && !b.parents) return "enqueue_frames: tiled extents need the parents";
     {
         // the chain walks go first, so that they overlap the candidate search
         ProfScope prof_scope_("candidate_kernel", s);
-        candidate_kernel<<<gi + chain.walker_blocks, kThreads, 0, s>>>(b.summary, b.points, b.counts, internal, cand,
-                                                                        b.nunits, b.keys, b.err, chain);
+        candidate_kernel<<<gi + chain.walker_blocks, kThreads, 0, s>>>(b.summary, b.points, b.counts, internal,
+                                                                            cand, b.nunits, b.keys, b.err, chain);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     if (tiled) {

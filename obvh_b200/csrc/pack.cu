@@ -266,6 +266,59 @@ kr_error run_sync(const kr_bvh_node* nodes, const kr_mat4* xfs, kr_bvh_node_pack
     return kr_success;
 }
 
+// One child of the compressed SoA OBVH (kr_cuda_soa_compressed_obvh,
+// transforms.cu:1475-1516): its box (column 1; 1 / column 2, IEEE division
+// as on the host) and its metadata word, shifted left a byte at a time
+// through the bytes of -trunc(127 x), -trunc(127 y), -trunc(127 z) and
+// trunc(127 w) of column 0 (the host's float -> int conversion truncates;
+// the narrowing to a byte keeps the low 8 bits).
+__device__ __forceinline__ uint32_t quant_byte(float v, bool negate) {
+    const float x = v * 127.0f;
+    // x86's cvttss2si: truncation, 0x80000000 outside the int32 range or NaN
+    const uint32_t q = fabsf(x) < 2147483648.0f ? static_cast<uint32_t>(__float2int_rz(x)) : 0x80000000u;
+    return (negate ? 0u - q : q) & 0xFFu;
+}
+
+__device__ __forceinline__ void compress_child(const kr_mat4& m, kr_aabb3* box, int32_t& word) {
+    const float* c = reinterpret_cast<const float*>(&m);  // column-major: column k at c[4k]
+    float* b = reinterpret_cast<float*>(box);
+    b[0] = c[4]; b[1] = c[5]; b[2] = c[6];
+    b[3] = 1.0f / c[8]; b[4] = 1.0f / c[9]; b[5] = 1.0f / c[10];
+    uint32_t w = static_cast<uint32_t>(word);
+    w = (w | quant_byte(c[0], true)) << 8;
+    w = (w | quant_byte(c[1], true)) << 8;
+    w = (w | quant_byte(c[2], true)) << 8;
+    w |= quant_byte(c[3], false);
+    word = static_cast<int32_t>(w);
+}
+
+__global__ void __launch_bounds__(kThreads)
+compress_kernel(const kr_bvh_node_packed* __restrict__ packed, const kr_bvh_transformation_pair* __restrict__ pairs,
+                kr_aabb3* lbounds, kr_aabb3* rbounds, kr_ivec4* meta, uint32_t node_count, uint32_t internal_count) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < node_count; i += gridDim.x * blockDim.x) {
+        const int4 m = __ldg(reinterpret_cast<const int4*>(&packed[i].metadata));
+        kr_ivec4 out;
+        out.x = m.x; out.y = m.y; out.z = m.z; out.w = m.w;
+        if (i < internal_count) {
+            const kr_bvh_transformation_pair p = pairs[i];
+            compress_child(p.l, lbounds + i, out.z);
+            compress_child(p.r, rbounds + i, out.w);
+        }
+        reinterpret_cast<int4*>(meta)[i] = make_int4(out.x, out.y, out.z, out.w);
+    }
+}
+
+kr_error enqueue_compress(const kr_bvh_node_packed* packed, const kr_bvh_transformation_pair* pairs,
+                          kr_aabb3* lbounds, kr_aabb3* rbounds, kr_ivec4* meta, uint32_t internal_count,
+                          uint32_t node_count, cudaStream_t s) {
+    if (node_count == 0) return kr_success;
+    ProfScope prof_scope_("compress_kernel", s);
+    compress_kernel<<<grid_for(node_count), kThreads, 0, s>>>(packed, pairs, lbounds, rbounds, meta, node_count,
+                                                               internal_count);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    return kr_success;
+}
+
 }  // namespace pack
 }  // namespace obvh
 
@@ -346,6 +399,83 @@ extern "C" kr_error obvh_soa_obvh_free(kr_SoA_OBVH* soa_bvh) {
         ce = cudaFree(soa_bvh);
     }
     kr_error e = ce == cudaSuccess ? kr_success : cuda_error(ce);
+    if (e) set_last_error(e);
+    return e;
+}
+
+namespace {
+kr_error soa_compressed(const kr_bvh_node_packed* packed, const kr_bvh_transformation_pair* pairs,
+                        kr_SoA_OBVH_Compressed** soa_bvh, kr_u32 internal_count, kr_u32 node_count) {
+    if (!packed || !pairs || !soa_bvh) return "kr_cuda_soa_compressed_obvh: null pointer argument";
+    if (internal_count > node_count) return "kr_cuda_soa_compressed_obvh: internal_count exceeds node_count";
+    if (!pack::aligned16(packed) || !pack::aligned16(pairs))
+        return "kr_cuda_soa_compressed_obvh: packed records and pairs must be 16-byte aligned";
+    *soa_bvh = nullptr;
+    kr_SoA_OBVH_Compressed h{};
+    void* d = nullptr;
+    cudaError_t ce = cudaMalloc(&d, sizeof(kr_aabb3) * (internal_count ? internal_count : 1));
+    h.lbounds = static_cast<kr_aabb3*>(d);
+    if (ce == cudaSuccess) ce = cudaMalloc(&d, sizeof(kr_aabb3) * (internal_count ? internal_count : 1));
+    if (ce == cudaSuccess) h.rbounds = static_cast<kr_aabb3*>(d);
+    if (ce == cudaSuccess) ce = cudaMalloc(&d, sizeof(kr_ivec4) * (node_count ? node_count : 1));
+    if (ce == cudaSuccess) h.metadata = static_cast<kr_ivec4*>(d);
+    kr_SoA_OBVH_Compressed* d_soa = nullptr;
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_soa, sizeof(kr_SoA_OBVH_Compressed));
+    kr_error e = kr_success;
+    if (ce == cudaSuccess)
+        e = pack::enqueue_compress(packed, pairs, h.lbounds, h.rbounds, h.metadata, internal_count, node_count,
+                                   nullptr);
+    if (ce == cudaSuccess && !e) ce = cudaMemcpy(d_soa, &h, sizeof h, cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess && !e) ce = cudaDeviceSynchronize();
+    if (ce != cudaSuccess || e) {
+        cudaFree(h.lbounds);
+        cudaFree(h.rbounds);
+        cudaFree(h.metadata);
+        cudaFree(d_soa);
+        return e ? e : cuda_error(ce);
+    }
+    *soa_bvh = d_soa;
+    return kr_success;
+}
+}  // namespace
+
+extern "C" kr_error kr_cuda_soa_compressed_obvh(const kr_bvh_node_packed* packed_bvh,
+                                                const kr_bvh_transformation_pair* packed_transforms,
+                                                kr_SoA_OBVH_Compressed** soa_bvh, kr_u32 internal_count,
+                                                kr_u32 node_count) {
+    kr_error e = soa_compressed(packed_bvh, packed_transforms, soa_bvh, internal_count, node_count);
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error obvh_soa_obvh_compressed_free(kr_SoA_OBVH_Compressed* soa_bvh) {
+    if (!soa_bvh) return kr_success;
+    kr_SoA_OBVH_Compressed h{};
+    cudaError_t ce = cudaMemcpy(&h, soa_bvh, sizeof h, cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess) {
+        cudaFree(h.lbounds);
+        cudaFree(h.rbounds);
+        cudaFree(h.metadata);
+        ce = cudaFree(soa_bvh);
+    }
+    kr_error e = ce == cudaSuccess ? kr_success : cuda_error(ce);
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error obvh_soa_compressed_obvh_async(const kr_bvh_node_packed* d_packed,
+                                                   const kr_bvh_transformation_pair* d_pairs, kr_aabb3* d_lbounds,
+                                                   kr_aabb3* d_rbounds, kr_ivec4* d_metadata, kr_u32 internal_count,
+                                                   kr_u32 node_count, void* stream) {
+    kr_error e = kr_success;
+    if (!d_packed || !d_pairs || !d_metadata || (internal_count && (!d_lbounds || !d_rbounds)))
+        e = "obvh_soa_compressed_obvh_async: null pointer argument";
+    else if (internal_count > node_count) e = "obvh_soa_compressed_obvh_async: internal_count exceeds node_count";
+    else if (!pack::aligned16(d_packed) || !pack::aligned16(d_pairs) || !pack::aligned16(d_metadata))
+        e = "obvh_soa_compressed_obvh_async: records, pairs and metadata must be 16-byte aligned";
+    else
+        e = pack::enqueue_compress(d_packed, d_pairs, d_lbounds, d_rbounds, d_metadata, internal_count, node_count,
+                                   static_cast<cudaStream_t>(stream));
     if (e) set_last_error(e);
     return e;
 }

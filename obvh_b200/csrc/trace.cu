@@ -1,6 +1,9 @@
 // trace.cu - closest-hit ray traversal of the SoA OBVH (the layout pack.cu
 // writes): kr_cuda_soa_obvh_intersect (soa_obvh_persistent_intersect,
-// src/ads/common/cuda/intersectors.cu:801-974, launched at :1452-1473).
+// src/ads/common/cuda/intersectors.cu:801-974, launched at :1452-1473), and
+// of the compressed SoA OBVH: kr_cuda_obvh_compressed_persistent_intersect
+// (soa_obvh_compressed_persistent_intersect, :975-1144, launched at
+// :1146-1172), the same kernel with another node test.
 //
 // Each ray follows exactly the reference's per-ray sequence, so results are
 // bit-identical: at an internal node both children's 4x3 transforms map the
@@ -54,14 +57,9 @@ __device__ __forceinline__ M43 load_m43(const kr_mat43* p) {
     return M43{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w}};
 }
 
-// (t0, t1) against the unit cube in the frame of `l`; (1, -1) on a miss
-// (kr_ray_unit_aabb_intersect of kr_n43transform3p / kr_v43transform3p).
-__device__ __forceinline__ float2 unit_box(const M43& l, V3 d, V3 o) {
-    const float* m = l.m;
-    const V3 rd = v3(m[0] * d.x + m[3] * d.y + m[6] * d.z, m[1] * d.x + m[4] * d.y + m[7] * d.z,
-                     m[2] * d.x + m[5] * d.y + m[8] * d.z);
-    const V3 ro = v3(m[0] * o.x + m[3] * o.y + m[6] * o.z + m[9], m[1] * o.x + m[4] * o.y + m[7] * o.z + m[10],
-                     m[2] * o.x + m[5] * o.y + m[8] * o.z + m[11]);
+// (t0, t1) of the ray (rd, ro) against the unit cube [-0.5, 0.5]^3; (1, -1)
+// on a miss (kr_ray_unit_aabb_intersect).
+__device__ __forceinline__ float2 unit_slabs(V3 rd, V3 ro) {
     const float nx = (-0.5f - ro.x) / rd.x, ny = (-0.5f - ro.y) / rd.y, nz = (-0.5f - ro.z) / rd.z;
     const float fx = (0.5f - ro.x) / rd.x, fy = (0.5f - ro.y) / rd.y, fz = (0.5f - ro.z) / rd.z;
     const float t0 = kmax(kmax(kmin(nx, fx), kmin(ny, fy)), kmin(nz, fz));
@@ -69,6 +67,64 @@ __device__ __forceinline__ float2 unit_box(const M43& l, V3 d, V3 o) {
     if (!(t0 <= t1 && t1 > 0.0f)) return make_float2(1.0f, -1.0f);
     return make_float2(t0, t1);
 }
+
+// (t0, t1) against the unit cube in the frame of `l` (kr_n43transform3p /
+// kr_v43transform3p, then kr_ray_unit_aabb_intersect).
+__device__ __forceinline__ float2 unit_box(const M43& l, V3 d, V3 o) {
+    const float* m = l.m;
+    const V3 rd = v3(m[0] * d.x + m[3] * d.y + m[6] * d.z, m[1] * d.x + m[4] * d.y + m[7] * d.z,
+                     m[2] * d.x + m[5] * d.y + m[8] * d.z);
+    const V3 ro = v3(m[0] * o.x + m[3] * o.y + m[6] * o.z + m[9], m[1] * o.x + m[4] * o.y + m[7] * o.z + m[10],
+                     m[2] * o.x + m[5] * o.y + m[8] * o.z + m[11]);
+    return unit_slabs(rd, ro);
+}
+
+// kr_vrotate_angle_axis3 (vecmath.h:1178-1189): Rodrigues' formula, with the
+// reference's cos/sin of a float (cosf, sinf) and its order of operations.
+__device__ __forceinline__ V3 rotate_angle_axis(V3 v, V3 axis, float radians) {
+    const float c = cosf(radians), s = sinf(radians);
+    const float d = dot(axis, v);
+    const V3 x = cross(axis, v);
+    return v3(c * v.x + s * x.x + (1.0f - c) * d * axis.x, c * v.y + s * x.y + (1.0f - c) * d * axis.y,
+              c * v.z + s * x.z + (1.0f - c) * d * axis.z);
+}
+
+// A child of the compressed SoA OBVH (intersectors.cu:1047-1071): the axis
+// and angle dequantised from the metadata word (byte / 127, the angle times
+// the reference's float pi), the ray rotated, offset by `min` and scaled by
+// `max`, then the unit cube.
+__device__ __forceinline__ float2 quant_box(const kr_aabb3* box, int32_t word, V3 d, V3 o) {
+    const float* b = reinterpret_cast<const float*>(box);
+    const V3 lo = v3(__ldg(b), __ldg(b + 1), __ldg(b + 2)), sc = v3(__ldg(b + 3), __ldg(b + 4), __ldg(b + 5));
+    const uint32_t w = static_cast<uint32_t>(word);
+    const V3 axis = v3(static_cast<float>(static_cast<int8_t>(w >> 24)) / 127.0f,
+                       static_cast<float>(static_cast<int8_t>(w >> 16)) / 127.0f,
+                       static_cast<float>(static_cast<int8_t>(w >> 8)) / 127.0f);
+    const float angle = (static_cast<float>(static_cast<int8_t>(w)) / 127.0f) * static_cast<float>(3.14159265359);
+    const V3 rd0 = rotate_angle_axis(d, axis, angle);
+    const V3 ro0 = rotate_angle_axis(sub(o, lo), axis, angle);
+    return unit_slabs(v3(rd0.x * sc.x, rd0.y * sc.y, rd0.z * sc.z), v3(ro0.x * sc.x, ro0.y * sc.y, ro0.z * sc.z));
+}
+
+// Node tests of the two layouts: both children's (t0, t1) at internal node i
+// (m: its metadata).
+struct SoaBoxes {
+    const kr_mat43* __restrict__ left_t;
+    const kr_mat43* __restrict__ right_t;
+    __device__ __forceinline__ void test(int32_t i, const int4& m, V3 d, V3 o, float2& li, float2& ri) const {
+        li = unit_box(load_m43(left_t + i), d, o);
+        ri = unit_box(load_m43(right_t + i), d, o);
+    }
+};
+
+struct QuantBoxes {
+    const kr_aabb3* __restrict__ lbounds;
+    const kr_aabb3* __restrict__ rbounds;
+    __device__ __forceinline__ void test(int32_t i, const int4& m, V3 d, V3 o, float2& li, float2& ri) const {
+        li = quant_box(lbounds + i, m.z, d, o);
+        ri = quant_box(rbounds + i, m.w, d, o);
+    }
+};
 
 __device__ __forceinline__ V3 vertex(const kr_vec3* v, uint32_t i) {
     const float* p = reinterpret_cast<const float*>(v) + 3ull * i;
@@ -115,9 +171,9 @@ __device__ __forceinline__ void finish(const RayState& st, const kr_vec3* verts,
 // every outer step (one descent to a leaf plus the leaves found, the body of
 // the reference's outer loop), so lanes do not wait for the warp's slowest
 // ray.  A ray's own steps are those of the reference, in the same order.
+template <class Boxes>
 __global__ void __launch_bounds__(kThreads)
-trace_kernel(const kr_mat43* __restrict__ left_t, const kr_mat43* __restrict__ right_t,
-             const kr_ivec4* __restrict__ meta, uint32_t internal_count, uint32_t node_count,
+trace_kernel(Boxes boxes, const kr_ivec4* __restrict__ meta, uint32_t internal_count, uint32_t node_count,
              const kr_vec3* __restrict__ verts, const kr_uvec4* __restrict__ faces, uint32_t face_count,
              const kr_u32* __restrict__ prims, uint32_t prim_slots, const kr_ray* __restrict__ rays,
              kr_intersection* isects, uint32_t ray_count, uint32_t per_warp, uint32_t* err) {
@@ -165,8 +221,8 @@ trace_kernel(const kr_mat43* __restrict__ left_t, const kr_mat43* __restrict__ r
                 break;
             }
             const int4 m = __ldg(reinterpret_cast<const int4*>(meta + st.inode));
-            const float2 li = unit_box(load_m43(left_t + st.inode), d, o);
-            const float2 ri = unit_box(load_m43(right_t + st.inode), d, o);
+            float2 li, ri;
+            boxes.test(st.inode, m, d, o, li, ri);
             const bool tl = (li.y >= li.x) && (li.y >= 0.0f) && (li.x <= st.hit_t);
             const bool tr = (ri.y >= ri.x) && (ri.y >= 0.0f) && (ri.x <= st.hit_t);
             int32_t inode = m.x;
@@ -251,11 +307,13 @@ trace_kernel(const kr_mat43* __restrict__ left_t, const kr_mat43* __restrict__ r
 // Persistent grid: every block resident at once (the occupancy of
 // trace_kernel, looked up once per device), and no more blocks than rays
 // need.
+template <class Boxes>
 inline unsigned grid_for(uint32_t n) {
     static int per_sm[64] = {0};
     const DeviceInfo& dev = device_info();
     int& k = per_sm[dev.device & 63];
-    if (k == 0 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, trace_kernel, kThreads, 0) != cudaSuccess) {
+    if (k == 0 &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, trace_kernel<Boxes>, kThreads, 0) != cudaSuccess) {
         (void)cudaGetLastError();
         k = 8;
     }
@@ -265,26 +323,56 @@ inline unsigned grid_for(uint32_t n) {
     return want < cap ? (want ? want : 1u) : cap;
 }
 
+
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+template <class Boxes>
+kr_error launch(const Boxes& boxes, const kr_ivec4* meta, uint32_t internal_count, uint32_t node_count,
+                const kr_vec3* verts, const kr_uvec4* faces, uint32_t face_count, const kr_u32* prims,
+                uint32_t prim_slots, const kr_ray* rays, kr_intersection* isects, uint32_t ray_count, uint32_t* err,
+                cudaStream_t s, const char* name) {
+    const unsigned g = grid_for<Boxes>(ray_count);
+    const uint64_t warps = static_cast<uint64_t>(g) * (kThreads / 32);
+    const uint32_t per_warp = static_cast<uint32_t>((ray_count + warps - 1) / warps);
+    ProfScope prof_scope_(name, s);
+    trace_kernel<Boxes><<<g, kThreads, 0, s>>>(boxes, meta, internal_count, node_count, verts, faces, face_count,
+                                               prims, prim_slots, rays, isects, ray_count, per_warp, err);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    return kr_success;
+}
+
+kr_error check_common(const kr_ivec4* meta, uint32_t internal_count, const kr_vec3* verts, const kr_uvec4* faces,
+                      const kr_ray* rays, kr_intersection* isects, uint32_t* err) {
+    if (!meta || !verts || !faces || !rays || !isects || !err) return "obvh trace: null pointer argument";
+    if (internal_count == 0) return "obvh trace: the tree has no internal node (one primitive) to traverse";
+    if (!aligned16(meta) || !aligned16(faces) || !aligned16(rays))
+        return "obvh trace: metadata, faces and rays must be 16-byte aligned";
+    return kr_success;
+}
 
 kr_error enqueue(const kr_mat43* left_t, const kr_mat43* right_t, const kr_ivec4* meta, uint32_t internal_count,
                  uint32_t node_count, const kr_vec3* verts, const kr_uvec4* faces, uint32_t face_count,
                  const kr_u32* prims, uint32_t prim_slots, const kr_ray* rays, kr_intersection* isects,
                  uint32_t ray_count, uint32_t* err, cudaStream_t s) {
     if (ray_count == 0) return kr_success;
-    if (!left_t || !right_t || !meta || !verts || !faces || !rays || !isects || !err)
-        return "obvh trace: null pointer argument";
-    if (internal_count == 0) return "obvh trace: the tree has no internal node (one primitive) to traverse";
-    if (!aligned16(left_t) || !aligned16(right_t) || !aligned16(meta) || !aligned16(faces) || !aligned16(rays))
-        return "obvh trace: SoA arrays, faces and rays must be 16-byte aligned";
-    const unsigned g = grid_for(ray_count);
-    const uint64_t warps = static_cast<uint64_t>(g) * (kThreads / 32);
-    const uint32_t per_warp = static_cast<uint32_t>((ray_count + warps - 1) / warps);
-    ProfScope prof_scope_("trace_kernel", s);
-    trace_kernel<<<g, kThreads, 0, s>>>(left_t, right_t, meta, internal_count, node_count, verts, faces, face_count,
-                                        prims, prim_slots, rays, isects, ray_count, per_warp, err);
-    OBVH_TRY_CUDA(cudaGetLastError());
-    return kr_success;
+    OBVH_TRY(check_common(meta, internal_count, verts, faces, rays, isects, err));
+    if (!left_t || !right_t) return "obvh trace: null pointer argument";
+    if (!aligned16(left_t) || !aligned16(right_t)) return "obvh trace: SoA arrays must be 16-byte aligned";
+    return launch(SoaBoxes{left_t, right_t}, meta, internal_count, node_count, verts, faces, face_count, prims,
+                  prim_slots, rays, isects, ray_count, err, s, "trace_kernel");
+}
+
+kr_error enqueue_compressed(const kr_aabb3* lbounds, const kr_aabb3* rbounds, const kr_ivec4* meta,
+                            uint32_t internal_count, uint32_t node_count, const kr_vec3* verts, const kr_uvec4* faces,
+                            uint32_t face_count, const kr_u32* prims, uint32_t prim_slots, const kr_ray* rays,
+                            kr_intersection* isects, uint32_t ray_count, uint32_t* err, cudaStream_t s) {
+    if (ray_count == 0) return kr_success;
+    OBVH_TRY(check_common(meta, internal_count, verts, faces, rays, isects, err));
+    if (!lbounds || !rbounds) return "obvh trace: null pointer argument";
+    if ((reinterpret_cast<uintptr_t>(lbounds) & 3) || (reinterpret_cast<uintptr_t>(rbounds) & 3))
+        return "obvh trace: boxes must be 4-byte aligned";
+    return launch(QuantBoxes{lbounds, rbounds}, meta, internal_count, node_count, verts, faces, face_count, prims,
+                  prim_slots, rays, isects, ray_count, err, s, "trace_compressed_kernel");
 }
 
 // The synchronous entry point's error word: one device word owned by the
@@ -355,6 +443,65 @@ extern "C" kr_error obvh_soa_obvh_intersect_async(const kr_mat43* d_left_t, cons
     kr_error e = trace::enqueue(d_left_t, d_right_t, d_metadata, internal_count, node_count, d_vertices, d_faces,
                                 face_count, d_primitives, primitive_slots, d_rays, d_isects, ray_count, d_error,
                                 static_cast<cudaStream_t>(stream));
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error kr_cuda_obvh_compressed_persistent_intersect(const kr_SoA_OBVH_Compressed* bvh,
+                                                                 const kr_vec3* vertices, const kr_uvec4* faces,
+                                                                 const kr_u32* primitives, const kr_ray* rays,
+                                                                 kr_intersection* isects, kr_u32 ray_count,
+                                                                 kr_u32 block_size, kr_u32 grid_size,
+                                                                 kr_u32* warp_counter) {
+    (void)block_size;
+    (void)grid_size;
+    (void)warp_counter;
+    kr_error e = kr_success;
+    if (!bvh) e = "kr_cuda_obvh_compressed_persistent_intersect: null pointer argument";
+    kr_SoA_OBVH_Compressed h{};
+    if (!e) {
+        cudaError_t ce = cudaMemcpy(&h, bvh, sizeof h, cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) e = cuda_error(ce);
+    }
+    if (!e) {
+        // no sizes in the reference's signature: indices are trusted (as in
+        // kr_cuda_soa_obvh_intersect)
+        trace::ErrWord& w = trace::err_word();
+        std::lock_guard<std::mutex> lock(w.mu);
+        e = w.buf.reserve(256);
+        uint32_t* d_err = static_cast<uint32_t*>(w.buf.ptr);
+        if (!e) {
+            cudaError_t ce = cudaMemsetAsync(d_err, 0, 4, nullptr);
+            if (ce != cudaSuccess) e = cuda_error(ce);
+        }
+        if (!e)
+            e = trace::enqueue_compressed(h.lbounds, h.rbounds, h.metadata, 0x7FFFFFFFu, 0x7FFFFFFFu, vertices, faces,
+                                          0x7FFFFFFFu, primitives, 0x7FFFFFFFu, rays, isects, ray_count, d_err,
+                                          nullptr);
+        uint32_t flag = 0;
+        if (!e) {
+            cudaError_t ce = cudaMemcpyAsync(&flag, d_err, 4, cudaMemcpyDeviceToHost, nullptr);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(nullptr);
+            if (ce != cudaSuccess) e = cuda_error(ce);
+        }
+        if (!e && flag)
+            e = "kr_cuda_obvh_compressed_persistent_intersect: a traversal index was negative or a stack passed 64 "
+                "entries";
+    }
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error obvh_soa_compressed_obvh_intersect_async(const kr_aabb3* d_lbounds, const kr_aabb3* d_rbounds,
+                                                             const kr_ivec4* d_metadata, kr_u32 internal_count,
+                                                             kr_u32 node_count, const kr_vec3* d_vertices,
+                                                             const kr_uvec4* d_faces, kr_u32 face_count,
+                                                             const kr_u32* d_primitives, kr_u32 primitive_slots,
+                                                             const kr_ray* d_rays, kr_intersection* d_isects,
+                                                             kr_u32 ray_count, kr_u32* d_error, void* stream) {
+    kr_error e = trace::enqueue_compressed(d_lbounds, d_rbounds, d_metadata, internal_count, node_count, d_vertices,
+                                           d_faces, face_count, d_primitives, primitive_slots, d_rays, d_isects,
+                                           ray_count, d_error, static_cast<cudaStream_t>(stream));
     if (e) set_last_error(e);
     return e;
 }

@@ -75,6 +75,12 @@ __device__ __forceinline__ f3 load_vertex(const kr_vec3* verts, uint32_t i) {
     return mk3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
 }
 
+// load_vertex for vertices written earlier in the same kernel (through L2).
+__device__ __forceinline__ f3 load_vertex_cg(const kr_vec3* verts, uint32_t i) {
+    const float* p = reinterpret_cast<const float*>(verts) + 3 * static_cast<size_t>(i);
+    return mk3(__ldcg(p), __ldcg(p + 1), __ldcg(p + 2));
+}
+
 // ---------------------------------------------------------------------------
 // 4x4 matrices (column-major, kr_mat4).
 struct M4 {
@@ -255,39 +261,36 @@ __device__ __forceinline__ void merge_right(Summary& a, const Summary& b) {
 
 // ---------------------------------------------------------------------------
 // DiTO-14 candidate of one internal node (calculate_candidate_obb_kernel,
-// transforms.cu:676-756, with the helpers at :413-674).  P holds the 14
-// extremal vertices interleaved (min, max) per slab as the reference reads its
-// kr_minmax_pair array.  Outputs the axes and the initial extents along them:
-// on a degenerate base triangle or a flat set the axes are the identity and
-// the extents keep the slab 3..5 values (lo/hi inputs), as in the reference.
+// transforms.cu:676-756, with the helpers at :413-674) from the 14 extremal
+// vertices of its summary (the reference's kr_minmax_pair array: min, max per
+// slab).  Outputs the axes and the initial extents along them: on a
+// degenerate base triangle or a flat set the axes are the identity and the
+// extents keep the slab 3..5 values (lo/hi inputs), as in the reference.
 struct Candidate {
     f3 b0, b1, b2;
     f3 lo, hi;  // slots 3..5
 };
 
-// The 14 summary points.  (Packed two-wide multiplies and adds are each exact,
+// The points of the frame search: the transform passes the 14 summary
+// vertices (K = 14).  (Packed two-wide multiplies and adds are each exact,
 // but a packed multiply feeding a packed add is contracted into a fused
 // multiply-add by the code generator even when both carry .rn, which changes
 // the rounding; the projections therefore stay scalar.)
-struct Points14 {
-    f3 p[14];
+template <int K>
+struct PointsK {
+    f3 p[K];
 };
 
-__device__ __forceinline__ Points14 pack14(const f3* P) {
-    Points14 q;
-#pragma unroll
-    for (int k = 0; k < 14; ++k) q.p[k] = P[k];
-    return q;
-}
-
-// Extent of the 14 points along d: min and max of their projections, two
+// Extent of the K points along d: min and max of their projections, two
 // points per three-input min/max.
-__device__ __forceinline__ void extent_proj(const Points14& Q, f3 d, float& lo, float& hi) {
+template <int K>
+__device__ __forceinline__ void extent_proj(const PointsK<K>& Q, f3 d, float& lo, float& hi) {
+    static_assert(K >= 2 && K % 2 == 0, "an even number of points");
     float a = dot3(Q.p[0], d), b = dot3(Q.p[1], d);
     lo = fminf(a, b);
     hi = fmaxf(a, b);
 #pragma unroll
-    for (int k = 1; k < 7; ++k) {
+    for (int k = 1; k < K / 2; ++k) {
         a = dot3(Q.p[2 * k], d);
         b = dot3(Q.p[2 * k + 1], d);
         lo = min3f(lo, a, b);
@@ -295,14 +298,15 @@ __device__ __forceinline__ void extent_proj(const Points14& Q, f3 d, float& lo, 
     }
 }
 
-// An edge direction of the candidate frames with its extent over the 14
-// points (computed once per node: an edge is shared by up to three frames).
+// An edge direction of the candidate frames with its extent over the points
+// (computed once per node: an edge is shared by up to three frames).
 struct EdgeX {
     f3 d;
     float lo, hi;
 };
 
-__device__ __forceinline__ EdgeX edge_x(const Points14& P, f3 d) {
+template <int K>
+__device__ __forceinline__ EdgeX edge_x(const PointsK<K>& P, f3 d) {
     EdgeX e;
     e.d = d;
     extent_proj(P, d, e.lo, e.hi);
@@ -312,7 +316,8 @@ __device__ __forceinline__ EdgeX edge_x(const Points14& P, f3 d) {
 // One candidate frame: normal n and its three edges in the reference's order.
 // Each edge e spans a box with n and m = e x n; the smallest half area wins,
 // ties to the earlier (frame, edge).
-__device__ __forceinline__ void score_frame(const Points14& P, f3 n, const EdgeX& x0, const EdgeX& x1,
+template <int K>
+__device__ __forceinline__ void score_frame(const PointsK<K>& P, f3 n, const EdgeX& x0, const EdgeX& x1,
                                             const EdgeX& x2, f3* b, f3& blen, f3& bmid, float& best) {
     float nlo, nhi;
     extent_proj(P, n, nlo, nhi);
@@ -335,45 +340,40 @@ __device__ __forceinline__ void score_frame(const Points14& P, f3 n, const EdgeX
     }
 }
 
-__device__ inline Candidate node_candidate(const f3* P, const Summary& s) {
+// The candidate search from the furthest slab pair p0 (min end), p1 (max
+// end) on; ties among the points go to the earliest, as over the
+// reference's kr_minmax_pair array.  lo6/hi6 are the summary's slabs 0..5:
+// the AABB (0..2) and the extents the reference leaves in slots 3..5 of a
+// degenerate node.
+template <int K>
+__device__ inline Candidate node_candidate(const PointsK<K>& Q, f3 p0, f3 p1, const float* lo6, const float* hi6) {
     const float eps = 0.000001f;
     Candidate c;
     c.b0 = mk3(1, 0, 0); c.b1 = mk3(0, 1, 0); c.b2 = mk3(0, 0, 1);
-    c.lo = mk3(s.lo[3], s.lo[4], s.lo[5]);
-    c.hi = mk3(s.hi[3], s.hi[4], s.hi[5]);
+    c.lo = mk3(lo6[3], lo6[4], lo6[5]);
+    c.hi = mk3(hi6[3], hi6[4], hi6[5]);
     const Candidate stale = c;
 
-    float best = half_area3(mk3(s.hi[0] - s.lo[0], s.hi[1] - s.lo[1], s.hi[2] - s.lo[2]));
+    float best = half_area3(mk3(hi6[0] - lo6[0], hi6[1] - lo6[1], hi6[2] - lo6[2]));
     f3 b[3] = {c.b0, c.b1, c.b2};
-    f3 blen = mk3(s.lo[0], s.lo[1], s.lo[2]), bmid = mk3(s.hi[0], s.hi[1], s.hi[2]);
+    f3 blen = mk3(lo6[0], lo6[1], lo6[2]), bmid = mk3(hi6[0], hi6[1], hi6[2]);
 
-    int at = 0;
-    float far = len2_3(sub3(P[1], P[0]));
-#pragma unroll
-    for (int k = 1; k < 7; ++k) {
-        float d = len2_3(sub3(P[2 * k + 1], P[2 * k]));
-        if (d > far) { far = d; at = k; }
-    }
-    f3 p0 = P[0], p1 = P[1];
-#pragma unroll
-    for (int k = 1; k < 7; ++k)
-        if (at == k) { p0 = P[2 * k]; p1 = P[2 * k + 1]; }
     if (len2_3(sub3(p1, p0)) < eps) return stale;
     const f3 e0 = unit3(sub3(p0, p1));
     const float l2 = len2_3(e0);
     f3 p2;
     float fd;
     {
-        f3 u = sub3(P[0], p0);
+        f3 u = sub3(Q.p[0], p0);
         float t = dot3(e0, u);
         fd = len2_3(u) - t * t / l2;
-        p2 = P[0];
+        p2 = Q.p[0];
 #pragma unroll
-        for (int i = 1; i < 14; ++i) {
-            u = sub3(P[i], p0);
+        for (int i = 1; i < K; ++i) {
+            u = sub3(Q.p[i], p0);
             t = dot3(e0, u);
             float d = len2_3(u) - t * t / l2;
-            if (d > fd) { fd = d; p2 = P[i]; }
+            if (d > fd) { fd = d; p2 = Q.p[i]; }
         }
     }
     if (fd < eps) return stale;
@@ -381,13 +381,13 @@ __device__ inline Candidate node_candidate(const f3* P, const Summary& s) {
     const f3 e2 = unit3(sub3(p2, p0));
     const f3 n = unit3(cross3(e1, e0));
 
-    float qlo = dot3(P[0], n), qhi = qlo;
-    f3 q1 = P[0], q0 = P[0];
+    float qlo = dot3(Q.p[0], n), qhi = qlo;
+    f3 q1 = Q.p[0], q0 = Q.p[0];
 #pragma unroll
-    for (int i = 1; i < 14; ++i) {
-        float q = dot3(P[i], n);
-        if (q < qlo) { qlo = q; q1 = P[i]; }
-        if (q > qhi) { qhi = q; q0 = P[i]; }
+    for (int i = 1; i < K; ++i) {
+        float q = dot3(Q.p[i], n);
+        if (q < qlo) { qlo = q; q1 = Q.p[i]; }
+        if (q > qhi) { qhi = q; q0 = Q.p[i]; }
     }
     const float tri = dot3(p0, n);
     const bool up = qhi - eps > tri, down = qlo + eps < tri;
@@ -398,7 +398,6 @@ __device__ inline Candidate node_candidate(const f3* P, const Summary& s) {
     // upper apex q0, then the three to the lower apex q1.  Face r of an apex
     // (r = 0, 1, 2) has the base edge e_r and the apex edges a_{r+1}, a_r
     // (a_i = unit(apex - p_i), indices mod 3) and the normal unit(a_{r+1} x e_r).
-    const Points14 Q = pack14(P);
     EdgeX x0 = edge_x(Q, e0), x1 = edge_x(Q, e1), x2 = edge_x(Q, e2);
     score_frame(Q, n, x0, x1, x2, b, blen, bmid, best);
 #pragma unroll 1

@@ -62,6 +62,8 @@ def _bind():
         "oracle_karras63": (None, [_u64, _u32, c.c_uint32, _i32, _i32, _i32, _i32]),
         "oracle_atrbvh_build": (c.c_int, [_f32, _u32, c.c_uint32, c.c_int, c.c_int, c.c_float, c.c_float, _node,
                                           _u32, _u32, _f32, _u64, _f32]),
+        "oracle_soa_compressed_obvh": (None, [c.c_void_p, c.c_void_p, c.c_uint32, c.c_uint32, c.c_void_p,
+                                              c.c_void_p, c.c_void_p]),
         "oracle_atrbvh_seed": (c.c_int, [_f32, _u32, c.c_uint32, _i32, _i32, _i32, _i32, _f32, _f32, _f32, _u64]),
         "oracle_atrbvh_optimize": (c.c_int, [c.c_uint32, c.c_int, c.c_int, c.c_float, c.c_float, _i32, _i32, _i32,
                                              _i32, _f32, _f32, _f32, _f32]),
@@ -619,6 +621,101 @@ def refgpu_soa_obvh_intersect(left_t, right_t, metadata, verts, faces, prims, ra
             0 if pr is None else pr.size, ry.ctypes.data, n, out.ctypes.data)
     if rc != 0:
         raise RuntimeError(f"refgpu_soa_obvh_intersect: CUDA error {rc}")
+    return out
+
+
+def compressed_pairs(nodes, obbs):
+    """TEST INPUT: transformation pairs in the form the compressed traversal
+    reads (intersectors.cu:1047-1071), one per internal node and child: column
+    0 = the axis and angle / pi of the box-to-world rotation (the packer
+    negates the axis, so the traversal applies world-to-box), column 1 = the
+    box centre, column 2 = twice the half-extents along unit axes (their
+    inverse scales the box to the unit cube).  The reference has no producer
+    of this form (kr_cuda_soa_compressed_obvh has no caller); a left-handed
+    frame is made right-handed by flipping its third axis, which leaves the
+    symmetric box unchanged."""
+    nodes = np.ascontiguousarray(nodes)
+    nn = nodes.shape[0]
+    ni = (nn - 1) // 2
+    obbs = np.asarray(obbs, np.float64).reshape(-1, 15)
+    pairs = np.zeros((ni, 32), np.float32)
+    for side, key in ((0, "left"), (1, "right")):
+        o = obbs[nodes[key][:ni].astype(np.int64)]
+        ax = o[:, 3:12].reshape(-1, 3, 3)
+        ln = np.linalg.norm(ax, axis=2)
+        u = ax / np.maximum(ln, 1e-300)[..., None]  # rows: unit box axes (world -> box)
+        flip = np.linalg.det(u) < 0
+        u[flip, 2] *= -1.0
+        rt = np.transpose(u, (0, 2, 1))  # box -> world
+        ang = np.arccos(np.clip((np.trace(rt, axis1=1, axis2=2) - 1.0) / 2.0, -1.0, 1.0))
+        axis = np.stack([rt[:, 2, 1] - rt[:, 1, 2], rt[:, 0, 2] - rt[:, 2, 0], rt[:, 1, 0] - rt[:, 0, 1]], 1)
+        norm = np.linalg.norm(axis, axis=1, keepdims=True)
+        axis = np.where(norm > 1e-12, axis / np.maximum(norm, 1e-300), np.array([1.0, 0.0, 0.0]))
+        m = np.zeros((ni, 16))
+        m[:, 0:3] = axis
+        m[:, 3] = ang / np.pi
+        m[:, 4:7] = o[:, 0:3]
+        m[:, 8:11] = 2.0 * o[:, 12:15] * ln
+        pairs[:, 16 * side:16 * side + 16] = m
+    return pairs
+
+
+def refgpu_soa_compressed_obvh(packed, pairs, internal_count, node_count, variant: str = "nofma"):
+    """The reference's kr_cuda_soa_compressed_obvh (a host loop between
+    copies) on the GPU build: dict of lbounds, rbounds [ni, 6], metadata
+    [nodes, 4]."""
+    l = ref_gpu(variant)
+    c = ctypes
+    f_ = l.refgpu_soa_compressed_obvh
+    f_.restype = c.c_int
+    f_.argtypes = [c.c_void_p, c.c_void_p, c.c_uint32, c.c_uint32, c.c_void_p, c.c_void_p, c.c_void_p]
+    pk = np.ascontiguousarray(packed).view(np.uint8)
+    pr = np.ascontiguousarray(pairs, np.float32)
+    out = {"lbounds": np.zeros((internal_count, 6), np.float32), "rbounds": np.zeros((internal_count, 6), np.float32),
+           "metadata": np.zeros((node_count, 4), np.int32)}
+    rc = f_(pk.ctypes.data, pr.ctypes.data, internal_count, node_count, out["lbounds"].ctypes.data,
+            out["rbounds"].ctypes.data, out["metadata"].ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"refgpu_soa_compressed_obvh: CUDA error {rc}")
+    return out
+
+
+def refgpu_compressed_intersect(lbounds, rbounds, metadata, verts, faces, prims, rays, variant: str = "nofma"):
+    """The reference's kr_cuda_obvh_compressed_persistent_intersect on the
+    GPU: ISECT records."""
+    l = ref_gpu(variant)
+    c = ctypes
+    f_ = l.refgpu_compressed_intersect
+    f_.restype = c.c_int
+    f_.argtypes = [c.c_void_p] * 3 + [c.c_uint32] * 2 + [c.c_void_p, c.c_uint32, c.c_void_p, c.c_uint32,
+                                                         c.c_void_p, c.c_uint32, c.c_void_p, c.c_uint32, c.c_void_p]
+    lb = np.ascontiguousarray(lbounds, np.float32).reshape(-1, 6)
+    rb = np.ascontiguousarray(rbounds, np.float32).reshape(-1, 6)
+    meta = np.ascontiguousarray(metadata, np.int32).reshape(-1, 4)
+    v, f, nf = _mesh(verts, faces)
+    pr = None if prims is None else np.ascontiguousarray(prims, np.uint32)
+    ry = np.ascontiguousarray(rays).view(np.uint8)
+    n = ry.nbytes // 32
+    out = np.zeros(n, ISECT)
+    rc = f_(lb.ctypes.data, rb.ctypes.data, meta.ctypes.data, lb.shape[0], meta.shape[0], v.ctypes.data, v.size // 3,
+            f.ctypes.data, nf, None if pr is None else pr.ctypes.data, 0 if pr is None else pr.size, ry.ctypes.data,
+            n, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"refgpu_compressed_intersect: CUDA error {rc}")
+    return out
+
+
+def soa_compressed_obvh(packed, pairs, internal_count, node_count):
+    """The oracle's restatement of kr_cuda_soa_compressed_obvh
+    (oracle_soa_compressed_obvh, pack_oracle.c): dict of lbounds, rbounds
+    [ni, 6], metadata [nodes, 4]."""
+    l = _bind()
+    pk = np.ascontiguousarray(packed).view(np.uint8)
+    pr = np.ascontiguousarray(pairs, np.float32)
+    out = {"lbounds": np.zeros((internal_count, 6), np.float32), "rbounds": np.zeros((internal_count, 6), np.float32),
+           "metadata": np.zeros((node_count, 4), np.int32)}
+    l.oracle_soa_compressed_obvh(pk.ctypes.data, pr.ctypes.data, internal_count, node_count,
+                                 out["lbounds"].ctypes.data, out["rbounds"].ctypes.data, out["metadata"].ctypes.data)
     return out
 
 

@@ -63,6 +63,10 @@ int oracle_collapse(const obvh_oracle_node* nodes, const uint32_t* parents, obvh
 /* traversal packing (pack_oracle.c) */
 void oracle_pack(const obvh_oracle_node* nodes, const float* transforms, uint32_t node_count, int with_obbs,
                  void* packed_io, float* pairs_io);
+/* kr_cuda_soa_compressed_obvh's host loop: lbounds/rbounds internal_count x 6,
+ * metadata node_count x 4 (pack_oracle.c). */
+void oracle_soa_compressed_obvh(const void* packed_in, const float* pairs, uint32_t internal_count,
+                                uint32_t node_count, float* lbounds, float* rbounds, int32_t* metadata);
 void oracle_soa_obvh(const void* packed_in, const float* pairs, uint32_t internal_count, uint32_t node_count,
                      float* left_t, float* right_t, int32_t* metadata);
 

@@ -14,6 +14,7 @@
  * (left, right, axis, w) 16; transformation pair 128 = two column-major
  * 4x4 matrices; mat43 48 = the first three rows of each column.
  */
+#include <math.h>
 #include <stdint.h>
 #include <string.h>
 
@@ -69,4 +70,38 @@ void oracle_soa_obvh(const void* packed_in, const float* pairs, uint32_t interna
         }
     }
     for (uint32_t i = 0; i < node_count; i++) memcpy(metadata + 4 * (size_t)i, packed[i].meta, 16);
+}
+
+/* kr_cuda_soa_compressed_obvh's host loop (transforms.cu:1452-1516):
+ * lbounds/rbounds = (column 1, 1 / column 2) of each child's 4x4, metadata
+ * = the record metadata with z (left) and w (right) shifted left a byte at a
+ * time through the bytes of -(int8)(127 c0.x), -(int8)(127 c0.y),
+ * -(int8)(127 c0.z), (int8)(127 c0.w).  The float -> integer conversion is
+ * x86's cvttss2si (truncation; 0x80000000 out of range or NaN), the
+ * narrowing keeps the low 8 bits, as the reference's host build does. */
+static uint32_t quant_byte(float v, int negate) {
+    const float x = v * 127.0f;
+    const uint32_t q = fabsf(x) < 2147483648.0f ? (uint32_t)(int32_t)x : 0x80000000u;
+    return (negate ? 0u - q : q) & 0xFFu;
+}
+
+static void compress_child(const float* m, float* box, int32_t* word) {
+    box[0] = m[4]; box[1] = m[5]; box[2] = m[6];
+    box[3] = 1.0f / m[8]; box[4] = 1.0f / m[9]; box[5] = 1.0f / m[10];
+    uint32_t w = (uint32_t)*word;
+    w = (w | quant_byte(m[0], 1)) << 8;
+    w = (w | quant_byte(m[1], 1)) << 8;
+    w = (w | quant_byte(m[2], 1)) << 8;
+    w |= quant_byte(m[3], 0);
+    *word = (int32_t)w;
+}
+
+void oracle_soa_compressed_obvh(const void* packed_in, const float* pairs, uint32_t internal_count,
+                                uint32_t node_count, float* lbounds, float* rbounds, int32_t* metadata) {
+    const packed_node* packed = (const packed_node*)packed_in;
+    for (uint32_t i = 0; i < node_count; i++) memcpy(metadata + 4 * (size_t)i, packed[i].meta, 16);
+    for (uint32_t i = 0; i < internal_count; i++) {
+        compress_child(pairs + 32 * (size_t)i, lbounds + 6 * (size_t)i, metadata + 4 * (size_t)i + 2);
+        compress_child(pairs + 32 * (size_t)i + 16, rbounds + 6 * (size_t)i, metadata + 4 * (size_t)i + 3);
+    }
 }

@@ -328,3 +328,66 @@ extern "C" int refgpu_soa_obvh_intersect_timed(const float* left_t, const float*
     *ms = total / reps;
     return static_cast<int>(a.err);
 }
+
+// The reference's compressed SoA OBVH (kr_cuda_soa_compressed_obvh,
+// transforms.cu:1452-1535, a host loop between copies): from node_count
+// packed records (64 bytes each) and internal_count transformation pairs
+// (32 floats each), host arrays.  Writes lbounds, rbounds (internal_count x 6
+// floats) and metadata (node_count x 4).  The reference's allocations are
+// freed here (it never frees them).  Returns 0 or the CUDA error code.
+extern "C" int refgpu_soa_compressed_obvh(const void* packed, const float* pairs, uint32_t internal_count,
+                                          uint32_t node_count, float* lbounds, float* rbounds, int32_t* metadata) {
+    if (internal_count == 0 || node_count == 0) return -1;
+    Arena a;
+    auto* d_packed = static_cast<kr_bvh_node_packed*>(a.copy(packed, sizeof(kr_bvh_node_packed) * node_count));
+    auto* d_pairs = static_cast<kr_bvh_transformation_pair*>(
+        a.copy(pairs, sizeof(kr_bvh_transformation_pair) * internal_count));
+    if (a.err != cudaSuccess) return static_cast<int>(a.err);
+    kr_SoA_OBVH_Compressed* d_soa = nullptr;
+    kr_cuda_soa_compressed_obvh(d_packed, d_pairs, d_soa, internal_count, node_count);
+    a.note(cudaGetLastError());
+    a.note(cudaDeviceSynchronize());
+    kr_SoA_OBVH_Compressed h;
+    memset(&h, 0, sizeof h);
+    if (d_soa) a.note(cudaMemcpy(&h, d_soa, sizeof h, cudaMemcpyDeviceToHost));
+    a.back(lbounds, h.lbounds, sizeof(aabb3) * internal_count);
+    a.back(rbounds, h.rbounds, sizeof(aabb3) * internal_count);
+    a.back(metadata, h.metadata, sizeof(ivec4) * node_count);
+    if (d_soa) {
+        cudaFree(h.lbounds);
+        cudaFree(h.rbounds);
+        cudaFree(h.metadata);
+        cudaFree(d_soa);
+    }
+    return static_cast<int>(a.err);
+}
+
+// The reference's compressed traversal (kr_cuda_obvh_compressed_persistent_
+// intersect) on host arrays: lbounds/rbounds internal_count x 6 floats,
+// metadata node_count x 4; the rest as refgpu_soa_obvh_intersect.
+extern "C" int refgpu_compressed_intersect(const float* lbounds, const float* rbounds, const int32_t* metadata,
+                                           uint32_t internal_count, uint32_t node_count, const float* verts,
+                                           uint32_t n_verts, const uint32_t* faces4, uint32_t face_count,
+                                           const uint32_t* prims, uint32_t prim_slots, const float* rays,
+                                           uint32_t ray_count, void* isects) {
+    if (internal_count == 0 || ray_count == 0) return -1;
+    Arena a;
+    kr_SoA_OBVH_Compressed h;
+    h.lbounds = static_cast<aabb3*>(a.copy(lbounds, sizeof(aabb3) * internal_count));
+    h.rbounds = static_cast<aabb3*>(a.copy(rbounds, sizeof(aabb3) * internal_count));
+    h.metadata = static_cast<ivec4*>(a.copy(metadata, sizeof(ivec4) * node_count));
+    auto* d_soa = static_cast<kr_SoA_OBVH_Compressed*>(a.copy(&h, sizeof h));
+    auto* d_verts = static_cast<kr_vec3*>(a.copy(verts, 12ull * n_verts));
+    auto* d_faces = static_cast<kr_uvec4*>(a.copy(faces4, 16ull * face_count));
+    auto* d_prims = prims ? static_cast<u32*>(a.copy(prims, 4ull * prim_slots)) : nullptr;
+    auto* d_rays = static_cast<kr_ray*>(a.copy(rays, sizeof(kr_ray) * ray_count));
+    auto* d_isects = static_cast<kr_intersection*>(a.zeroed(sizeof(kr_intersection) * ray_count));
+    auto* d_counter = static_cast<u32*>(a.zeroed(4));
+    if (a.err != cudaSuccess) return static_cast<int>(a.err);
+    kr_cuda_obvh_compressed_persistent_intersect(d_soa, d_verts, d_faces, d_prims, d_rays, d_isects, ray_count, 128,
+                                                 0, d_counter);
+    a.note(cudaGetLastError());
+    a.note(cudaDeviceSynchronize());
+    a.back(isects, d_isects, sizeof(kr_intersection) * ray_count);
+    return static_cast<int>(a.err);
+}

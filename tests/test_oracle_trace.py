@@ -53,3 +53,44 @@ def test_oracle_traversal_finds_the_closest_hit(n, collapsed):
     miss = want == 0xFFFFFFFF
     assert np.all(hits["barys"][miss] == 0.5)
     assert np.array_equal(hits["normal"][miss], rays["direction"][miss])
+
+
+def _quant(v, negate):
+    """kr_cuda_soa_compressed_obvh's byte of a float (transforms.cu:1482-1485):
+    x86 truncation to int32 (0x80000000 outside the range), then the low
+    8 bits, of -(v * 127) or v * 127, in float arithmetic."""
+    x = np.float32(v) * np.float32(127.0)
+    q = int(np.trunc(x)) & 0xFFFFFFFF if abs(float(x)) < 2.0 ** 31 else 0x80000000
+    return ((-q if negate else q) & 0xFF)
+
+
+def test_compressed_packing_restatement():
+    """The oracle's compressed packing on hand-made records and pairs, held to
+    a separate evaluation of the reference's host loop: boxes (column 1,
+    1 / column 2) and metadata words shifted through the quantised bytes,
+    on top of the records' own words; leaf records copied unchanged."""
+    rng = np.random.default_rng(5)
+    nn, ni = 7, 3
+    packed = np.zeros(nn, ref.PACKED)
+    packed["meta"] = rng.integers(-2 ** 31, 2 ** 31, size=(nn, 4), dtype=np.int64).astype(np.int32)
+    pairs = rng.uniform(-3, 3, size=(ni, 32)).astype(np.float32)
+    pairs[0, 0] = 1e12    # out of the int32 range after scaling
+    pairs[1, 17] = -0.0
+    pairs[2, 3] = np.nan
+    got = ref.soa_compressed_obvh(packed, pairs, ni, nn)
+    for i in range(nn):
+        m = packed["meta"][i].astype(np.int64) & 0xFFFFFFFF
+        want = [int(m[0]), int(m[1]), int(m[2]), int(m[3])]
+        if i < ni:
+            for side in range(2):
+                c = pairs[i, 16 * side:16 * side + 16]
+                w = want[2 + side]
+                for k in range(3):
+                    w = ((w | _quant(c[k], True)) << 8) & 0xFFFFFFFF
+                w |= _quant(c[3], False)
+                want[2 + side] = w
+                box = got["lbounds" if side == 0 else "rbounds"][i]
+                assert np.array_equal(box[:3].view(np.uint32), c[4:7].view(np.uint32))
+                inv = (np.float32(1.0) / c[8:11]).astype(np.float32)
+                assert np.array_equal(box[3:].view(np.uint32), inv.view(np.uint32))
+        assert [int(x) & 0xFFFFFFFF for x in got["metadata"][i]] == want, i

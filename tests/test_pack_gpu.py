@@ -126,3 +126,32 @@ def test_malformed_tree_is_reported():
     f = bvh.obvh_pack(_dev(bad), nn, (nn - 1) // 2, _dev(xfs))
     torch.cuda.synchronize()
     assert int(f["error"].item()) == 1
+
+
+@pytest.mark.parametrize("n,collapse", [(2, True), (3, False), (1000, True), (65_537, True), (300_000, True)])
+@pytest.mark.parametrize("prefill", [False, True])
+def test_compressed_soa_matches_the_oracle_and_the_reference(n, collapse, prefill):
+    """kr_cuda_soa_compressed_obvh on the persistent packing's records and
+    pairs (prefilled records carry random metadata words, which the
+    compression shifts through): byte-identical to the oracle's restatement
+    and to the reference's own host loop; the stream form equals both."""
+    import torch
+    nodes, xfs = _tree(n, 900 + n, collapse)
+    nn = nodes.shape[0]
+    ni = (nn - 1) // 2
+    pk0 = _garbage(nn * 64, 3).view(ref.PACKED) if prefill else np.zeros(nn, ref.PACKED)
+    pr0 = np.zeros((max(ni, 1), 32), np.float32)
+    pk, pr = ref.pack(nodes, xfs, pk0, pr0)
+    want = ref.soa_compressed_obvh(pk, pr, ni, nn)
+    got = bvh.soa_compressed_obvh_sync(_dev(pk), _dev(pr), ni, nn)
+    for k in ("lbounds", "rbounds", "metadata"):
+        assert got[k].tobytes() == want[k].tobytes(), k
+    if ref.ref_gpu_available("nofma"):
+        theirs = ref.refgpu_soa_compressed_obvh(pk, pr, ni, nn)
+        for k in ("lbounds", "rbounds", "metadata"):
+            assert theirs[k].tobytes() == want[k].tobytes(), k
+    s = bvh.soa_compressed_obvh(_dev(pk), _dev(pr).view(torch.float32), ni, nn)
+    torch.cuda.synchronize()
+    assert s["lbounds"].cpu().numpy()[:ni].tobytes() == want["lbounds"].tobytes()
+    assert s["rbounds"].cpu().numpy()[:ni].tobytes() == want["rbounds"].tobytes()
+    assert s["metadata"].cpu().numpy()[:nn].tobytes() == want["metadata"].tobytes()
