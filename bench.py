@@ -366,9 +366,16 @@ def bench_tree_ours(a, dist, atrbvh=False):
     ms_step = total_ms / a.steps
     value = dist.world * nn * a.steps / (total_ms / 1e3) / 1e6
     peak, peak_kind = peaks()
-    kern = kernel_table(prof, a.steps, tree_bytes_per_launch(n), peak)
-    roof = roofline(prof, tree_bytes_per_launch(n), peak, peak_kind,
-                    os.path.join(ROOT, "profiles", f"{wname}_traffic.json"))
+    algo = tree_bytes_per_launch(n)
+    # the fused build searches the candidate frames in two launches per step
+    # (the nodes completed inside CTA blocks, then those across them): their
+    # bytes per step are spread over the launches, so that achieved GB/s is
+    # the step's candidate bytes over the step's candidate time
+    cl = prof.get("candidate_kernel", (0, 0.0))[0] / a.steps
+    if cl > 1:
+        algo["candidate_kernel"] = algo["candidate_kernel"] / cl
+    kern = kernel_table(prof, a.steps, algo, peak)
+    roof = roofline(prof, algo, peak, peak_kind, os.path.join(ROOT, "profiles", f"{wname}_traffic.json"))
     launches = sum(v[0] for v in prof.values())
 
     # End to end through the C ABI: every step copies its mesh in from pinned
@@ -1050,21 +1057,36 @@ def bench_batch_ours(a, dist):
     calls = [(ctypes.c_void_p(base + 12 * int(offsets[s])), int(offsets[s + 1] - offsets[s]),
               ctypes.c_void_p(obase + 60 * s)) for s in range(a.sets)]
 
-    def per_call():
+    def per_call(st):
         for p, n, o in calls:
-            e = lib.obvh_dito_fit_async(p, n, 0, o, W, S)
+            e = lib.obvh_dito_fit_async(p, n, 0, o, W, st)
             if e:
                 _native.check(e)
-    per_call()
+    per_call(S)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = 2
     e0.record(stream)
     for _ in range(reps):
-        per_call()
+        per_call(S)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    host_loop_ms = e0.elapsed_time(e1) / reps
+    # the same per-set launches captured once into a CUDA graph and replayed:
+    # the per-call path without the host's launch overhead, i.e. what the
+    # device itself spends on one fit per call
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        per_call(ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    g.replay()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        g.replay()
     e1.record(stream)
     torch.cuda.synchronize()
     pc_ms = e0.elapsed_time(e1) / reps
+    del g
     pc_value = -dist.max(-(total / (pc_ms / 1e3) / 1e6)) * dist.world
 
     host = torch.empty((total, 3), dtype=torch.float32, pin_memory=True)
@@ -1090,8 +1112,11 @@ def bench_batch_ours(a, dist):
         "kernels": kernel_table(prof, a.steps, batch_bytes, peak),
         "gpu_launches": sum(v[0] for v in prof.values()), "roofline": roof,
         "per_call": {"value": round(pc_value, 3), "unit": "Mpoints/s", "ms_per_batch": round(pc_ms, 3),
-                     "api": "obvh_dito_fit_async per set (2 kernels per set), same device buffer",
-                     "speedup": round(value / pc_value, 2)},
+                     "api": "obvh_dito_fit_async per set (2 kernels per set, grid sized to the set's 2,048-point "
+                            "tiles), same device buffer, the 4,096 calls replayed from one CUDA graph",
+                     "speedup": round(value / pc_value, 2),
+                     "host_loop_ms_per_batch": round(host_loop_ms, 3),
+                     "host_loop_speedup": round(value / (total / (host_loop_ms / 1e3) / 1e6), 2)},
         "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mpoints/s", "h2d_bytes_per_step": 12 * total,
                 "d2h_bytes_per_step": 60 * a.sets + 4, "api": "obvh_points_obb_batch, pinned host"},
         "clocks": clocks,
@@ -1373,7 +1398,11 @@ def bench_serve_ours(a, dist):
     outs = builder.outputs(nmax)
     obb = torch.empty(15, dtype=torch.float32, device=dev)
 
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    device_ms = {"fit": 0.0, "build": 0.0}
+
     def plain(r):
+        ev[0].record(stream)
         if r[0] == "fit":
             p = r[1]
             _native.check(lib.obvh_dito_fit_async(ctypes.c_void_p(p.data_ptr()), r[2], 0, ctypes.c_void_p(obb.data_ptr()),
@@ -1381,10 +1410,13 @@ def bench_serve_ours(a, dist):
         else:
             v, f = r[1]
             builder.build(bvh.Mesh.from_device(v, f), flags=3, ci=1.2, ct=1.0, stream=stream, out=outs)
+        ev[1].record(stream)
         stream.synchronize()
+        device_ms[r[0]] += ev[0].elapsed_time(ev[1])
 
     for r in reqs:  # warm-up over the whole list: workspaces sized, every kernel loaded
         plain(r)
+    device_ms = {"fit": 0.0, "build": 0.0}
     t0 = time.perf_counter()
     for r in reqs:
         plain(r)
@@ -1469,7 +1501,10 @@ def bench_serve_ours(a, dist):
                    "mnodes_per_s": round(nodes / sat["span_s"] / 1e6, 2)},
         "per_call": {"value": round(serial_rps, 3), "unit": "requests/s", "seconds": round(serial_s, 4),
                      "api": "obvh_dito_fit_async / obvh_build_async, one request at a time, each waited for",
-                     "speedup": round(served_rps / serial_rps, 2)},
+                     "speedup": round(served_rps / serial_rps, 2),
+                     "lone_device_ms": {k: round(x, 3) for k, x in device_ms.items()},
+                     "lone_device_note": "each request's own device time in the serial loop (CUDA events around "
+                                         "its kernels, GPU otherwise idle), summed"},
         "poisson_sweep": sweep,
         "kernels": {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()},
         "gpu_launches": sum(v[0] for v in prof.values()),
@@ -1502,10 +1537,21 @@ def extra_workloads(a, dist, line):
         line[key] = sub
         gc.collect()
         torch.cuda.empty_cache()
+    # What any schedule of the served mix needs at least: its build nodes at
+    # the 2M-triangle build's own rate (this line's value, a build that fills
+    # the GPU alone) plus its fit points at 24 B/point at the HBM peak; the
+    # serial per-call time over that bounds the served speed-up on this mix.
+    sv = line["serve"]
+    peak, peak_kind = peaks()
+    floor_s = (sv["config"]["build_nodes"] / (line["value"] * 1e6 / dist.world)
+               + 24 * sv["config"]["points"] / (peak * 1e9))
+    pc = sv["per_call"]
+    pc["speedup_bound"] = round(pc["seconds"] / floor_s, 2)
+    pc["bound_note"] = ("serial per-call seconds over (build nodes at this line's 2M-triangle build rate + fit points "
+                        f"at 24 B/point at the {peak_kind} HBM peak): the mix is build-bound")
     d = line["dito_100M"]
     # the whole fit against 24 B/point (two compulsory passes over 12-byte points)
     fit_gbs = 24 * d["config"]["points_per_gpu"] / (d["ms_per_step"] / 1e3) / 1e9
-    peak, peak_kind = peaks()
     d["fit_roofline"] = {"bound": "hbm", "achieved": round(fit_gbs, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(fit_gbs / peak, 4), "bytes_per_point": 24,
                          "note": f"both passes, one fit per step, peak {peak_kind}"}

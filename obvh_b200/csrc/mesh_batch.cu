@@ -48,7 +48,7 @@ namespace meshbatch {
 using namespace tree;
 
 #ifndef OBVH_MESH_BATCH_THREADS
-#define OBVH_MESH_BATCH_THREADS 512
+#define OBVH_MESH_BATCH_THREADS 256
 #endif
 constexpr int kThreads = OBVH_MESH_BATCH_THREADS;  // one mesh per CTA of this many threads
 constexpr int kCtasPerSm = 512 / kThreads;           // the SM's registers at 128 per thread
@@ -114,6 +114,7 @@ struct Args {
     SlotLayout slot;
     uint32_t* err;
     uint32_t* mesh_slots;  // per mesh: primitive slots of the collapsed leaves
+    float nz;              // -0.0f (tree::mul2)
 };
 
 struct Smem {
@@ -202,22 +203,6 @@ __device__ void sort_pass(const uint32_t* kin, const uint32_t* vin, uint32_t* ko
         }
     }
     stage_sync();
-}
-
-__device__ __forceinline__ void project_tri_cg(const float* t, const obbtree::Axes& ax, float lo[3], float hi[3]) {
-    float q[3][3];
-#pragma unroll
-    for (int v = 0; v < 3; ++v) {
-        const f3 p = mk3(__ldcg(t + 3 * v), __ldcg(t + 3 * v + 1), __ldcg(t + 3 * v + 2));
-        q[0][v] = dot3(p, ax.b0);
-        q[1][v] = dot3(p, ax.b1);
-        q[2][v] = dot3(p, ax.b2);
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        lo[k] = fminf(min3f(lo[k], q[k][0], q[k][1]), q[k][2]);
-        hi[k] = fmaxf(max3f(hi[k], q[k][0], q[k][1]), q[k][2]);
-    }
 }
 
 __device__ __forceinline__ obbtree::Cand load_cand_cg(const obbtree::Cand* cand, uint32_t a) {
@@ -364,25 +349,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
         const kr_vec3* pts = reinterpret_cast<const kr_vec3*>(tris);
         for (uint32_t i = t; i < ni; i += kThreads) {
             Summary s;
-            load_summary(summary + 7 * static_cast<size_t>(i), s);
-            PointsK<14> P;
-#pragma unroll
-            for (int k = 0; k < 7; ++k) {
-                P.p[2 * k] = load_vertex_cg(pts, s.ilo[k]);
-                P.p[2 * k + 1] = load_vertex_cg(pts, s.ihi[k]);
-            }
-            int at = 0;
-            float far = len2_3(sub3(P.p[1], P.p[0]));
-#pragma unroll
-            for (int k = 1; k < 7; ++k) {
-                const float d = len2_3(sub3(P.p[2 * k + 1], P.p[2 * k]));
-                if (d > far) { far = d; at = k; }
-            }
-            f3 p0 = P.p[0], p1 = P.p[1];
-#pragma unroll
-            for (int k = 1; k < 7; ++k)
-                if (at == k) { p0 = P.p[2 * k]; p1 = P.p[2 * k + 1]; }
-            const Candidate c = node_candidate<14>(P, p0, p1, s.lo, s.hi);
+            const Candidate c = summary_candidate<true>(summary, pts, i, a.nz, s);
             obbtree::Cand out;
             out.ax[0] = c.b0.x; out.ax[1] = c.b0.y; out.ax[2] = c.b0.z;
             out.ax[3] = c.b1.x; out.ax[4] = c.b1.y; out.ax[5] = c.b1.z;
@@ -405,10 +372,10 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
             if (cnt > kThreadLeaves) continue;
             const obbtree::Cand c = load_cand_cg(cand, i);
             const obbtree::Axes ax = obbtree::make_axes(mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
-                                                        mk3(c.ax[6], c.ax[7], c.ax[8]));
+                                                        mk3(c.ax[6], c.ax[7], c.ax[8]), a.nz);
             float lo[3] = {c.olo[0], c.olo[1], c.olo[2]}, hi[3] = {c.ohi[0], c.ohi[1], c.ohi[2]};
             const float* tp = tris + 9 * static_cast<size_t>(__ldcg(first + i));
-            for (uint32_t k = 0; k < cnt; ++k) project_tri_cg(tp + 9 * k, ax, lo, hi);
+            for (uint32_t k = 0; k < cnt; ++k) obbtree::project_tri_cg(tp + 9 * k, ax, lo, hi);
             obbtree::finalize_node(c, mk3(lo[0], lo[1], lo[2]), mk3(hi[0], hi[1], hi[2]), obbs + i, xfs + i);
         }
         for (uint32_t i = w; i < ni; i += kWarps) {
@@ -416,10 +383,10 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
             if (cnt <= kThreadLeaves) continue;
             const obbtree::Cand c = load_cand_cg(cand, i);
             const obbtree::Axes ax = obbtree::make_axes(mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
-                                                        mk3(c.ax[6], c.ax[7], c.ax[8]));
+                                                        mk3(c.ax[6], c.ax[7], c.ax[8]), a.nz);
             float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
             const float* tp = tris + 9 * static_cast<size_t>(__ldcg(first + i));
-            for (uint32_t k = lane; k < cnt; k += 32) project_tri_cg(tp + 9 * k, ax, lo, hi);
+            for (uint32_t k = lane; k < cnt; k += 32) obbtree::project_tri_cg(tp + 9 * k, ax, lo, hi);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 lo[k] = fminf(c.olo[k], warp_min(lo[k]));
@@ -601,6 +568,7 @@ kr_error enqueue(Plan& P, const Buffers& b, cudaStream_t s) {
         a.slot = P.slot;
         a.err = status;
         a.mesh_slots = status + 2;
+        a.nz = -0.0f;
         ProfScope prof_scope_("mesh_batch_kernel", s);
         mesh_batch_kernel<<<P.grid, kThreads, 0, s>>>(a);
         OBVH_TRY_CUDA(cudaGetLastError());

@@ -366,6 +366,11 @@ struct ChainArgs {
     uint32_t* err;
     uint32_t* final_list;     // tiles: the nodes finalize_list_kernel finishes
     uint32_t* final_count;
+    float nz;                 // -0.0f (tree::mul2)
+    uint32_t which;           // FrameNodes: all nodes, or those inside / across aligned leaf blocks
+    uint32_t block_shift;     // the blocks hold 2^block_shift leaves
+    const uint32_t* list;     // kAcross: the nodes, list_count of them
+    const uint32_t* list_count;
 };
 
 // The ancestors of tile tau's first leaf (side 0) and last leaf (side 1) whose
@@ -393,43 +398,13 @@ __device__ void walk_chain(const ChainArgs& c, const uint32_t* counts, uint32_t 
     c.chain_counts[w] = count;
 }
 
-__global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* summary, const kr_vec3* verts,
-                                                             const uint32_t* counts, uint32_t internal, Cand* cand,
-                                                             uint32_t* nunits, uint32_t* keys, const uint32_t* err,
-                                                             ChainArgs chain) {
-    if (blockIdx.x < chain.walker_blocks) {
-        if (!*err) walk_chain(chain, counts, blockIdx.x * blockDim.x + threadIdx.x);
-        return;
-    }
-    const uint32_t a = (blockIdx.x - chain.walker_blocks) * blockDim.x + threadIdx.x;
-    if (a >= internal) return;
-    if (*err) {  // malformed tree: no summaries to read; nothing is scheduled after this
-        nunits[a] = 0;
-        return;
-    }
+// The candidate of internal node a and its extents plan (nunits, keys, the
+// finalize list).
+__device__ __forceinline__ void candidate_node(uint32_t a, const uint4* summary, const kr_vec3* verts,
+                                               const uint32_t* counts, Cand* cand, uint32_t* nunits, uint32_t* keys,
+                                               const ChainArgs& chain) {
     Summary s;
-    load_summary(summary + 7 * static_cast<size_t>(a), s);
-    f3 P[14];
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-        P[2 * k] = load_vertex(verts, s.ilo[k]);
-        P[2 * k + 1] = load_vertex(verts, s.ihi[k]);
-    }
-    int at = 0;
-    float far = len2_3(sub3(P[1], P[0]));
-#pragma unroll
-    for (int k = 1; k < 7; ++k) {
-        const float d = len2_3(sub3(P[2 * k + 1], P[2 * k]));
-        if (d > far) { far = d; at = k; }
-    }
-    f3 p0 = P[0], p1 = P[1];
-#pragma unroll
-    for (int k = 1; k < 7; ++k)
-        if (at == k) { p0 = P[2 * k]; p1 = P[2 * k + 1]; }
-    PointsK<14> Q;
-#pragma unroll
-    for (int k = 0; k < 14; ++k) Q.p[k] = P[k];
-    const Candidate c = node_candidate<14>(Q, p0, p1, s.lo, s.hi);
+    const Candidate c = summary_candidate<false>(summary, verts, a, chain.nz, s);
     Cand out;
     out.ax[0] = c.b0.x; out.ax[1] = c.b0.y; out.ax[2] = c.b0.z;
     out.ax[3] = c.b1.x; out.ax[4] = c.b1.y; out.ax[5] = c.b1.z;
@@ -467,11 +442,50 @@ __global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* sum
     }
 }
 
+__global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* summary, const kr_vec3* verts,
+                                                             const uint32_t* counts, uint32_t internal, Cand* cand,
+                                                             uint32_t* nunits, uint32_t* keys, const uint32_t* err,
+                                                             ChainArgs chain) {
+    if (chain.which == static_cast<uint32_t>(FrameNodes::kAcross)) {
+        // the listed nodes (written by the walk that completed them), a
+        // grid-stride loop so that warps stay full
+        const uint32_t total = min(*chain.list_count, internal);
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+            const uint32_t a = chain.list[i];
+            if (a >= internal) {
+                atomicOr(chain.err, kErrBadInput);
+                continue;
+            }
+            if (*err) {
+                nunits[a] = 0;
+                continue;
+            }
+            candidate_node(a, summary, verts, counts, cand, nunits, keys, chain);
+        }
+        return;
+    }
+    if (blockIdx.x < chain.walker_blocks) {
+        if (!*err) walk_chain(chain, counts, blockIdx.x * blockDim.x + threadIdx.x);
+        return;
+    }
+    const uint32_t a = (blockIdx.x - chain.walker_blocks) * blockDim.x + threadIdx.x;
+    if (a >= internal) return;
+    if (chain.which == static_cast<uint32_t>(FrameNodes::kInside)) {
+        const uint32_t f = __ldg(chain.first + a), cnt = __ldg(counts + a);
+        if ((f >> chain.block_shift) != ((f + cnt - 1) >> chain.block_shift)) return;
+    }
+    if (*err) {  // malformed tree: no summaries to read; nothing is scheduled after this
+        nunits[a] = 0;
+        return;
+    }
+    candidate_node(a, summary, verts, counts, cand, nunits, keys, chain);
+}
+
 // Nodes of at most kThreadMax leaves: one thread each, finalised here.
 __global__ void __launch_bounds__(kThreads) extents_small_kernel(const Cand* cand, const uint32_t* counts,
                                                                  const uint32_t* first, const float* tris,
                                                                  uint32_t internal, kr_obb3* obbs, kr_mat4* xfs,
-                                                                 const uint32_t* err) {
+                                                                 const uint32_t* err, float nz) {
     const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= internal || *err) return;
     const uint32_t cnt = counts[a];
@@ -480,7 +494,7 @@ __global__ void __launch_bounds__(kThreads) extents_small_kernel(const Cand* can
     const f3 b0 = mk3(c.ax[0], c.ax[1], c.ax[2]), b1 = mk3(c.ax[3], c.ax[4], c.ax[5]), b2 = mk3(c.ax[6], c.ax[7], c.ax[8]);
     float lo[3] = {c.olo[0], c.olo[1], c.olo[2]}, hi[3] = {c.ohi[0], c.ohi[1], c.ohi[2]};
     const float* t = tris + 9 * static_cast<size_t>(first[a]);
-    const Axes ax = make_axes(b0, b1, b2);
+    const Axes ax = make_axes(b0, b1, b2, nz);
     for (uint32_t i = 0; i < cnt; ++i) project_tri(t + 9 * i, ax, lo, hi);
     finalize_node(c, mk3(lo[0], lo[1], lo[2]), mk3(hi[0], hi[1], hi[2]), obbs + a, xfs + a);
 }
@@ -491,7 +505,7 @@ __global__ void __launch_bounds__(kThreads) extents_units_kernel(const Cand* can
                                                                  const uint32_t* nunits, const uint32_t* unit_start,
                                                                  uint32_t internal, const uint32_t* err,
                                                                  const uint32_t* total_units, uint32_t* keys,
-                                                                 kr_obb3* obbs, kr_mat4* xfs) {
+                                                                 kr_obb3* obbs, kr_mat4* xfs, float nz) {
     const int lane = threadIdx.x & 31;
     const uint32_t total = *err ? 0u : *total_units;
     // Warps take runs of kUnitRun consecutive units round-robin: one binary
@@ -521,7 +535,7 @@ __global__ void __launch_bounds__(kThreads) extents_units_kernel(const Cand* can
                      b2 = mk3(c.ax[6], c.ax[7], c.ax[8]);
             float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
             const float* t = tris + 9 * static_cast<size_t>(__ldg(first + a));
-            const Axes ax = make_axes(b0, b1, b2);
+            const Axes ax = make_axes(b0, b1, b2, nz);
             for (uint32_t i = begin + lane; i < end; i += 32) project_tri(t + 9 * static_cast<size_t>(i), ax, lo, hi);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
@@ -556,7 +570,7 @@ __global__ void __launch_bounds__(kThreads) extents_tile_kernel(const Cand* cand
                                                                 const uint32_t* first, const float* tris, uint32_t n,
                                                                 const uint32_t* chains, const uint32_t* chain_counts,
                                                                 uint32_t* keys, kr_obb3* obbs, kr_mat4* xfs,
-                                                                const uint32_t* err) {
+                                                                const uint32_t* err, float nz) {
     __shared__ __align__(16) float tri[kTile * 9];
     __shared__ uint32_t item_node[kTileItems];
     __shared__ uint16_t item_b[kTileItems], item_e[kTileItems];
@@ -590,7 +604,7 @@ __global__ void __launch_bounds__(kThreads) extents_tile_kernel(const Cand* cand
         // list full: this thread does the item alone
         const Cand c = load_cand(cand, a);
         const Axes ax = make_axes(mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
-                                  mk3(c.ax[6], c.ax[7], c.ax[8]));
+                                  mk3(c.ax[6], c.ax[7], c.ax[8]), nz);
         float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
         for (uint32_t i = b; i < e; ++i) project_tri_s(tri + 9 * i, ax, lo, hi);
         for (int k = 0; k < 3; ++k) {
@@ -614,7 +628,7 @@ __global__ void __launch_bounds__(kThreads) extents_tile_kernel(const Cand* cand
             const Cand c = load_cand(cand, a);
             float lo[3] = {c.olo[0], c.olo[1], c.olo[2]}, hi[3] = {c.ohi[0], c.ohi[1], c.ohi[2]};
             const Axes ax = make_axes(mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
-                                      mk3(c.ax[6], c.ax[7], c.ax[8]));
+                                      mk3(c.ax[6], c.ax[7], c.ax[8]), nz);
             const float* tp = tri + 9 * (f - t0);
             for (uint32_t k = 0; k < cnt; ++k) project_tri_s(tp + 9 * k, ax, lo, hi);
             finalize_node(c, mk3(lo[0], lo[1], lo[2]), mk3(hi[0], hi[1], hi[2]), obbs + a, xfs + a);
@@ -644,7 +658,7 @@ __global__ void __launch_bounds__(kThreads) extents_tile_kernel(const Cand* cand
         const uint32_t b = item_b[it], e = item_e[it];
         const Cand c = load_cand(cand, a);
         const Axes ax = make_axes(mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
-                                  mk3(c.ax[6], c.ax[7], c.ax[8]));
+                                  mk3(c.ax[6], c.ax[7], c.ax[8]), nz);
         float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
         for (uint32_t i = b + lane; i < e; i += 32) project_tri_s(tri + 9 * i, ax, lo, hi);
 #pragma unroll
@@ -790,29 +804,59 @@ size_t cand_bytes(uint32_t internal) { return sizeof(Cand) * (internal > 0 ? int
 size_t chain_bytes(uint32_t n) { return 2ull * kChain * 4 * (((n > 0 ? n : 1) + kTile - 1) >> kTileShift); }
 size_t chain_count_bytes(uint32_t n) { return 2ull * 4 * (((n > 0 ? n : 1) + kTile - 1) >> kTileShift); }
 
+namespace {
+ChainArgs chain_args(const FrameBuffers& b, uint32_t internal, FrameNodes which, uint32_t block_shift) {
+    const uint32_t n = internal + 1;
+    const bool tiled = b.chains != nullptr;
+    const uint32_t ntiles = (n + kTile - 1) >> kTileShift;
+    // the chain walks ride along with the first (or only) candidate launch
+    const bool walks = tiled && which != FrameNodes::kAcross;
+    return ChainArgs{tiled ? b.parents : nullptr, b.first, n,
+                     walks ? (2 * ntiles + kThreads - 1) / kThreads : 0u,
+                     b.chains, b.chain_counts, b.err, b.ustart, b.total_units, -0.0f,
+                     static_cast<uint32_t>(which), block_shift, b.across_list, b.across_count};
+}
+}  // namespace
+
+kr_error enqueue_candidates(const FrameBuffers& b, uint32_t internal, FrameNodes which, uint32_t block_shift,
+                            cudaStream_t s) {
+    if (internal == 0) return kr_success;
+    const bool tiled = b.chains != nullptr;
+    if (tiled && !b.parents) return "enqueue_frames: tiled extents need the parents";
+    if (which != FrameNodes::kAll && (!tiled || block_shift > 31))
+        return "enqueue_candidates: node classes need the tiled path and a block shift below 32";
+    if (which == FrameNodes::kAcross && (!b.across_list || !b.across_count))
+        return "enqueue_candidates: the nodes across blocks come as a list";
+    const ChainArgs chain = chain_args(b, internal, which, block_shift);
+    // kAcross loops over its list: two CTAs per SM
+    const unsigned gi = which == FrameNodes::kAcross ? 2u * static_cast<unsigned>(device_info().sm_count)
+                                                     : (internal + kThreads - 1) / kThreads;
+    // the chain walks go first, so that they overlap the candidate search
+    ProfScope prof_scope_("candidate_kernel", s);
+    candidate_kernel<<<gi + chain.walker_blocks, kThreads, 0, s>>>(b.summary, b.points, b.counts, internal,
+                                                                        static_cast<Cand*>(b.cand), b.nunits, b.keys,
+                                                                        b.err, chain);
+    OBVH_TRY_CUDA(cudaGetLastError());
+    return kr_success;
+}
+
 kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs, kr_mat4* xfs, cudaStream_t s) {
+    OBVH_TRY(enqueue_candidates(b, internal, FrameNodes::kAll, 0, s));
+    return enqueue_extents(b, internal, obbs, xfs, s);
+}
+
+kr_error enqueue_extents(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs, kr_mat4* xfs, cudaStream_t s) {
     if (internal == 0) return kr_success;
     const unsigned gi = (internal + kThreads - 1) / kThreads;
     Cand* cand = static_cast<Cand*>(b.cand);
     const uint32_t n = internal + 1;
     const bool tiled = b.chains != nullptr;
     const uint32_t ntiles = (n + kTile - 1) >> kTileShift;
-    ChainArgs chain{tiled ? b.parents : nullptr, b.first, n,
-                    tiled ? (2 * ntiles + kThreads - 1) / kThreads : 0u,
-                    b.chains, b.chain_counts, b.err, b.ustart, b.total_units};
-    if (tiled && !b.parents) return "enqueue_frames: tiled extents need the parents";
-    {
-        // the chain walks go first, so that they overlap the candidate search
-        ProfScope prof_scope_("candidate_kernel", s);
-        candidate_kernel<<<gi + chain.walker_blocks, kThreads, 0, s>>>(b.summary, b.points, b.counts, internal,
-                                                                            cand, b.nunits, b.keys, b.err, chain);
-    }
-    OBVH_TRY_CUDA(cudaGetLastError());
     if (tiled) {
         {
             ProfScope prof_scope_("extents_tile_kernel", s);
             extents_tile_kernel<<<ntiles, kThreads, 0, s>>>(cand, b.counts, b.first, b.tris, n, b.chains,
-                                                            b.chain_counts, b.keys, obbs, xfs, b.err);
+                                                            b.chain_counts, b.keys, obbs, xfs, b.err, -0.0f);
         }
         OBVH_TRY_CUDA(cudaGetLastError());
         {
@@ -827,7 +871,8 @@ kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs,
     }
     {
         ProfScope prof_scope_("extents_small_kernel", s);
-        extents_small_kernel<<<gi, kThreads, 0, s>>>(cand, b.counts, b.first, b.tris, internal, obbs, xfs, b.err);
+        extents_small_kernel<<<gi, kThreads, 0, s>>>(cand, b.counts, b.first, b.tris, internal, obbs, xfs, b.err,
+                                                     -0.0f);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     OBVH_TRY(exclusive_scan_u32(b.nunits, b.ustart, internal, b.total_units, b.scan, s));
@@ -835,7 +880,7 @@ kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs,
     {
         ProfScope prof_scope_("extents_units_kernel", s);
         extents_units_kernel<<<grid, kThreads, 0, s>>>(cand, b.counts, b.first, b.tris, b.nunits, b.ustart, internal,
-                                                       b.err, b.total_units, b.keys, obbs, xfs);
+                                                       b.err, b.total_units, b.keys, obbs, xfs, -0.0f);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     {

@@ -67,11 +67,25 @@ struct FrameBuffers {
     const uint32_t* parents = nullptr;
     uint32_t* chains = nullptr;        // chain_bytes(n)
     uint32_t* chain_counts = nullptr;  // chain_count_bytes(n)
+    // FrameNodes::kAcross: those nodes, as a list of across_count entries
+    const uint32_t* across_list = nullptr;
+    const uint32_t* across_count = nullptr;
 };
 size_t cand_bytes(uint32_t internal);
 size_t chain_bytes(uint32_t n);
 size_t chain_count_bytes(uint32_t n);
 kr_error enqueue_frames(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs, kr_mat4* xfs, cudaStream_t s);
+
+// enqueue_frames in two parts, so that candidate frames can be searched for
+// part of the nodes while another stream completes the summaries of the rest.
+// Tiled path only.  With block_shift = b, the nodes whose leaves lie inside
+// one aligned block of 2^b leaves are kInside, the others kAcross (given as
+// the list b.across_list, e.g. written by the walk that completes them).
+enum class FrameNodes : uint32_t { kAll = 0, kInside = 1, kAcross = 2 };
+kr_error enqueue_candidates(const FrameBuffers& b, uint32_t internal, FrameNodes which, uint32_t block_shift,
+                            cudaStream_t s);
+// The extents and final boxes, after the candidates of every node.
+kr_error enqueue_extents(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs, kr_mat4* xfs, cudaStream_t s);
 
 }  // namespace obbtree
 }  // namespace obvh

@@ -39,13 +39,16 @@ namespace pipeline {
 using namespace tree;
 
 constexpr int kThreads = 256;
+constexpr uint32_t kLocalShift = 8;  // fused_up_local covers 2^kLocalShift = kThreads leaves per CTA
+static_assert((1 << kLocalShift) == kThreads, "CTA leaf blocks are aligned powers of two");
 
 struct Ctl {
     uint32_t error;
     uint32_t total_units;
     uint32_t total_slots;
     uint32_t frontier;  // walks left for the cross-CTA pass
-    uint32_t pad[60];
+    uint32_t across;    // nodes the cross-CTA pass completed (listed at Layout::across)
+    uint32_t pad[59];
 };
 
 // Writes `words` staged words to dst with coalesced stores: 4-byte stores up
@@ -515,7 +518,9 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(const uint32_t* sizes,
 #pragma unroll
     for (uint32_t q = 0; q < kMaxLeafSize; ++q)
         if (q < pos) primitives[off + q] = out[q];
-    counts[c] = pos;
+    // pos equals cnt for a permutation order; the count is rewritten only if
+    // not, so that the OBB extents (on another stream) read it undisturbed
+    if (pos != cnt) counts[c] = pos;
     uint32_t* cw = reinterpret_cast<uint32_t*>(collapsed + c);
     cw[6] = off;
     cw[8] = (cw[8] & 0xffff0000u) | pos;
@@ -526,7 +531,7 @@ size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
 struct Layout {
     size_t lbvh, ctl, first, tris, summary, flags, cand, nunits, ustart, keys, sizes, offsets, scan, frontier, chains,
-        chain_counts, total;
+        chain_counts, across, total;
 };
 
 Layout layout(uint32_t n) {
@@ -550,6 +555,7 @@ Layout layout(uint32_t n) {
     L.frontier = o; o += align256(4 * nn);
     L.chains = o;   o += align256(obbtree::chain_bytes(n));
     L.chain_counts = o; o += align256(obbtree::chain_count_bytes(n));
+    L.across = o;   o += align256(4 * ni);
     L.total = o;
     return L;
 }
@@ -603,27 +609,17 @@ kr_error enqueue(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32
     if (internal > 0) OBVH_TRY_CUDA(cudaMemsetAsync(c.visits, 0, 4ull * internal, s));
     if (want_collapse) OBVH_TRY_CUDA(cudaMemsetAsync(cflags, 0, nn, s));
     OBVH_TRY(allow_dynamic_smem(reinterpret_cast<const void*>(fused_up_local_kernel), kFusedSmemBytes));
-    {
-        UpArgs a{nodes, want_collapse ? collapsed : nullptr, parents, first, tris, n, counts, costs,
-                 want_collapse ? cflags : nullptr, ci, ct, want_obbs ? summary : nullptr, c.visits, &ctl->error};
-        uint32_t* frontier = reinterpret_cast<uint32_t*>(ws + L.frontier);
-        {
-            ProfScope prof_scope_("fused_up_local_kernel", s);
-            fused_up_local_kernel<<<gn, kThreads, kFusedSmemBytes, s>>>(a, frontier, &ctl->frontier);
-        }
-        OBVH_TRY_CUDA(cudaGetLastError());
-        // at most one walk per leaf and per internal node; most of the grid
-        // finds nothing to do, so it is capped at a few CTAs per SM
-        const unsigned cap = 8u * static_cast<unsigned>(device_info().sm_count);
-        const unsigned gx = (nn + kThreads - 1) / kThreads;
-        {
-            ProfScope prof_scope_("fused_up_cross_kernel", s);
-            fused_up_cross_kernel<<<gx < cap ? gx : cap, kThreads, 0, s>>>(a, frontier, &ctl->frontier);
-        }
-    }
-    OBVH_TRY_CUDA(cudaGetLastError());
-    if (want_obbs && internal > 0) {
-        obbtree::FrameBuffers fb;
+    // Two helper streams.  aux[0] (the highest priority, so that its CTAs
+    // are placed first) takes the latency-bound walk up the top of the tree
+    // and then the candidate frames of the nodes it completed, while the
+    // caller's stream searches the frames of the nodes fused_up_local
+    // completed; aux[1] takes the collapse's gather beside the extents.
+    const bool frames = want_obbs && internal > 0;
+    ForkStreams* fk = nullptr;
+    OBVH_TRY(fork_streams(s, &fk));
+    obbtree::FrameBuffers fb;
+    uint32_t* across = reinterpret_cast<uint32_t*>(ws + L.across);
+    if (frames) {
         fb.summary = summary;
         fb.points = reinterpret_cast<const kr_vec3*>(tris);
         fb.counts = counts;
@@ -639,25 +635,63 @@ kr_error enqueue(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32
         fb.parents = parents;
         fb.chains = reinterpret_cast<uint32_t*>(ws + L.chains);
         fb.chain_counts = reinterpret_cast<uint32_t*>(ws + L.chain_counts);
-        OBVH_TRY(obbtree::enqueue_frames(fb, internal, obbs, xfs, s));
+        fb.across_list = across;
+        fb.across_count = &ctl->across;
     }
-    if (want_collapse) {
-        uint32_t* sizes = reinterpret_cast<uint32_t*>(ws + L.sizes);
-        uint32_t* offsets = reinterpret_cast<uint32_t*>(ws + L.offsets);
-        const unsigned gnn = (nn + kThreads - 1) / kThreads;
+    {
+        UpArgs a{nodes, want_collapse ? collapsed : nullptr, parents, first, tris, n, counts, costs,
+                 want_collapse ? cflags : nullptr, ci, ct, want_obbs ? summary : nullptr, c.visits, &ctl->error};
+        uint32_t* frontier = reinterpret_cast<uint32_t*>(ws + L.frontier);
         {
-            ProfScope prof_scope_("roots_kernel", s);
-            roots_kernel<<<gnn, kThreads, 0, s>>>(parents, cflags, counts, nn, sizes, &ctl->error);
+            ProfScope prof_scope_("fused_up_local_kernel", s);
+            fused_up_local_kernel<<<gn, kThreads, kFusedSmemBytes, s>>>(a, frontier, &ctl->frontier);
         }
         OBVH_TRY_CUDA(cudaGetLastError());
-        OBVH_TRY(exclusive_scan_u32(sizes, offsets, nn, &ctl->total_slots, ws + L.scan, s));
+        OBVH_TRY(fork_to(*fk, 0, s));
+        cudaStream_t ws0 = fk->aux[0];
+        if (frames) {
+            a.done_list = across;
+            a.done_count = &ctl->across;
+        }
+        // at most one walk per leaf and per internal node; most of the grid
+        // finds nothing to do, so it is capped at a few CTAs per SM
+        const unsigned cap = 8u * static_cast<unsigned>(device_info().sm_count);
+        const unsigned gx = (nn + kThreads - 1) / kThreads;
         {
-            ProfScope prof_scope_("gather_kernel", s);
-            gather_kernel<<<gnn, kThreads, 0, s>>>(sizes, offsets, first, c.order, nn, collapsed, counts, primitives,
-                                                   &ctl->error);
+            ProfScope prof_scope_("fused_up_cross_kernel", ws0);
+            fused_up_cross_kernel<<<gx < cap ? gx : cap, kThreads, 0, ws0>>>(a, frontier, &ctl->frontier);
         }
         OBVH_TRY_CUDA(cudaGetLastError());
+        if (want_collapse) {
+            // reads the collapse marks, counts and first leaves (final after
+            // the walk); writes only collapse outputs, which the frames never read
+            OBVH_TRY(fork_to(*fk, 1, ws0));
+            cudaStream_t cs = fk->aux[1];
+            uint32_t* sizes = reinterpret_cast<uint32_t*>(ws + L.sizes);
+            uint32_t* offsets = reinterpret_cast<uint32_t*>(ws + L.offsets);
+            const unsigned gnn = (nn + kThreads - 1) / kThreads;
+            {
+                ProfScope prof_scope_("roots_kernel", cs);
+                roots_kernel<<<gnn, kThreads, 0, cs>>>(parents, cflags, counts, nn, sizes, &ctl->error);
+            }
+            OBVH_TRY_CUDA(cudaGetLastError());
+            OBVH_TRY(exclusive_scan_u32(sizes, offsets, nn, &ctl->total_slots, ws + L.scan, cs));
+            {
+                ProfScope prof_scope_("gather_kernel", cs);
+                gather_kernel<<<gnn, kThreads, 0, cs>>>(sizes, offsets, first, c.order, nn, collapsed, counts,
+                                                        primitives, &ctl->error);
+            }
+            OBVH_TRY_CUDA(cudaGetLastError());
+        }
+        if (frames) {
+            OBVH_TRY(obbtree::enqueue_candidates(fb, internal, obbtree::FrameNodes::kAcross, kLocalShift, ws0));
+            // a node is completed by fused_up_local iff its leaves lie inside one CTA's kThreads leaves
+            OBVH_TRY(obbtree::enqueue_candidates(fb, internal, obbtree::FrameNodes::kInside, kLocalShift, s));
+        }
+        OBVH_TRY(join_from(*fk, 0, s));
     }
+    if (frames) OBVH_TRY(obbtree::enqueue_extents(fb, internal, obbs, xfs, s));
+    if (want_collapse) OBVH_TRY(join_from(*fk, 1, s));
     if (bounds) OBVH_TRY_CUDA(cudaMemcpyAsync(bounds, c.boxes, 2 * sizeof(kr_aabb3), cudaMemcpyDeviceToDevice, s));
     return kr_success;
 }

@@ -5,6 +5,7 @@
 
 #include <atomic>
 #include <cstdio>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <string>
@@ -27,6 +28,63 @@ kr_error cuda_error(cudaError_t e) {
 }
 
 void set_last_error(kr_error e) { t_last_error = e; }
+
+namespace {
+struct ForkSlot {
+    int device = -1;
+    cudaStream_t caller = nullptr;
+    ForkStreams f;
+};
+constexpr size_t kForkSlots = 8;
+thread_local std::deque<ForkSlot>* t_fork_slots = nullptr;  // never freed: streams may outlive thread exit
+}  // namespace
+
+kr_error fork_streams(cudaStream_t s, ForkStreams** out) {
+    int dev = 0;
+    OBVH_TRY_CUDA(cudaGetDevice(&dev));
+    if (!t_fork_slots) t_fork_slots = new std::deque<ForkSlot>();
+    std::deque<ForkSlot>& slots = *t_fork_slots;  // references stay valid as it grows
+    ForkSlot* shared = nullptr;
+    for (ForkSlot& x : slots) {
+        if (x.device != dev) continue;
+        if (x.caller == s) {
+            *out = &x.f;
+            return kr_success;
+        }
+        shared = &x;  // the last slot of this device
+    }
+    size_t on_dev = 0;
+    for (const ForkSlot& x : slots) on_dev += x.device == dev;
+    if (on_dev >= kForkSlots && shared) {
+        *out = &shared->f;
+        return kr_success;
+    }
+    ForkSlot x;
+    x.device = dev;
+    x.caller = s;
+    int least = 0, greatest = 0;
+    OBVH_TRY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    for (int i = 0; i < 2; ++i) {
+        OBVH_TRY_CUDA(cudaStreamCreateWithPriority(&x.f.aux[i], cudaStreamNonBlocking, i == 0 ? greatest : least));
+        OBVH_TRY_CUDA(cudaEventCreateWithFlags(&x.f.fork[i], cudaEventDisableTiming));
+        OBVH_TRY_CUDA(cudaEventCreateWithFlags(&x.f.join[i], cudaEventDisableTiming));
+    }
+    slots.push_back(x);
+    *out = &slots.back().f;
+    return kr_success;
+}
+
+kr_error fork_to(ForkStreams& f, int i, cudaStream_t s) {
+    OBVH_TRY_CUDA(cudaEventRecord(f.fork[i], s));
+    OBVH_TRY_CUDA(cudaStreamWaitEvent(f.aux[i], f.fork[i], 0));
+    return kr_success;
+}
+
+kr_error join_from(ForkStreams& f, int i, cudaStream_t s) {
+    OBVH_TRY_CUDA(cudaEventRecord(f.join[i], f.aux[i]));
+    OBVH_TRY_CUDA(cudaStreamWaitEvent(s, f.join[i], 0));
+    return kr_success;
+}
 
 const DeviceInfo& device_info() {
     int dev = 0;

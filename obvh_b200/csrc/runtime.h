@@ -59,6 +59,27 @@ struct PinnedBuffer {
 };
 
 // ---------------------------------------------------------------------------
+// Fork and join inside one enqueue: work that does not depend on what the
+// caller's stream runs next goes to a helper stream, ordered by events (so a
+// stream under graph capture captures the helper's work as parallel branches
+// of the same graph).  Each (thread, device, caller stream) gets its own two
+// helper streams, up to eight caller streams per thread; further streams share
+// the eighth set, which is still correct, only less parallel.  aux[0] has the
+// device's highest stream priority (its CTAs are placed before those of
+// kernels already waiting), aux[1] the lowest.
+struct ForkStreams {
+    cudaStream_t aux[2] = {nullptr, nullptr};
+    cudaEvent_t fork[2] = {nullptr, nullptr};  // recorded on the caller's stream
+    cudaEvent_t join[2] = {nullptr, nullptr};  // recorded on aux[i]
+};
+// The helper set of caller stream s on the current device (created once).
+kr_error fork_streams(cudaStream_t s, ForkStreams** out);
+// aux[i] waits for everything enqueued on s so far.
+kr_error fork_to(ForkStreams& f, int i, cudaStream_t s);
+// s waits for everything enqueued on aux[i] so far.
+kr_error join_from(ForkStreams& f, int i, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
 // Per-kernel timing, off by default (obvh_profile_enable).  A ProfScope around
 // a launch records an event pair on the launching stream; the summary gives
 // launches and total device time per kernel name.

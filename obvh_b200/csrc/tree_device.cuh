@@ -271,30 +271,65 @@ struct Candidate {
     f3 lo, hi;  // slots 3..5
 };
 
-// The points of the frame search: the transform passes the 14 summary
-// vertices (K = 14).  (Packed two-wide multiplies and adds are each exact,
-// but a packed multiply feeding a packed add is contracted into a fused
-// multiply-add by the code generator even when both carry .rn, which changes
-// the rounding; the projections therefore stay scalar.)
+// Two-wide products.  sm_100 multiplies and adds float pairs in one
+// instruction (FMUL2/FADD2/FFMA2), each lane rounded like the scalar
+// operation.  A two-wide multiply feeding a two-wide add is fused into a
+// two-wide FMA by the code generator even when both carry .rn (which changes
+// the rounding), so a product is formed as fma(a, b, -0): the exact product
+// rounded once, which equals the rounded product for every input (a zero
+// product keeps its sign, since -0 is the additive identity under
+// round-to-nearest).  The -0 comes from a kernel argument, so that the
+// compiler cannot fold the FMA back into a multiply.
+// OBVH_SCALAR_PAIRS forms the pairs with scalar operations instead (the
+// same bits, twice the instructions), to hold the two-wide path against.
+#ifdef OBVH_SCALAR_PAIRS
+__device__ __forceinline__ float2 mul2(float2 a, float2 b, float2) {
+    return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y)); }
+#else
+__device__ __forceinline__ float2 mul2(float2 a, float2 b, float2 nz) { return __ffma2_rn(a, b, nz); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+#endif
+__device__ __forceinline__ float2 splat2(float v) { return make_float2(v, v); }
+
+// The points of the frame search (the transform passes the 14 summary
+// vertices, K = 14), two to a register pair: pair j holds point 2j in .x and
+// point 2j + 1 in .y, so that a projection of two points costs five
+// instructions instead of ten, with the same bits.
 template <int K>
 struct PointsK {
-    f3 p[K];
+    static_assert(K >= 2 && K % 2 == 0, "an even number of points");
+    float2 x[K / 2], y[K / 2], z[K / 2];
+    float2 nz;  // (-0, -0): see mul2
+    __device__ __forceinline__ void set(int i, f3 p) {
+        if (i & 1) { x[i >> 1].y = p.x; y[i >> 1].y = p.y; z[i >> 1].y = p.z; }
+        else { x[i >> 1].x = p.x; y[i >> 1].x = p.y; z[i >> 1].x = p.z; }
+    }
+    __device__ __forceinline__ f3 get(int i) const {
+        return (i & 1) ? mk3(x[i >> 1].y, y[i >> 1].y, z[i >> 1].y) : mk3(x[i >> 1].x, y[i >> 1].x, z[i >> 1].x);
+    }
 };
+
+// dot3 of the pair's two points with d: (x dx + y dy) + z dz, each rounded.
+template <int K>
+__device__ __forceinline__ float2 proj2(const PointsK<K>& P, int j, f3 d) {
+    const float2 xy = add2(mul2(P.x[j], splat2(d.x), P.nz), mul2(P.y[j], splat2(d.y), P.nz));
+    return add2(xy, mul2(P.z[j], splat2(d.z), P.nz));
+}
 
 // Extent of the K points along d: min and max of their projections, two
 // points per three-input min/max.
 template <int K>
-__device__ __forceinline__ void extent_proj(const PointsK<K>& Q, f3 d, float& lo, float& hi) {
-    static_assert(K >= 2 && K % 2 == 0, "an even number of points");
-    float a = dot3(Q.p[0], d), b = dot3(Q.p[1], d);
-    lo = fminf(a, b);
-    hi = fmaxf(a, b);
+__device__ __forceinline__ void extent_proj(const PointsK<K>& P, f3 d, float& lo, float& hi) {
+    float2 r = proj2(P, 0, d);
+    lo = fminf(r.x, r.y);
+    hi = fmaxf(r.x, r.y);
 #pragma unroll
-    for (int k = 1; k < K / 2; ++k) {
-        a = dot3(Q.p[2 * k], d);
-        b = dot3(Q.p[2 * k + 1], d);
-        lo = min3f(lo, a, b);
-        hi = max3f(hi, a, b);
+    for (int j = 1; j < K / 2; ++j) {
+        r = proj2(P, j, d);
+        lo = min3f(lo, r.x, r.y);
+        hi = max3f(hi, r.x, r.y);
     }
 }
 
@@ -361,33 +396,45 @@ __device__ inline Candidate node_candidate(const PointsK<K>& Q, f3 p0, f3 p1, co
     if (len2_3(sub3(p1, p0)) < eps) return stale;
     const f3 e0 = unit3(sub3(p0, p1));
     const float l2 = len2_3(e0);
-    f3 p2;
-    float fd;
-    {
-        f3 u = sub3(Q.p[0], p0);
-        float t = dot3(e0, u);
-        fd = len2_3(u) - t * t / l2;
-        p2 = Q.p[0];
+    // furthest point from the line p0 + s e0: |u|^2 - (e0.u)^2 / |e0|^2, u = p - p0
+    f3 p2 = Q.get(0);
+    float fd = 0.f;
 #pragma unroll
-        for (int i = 1; i < K; ++i) {
-            u = sub3(Q.p[i], p0);
-            t = dot3(e0, u);
-            float d = len2_3(u) - t * t / l2;
-            if (d > fd) { fd = d; p2 = Q.p[i]; }
+    for (int j = 0; j < K / 2; ++j) {
+        const float2 ux = add2(Q.x[j], splat2(-p0.x));
+        const float2 uy = add2(Q.y[j], splat2(-p0.y));
+        const float2 uz = add2(Q.z[j], splat2(-p0.z));
+        const float2 t = add2(add2(mul2(splat2(e0.x), ux, Q.nz), mul2(splat2(e0.y), uy, Q.nz)),
+                              mul2(splat2(e0.z), uz, Q.nz));
+        const float2 uu = add2(add2(mul2(ux, ux, Q.nz), mul2(uy, uy, Q.nz)), mul2(uz, uz, Q.nz));
+        const float2 tt = mul2(t, t, Q.nz);
+        const float2 d = add2(uu, make_float2(-(tt.x / l2), -(tt.y / l2)));
+        if (j == 0) {
+            fd = d.x;
+        } else if (d.x > fd) {
+            fd = d.x; p2 = Q.get(2 * j);
         }
+        if (d.y > fd) { fd = d.y; p2 = Q.get(2 * j + 1); }
     }
     if (fd < eps) return stale;
     const f3 e1 = unit3(sub3(p1, p2));
     const f3 e2 = unit3(sub3(p2, p0));
     const f3 n = unit3(cross3(e1, e0));
 
-    float qlo = dot3(Q.p[0], n), qhi = qlo;
-    f3 q1 = Q.p[0], q0 = Q.p[0];
+    // the points furthest below (q1) and above (q0) the base triangle's plane
+    float qlo = 0.f, qhi = 0.f;
+    f3 q1 = Q.get(0), q0 = Q.get(0);
 #pragma unroll
-    for (int i = 1; i < K; ++i) {
-        float q = dot3(Q.p[i], n);
-        if (q < qlo) { qlo = q; q1 = Q.p[i]; }
-        if (q > qhi) { qhi = q; q0 = Q.p[i]; }
+    for (int j = 0; j < K / 2; ++j) {
+        const float2 q = proj2(Q, j, n);
+        if (j == 0) {
+            qlo = qhi = q.x;
+        } else {
+            if (q.x < qlo) { qlo = q.x; q1 = Q.get(2 * j); }
+            if (q.x > qhi) { qhi = q.x; q0 = Q.get(2 * j); }
+        }
+        if (q.y < qlo) { qlo = q.y; q1 = Q.get(2 * j + 1); }
+        if (q.y > qhi) { qhi = q.y; q0 = Q.get(2 * j + 1); }
     }
     const float tri = dot3(p0, n);
     const bool up = qhi - eps > tri, down = qlo + eps < tri;
@@ -421,6 +468,35 @@ __device__ inline Candidate node_candidate(const PointsK<K>& Q, f3 p0, f3 p1, co
     c.lo = blen;
     c.hi = bmid;
     return c;
+}
+
+// The candidate of internal node a from its stored summary: the 14 extremal
+// vertices (min, max per slab), the furthest slab pair (first on ties), then
+// node_candidate.  kCg reads the vertices through L2 (vertices written
+// earlier in the same kernel); nz is -0.0f from a kernel argument (mul2).
+template <bool kCg>
+__device__ __forceinline__ Candidate summary_candidate(const uint4* summary, const kr_vec3* verts, size_t a,
+                                                       float nz, Summary& s) {
+    load_summary(summary + 7 * a, s);
+    PointsK<14> P;
+    P.nz = splat2(nz);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        P.set(2 * k, kCg ? load_vertex_cg(verts, s.ilo[k]) : load_vertex(verts, s.ilo[k]));
+        P.set(2 * k + 1, kCg ? load_vertex_cg(verts, s.ihi[k]) : load_vertex(verts, s.ihi[k]));
+    }
+    int at = 0;
+    float far = len2_3(sub3(P.get(1), P.get(0)));
+#pragma unroll
+    for (int k = 1; k < 7; ++k) {
+        const float d = len2_3(sub3(P.get(2 * k + 1), P.get(2 * k)));
+        if (d > far) { far = d; at = k; }
+    }
+    f3 p0 = P.get(0), p1 = P.get(1);
+#pragma unroll
+    for (int k = 1; k < 7; ++k)
+        if (at == k) { p0 = P.get(2 * k); p1 = P.get(2 * k + 1); }
+    return node_candidate<14>(P, p0, p1, s.lo, s.hi);
 }
 
 }  // namespace tree

@@ -104,6 +104,10 @@ struct UpArgs {
     uint4* summary;  // null: no summaries
     uint32_t* visits;
     uint32_t* err;
+    // null, or the nodes walk_up completes are appended here (done_count of
+    // them; at most the internal nodes)
+    uint32_t* done_list = nullptr;
+    uint32_t* done_count = nullptr;
 };
 
 // Completes internal node p (children L, R; count primitives) from its
@@ -210,6 +214,7 @@ __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Su
                 store_slab(a.summary, p, k, m);
             }
         }
+        if (a.done_list) a.done_list[atomicAdd(a.done_count, 1u)] = p;
         child = p;
         p = grand;
     }
