@@ -55,7 +55,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["lbvh_obb_tree", "atrbvh_obb_tree", "dito", "dito_batch", "serve",
-                                           "obvh_pack", "obvh_trace", "mesh_batch"],
+                                           "obvh_pack", "obvh_trace", "obvh_trace_compressed", "mesh_batch"],
                     default="lbvh_obb_tree")
     ap.add_argument("--treelet", type=int, default=7, help="atrbvh_obb_tree: treelet size")
     ap.add_argument("--requests", type=int, default=300, help="serve: requests in the stream")
@@ -794,7 +794,7 @@ def _trace_scene(n, dev):
         raise RuntimeError("build failed")
     s = bvh.obvh_pack(o["collapsed"], 2 * n - 1, n - 1, o["transforms"])
     torch.cuda.synchronize()
-    return v, f, mesh, s, o["primitives"]
+    return v, f, mesh, s, o["primitives"], o
 
 
 def bench_trace_ours(a, dist):
@@ -806,7 +806,7 @@ def bench_trace_ours(a, dist):
     from obvh_b200 import _native, bvh, workloads
     n = a.tris
     dev = torch.device("cuda", torch.cuda.current_device())
-    v, f, mesh, soa, prims = _trace_scene(n, dev)
+    v, f, mesh, soa, prims, _ = _trace_scene(n, dev)
     nn, ni = 2 * n - 1, n - 1
     ray_sets = [workloads.probe_rays(a.rays, [0, 0, 0], [1, 1, 1], seed=21 + 2 * dist.rank + j) for j in range(2)]
     d_rays = [torch.from_numpy(r.view(np.uint8).copy()).to(dev) for r in ray_sets]
@@ -896,6 +896,114 @@ def bench_trace_ours(a, dist):
                                 "kind": "port",
                                 "sample": f"{len(sample)} of the rays ({dt:.1f} s), oracle C restatement"}
     return line
+
+
+def bench_trace_compressed_ours(a, dist):
+    """Closest-hit traversal of a.rays probe rays through the compressed SoA
+    OBVH (24-byte boxes per child, quantised frames) of the collapsed
+    2M-triangle soup tree, beside the SoA OBVH traversal on the same rays."""
+    import ctypes as c
+    import numpy as np
+    import torch
+    from obvh_b200 import _native, bvh, workloads
+    n = a.tris
+    dev = torch.device("cuda", torch.cuda.current_device())
+    v, f, mesh, soa, prims, o = _trace_scene(n, dev)
+    nn, ni = 2 * n - 1, n - 1
+    pairs = bvh.compressed_pairs_from_obbs(bvh.nodes_numpy(o["collapsed"]), o["obbs"].cpu().numpy())
+    d_pairs = torch.from_numpy(pairs).to(dev)
+    comp = bvh.soa_compressed_obvh(soa["packed"], d_pairs, ni, nn)
+    torch.cuda.synchronize()
+    ray_sets = [workloads.probe_rays(a.rays, [0, 0, 0], [1, 1, 1], seed=21 + 2 * dist.rank + j) for j in range(2)]
+    d_rays = [torch.from_numpy(r.view(np.uint8).copy()).to(dev) for r in ray_sets]
+    isects = torch.empty(28 * a.rays, dtype=torch.uint8, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    lib = _native.lib()
+    stream = torch.cuda.current_stream(dev)
+    P = lambda t: c.c_void_p(t.data_ptr())  # noqa: E731
+
+    def step(j):
+        _native.check(lib.obvh_soa_compressed_obvh_intersect_async(
+            P(comp["lbounds"]), P(comp["rbounds"]), P(comp["metadata"]), ni, nn, P(mesh.verts), P(mesh.faces), n,
+            P(prims), prims.numel(), P(d_rays[j & 1]), P(isects), a.rays, P(err), c.c_void_p(stream.cuda_stream)))
+
+    def step_soa(j):
+        _native.check(lib.obvh_soa_obvh_intersect_async(P(soa["left_T"]), P(soa["right_T"]), P(soa["metadata"]), ni,
+                                                        nn, P(mesh.verts), P(mesh.faces), n, P(prims), prims.numel(),
+                                                        P(d_rays[j & 1]), P(isects), a.rays, P(err),
+                                                        c.c_void_p(stream.cuda_stream)))
+
+    sampler = ClockSampler(dev.index, enabled=not a.profile)
+    total_ms, prof, clocks = timed_steps(a, dist, step, sampler, stream)
+    if int(err.item()):
+        raise RuntimeError("compressed traversal reported a bad index")
+    if a.profile:
+        return {"profile": "obvh_trace_compressed", "rays": a.rays, "ms_per_step": total_ms / a.steps,
+                "kernels": prof}
+    hits = np.frombuffer(isects.cpu().numpy().tobytes(), dtype=workloads.ISECT)
+    hit_fraction = float((hits["primitive"] != 0xFFFFFFFF).mean())
+    value = dist.world * a.rays * a.steps / (total_ms / 1e3) / 1e6
+    soa_ms, _, _ = timed_steps(a, dist, step_soa, ClockSampler(dev.index, enabled=False), stream)
+    soa_value = dist.world * a.rays * a.steps / (soa_ms / 1e3) / 1e6
+    exact = np.frombuffer(isects.cpu().numpy().tobytes(), dtype=workloads.ISECT)
+    exact_hits = float((exact["primitive"] != 0xFFFFFFFF).mean())
+    node_bytes = {"compressed": 48 * ni + 16 * nn, "soa_obvh": 96 * ni + 16 * nn}
+
+    # end to end through kr_cuda_soa_compressed_obvh + kr_cuda_obvh_compressed_persistent_intersect:
+    # the scene resident, the rays copied from pinned host memory and the records read back each step
+    d_soa = c.c_void_p(0)
+    _native.check(lib.kr_cuda_soa_compressed_obvh(P(soa["packed"]), P(d_pairs), c.byref(d_soa), ni, nn))
+    h_rays = torch.empty(32 * a.rays, dtype=torch.uint8, pin_memory=True)
+    h_rays.copy_(d_rays[0])
+    h_isects = torch.empty(28 * a.rays, dtype=torch.uint8, pin_memory=True)
+    counter = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def e2e_step():
+        d_rays[1].copy_(h_rays, non_blocking=True)
+        torch.cuda.synchronize()
+        _native.check(lib.kr_cuda_obvh_compressed_persistent_intersect(d_soa, P(mesh.verts), P(mesh.faces), P(prims),
+                                                                       P(d_rays[1]), P(isects), a.rays, 128, 0,
+                                                                       P(counter)))
+        h_isects.copy_(isects)
+
+    try:
+        e2e_step()
+        e2e_steps = max(3, min(a.steps, 10))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        e2e_s = time.perf_counter() - t0
+    finally:
+        _native.check(lib.obvh_soa_obvh_compressed_free(d_soa))
+    e2e_min = -dist.max(-(a.rays * e2e_steps / e2e_s / 1e6))
+    peak, peak_kind = peaks()
+    name, (launches, kms) = max(prof.items(), key=lambda kv: kv[1][1])
+    return {
+        "metric": "Compressed OBVH closest-hit traversal throughput (Mrays/s)", "value": round(value, 3),
+        "unit": "Mrays/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": round(total_ms / a.steps, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: probe rays from a sphere around [0,1]^3 towards uniform points in it, through the "
+                "compressed form of the collapsed OBB tree of the 2M thin-triangle soup (pairs from the tree's "
+                "own boxes, obvh_b200.bvh.compressed_pairs_from_obbs)",
+        "config": {"workload": "obvh_trace_compressed_collapsed_tree", "triangles": n, "rays_per_gpu": a.rays,
+                   "hit_fraction": round(hit_fraction, 4), "hit_fraction_soa_obvh": round(exact_hits, 4),
+                   "node_array_bytes": node_bytes,
+                   "l2": "two ray sets of 128 MB alternated; node arrays and mesh exceed L2",
+                   "parallelism": f"replicas{dist.world}"},
+        "kernels": kernel_table(prof, a.steps, {}, peak), "gpu_launches": sum(x[0] for x in prof.values()),
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                     "traffic": None, "peak_source": peak_kind, "launches": launches,
+                     "ms_per_launch": round(kms / max(launches, 1), 5),
+                     "note": "work per ray (node and triangle fetches) is not counted for the compressed form"},
+        "soa_obvh": {"value": round(soa_value, 3), "unit": "Mrays/s", "ms_per_step": round(soa_ms / a.steps, 5),
+                     "api": "obvh_soa_obvh_intersect_async on the same tree and rays"},
+        "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 32 * a.rays,
+                "d2h_bytes_per_step": 28 * a.rays,
+                "api": "kr_cuda_obvh_compressed_persistent_intersect, rays from pinned host memory, records read "
+                       "back to pinned memory"},
+        "clocks": clocks,
+    }
 
 
 def bench_trace_reference(a, dist):
@@ -1578,6 +1686,9 @@ def main():
             print(json.dumps(bench_trace_reference(a, dist)), flush=True)
         elif a.workload == "mesh_batch":
             print(json.dumps(bench_mesh_batch_reference(a, dist)), flush=True)
+        elif a.workload == "obvh_trace_compressed":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's compressed traversal exists only "
+                              "as a GPU kernel (pinned against this build in the GPU tests); there is no CPU form"}))
         else:
             print(json.dumps(bench_tree_reference(a, dist)), flush=True)
         return
@@ -1585,7 +1696,8 @@ def main():
     try:
         run = {"lbvh_obb_tree": bench_tree_ours, "atrbvh_obb_tree": lambda a, d: bench_tree_ours(a, d, atrbvh=True),
                "dito": bench_dito_ours, "dito_batch": bench_batch_ours, "serve": bench_serve_ours,
-               "obvh_pack": bench_pack_ours, "obvh_trace": bench_trace_ours, "mesh_batch": bench_mesh_batch_ours}
+               "obvh_pack": bench_pack_ours, "obvh_trace": bench_trace_ours,
+               "obvh_trace_compressed": bench_trace_compressed_ours, "mesh_batch": bench_mesh_batch_ours}
         line = run[a.workload](a, dist)
         if a.workload == "lbvh_obb_tree" and dist.world == 1 and not (a.profile or a.no_extras):
             extra_workloads(a, dist, line)

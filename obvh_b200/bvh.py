@@ -435,6 +435,48 @@ def soa_compressed_obvh_sync(packed, pairs, internal_count: int, node_count: int
         _native.check(lib.obvh_soa_obvh_compressed_free(d_soa))
 
 
+def compressed_pairs_from_obbs(nodes: np.ndarray, obbs: np.ndarray) -> np.ndarray:
+    """Transformation pairs in the form the compressed OBVH reads, one per
+    internal node and child (float32 [internal, 32]: left pair, then right):
+    column 0 the axis and angle / pi of the child box's rotation (box to
+    world; kr_cuda_soa_compressed_obvh negates the axis, so the traversal
+    applies world to box), column 1 the box centre, column 2 the box's full
+    size along its unit axes.  The reference has no producer of this form
+    (kr_cuda_soa_compressed_obvh, src/ads/common/cuda/transforms.cu:1452-1535,
+    has no caller); this one derives it from an OBB tree (NODE records and
+    kr_obb3 rows).  A left-handed frame is made right-handed by reversing its
+    third axis, which leaves the symmetric box unchanged; rotations by about
+    pi take their axis from R + I, where the skew part vanishes."""
+    nodes = np.ascontiguousarray(nodes)
+    ni = (nodes.shape[0] - 1) // 2
+    o_all = np.asarray(obbs, np.float64).reshape(-1, 15)
+    pairs = np.zeros((max(ni, 0), 32), np.float32)
+    for side, key in ((0, "left"), (1, "right")):
+        o = o_all[nodes[key][:ni].astype(np.int64)]
+        axes = o[:, 3:12].reshape(-1, 3, 3)                  # rows a0, a1, a2
+        length = np.linalg.norm(axes, axis=2)
+        unit = axes / np.where(length > 0, length, 1.0)[..., None]
+        unit[np.linalg.det(unit) < 0, 2] *= -1.0
+        r = np.transpose(unit, (0, 2, 1))                      # columns: the box axes in world coordinates
+        cos = np.clip((np.trace(r, axis1=1, axis2=2) - 1.0) * 0.5, -1.0, 1.0)
+        angle = np.arccos(cos)
+        axis = np.stack([r[:, 2, 1] - r[:, 1, 2], r[:, 0, 2] - r[:, 2, 0], r[:, 1, 0] - r[:, 0, 1]], 1)
+        skew = np.linalg.norm(axis, axis=1)
+        near_pi = skew < 1e-6
+        if near_pi.any():
+            sym = r[near_pi] + np.eye(3)                        # columns ~ 2 (axis . x) axis
+            pick = np.argmax(np.linalg.norm(sym, axis=1), axis=1)
+            axis[near_pi] = sym[np.arange(sym.shape[0]), :, pick]
+            skew = np.linalg.norm(axis, axis=1)
+        axis = np.where(skew[:, None] > 0, axis / np.where(skew > 0, skew, 1.0)[:, None], [1.0, 0.0, 0.0])
+        m = pairs[:, 16 * side:16 * side + 16]
+        m[:, 0:3] = axis
+        m[:, 3] = angle / np.pi
+        m[:, 4:7] = o[:, 0:3]
+        m[:, 8:11] = 2.0 * o[:, 12:15] * length
+    return pairs
+
+
 def soa_compressed_obvh_intersect(soa: dict, mesh: "Mesh", primitives, rays, node_count: int, internal_count: int,
                                   isects=None, stream=None):
     """obvh_soa_compressed_obvh_intersect_async: closest hits of `rays`

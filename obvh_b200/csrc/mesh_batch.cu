@@ -68,7 +68,7 @@ static_assert(sizeof(Job) == 40, "Job layout");
 
 // Per-CTA scratch for meshes of up to `max_faces` triangles.
 struct SlotLayout {
-    size_t boxes, keys_a, vals_a, keys_b, vals_b, tris, summary, cand, first, visits, flags, sizes, offsets, total;
+    size_t boxes, keys_a, vals_a, keys_b, vals_b, tris, summary, cand, first, flags, sizes, offsets, total;
 };
 
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
@@ -85,7 +85,6 @@ SlotLayout slot_layout(uint32_t m) {
     L.summary = o; o += align256(112ull * m);
     L.cand = o;    o += align256(sizeof(obbtree::Cand) * m);
     L.first = o;   o += align256(4ull * m);
-    L.visits = o;  o += align256(4ull * m);
     L.flags = o;   o += align256(2ull * m);
     L.sizes = o;   o += align256(8ull * m);
     L.offsets = o; o += align256(8ull * m);
@@ -119,10 +118,28 @@ struct Args {
 
 struct Smem {
     uint16_t table[16 * kMaxRounds * kWarps];  // sort: digit counts per (digit, round, warp)
+    uint32_t visits[kMaxFaces / 4];            // bottom-up arrivals: one byte per internal node
     float red[kWarps][12];
     float box[12];  // scene lo, hi; centroid lo, hi
     uint32_t part[kWarps];
     uint32_t job;
+};
+
+// Arrival at internal node p of the mesh in the bottom-up pass: the mesh is
+// the CTA's alone, so a shared-memory byte counter with CTA-scope fences
+// orders the children's outputs (written to global memory by threads of
+// this CTA) before the second arrival, much as the chain's GPU-scope
+// acquire/release counter does across CTAs, at a fraction of the latency.
+// A byte counts at most 2, so adding 1 at its position never carries.
+struct CtaArrive {
+    uint32_t* words;  // Smem::visits
+    __device__ __forceinline__ uint32_t operator()(const pipeline::UpArgs&, uint32_t p) const {
+        const uint32_t shift = 8u * (p & 3u);
+        __threadfence_block();  // release: this thread's child outputs before its arrival
+        const uint32_t old = atomicAdd(words + (p >> 2), 1u << shift);
+        __threadfence_block();  // acquire: the sibling's outputs after the arrival
+        return (old >> shift) & 0xffu;
+    }
 };
 
 // Global writes of one stage are read by other threads of the CTA in the next.
@@ -235,7 +252,6 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
     uint4* summary = reinterpret_cast<uint4*>(slot + a.slot.summary);
     obbtree::Cand* cand = reinterpret_cast<obbtree::Cand*>(slot + a.slot.cand);
     uint32_t* first = reinterpret_cast<uint32_t*>(slot + a.slot.first);
-    uint32_t* visits = reinterpret_cast<uint32_t*>(slot + a.slot.visits);
     uint8_t* flags = reinterpret_cast<uint8_t*>(slot + a.slot.flags);
     uint32_t* sizes = reinterpret_cast<uint32_t*>(slot + a.slot.sizes);
     uint32_t* offsets = reinterpret_cast<uint32_t*>(slot + a.slot.offsets);
@@ -243,7 +259,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
     const float leaf_ct = want_collapse ? a.ct : 1.0f;
 
     // ---- 1: triangle boxes; scene and centroid boxes (tri_bounds_kernel) ----
-    for (uint32_t i = t; i < ni; i += kThreads) visits[i] = 0;
+    for (uint32_t i = t; i < (ni + 3) / 4; i += kThreads) sm.visits[i] = 0;
     if (want_collapse)
         for (uint32_t i = t; i < nn; i += kThreads) flags[i] = 0;
     float acc[12];
@@ -319,7 +335,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
     // ---- 6: bottom-up pass from every leaf (walk_up of the chain) ------------
     {
         pipeline::UpArgs ua{nodes,  collapsed, parents, first, tris, n, counts, costs, want_collapse ? flags : nullptr,
-                            a.ci,   a.ct,      want_obbs ? summary : nullptr, visits, a.err};
+                            a.ci,   a.ct,      want_obbs ? summary : nullptr, nullptr, a.err};
         for (uint32_t j = t; j < n; j += kThreads) {
             const uint32_t x = ni + j;
             pipeline::Carry c;
@@ -339,7 +355,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
 #pragma unroll
                 for (int k = 0; k < 7; ++k) pipeline::set_slab(s, k, pipeline::leaf_slab(v, j, k));
             }
-            pipeline::walk_up<true>(ua, x, c, s);
+            pipeline::walk_up<true>(ua, x, c, s, CtaArrive{sm.visits});
         }
     }
     stage_sync();

@@ -154,14 +154,22 @@ __device__ __forceinline__ Carry complete_node(const UpArgs& a, uint32_t p, uint
 
 // Leaf-to-root walk from node x (carry c, summary s) through nodes whose
 // leaf ranges cross a CTA's edge: the second thread to arrive at a node
-// (GPU-scope acquire/release counter) completes it from the sibling's outputs.
+// (arrive_at: a GPU-scope acquire/release counter by default) completes it
+// from the sibling's outputs.
 //
 // Fresh: the node records' children, the parents, the counts and the sorted
 // triangles were written earlier in the same kernel (the one-CTA-per-mesh
 // batch build), so they are read through L2 like the rest; otherwise they
 // were written before the kernel and go through the read-only path.
-template <bool Fresh = false>
-__device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Summary s) {
+// Arrival at internal node p through the global counters a.visits
+// (GPU-scope acquire/release): walks from any CTA.
+struct GlobalArrive {
+    __device__ __forceinline__ uint32_t operator()(const UpArgs& a, uint32_t p) const { return arrive(a.visits + p); }
+};
+
+template <bool Fresh = false, class Arrive = GlobalArrive>
+__device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Summary s,
+                                        Arrive arrive_at = Arrive{}) {
     const uint32_t internal = a.n - 1;
     uint32_t child = x;
     uint32_t p = a.parents[x];
@@ -175,7 +183,7 @@ __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Su
         const uint32_t L = Fresh ? __ldcg(pw + 6) : __ldg(pw + 6), R = Fresh ? __ldcg(pw + 7) : __ldg(pw + 7);
         const uint32_t grand = Fresh ? __ldcg(a.parents + p) : __ldg(a.parents + p);
         const uint32_t count = Fresh ? __ldcg(a.counts + p) : __ldg(a.counts + p);
-        if (arrive(a.visits + p) == 0) return;
+        if (arrive_at(a, p) == 0) return;
         const bool from_left = (L == child);
         const uint32_t other = from_left ? R : L;
         Carry o;
