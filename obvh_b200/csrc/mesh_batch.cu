@@ -53,6 +53,9 @@ using namespace tree;
 constexpr int kThreads = OBVH_MESH_BATCH_THREADS;  // one mesh per CTA of this many threads
 constexpr int kCtasPerSm = 512 / kThreads;           // the SM's registers at 128 per thread
 constexpr int kWarps = kThreads / 32;
+// Shared-memory carveout, in percent of the SM's maximum: room for kCtasPerSm
+// CTAs of static shared memory (33 KB each), the rest of the unified memory L1.
+constexpr int kSmemCarveout = 32;
 constexpr uint32_t kMaxFaces = OBVH_BUILD_BATCH_CTA_MAX_FACES;
 constexpr uint32_t kMaxRounds = kMaxFaces / kThreads;  // sort rounds of kThreads keys
 constexpr uint32_t kThreadLeaves = 32;                  // extents: one thread per node up to this many leaves
@@ -125,15 +128,34 @@ struct Smem {
     uint32_t job;
 };
 
-// Arrival at internal node p of the mesh in the bottom-up pass: the mesh is
-// the CTA's alone, so a shared-memory byte counter with CTA-scope fences
-// orders the children's outputs (written to global memory by threads of
-// this CTA) before the second arrival, much as the chain's GPU-scope
-// acquire/release counter does across CTAs, at a fraction of the latency.
-// A byte counts at most 2, so adding 1 at its position never carries.
+// A load of data this CTA wrote earlier in the kernel (its scratch slot and
+// its mesh's outputs): a plain load, cached in L1, which stays coherent with
+// the SM's own stores; the barriers and CTA-scope fences order them.
+template <class T>
+__device__ __forceinline__ T ld_own(const T* p) { return ld_src<Src::kOwnCta>(p); }
+
+// Arrival at internal node p of the mesh in the bottom-up pass.  Thread t
+// walks up from the leaves of its run [t R, (t + 1) R): a node whose leaves
+// all lie in that run has both arrivals from this thread, so a plain
+// shared-memory byte counts them.  Other nodes are reached from two threads:
+// the same byte, updated by an atomic add on its word between CTA-scope
+// fences, orders the children's outputs (written to global memory by threads
+// of this CTA) before the second arrival.  A node keeps one mode for both of
+// its arrivals, a byte counts at most 2 (so adding 1 at its position never
+// carries), and byte stores leave the word's other bytes alone.
 struct CtaArrive {
-    uint32_t* words;  // Smem::visits
+    uint32_t* words;        // Smem::visits
+    const uint32_t* first;  // per internal node: its first leaf
+    const uint32_t* counts; // and its leaf count
+    uint32_t run, me;       // leaves per thread, this thread's run
     __device__ __forceinline__ uint32_t operator()(const pipeline::UpArgs&, uint32_t p) const {
+        const uint32_t f = ld_own(first + p), last = f + ld_own(counts + p) - 1;
+        if (f / run == me && last / run == me) {
+            uint8_t* b = reinterpret_cast<uint8_t*>(words) + p;
+            const uint32_t old = *b;
+            *b = static_cast<uint8_t>(old + 1);
+            return old;
+        }
         const uint32_t shift = 8u * (p & 3u);
         __threadfence_block();  // release: this thread's child outputs before its arrival
         const uint32_t old = atomicAdd(words + (p >> 2), 1u << shift);
@@ -200,7 +222,7 @@ __device__ void sort_pass(const uint32_t* kin, const uint32_t* vin, uint32_t* ko
     __syncthreads();
     for (uint32_t r = 0; r < rounds; ++r) {
         const uint32_t e = r * kThreads + t;
-        const uint32_t d = e < n ? (__ldcg(kin + e) >> shift) & 15u : 16u;
+        const uint32_t d = e < n ? (ld_own(kin + e) >> shift) & 15u : 16u;
         const uint32_t same = __match_any_sync(0xffffffffu, d);
         if (d < 16 && lane == static_cast<uint32_t>(__ffs(same) - 1))
             sm.table[d * cols + r * kWarps + w] = static_cast<uint16_t>(__popc(same));
@@ -210,24 +232,24 @@ __device__ void sort_pass(const uint32_t* kin, const uint32_t* vin, uint32_t* ko
     const uint32_t below = (1u << lane) - 1u;
     for (uint32_t r = 0; r < rounds; ++r) {
         const uint32_t e = r * kThreads + t;
-        const uint32_t key = e < n ? __ldcg(kin + e) : 0u;
+        const uint32_t key = e < n ? ld_own(kin + e) : 0u;
         const uint32_t d = e < n ? (key >> shift) & 15u : 16u;
         const uint32_t same = __match_any_sync(0xffffffffu, d);
         if (e < n) {
             const uint32_t rank = sm.table[d * cols + r * kWarps + w] + __popc(same & below);
             kout[rank] = key;
-            vout[rank] = __ldcg(vin + e);
+            vout[rank] = ld_own(vin + e);
         }
     }
     stage_sync();
 }
 
-__device__ __forceinline__ obbtree::Cand load_cand_cg(const obbtree::Cand* cand, uint32_t a) {
+__device__ __forceinline__ obbtree::Cand load_cand_own(const obbtree::Cand* cand, uint32_t a) {
     obbtree::Cand c;
     float4* d = reinterpret_cast<float4*>(&c);
     const float4* s = reinterpret_cast<const float4*>(cand + a);
 #pragma unroll
-    for (int q = 0; q < 6; ++q) d[q] = __ldcg(s + q);
+    for (int q = 0; q < 6; ++q) d[q] = ld_own(s + q);
     return c;
 }
 
@@ -306,11 +328,11 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
 
     // ---- 4: leaves (leaves_fused_kernel) ---------------------------------------
     for (uint32_t j = t; j < n; j += kThreads) {
-        const uint32_t i = __ldcg(vals_a + j);
+        const uint32_t i = ld_own(vals_a + j);
         const float* b = boxes + 6 * static_cast<size_t>(i);
         uint32_t wd[9];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) wd[k] = __float_as_uint(__ldcg(b + k));
+        for (int k = 0; k < 6; ++k) wd[k] = __float_as_uint(ld_own(b + k));
         wd[6] = i;  // primitivesOffset
         wd[7] = 0;
         wd[8] = 1;  // one primitive, axis 0
@@ -336,14 +358,17 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
     {
         pipeline::UpArgs ua{nodes,  collapsed, parents, first, tris, n, counts, costs, want_collapse ? flags : nullptr,
                             a.ci,   a.ct,      want_obbs ? summary : nullptr, nullptr, a.err};
-        for (uint32_t j = t; j < n; j += kThreads) {
+        // thread t walks up from the leaves of its run [t R, (t + 1) R), in order
+        const uint32_t run = (n + kThreads - 1) / kThreads;
+        const CtaArrive arrive{sm.visits, first, counts, run, t};
+        for (uint32_t j = t * run, jend = min(n, (t + 1) * run); j < jend; ++j) {
             const uint32_t x = ni + j;
             pipeline::Carry c;
             const uint32_t* wd = reinterpret_cast<const uint32_t*>(nodes + x);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                c.lo[k] = __uint_as_float(__ldcg(wd + k));
-                c.hi[k] = __uint_as_float(__ldcg(wd + 3 + k));
+                c.lo[k] = __uint_as_float(ld_own(wd + k));
+                c.hi[k] = __uint_as_float(ld_own(wd + 3 + k));
             }
             c.cost = leaf_ct * box_area(c.lo, c.hi);
             Summary s;
@@ -351,11 +376,11 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
                 const kr_vec3* pts = reinterpret_cast<const kr_vec3*>(tris);
                 f3 v[3];
 #pragma unroll
-                for (int k = 0; k < 3; ++k) v[k] = load_vertex_cg(pts, 3 * j + k);
+                for (int k = 0; k < 3; ++k) v[k] = load_vertex_src<Src::kOwnCta>(pts, 3 * j + k);
 #pragma unroll
                 for (int k = 0; k < 7; ++k) pipeline::set_slab(s, k, pipeline::leaf_slab(v, j, k));
             }
-            pipeline::walk_up<true>(ua, x, c, s, CtaArrive{sm.visits});
+            pipeline::walk_up<Src::kOwnCta, Src::kOwnCta>(ua, x, c, s, arrive);
         }
     }
     stage_sync();
@@ -365,7 +390,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
         const kr_vec3* pts = reinterpret_cast<const kr_vec3*>(tris);
         for (uint32_t i = t; i < ni; i += kThreads) {
             Summary s;
-            const Candidate c = summary_candidate<true>(summary, pts, i, a.nz, s);
+            const Candidate c = summary_candidate<Src::kOwnCta, Src::kOwnCta>(summary, pts, i, a.nz, s);
             obbtree::Cand out;
             out.ax[0] = c.b0.x; out.ax[1] = c.b0.y; out.ax[2] = c.b0.z;
             out.ax[3] = c.b1.x; out.ax[4] = c.b1.y; out.ax[5] = c.b1.z;
@@ -384,25 +409,25 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
 
         // ---- 8: extents over each node's leaf run; final boxes ---------------
         for (uint32_t i = t; i < ni; i += kThreads) {
-            const uint32_t cnt = __ldcg(counts + i);
+            const uint32_t cnt = ld_own(counts + i);
             if (cnt > kThreadLeaves) continue;
-            const obbtree::Cand c = load_cand_cg(cand, i);
+            const obbtree::Cand c = load_cand_own(cand, i);
             const obbtree::Axes ax = obbtree::make_axes(mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
                                                         mk3(c.ax[6], c.ax[7], c.ax[8]), a.nz);
             float lo[3] = {c.olo[0], c.olo[1], c.olo[2]}, hi[3] = {c.ohi[0], c.ohi[1], c.ohi[2]};
-            const float* tp = tris + 9 * static_cast<size_t>(__ldcg(first + i));
-            for (uint32_t k = 0; k < cnt; ++k) obbtree::project_tri_cg(tp + 9 * k, ax, lo, hi);
+            const float* tp = tris + 9 * static_cast<size_t>(ld_own(first + i));
+            for (uint32_t k = 0; k < cnt; ++k) obbtree::project_tri_own(tp + 9 * k, ax, lo, hi);
             obbtree::finalize_node(c, mk3(lo[0], lo[1], lo[2]), mk3(hi[0], hi[1], hi[2]), obbs + i, xfs + i);
         }
         for (uint32_t i = w; i < ni; i += kWarps) {
-            const uint32_t cnt = __ldcg(counts + i);
+            const uint32_t cnt = ld_own(counts + i);
             if (cnt <= kThreadLeaves) continue;
-            const obbtree::Cand c = load_cand_cg(cand, i);
+            const obbtree::Cand c = load_cand_own(cand, i);
             const obbtree::Axes ax = obbtree::make_axes(mk3(c.ax[0], c.ax[1], c.ax[2]), mk3(c.ax[3], c.ax[4], c.ax[5]),
                                                         mk3(c.ax[6], c.ax[7], c.ax[8]), a.nz);
             float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
-            const float* tp = tris + 9 * static_cast<size_t>(__ldcg(first + i));
-            for (uint32_t k = lane; k < cnt; k += 32) obbtree::project_tri_cg(tp + 9 * k, ax, lo, hi);
+            const float* tp = tris + 9 * static_cast<size_t>(ld_own(first + i));
+            for (uint32_t k = lane; k < cnt; k += 32) obbtree::project_tri_own(tp + 9 * k, ax, lo, hi);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 lo[k] = fminf(c.olo[k], warp_min(lo[k]));
@@ -416,31 +441,31 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
     // ---- 9: collapse (roots_kernel, exclusive scan, gather_kernel) ----------
     if (want_collapse) {
         for (uint32_t c = t; c < nn; c += kThreads) {
-            const uint32_t p = __ldcg(parents + c);
-            const uint32_t cnt = __ldcg(counts + c);
-            sizes[c] = (c != 0 && p < nn && __ldcg(flags + c) && !__ldcg(flags + p) && cnt > 1) ? cnt : 0u;
+            const uint32_t p = ld_own(parents + c);
+            const uint32_t cnt = ld_own(counts + c);
+            sizes[c] = (c != 0 && p < nn && ld_own(flags + c) && !ld_own(flags + p) && cnt > 1) ? cnt : 0u;
         }
         stage_sync();
-        for (uint32_t c = t; c < nn; c += kThreads) offsets[c] = __ldcg(sizes + c);
+        for (uint32_t c = t; c < nn; c += kThreads) offsets[c] = ld_own(sizes + c);
         stage_sync();
         const uint32_t total = block_scan(offsets, nn, sm);
         if (t == 0) a.mesh_slots[J.mesh] = total;
         stage_sync();
         uint32_t* prims = a.primitives + J.fbase;
         for (uint32_t c = t; c < nn; c += kThreads) {
-            const uint32_t cnt = __ldcg(sizes + c);
+            const uint32_t cnt = ld_own(sizes + c);
             if (cnt == 0) continue;
             if (cnt > pipeline::kMaxLeafSize) {
                 atomicOr(a.err, kErrBadInput);
                 continue;
             }
-            const uint32_t f = __ldcg(first + c), off = __ldcg(offsets + c);
+            const uint32_t f = ld_own(first + c), off = ld_own(offsets + c);
             uint32_t out[pipeline::kMaxLeafSize];
             uint32_t pos = 0;
 #pragma unroll
             for (uint32_t q = 0; q < pipeline::kMaxLeafSize; ++q) {
                 if (q < cnt) {
-                    const uint32_t prim = __ldcg(vals_a + f + cnt - 1 - q);
+                    const uint32_t prim = ld_own(vals_a + f + cnt - 1 - q);
                     bool uniq = true;
 #pragma unroll
                     for (uint32_t r = 0; r < pipeline::kMaxLeafSize; ++r) uniq = uniq && !(r < pos && out[r] == prim);
@@ -458,7 +483,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
             counts[c] = pos;
             uint32_t* cw = reinterpret_cast<uint32_t*>(collapsed + c);
             cw[6] = off;
-            cw[8] = (__ldcg(cw + 8) & 0xffff0000u) | pos;
+            cw[8] = (ld_own(cw + 8) & 0xffff0000u) | pos;
         }
     } else if (t == 0) {
         a.mesh_slots[J.mesh] = 0;
@@ -615,6 +640,10 @@ kr_error plan(Plan& P, const kr_size* voff, const kr_size* foff, kr_size meshes)
     P.slot = slot_layout(P.cta_max);
     const int sms = device_info().sm_count;
     P.grid = static_cast<int>(std::min<size_t>(P.cta_jobs.size(), static_cast<size_t>(sms) * kCtasPerSm));
+    // The kernel reads its own writes through L1: leave L1 the SM's unified
+    // memory beyond the CTAs' static shared memory (a hint, per device).
+    OBVH_TRY_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(mesh_batch_kernel),
+                                       cudaFuncAttributePreferredSharedMemoryCarveout, kSmemCarveout));
     OBVH_TRY(P.status.reserve(4ull * (2 + meshes)));
     OBVH_TRY_CUDA(cudaMemset(P.status.ptr, 0, 4ull * (2 + meshes)));
     if (!P.cta_jobs.empty()) {

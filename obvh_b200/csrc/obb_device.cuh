@@ -114,5 +114,10 @@ __device__ __forceinline__ void project_tri_cg(const float* t, const Axes& ax, f
     project_tri_from<From::kL2>(t, ax, lo, hi);
 }
 
+// project_tri for triangles this CTA wrote (plain loads, as from shared memory)
+__device__ __forceinline__ void project_tri_own(const float* t, const Axes& ax, float lo[3], float hi[3]) {
+    project_tri_from<From::kShared>(t, ax, lo, hi);
+}
+
 }  // namespace obbtree
 }  // namespace obvh

@@ -404,7 +404,7 @@ __device__ __forceinline__ void candidate_node(uint32_t a, const uint4* summary,
                                                const uint32_t* counts, Cand* cand, uint32_t* nunits, uint32_t* keys,
                                                const ChainArgs& chain) {
     Summary s;
-    const Candidate c = summary_candidate<false>(summary, verts, a, chain.nz, s);
+    const Candidate c = summary_candidate<Src::kL2, Src::kReadOnly>(summary, verts, a, chain.nz, s);
     Cand out;
     out.ax[0] = c.b0.x; out.ax[1] = c.b0.y; out.ax[2] = c.b0.z;
     out.ax[3] = c.b1.x; out.ax[4] = c.b1.y; out.ax[5] = c.b1.z;

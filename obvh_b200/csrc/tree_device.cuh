@@ -81,6 +81,25 @@ __device__ __forceinline__ f3 load_vertex_cg(const kr_vec3* verts, uint32_t i) {
     return mk3(__ldcg(p), __ldcg(p + 1), __ldcg(p + 2));
 }
 
+// Where the data a load reads was written: before the kernel (the read-only
+// path), earlier in the kernel by other SMs (through L2), or earlier in the
+// kernel by this CTA (a plain load, cached in L1: an SM's own stores keep its
+// L1 coherent, and a barrier or CTA-scope fence orders them).
+enum class Src { kReadOnly, kL2, kOwnCta };
+
+template <Src S, class T>
+__device__ __forceinline__ T ld_src(const T* p) {
+    if constexpr (S == Src::kReadOnly) return __ldg(p);
+    else if constexpr (S == Src::kL2) return __ldcg(p);
+    else return *p;
+}
+
+template <Src S>
+__device__ __forceinline__ f3 load_vertex_src(const kr_vec3* verts, uint32_t i) {
+    const float* p = reinterpret_cast<const float*>(verts) + 3 * static_cast<size_t>(i);
+    return mk3(ld_src<S>(p), ld_src<S>(p + 1), ld_src<S>(p + 2));
+}
+
 // ---------------------------------------------------------------------------
 // 4x4 matrices (column-major, kr_mat4).
 struct M4 {
@@ -239,10 +258,11 @@ __device__ __forceinline__ void store_summary(uint4* dst, const Summary& s) {
         __stcg(dst + k, make_uint4(__float_as_uint(s.lo[k]), __float_as_uint(s.hi[k]), s.ilo[k], s.ihi[k]));
 }
 
+template <Src S = Src::kL2>
 __device__ __forceinline__ void load_summary(const uint4* src, Summary& s) {
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
-        uint4 w = __ldcg(src + k);
+        uint4 w = ld_src<S>(src + k);
         s.lo[k] = __uint_as_float(w.x);
         s.hi[k] = __uint_as_float(w.y);
         s.ilo[k] = w.z;
@@ -472,18 +492,18 @@ __device__ inline Candidate node_candidate(const PointsK<K>& Q, f3 p0, f3 p1, co
 
 // The candidate of internal node a from its stored summary: the 14 extremal
 // vertices (min, max per slab), the furthest slab pair (first on ties), then
-// node_candidate.  kCg reads the vertices through L2 (vertices written
-// earlier in the same kernel); nz is -0.0f from a kernel argument (mul2).
-template <bool kCg>
+// node_candidate.  SumSrc / VertSrc say where the summaries and the vertices
+// were written (ld_src); nz is -0.0f from a kernel argument (mul2).
+template <Src SumSrc, Src VertSrc>
 __device__ __forceinline__ Candidate summary_candidate(const uint4* summary, const kr_vec3* verts, size_t a,
                                                        float nz, Summary& s) {
-    load_summary(summary + 7 * a, s);
+    load_summary<SumSrc>(summary + 7 * a, s);
     PointsK<14> P;
     P.nz = splat2(nz);
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
-        P.set(2 * k, kCg ? load_vertex_cg(verts, s.ilo[k]) : load_vertex(verts, s.ilo[k]));
-        P.set(2 * k + 1, kCg ? load_vertex_cg(verts, s.ihi[k]) : load_vertex(verts, s.ihi[k]));
+        P.set(2 * k, load_vertex_src<VertSrc>(verts, s.ilo[k]));
+        P.set(2 * k + 1, load_vertex_src<VertSrc>(verts, s.ihi[k]));
     }
     int at = 0;
     float far = len2_3(sub3(P.get(1), P.get(0)));

@@ -157,17 +157,17 @@ __device__ __forceinline__ Carry complete_node(const UpArgs& a, uint32_t p, uint
 // (arrive_at: a GPU-scope acquire/release counter by default) completes it
 // from the sibling's outputs.
 //
-// Fresh: the node records' children, the parents, the counts and the sorted
-// triangles were written earlier in the same kernel (the one-CTA-per-mesh
-// batch build), so they are read through L2 like the rest; otherwise they
-// were written before the kernel and go through the read-only path.
+// Pre says where the node records' children, the parents, the counts and
+// the sorted triangles were written (before the kernel in the chain, by this
+// CTA in the one-CTA-per-mesh batch build), Sib where the sibling's outputs
+// were (in this kernel by any SM in the chain, by this CTA in the batch).
 // Arrival at internal node p through the global counters a.visits
 // (GPU-scope acquire/release): walks from any CTA.
 struct GlobalArrive {
     __device__ __forceinline__ uint32_t operator()(const UpArgs& a, uint32_t p) const { return arrive(a.visits + p); }
 };
 
-template <bool Fresh = false, class Arrive = GlobalArrive>
+template <Src Pre = Src::kReadOnly, Src Sib = Src::kL2, class Arrive = GlobalArrive>
 __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Summary s,
                                         Arrive arrive_at = Arrive{}) {
     const uint32_t internal = a.n - 1;
@@ -180,9 +180,9 @@ __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Su
         }
         // written before this kernel: read ahead of the arrival
         const uint32_t* pw = reinterpret_cast<const uint32_t*>(a.nodes + p);
-        const uint32_t L = Fresh ? __ldcg(pw + 6) : __ldg(pw + 6), R = Fresh ? __ldcg(pw + 7) : __ldg(pw + 7);
-        const uint32_t grand = Fresh ? __ldcg(a.parents + p) : __ldg(a.parents + p);
-        const uint32_t count = Fresh ? __ldcg(a.counts + p) : __ldg(a.counts + p);
+        const uint32_t L = ld_src<Pre>(pw + 6), R = ld_src<Pre>(pw + 7);
+        const uint32_t grand = ld_src<Pre>(a.parents + p);
+        const uint32_t count = ld_src<Pre>(a.counts + p);
         if (arrive_at(a, p) == 0) return;
         const bool from_left = (L == child);
         const uint32_t other = from_left ? R : L;
@@ -191,11 +191,11 @@ __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Su
             const uint32_t* sw = reinterpret_cast<const uint32_t*>(a.nodes + other);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                o.lo[k] = __uint_as_float(__ldcg(sw + k));
-                o.hi[k] = __uint_as_float(__ldcg(sw + 3 + k));
+                o.lo[k] = __uint_as_float(ld_src<Sib>(sw + k));
+                o.hi[k] = __uint_as_float(ld_src<Sib>(sw + 3 + k));
             }
         }
-        o.cost = __ldcg(a.costs + other);
+        o.cost = ld_src<Sib>(a.costs + other);
         c = from_left ? complete_node(a, p, L, R, count, c, o) : complete_node(a, p, L, R, count, o, c);
         if (a.summary) {
             const bool sleaf = other >= internal;
@@ -204,8 +204,7 @@ __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Su
                 const kr_vec3* pts = reinterpret_cast<const kr_vec3*>(a.tris);
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
-                    v[i] = Fresh ? load_vertex_cg(pts, 3 * (other - internal) + i)
-                                 : load_vertex(pts, 3 * (other - internal) + i);
+                    v[i] = load_vertex_src<Pre>(pts, 3 * (other - internal) + i);
             }
 #pragma unroll
             for (int k = 0; k < 7; ++k) {
@@ -213,7 +212,7 @@ __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Su
                 if (sleaf) {
                     sib = leaf_slab(v, other - internal, k);
                 } else {
-                    const uint4 q = __ldcg(a.summary + 7 * static_cast<size_t>(other) + k);
+                    const uint4 q = ld_src<Sib>(a.summary + 7 * static_cast<size_t>(other) + k);
                     sib = Slab{__uint_as_float(q.x), __uint_as_float(q.y), q.z, q.w};
                 }
                 const Slab own = slab_of(s, k);
