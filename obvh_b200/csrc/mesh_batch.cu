@@ -336,8 +336,8 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
         wd[6] = i;  // primitivesOffset
         wd[7] = 0;
         wd[8] = 1;  // one primitive, axis 0
-        pipeline::store_words(nodes, ni + j, wd, 9);
-        if (want_collapse) pipeline::store_words(collapsed, ni + j, wd, 9);
+        pipeline::store_words<Src::kOwnCta>(nodes, ni + j, wd, 9);
+        if (want_collapse) pipeline::store_words<Src::kOwnCta>(collapsed, ni + j, wd, 9);
         const uint4 f = __ldg(F + i);
         const f3 v0 = load_vertex(V, f.x), v1 = load_vertex(V, f.y), v2 = load_vertex(V, f.z);
         float* tp = tris + 9 * static_cast<size_t>(j);
@@ -416,6 +416,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
                                                         mk3(c.ax[6], c.ax[7], c.ax[8]), a.nz);
             float lo[3] = {c.olo[0], c.olo[1], c.olo[2]}, hi[3] = {c.ohi[0], c.ohi[1], c.ohi[2]};
             const float* tp = tris + 9 * static_cast<size_t>(ld_own(first + i));
+#pragma unroll 4
             for (uint32_t k = 0; k < cnt; ++k) obbtree::project_tri_own(tp + 9 * k, ax, lo, hi);
             obbtree::finalize_node(c, mk3(lo[0], lo[1], lo[2]), mk3(hi[0], hi[1], hi[2]), obbs + i, xfs + i);
         }
@@ -427,6 +428,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
                                                         mk3(c.ax[6], c.ax[7], c.ax[8]), a.nz);
             float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
             const float* tp = tris + 9 * static_cast<size_t>(ld_own(first + i));
+#pragma unroll 4
             for (uint32_t k = lane; k < cnt; k += 32) obbtree::project_tri_own(tp + 9 * k, ax, lo, hi);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {

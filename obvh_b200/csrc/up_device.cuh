@@ -21,9 +21,19 @@ using namespace tree;
 constexpr uint32_t kMaxLeafSize = 8;
 constexpr uint32_t kHidden = 0xffffu;
 
+// A store of data that the same kernel reads back later: through L2
+// (__stcg) for readers on any SM, a plain store for readers in this CTA
+// (Src::kOwnCta, which then read it through L1).
+template <Src S, class T>
+__device__ __forceinline__ void st_dst(T* p, T v) {
+    if constexpr (S == Src::kOwnCta) *p = v;
+    else __stcg(p, v);
+}
+
+template <Src S = Src::kL2>
 __device__ __forceinline__ void store_words(kr_bvh_node* nodes, uint32_t i, const uint32_t* w, int count) {
     uint32_t* d = reinterpret_cast<uint32_t*>(nodes + i);
-    for (int k = 0; k < count; ++k) __stcg(d + k, w[k]);
+    for (int k = 0; k < count; ++k) st_dst<S>(d + k, w[k]);
 }
 
 // Summary of sorted leaf j; its vertex ids are the triangle slots 3j..3j+2.
@@ -85,9 +95,10 @@ __device__ __forceinline__ Slab leaf_slab(const f3* v, uint32_t j, int k) {
     return o;
 }
 
+template <Src S = Src::kL2>
 __device__ __forceinline__ void store_slab(uint4* summary, uint32_t p, int k, const Slab& v) {
-    __stcg(summary + 7 * static_cast<size_t>(p) + k,
-           make_uint4(__float_as_uint(v.lo), __float_as_uint(v.hi), v.ilo, v.ihi));
+    st_dst<S>(summary + 7 * static_cast<size_t>(p) + k,
+              make_uint4(__float_as_uint(v.lo), __float_as_uint(v.hi), v.ilo, v.ihi));
 }
 
 struct UpArgs {
@@ -113,6 +124,7 @@ struct UpArgs {
 // Completes internal node p (children L, R; count primitives) from its
 // children's carries: writes its bounds, cost and collapse marks and returns
 // its carry.  (The summary is merged by the caller.)
+template <Src S = Src::kL2>
 __device__ __forceinline__ Carry complete_node(const UpArgs& a, uint32_t p, uint32_t L, uint32_t R, uint32_t count,
                                                const Carry& l, const Carry& r) {
     Carry o;
@@ -126,8 +138,8 @@ __device__ __forceinline__ Carry complete_node(const UpArgs& a, uint32_t p, uint
     w[6] = L;
     w[7] = R;
     w[8] = 0;
-    store_words(a.nodes, p, w, 6);
-    if (a.collapsed) store_words(a.collapsed, p, w, 9);
+    store_words<S>(a.nodes, p, w, 6);
+    if (a.collapsed) store_words<S>(a.collapsed, p, w, 9);
     const float area = box_area(o.lo, o.hi);
     if (a.flags) {
         // bvh_mark_collapse_kernel (transforms.cu:111-133)
@@ -140,15 +152,15 @@ __device__ __forceinline__ Carry complete_node(const UpArgs& a, uint32_t p, uint
             a.flags[R] = 1;
             // nPrimitives = 0xFFFF; the axis byte and the pad of every node
             // record are zero here, so the whole word is written
-            __stcg(reinterpret_cast<uint32_t*>(a.collapsed + L) + 8, kHidden);
-            __stcg(reinterpret_cast<uint32_t*>(a.collapsed + R) + 8, kHidden);
+            st_dst<S>(reinterpret_cast<uint32_t*>(a.collapsed + L) + 8, kHidden);
+            st_dst<S>(reinterpret_cast<uint32_t*>(a.collapsed + R) + 8, kHidden);
         } else {
             o.cost = node_cost;
         }
     } else {
         o.cost = 1.2f * area + r.cost + l.cost;  // calculate_aabbs_kernel (lbvh.cu:452)
     }
-    __stcg(a.costs + p, o.cost);
+    st_dst<S>(a.costs + p, o.cost);
     return o;
 }
 
@@ -196,7 +208,7 @@ __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Su
             }
         }
         o.cost = ld_src<Sib>(a.costs + other);
-        c = from_left ? complete_node(a, p, L, R, count, c, o) : complete_node(a, p, L, R, count, o, c);
+        c = from_left ? complete_node<Sib>(a, p, L, R, count, c, o) : complete_node<Sib>(a, p, L, R, count, o, c);
         if (a.summary) {
             const bool sleaf = other >= internal;
             f3 v[3];
@@ -218,7 +230,7 @@ __device__ __forceinline__ void walk_up(const UpArgs& a, uint32_t x, Carry c, Su
                 const Slab own = slab_of(s, k);
                 const Slab m = from_left ? merge_slab(own, sib) : merge_slab(sib, own);
                 set_slab(s, k, m);
-                store_slab(a.summary, p, k, m);
+                store_slab<Sib>(a.summary, p, k, m);
             }
         }
         if (a.done_list) a.done_list[atomicAdd(a.done_count, 1u)] = p;
