@@ -121,3 +121,12 @@ def test_many_uneven_meshes_in_a_graph():
     rng = np.random.default_rng(40)
     sizes = [int(x) for x in np.exp(rng.uniform(np.log(2), np.log(16384), size=300))]
     _check(_meshes(sizes, seed=40), graph=True)
+
+
+def test_chain_meshes_in_a_graph():
+    """Meshes above the CTA limit go through the whole-GPU chain, which forks
+    onto helper streams (the walk up the tree beside the candidate search, the
+    collapse beside the extents); captured into the batch's graph, the forks
+    become parallel branches and every result stays its lone build's."""
+    batch = _check(_meshes([20000, 40000, 700, "knot"], seed=50), graph=True)
+    assert batch.info()["chain_meshes"] >= 2
