@@ -43,6 +43,7 @@ typedef struct obvh_server_stats {
     kr_scalar p50_ms, p99_ms, mean_ms, max_ms; /* submit -> result ready, over completed requests */
     kr_size arena_bytes, peak_bytes, in_use_bytes;
     kr_scalar span_s;                          /* first submit -> last completion */
+    kr_u64 build_batches;                      /* launches that built several small meshes at once */
 } obvh_server_stats;
 
 /* Device pointers of a completed build, valid until obvh_server_release.

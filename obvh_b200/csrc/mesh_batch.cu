@@ -37,6 +37,7 @@
 #include "obb_device.cuh"
 #include "obvh_build.h"
 #include "obvh_build_batch.h"
+#include "mesh_batch_host.h"
 #include "pipeline_host.h"
 #include "runtime.h"
 #include "tree_device.cuh"
@@ -97,6 +98,7 @@ SlotLayout slot_layout(uint32_t m) {
 
 struct Args {
     const Job* jobs;
+    const JobBases* bases;  // null: the CSR arrays below, else bases[J.mesh] (mesh_batch_host.h)
     uint32_t njobs;
     uint32_t* next_job;  // zeroed before the launch
     const kr_vec3* verts;
@@ -256,15 +258,33 @@ __device__ __forceinline__ obbtree::Cand load_cand_own(const obbtree::Cand* cand
 __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
     const uint32_t t = threadIdx.x, lane = t & 31, w = t >> 5;
     const uint32_t n = J.n, ni = n - 1, nn = 2 * n - 1;
-    const kr_vec3* V = a.verts + J.vbase;
-    const uint4* F = a.faces + J.fbase;
-    kr_bvh_node* nodes = a.nodes + J.nbase;
-    uint32_t* parents = a.parents + J.nbase;
-    uint32_t* counts = a.counts + J.nbase;
-    float* costs = a.costs + J.nbase;
-    kr_obb3* obbs = a.obbs ? a.obbs + J.nbase : nullptr;
-    kr_mat4* xfs = a.obbs ? a.xfs + J.nbase : nullptr;
-    kr_bvh_node* collapsed = a.collapsed ? a.collapsed + J.nbase : nullptr;
+    JobBases B;
+    if (a.bases) {
+        B = a.bases[J.mesh];
+    } else {
+        B.verts = a.verts + J.vbase;
+        B.faces = a.faces + J.fbase;
+        B.nodes = a.nodes + J.nbase;
+        B.parents = a.parents + J.nbase;
+        B.counts = a.counts + J.nbase;
+        B.costs = a.costs + J.nbase;
+        B.bounds = a.bounds ? a.bounds + 2 * static_cast<size_t>(J.mesh) : nullptr;
+        B.obbs = a.obbs ? a.obbs + J.nbase : nullptr;
+        B.xfs = a.obbs ? a.xfs + J.nbase : nullptr;
+        B.collapsed = a.collapsed ? a.collapsed + J.nbase : nullptr;
+        B.primitives = a.collapsed ? a.primitives + J.fbase : nullptr;
+        B.ci = a.ci;
+        B.ct = a.ct;
+    }
+    const kr_vec3* V = B.verts;
+    const uint4* F = B.faces;
+    kr_bvh_node* nodes = B.nodes;
+    uint32_t* parents = B.parents;
+    uint32_t* counts = B.counts;
+    float* costs = B.costs;
+    kr_obb3* obbs = B.obbs;
+    kr_mat4* xfs = B.xfs;
+    kr_bvh_node* collapsed = B.collapsed;
     float* boxes = reinterpret_cast<float*>(slot + a.slot.boxes);
     uint32_t* keys_a = reinterpret_cast<uint32_t*>(slot + a.slot.keys_a);
     uint32_t* vals_a = reinterpret_cast<uint32_t*>(slot + a.slot.vals_a);
@@ -277,8 +297,8 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
     uint8_t* flags = reinterpret_cast<uint8_t*>(slot + a.slot.flags);
     uint32_t* sizes = reinterpret_cast<uint32_t*>(slot + a.slot.sizes);
     uint32_t* offsets = reinterpret_cast<uint32_t*>(slot + a.slot.offsets);
-    const bool want_obbs = a.obbs != nullptr, want_collapse = a.collapsed != nullptr;
-    const float leaf_ct = want_collapse ? a.ct : 1.0f;
+    const bool want_obbs = obbs != nullptr, want_collapse = collapsed != nullptr;
+    const float leaf_ct = want_collapse ? B.ct : 1.0f;
 
     // ---- 1: triangle boxes; scene and centroid boxes (tri_bounds_kernel) ----
     for (uint32_t i = t; i < (ni + 3) / 4; i += kThreads) sm.visits[i] = 0;
@@ -311,7 +331,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
         float v = sm.red[0][t];
         for (int q = 1; q < kWarps; ++q) v = mn ? fminf(v, sm.red[q][t]) : fmaxf(v, sm.red[q][t]);
         sm.box[t] = v;
-        if (a.bounds) reinterpret_cast<float*>(a.bounds + 2 * static_cast<size_t>(J.mesh))[t] = v;
+        if (B.bounds) reinterpret_cast<float*>(B.bounds)[t] = v;
     }
     stage_sync();
 
@@ -357,7 +377,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
     // ---- 6: bottom-up pass from every leaf (walk_up of the chain) ------------
     {
         pipeline::UpArgs ua{nodes,  collapsed, parents, first, tris, n, counts, costs, want_collapse ? flags : nullptr,
-                            a.ci,   a.ct,      want_obbs ? summary : nullptr, nullptr, a.err};
+                            B.ci,   B.ct,      want_obbs ? summary : nullptr, nullptr, a.err};
         // thread t walks up from the leaves of its run [t R, (t + 1) R), in order
         const uint32_t run = (n + kThreads - 1) / kThreads;
         const CtaArrive arrive{sm.visits, first, counts, run, t};
@@ -453,7 +473,7 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
         const uint32_t total = block_scan(offsets, nn, sm);
         if (t == 0) a.mesh_slots[J.mesh] = total;
         stage_sync();
-        uint32_t* prims = a.primitives + J.fbase;
+        uint32_t* prims = B.primitives;
         for (uint32_t c = t; c < nn; c += kThreads) {
             const uint32_t cnt = ld_own(sizes + c);
             if (cnt == 0) continue;
@@ -591,6 +611,7 @@ kr_error enqueue(Plan& P, const Buffers& b, cudaStream_t s) {
     if (!P.cta_jobs.empty()) {
         Args a;
         a.jobs = static_cast<const Job*>(P.jobs.ptr);
+        a.bases = nullptr;
         a.njobs = static_cast<uint32_t>(P.cta_jobs.size());
         a.next_job = status + 1;
         a.verts = b.verts;
@@ -659,6 +680,101 @@ kr_error plan(Plan& P, const kr_size* voff, const kr_size* foff, kr_size meshes)
         OBVH_TRY(obvh_build_workspace_init(P.chain_ws.ptr, P.chain_max, nullptr));
         OBVH_TRY_CUDA(cudaDeviceSynchronize());
     }
+    return kr_success;
+}
+
+struct Runner {
+    int device = 0;
+    int grid = 0;
+    uint32_t capacity = 0;
+    SlotLayout slot{};
+    DeviceBuffer scratch, jobs, bases, status;
+    PinnedBuffer staging;  // the jobs, then the bases, on their way up
+    std::vector<uint32_t> order;
+    ~Runner() {
+        scratch.release();
+        jobs.release();
+        bases.release();
+        status.release();
+        staging.release();
+    }
+};
+
+uint32_t runner_max_faces() { return kMaxFaces; }
+
+kr_error make_runner(uint32_t capacity, Runner** out) {
+    *out = nullptr;
+    if (capacity == 0) return "make_runner: no capacity";
+    Runner* r = new Runner();
+    r->capacity = capacity;
+    r->slot = slot_layout(kMaxFaces);
+    r->grid = device_info().sm_count;  // one CTA per SM: a server round holds a few meshes
+    kr_error e = kr_success;
+    if (cudaGetDevice(&r->device) != cudaSuccess) e = "make_runner: no current device";
+    if (!e) e = r->scratch.reserve(r->slot.total * static_cast<size_t>(r->grid));
+    if (!e) e = r->jobs.reserve(sizeof(Job) * capacity);
+    if (!e) e = r->bases.reserve(sizeof(JobBases) * capacity);
+    if (!e) e = r->status.reserve(4ull * (2 + capacity));
+    if (!e) e = r->staging.reserve((sizeof(Job) + sizeof(JobBases)) * capacity);
+    if (!e && cudaFuncSetAttribute(reinterpret_cast<const void*>(mesh_batch_kernel),
+                                   cudaFuncAttributePreferredSharedMemoryCarveout, kSmemCarveout) != cudaSuccess)
+        e = "make_runner: setting the kernel's carveout failed";
+    if (e) {
+        delete r;
+        return e;
+    }
+    *out = r;
+    return kr_success;
+}
+
+void free_runner(Runner* r) { delete r; }
+
+size_t runner_device_bytes(const Runner& r) {
+    return r.scratch.bytes + r.jobs.bytes + r.bases.bytes + r.status.bytes;
+}
+
+const uint32_t* status(const Runner& r) { return static_cast<const uint32_t*>(r.status.ptr); }
+
+kr_error run(Runner& r, const JobBases* bases, const uint32_t* faces, uint32_t count, cudaStream_t s) {
+    if (count == 0) return kr_success;
+    if (count > r.capacity) return "meshbatch::run: more meshes than the runner's capacity";
+    int dev = 0;
+    OBVH_TRY_CUDA(cudaGetDevice(&dev));
+    if (dev != r.device) return "meshbatch::run: the runner belongs to another device";
+    for (uint32_t i = 0; i < count; ++i)
+        if (faces[i] < 2 || faces[i] > kMaxFaces) return "meshbatch::run: a mesh outside 2..runner_max_faces() faces";
+    // largest first, as the CSR batch plans its jobs
+    r.order.resize(count);
+    for (uint32_t i = 0; i < count; ++i) r.order[i] = i;
+    std::stable_sort(r.order.begin(), r.order.end(), [&](uint32_t x, uint32_t y) { return faces[x] > faces[y]; });
+    Job* jh = static_cast<Job*>(r.staging.ptr);
+    JobBases* bh = reinterpret_cast<JobBases*>(jh + r.capacity);
+    for (uint32_t k = 0; k < count; ++k) {
+        Job J{};
+        J.n = faces[r.order[k]];
+        J.mesh = r.order[k];
+        jh[k] = J;
+    }
+    std::copy(bases, bases + count, bh);
+    uint32_t* st = static_cast<uint32_t*>(r.status.ptr);
+    OBVH_TRY_CUDA(cudaMemcpyAsync(r.jobs.ptr, jh, sizeof(Job) * count, cudaMemcpyHostToDevice, s));
+    OBVH_TRY_CUDA(cudaMemcpyAsync(r.bases.ptr, bh, sizeof(JobBases) * count, cudaMemcpyHostToDevice, s));
+    OBVH_TRY_CUDA(cudaMemsetAsync(st, 0, 4ull * (2 + count), s));
+    Args a{};
+    a.jobs = static_cast<const Job*>(r.jobs.ptr);
+    a.bases = static_cast<const JobBases*>(r.bases.ptr);
+    a.njobs = count;
+    a.next_job = st + 1;
+    a.scratch = static_cast<char*>(r.scratch.ptr);
+    a.slot_bytes = r.slot.total;
+    a.slot = r.slot;
+    a.err = st;
+    a.mesh_slots = st + 2;
+    a.nz = -0.0f;
+    const int grid = static_cast<int>(std::min<uint32_t>(count, static_cast<uint32_t>(r.grid)));
+    ProfScope prof_scope_("mesh_batch_kernel", s);
+    mesh_batch_kernel<<<grid, kThreads, 0, s>>>(a);
+    OBVH_TRY_CUDA(cudaGetLastError());
     return kr_success;
 }
 

@@ -10,7 +10,10 @@
 //      waiting only for a free lane lets later fits pass);
 //   3. launches all admitted fits as one batched persistent kernel on a free
 //      fit round (two rounds alternate, so the next batch's copies overlap the
-//      running one), and each admitted build on a free lane's stream.
+//      running one), the admitted builds of up to 16,384 triangles as one
+//      launch of the one-CTA-per-mesh build kernel on the batch round's
+//      stream, and each larger build on a free lane's stream (the whole-GPU
+//      chain).
 // Callers' threads only touch host-side state under the mutex.
 #include <cuda_runtime.h>
 
@@ -27,6 +30,7 @@
 #include <vector>
 
 #include "dito_batch_host.h"
+#include "mesh_batch_host.h"
 #include "obvh_build.h"
 #include "obvh_server.h"
 #include "pipeline_host.h"
@@ -128,6 +132,18 @@ struct FitRound {
     bool busy = false;
 };
 
+// The small builds admitted together, built by one launch of the
+// one-CTA-per-mesh kernel (mesh_batch_host.h) into their own arena blocks.
+struct BuildBatchRound {
+    meshbatch::Runner* runner = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    PinnedBuffer words;  // the run's status: error, job counter, each mesh's primitive slots
+    std::vector<Request*> reqs;
+    bool busy = false;
+};
+constexpr uint32_t kSmallBuildsPerRound = 1024;
+
 struct BuildLane {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
@@ -173,16 +189,18 @@ public:
     std::deque<Request*> pending;
     std::vector<Request*> admitted_fits;
     std::vector<Request*> admitted_builds;
+    std::vector<Request*> admitted_small;  // builds of 2..runner_max_faces() triangles, for a batch round
     std::unordered_map<uint64_t, std::unique_ptr<Request>> all;
     uint64_t next_id = 1;
     std::vector<FitRound> rounds;
     std::vector<BuildLane> lanes;
+    BuildBatchRound brd;
     std::thread worker;
     bool stop = false;
     bool kick = false;       // a submit or a release since the scheduler last looked
     uint64_t in_flight = 0;  // submitted, not yet done or failed
     // statistics
-    uint64_t submitted = 0, completed = 0, failed = 0, fits = 0, builds = 0, fit_batches = 0;
+    uint64_t submitted = 0, completed = 0, failed = 0, fits = 0, builds = 0, fit_batches = 0, build_batches = 0;
     std::vector<float> latencies;
     Clock::time_point first_submit{}, last_done{};
     kr_error fatal = nullptr;
@@ -207,6 +225,10 @@ public:
             if (l.stream) cudaStreamDestroy(l.stream);
             l.words.release();
         }
+        if (brd.runner) meshbatch::free_runner(brd.runner);
+        if (brd.done) cudaEventDestroy(brd.done);
+        if (brd.stream) cudaStreamDestroy(brd.stream);
+        brd.words.release();
         if (base) cudaFree(base);
     }
 
@@ -230,6 +252,10 @@ public:
             OBVH_TRY_CUDA(cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming));
             OBVH_TRY(l.words.reserve(16));
         }
+        OBVH_TRY_CUDA(cudaStreamCreateWithFlags(&brd.stream, cudaStreamNonBlocking));
+        OBVH_TRY_CUDA(cudaEventCreateWithFlags(&brd.done, cudaEventDisableTiming));
+        OBVH_TRY(meshbatch::make_runner(kSmallBuildsPerRound, &brd.runner));
+        OBVH_TRY(brd.words.reserve(4ull * (2 + kSmallBuildsPerRound)));
         worker = std::thread([this] { loop(); });
         return kr_success;
     }
@@ -314,6 +340,22 @@ public:
                 it = pending.erase(it);
                 continue;
             }
+            if (r->nfaces >= 2 && r->nfaces <= meshbatch::runner_max_faces()) {
+                // a small build: the next batch round builds it, with the
+                // round's own scratch
+                Block in, out;
+                if (!take_block(in, in_bytes)) break;
+                if (!take_block(out, o.total)) {
+                    free_block(in);
+                    break;
+                }
+                r->input = in;
+                r->output = out;
+                r->state = State::Admitted;
+                admitted_small.push_back(r);
+                it = pending.erase(it);
+                continue;
+            }
             if (free_lanes == 0) {  // memory may be there; let fits behind pass
                 ++it;
                 continue;
@@ -341,6 +383,20 @@ public:
 
     // Retire finished rounds and lanes (under the lock).
     void retire() {
+        if (brd.busy && cudaEventQuery(brd.done) != cudaErrorNotReady) {
+            const cudaError_t e = cudaEventQuery(brd.done);
+            const uint32_t* w = static_cast<const uint32_t*>(brd.words.ptr);
+            const kr_error ke = e != cudaSuccess ? cuda_error(e) : (w[0] ? "obvh_server: device error in a build" : nullptr);
+            for (size_t i = 0; i < brd.reqs.size(); ++i) {
+                Request* r = brd.reqs[i];
+                r->view.primitive_slots = w[2 + i];
+                free_block(r->input);
+                if (ke) free_block(r->output);
+                finish(r, ke);
+            }
+            brd.reqs.clear();
+            brd.busy = false;
+        }
         for (FitRound& rd : rounds) {
             if (!rd.busy || cudaEventQuery(rd.done) == cudaErrorNotReady) continue;
             const cudaError_t e = cudaEventQuery(rd.done);
@@ -425,22 +481,23 @@ public:
         for (Request* r : batch) r->state = State::Running;
     }
 
-    void launch_build(BuildLane& l, Request* r) {
+    // A build's inputs on the device (copied in on `s` from host memory) and
+    // its output view over its output block.
+    kr_error stage_build(Request* r, cudaStream_t s, const kr_vec3** dv, const kr_uvec4** df) {
         const BuildOutputs o = build_outputs(r->nfaces, r->flags);
         char* out = base + r->output.off;
-        const kr_vec3* dv = r->verts;
-        const kr_uvec4* df = r->faces;
+        *dv = r->verts;
+        *df = r->faces;
         kr_error e = kr_success;
         if (!r->device_input) {
             char* in = base + r->input.off;
             kr_vec3* v = reinterpret_cast<kr_vec3*>(in);
             kr_uvec4* f = reinterpret_cast<kr_uvec4*>(in + (12 * r->nverts + 255) / 256 * 256);
-            cudaError_t ce = cudaMemcpyAsync(v, r->verts, 12 * r->nverts, cudaMemcpyHostToDevice, l.stream);
-            if (ce == cudaSuccess)
-                ce = cudaMemcpyAsync(f, r->faces, 16ull * r->nfaces, cudaMemcpyHostToDevice, l.stream);
+            cudaError_t ce = cudaMemcpyAsync(v, r->verts, 12 * r->nverts, cudaMemcpyHostToDevice, s);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(f, r->faces, 16ull * r->nfaces, cudaMemcpyHostToDevice, s);
             if (ce != cudaSuccess) e = cuda_error(ce);
-            dv = v;
-            df = f;
+            *dv = v;
+            *df = f;
         }
         obvh_server_build_view& vw = r->view;
         vw.nodes = reinterpret_cast<kr_bvh_node*>(out + o.nodes);
@@ -453,6 +510,55 @@ public:
         vw.collapsed = (r->flags & OBVH_BUILD_COLLAPSE) ? reinterpret_cast<kr_bvh_node*>(out + o.collapsed) : nullptr;
         vw.primitives = (r->flags & OBVH_BUILD_COLLAPSE) ? reinterpret_cast<kr_u32*>(out + o.prims) : nullptr;
         vw.face_count = r->nfaces;
+        return e;
+    }
+
+    // The small builds of a batch round, one launch for all of them.
+    void launch_small_builds(std::vector<Request*>& batch) {
+        std::vector<meshbatch::JobBases> bases(batch.size());
+        std::vector<uint32_t> faces(batch.size());
+        kr_error e = kr_success;
+        for (size_t i = 0; i < batch.size() && !e; ++i) {
+            Request* r = batch[i];
+            const kr_vec3* dv = nullptr;
+            const kr_uvec4* df = nullptr;
+            e = stage_build(r, brd.stream, &dv, &df);
+            const obvh_server_build_view& vw = r->view;
+            bases[i] = meshbatch::JobBases{dv, reinterpret_cast<const uint4*>(df), vw.nodes, vw.parents,
+                                           vw.primitive_counts, vw.costs, vw.bounds, vw.obbs, vw.transforms,
+                                           vw.collapsed, vw.primitives, r->ci, r->ct};
+            faces[i] = r->nfaces;
+        }
+        const uint32_t k = static_cast<uint32_t>(batch.size());
+        if (!e) e = meshbatch::run(*brd.runner, bases.data(), faces.data(), k, brd.stream);
+        if (!e) {
+            cudaError_t ce = cudaMemcpyAsync(brd.words.ptr, meshbatch::status(*brd.runner), 4ull * (2 + k),
+                                             cudaMemcpyDeviceToHost, brd.stream);
+            if (ce == cudaSuccess) ce = cudaEventRecord(brd.done, brd.stream);
+            if (ce != cudaSuccess) e = cuda_error(ce);
+        }
+        std::lock_guard<std::mutex> lock(m);
+        ++build_batches;
+        if (e) {
+            cudaStreamSynchronize(brd.stream);
+            for (Request* r : batch) {
+                free_block(r->input);
+                free_block(r->output);
+                finish(r, e);
+            }
+            brd.busy = false;
+            done.notify_all();
+            return;
+        }
+        brd.reqs = batch;
+        for (Request* r : batch) r->state = State::Running;
+    }
+
+    void launch_build(BuildLane& l, Request* r) {
+        const kr_vec3* dv = nullptr;
+        const kr_uvec4* df = nullptr;
+        kr_error e = stage_build(r, l.stream, &dv, &df);
+        obvh_server_build_view& vw = r->view;
         void* ws = base + r->scratch.off;
         if (!e) e = obvh_build_workspace_init(ws, r->nfaces, l.stream);
         if (!e)
@@ -506,6 +612,13 @@ public:
                     rd->busy = true;
                 }
             }
+            std::vector<Request*> small;
+            if (!brd.busy && !admitted_small.empty()) {
+                const size_t k = std::min<size_t>(admitted_small.size(), kSmallBuildsPerRound);
+                small.insert(small.end(), admitted_small.begin(), admitted_small.begin() + k);
+                admitted_small.erase(admitted_small.begin(), admitted_small.begin() + k);
+                brd.busy = true;
+            }
             std::vector<std::pair<BuildLane*, Request*>> starts;
             for (BuildLane& l : lanes) {
                 if (admitted_builds.empty()) break;
@@ -515,10 +628,12 @@ public:
                 starts.emplace_back(&l, l.req);
             }
             const bool busy = std::any_of(rounds.begin(), rounds.end(), [](const FitRound& r) { return r.busy; }) ||
-                              std::any_of(lanes.begin(), lanes.end(), [](const BuildLane& l) { return l.req; });
-            if (rd || !starts.empty()) {
+                              std::any_of(lanes.begin(), lanes.end(), [](const BuildLane& l) { return l.req; }) ||
+                              brd.busy;
+            if (rd || !starts.empty() || !small.empty()) {
                 lock.unlock();
                 if (rd) launch_fits(*rd, batch);
+                if (!small.empty()) launch_small_builds(small);
                 for (auto& sl : starts) launch_build(*sl.first, sl.second);
                 lock.lock();
                 continue;
@@ -527,7 +642,7 @@ public:
                 for (Request* r : pending) finish(r, "obvh_server: shut down before the request was admitted");
                 pending.clear();
                 done.notify_all();
-                if (!busy && admitted_fits.empty() && admitted_builds.empty()) break;
+                if (!busy && admitted_fits.empty() && admitted_builds.empty() && admitted_small.empty()) break;
             }
             if (busy) {
                 wake.wait_for(lock, std::chrono::microseconds(20));
@@ -735,6 +850,7 @@ extern "C" kr_error obvh_server_get_stats(obvh_server server, obvh_server_stats*
     o.fits = s.fits;
     o.builds = s.builds;
     o.fit_batches = s.fit_batches;
+    o.build_batches = s.build_batches;
     std::vector<float> l = s.latencies;
     if (!l.empty()) {
         std::sort(l.begin(), l.end());

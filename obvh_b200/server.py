@@ -25,7 +25,7 @@ class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("submitted", "completed", "failed", "fits", "builds", "fit_batches")] + \
                [(n, ctypes.c_float) for n in ("p50_ms", "p99_ms", "mean_ms", "max_ms")] + \
                [(n, ctypes.c_uint64) for n in ("arena_bytes", "peak_bytes", "in_use_bytes")] + \
-               [("span_s", ctypes.c_float)]
+               [("span_s", ctypes.c_float), ("build_batches", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -99,6 +99,7 @@ def test_results_alone_equal_results_in_the_mix(torch):
     st = srv.stats()
     assert st["completed"] == len(jobs) and st["failed"] == 0
     assert st["fit_batches"] >= 1 and st["peak_bytes"] <= st["arena_bytes"]
+    assert st["build_batches"] >= 1  # the builds of up to 16,384 triangles went through batch rounds
     assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
 
     builder = bvh.ObvhBuilder()
@@ -161,4 +162,31 @@ def test_many_small_fits_are_batched(torch):
     assert st["completed"] == 2000 and st["fit_batches"] < 2000
     for s, rid in zip(sets[::50], ids[::50]):
         assert same_bits(srv.fit_result(rid), dito.points_obb(s))
+    srv.close()
+
+
+def test_small_builds_batched_in_one_round_equal_their_lone_builds(torch):
+    """Builds of up to 16,384 triangles admitted together go to one launch of
+    the one-CTA-per-mesh kernel, each into its own arena blocks, with its own
+    flags and SAH constants; every result equals its lone obvh_build_async,
+    bit for bit, and the larger builds beside them still go through lanes."""
+    from obvh_b200.server import Server
+    rng = np.random.default_rng(21)
+    sizes = [2, 3, 64, 255, 256, 257, 1000, 5000, 16384, 16385, 40000] + \
+            [int(np.exp(rng.uniform(np.log(2), np.log(16384)))) for _ in range(40)]
+    meshes = [workloads.triangle_soup(n, seed=1300 + i) for i, n in enumerate(sizes)]
+    flags = [[3, 1, 2, 0][i % 4] for i in range(len(meshes))]
+    consts = [(1.2, 1.0) if i % 3 else (0.8, 1.3) for i in range(len(meshes))]
+    srv = Server(budget_bytes=4 << 30, build_lanes=2)
+    ids = [srv.submit_build(v, f, flags=flags[i], ci=consts[i][0], ct=consts[i][1]) for i, (v, f) in enumerate(meshes)]
+    srv.drain()
+    st = srv.stats()
+    assert st["completed"] == len(meshes) and st["failed"] == 0
+    assert 1 <= st["build_batches"] < len(meshes)
+    builder = bvh.ObvhBuilder()
+    for i, (v, f) in enumerate(meshes):
+        alone, slots = _alone_build(builder, v, f, flags[i], *consts[i])
+        _check_build(srv.build_result(ids[i]), alone, slots, flags[i])
+        srv.release(ids[i])
+    assert srv.stats()["in_use_bytes"] == 0
     srv.close()
