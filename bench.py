@@ -283,8 +283,8 @@ def tree_bytes_per_launch(n):
         # tiles: ordered triangles, frames, first leaves and counts in; boxes + transforms (or extent keys) out
         "extents_tile_kernel": 36 * n + 104 * ni + 124 * ni,
         "mark_up_kernel": 36 * nn + 16 * nn + 36 * n,
-        # fused build: leaf node (x2), ordered triangle, leaf box + transform out; box, face, vertices in
-        "leaves_fused_kernel": 4 * n + 24 * n + 52 * n + 72 * n + 36 * n + 124 * n,
+        # fused build: order, face, vertices in; leaf node (x2), ordered triangle, leaf box + transform out
+        "leaves_fused_kernel": 4 * n + 52 * n + 72 * n + 36 * n + 124 * n,
         # fused leaf-to-root pass over the CTA-local nodes: leaf nodes + triangles in, leaf costs + counts out;
         # children, first leaf, count in; bounds, collapsed node, cost, summary out; collapse marks
         "fused_up_local_kernel": 36 * n + 36 * n + 8 * n + 16 * ni + 24 * ni + 36 * ni + 4 * ni + 112 * ni + nn,

@@ -73,7 +73,7 @@ __device__ __forceinline__ uint32_t* stage_at(uint32_t* stage, const void* dst, 
 // Sorted leaf j: node internal + j, its triangle at slot j, its own box.  The
 // CTA's leaves are consecutive, so every output is one contiguous run per CTA:
 // records are staged in shared memory and written out coalesced.
-__global__ void __launch_bounds__(kThreads) leaves_fused_kernel(const float* tri_boxes, const uint32_t* order,
+__global__ void __launch_bounds__(kThreads) leaves_fused_kernel(const uint32_t* order,
                                                                 const kr_vec3* verts, const uint4* faces, uint32_t n,
                                                                 kr_bvh_node* nodes, kr_bvh_node* collapsed,
                                                                 float* tris, kr_obb3* obbs, kr_mat4* xfs) {
@@ -88,15 +88,19 @@ __global__ void __launch_bounds__(kThreads) leaves_fused_kernel(const float* tri
     f3 v0 = mk3(0, 0, 0), v1 = v0, v2 = v0;
     if (live) {
         const uint32_t i = order[j];
-        const float* b = tri_boxes + 6 * static_cast<size_t>(i);
-        for (int k = 0; k < 6; ++k) w[k] = __float_as_uint(b[k]);
-        w[6] = i;  // primitivesOffset
-        w[7] = 0;
-        w[8] = 1;  // one primitive, axis 0
         const uint4 f = __ldg(faces + i);
         v0 = load_vertex(verts, f.x);
         v1 = load_vertex(verts, f.y);
         v2 = load_vertex(verts, f.z);
+        // the triangle's box, as tri_bounds_kernel computed it (lbvh::tri_box:
+        // exact min/max, so recomputing it from the vertices read here gives
+        // the same bits as reading it back)
+        const f3 lo = vmin3(vmin3(v0, v1), v2), hi = vmax3(vmax3(v0, v1), v2);
+        w[0] = __float_as_uint(lo.x); w[1] = __float_as_uint(lo.y); w[2] = __float_as_uint(lo.z);
+        w[3] = __float_as_uint(hi.x); w[4] = __float_as_uint(hi.y); w[5] = __float_as_uint(hi.z);
+        w[6] = i;  // primitivesOffset
+        w[7] = 0;
+        w[8] = 1;  // one primitive, axis 0
     }
     for (int out = 0; out < 2; ++out) {
         kr_bvh_node* dst = out == 0 ? nodes : collapsed;
@@ -600,7 +604,7 @@ kr_error enqueue(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32
     OBVH_TRY(lbvh::enqueue_codes(verts, faces, n, ws + L.lbvh, s, &c));
     {
         ProfScope prof_scope_("leaves_fused_kernel", s);
-        leaves_fused_kernel<<<gn, kThreads, 0, s>>>(c.tri_boxes, c.order, verts, reinterpret_cast<const uint4*>(faces),
+        leaves_fused_kernel<<<gn, kThreads, 0, s>>>(c.order, verts, reinterpret_cast<const uint4*>(faces),
                                                     n, nodes, want_collapse ? collapsed : nullptr, tris,
                                                     want_obbs ? obbs : nullptr, xfs);
     }
