@@ -285,9 +285,10 @@ def tree_bytes_per_launch(n):
         "mark_up_kernel": 36 * nn + 16 * nn + 36 * n,
         # fused build: order, face, vertices in; leaf node (x2), ordered triangle, leaf box + transform out
         "leaves_fused_kernel": 4 * n + 52 * n + 72 * n + 36 * n + 124 * n,
-        # fused leaf-to-root pass over the CTA-local nodes: leaf nodes + triangles in, leaf costs + counts out;
-        # children, first leaf, count in; bounds, collapsed node, cost, summary out; collapse marks
-        "fused_up_local_kernel": 36 * n + 36 * n + 8 * n + 16 * ni + 24 * ni + 36 * ni + 4 * ni + 112 * ni + nn,
+        # fused leaf-to-root pass over the CTA-local nodes: triangles in (the leaf bounds are recomputed from
+        # them), leaf costs + counts out; children, first leaf, count in; bounds, collapsed node, cost, summary
+        # out; collapse marks
+        "fused_up_local_kernel": 36 * n + 8 * n + 16 * ni + 24 * ni + 36 * ni + 4 * ni + 112 * ni + nn,
         # ATRBVH: triangle in, 63-bit key + index out; sorted keys in, working nodes out;
         # leaf triangles + nodes in/out bottom-up; one pass over the working tree per iteration
         "morton63_kernel": 52 * n + 12 * n,

@@ -349,17 +349,18 @@ __device__ void build_mesh(const Args& a, const Job& J, char* slot, Smem& sm) {
     // ---- 4: leaves (leaves_fused_kernel) ---------------------------------------
     for (uint32_t j = t; j < n; j += kThreads) {
         const uint32_t i = ld_own(vals_a + j);
-        const float* b = boxes + 6 * static_cast<size_t>(i);
+        const uint4 f = __ldg(F + i);
+        const f3 v0 = load_vertex(V, f.x), v1 = load_vertex(V, f.y), v2 = load_vertex(V, f.z);
+        // the triangle's box (lbvh::tri_box, exact min/max) from the vertices
+        const f3 blo = vmin3(vmin3(v0, v1), v2), bhi = vmax3(vmax3(v0, v1), v2);
         uint32_t wd[9];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) wd[k] = __float_as_uint(ld_own(b + k));
+        wd[0] = __float_as_uint(blo.x); wd[1] = __float_as_uint(blo.y); wd[2] = __float_as_uint(blo.z);
+        wd[3] = __float_as_uint(bhi.x); wd[4] = __float_as_uint(bhi.y); wd[5] = __float_as_uint(bhi.z);
         wd[6] = i;  // primitivesOffset
         wd[7] = 0;
         wd[8] = 1;  // one primitive, axis 0
         pipeline::store_words<Src::kOwnCta>(nodes, ni + j, wd, 9);
         if (want_collapse) pipeline::store_words<Src::kOwnCta>(collapsed, ni + j, wd, 9);
-        const uint4 f = __ldg(F + i);
-        const f3 v0 = load_vertex(V, f.x), v1 = load_vertex(V, f.y), v2 = load_vertex(V, f.z);
         float* tp = tris + 9 * static_cast<size_t>(j);
         tp[0] = v0.x; tp[1] = v0.y; tp[2] = v0.z; tp[3] = v1.x; tp[4] = v1.y; tp[5] = v1.z;
         tp[6] = v2.x; tp[7] = v2.y; tp[8] = v2.z;

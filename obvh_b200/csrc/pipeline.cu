@@ -235,26 +235,27 @@ __global__ void __launch_bounds__(kThreads, 4) fused_up_local_kernel(UpArgs a, u
     const bool with_summary = a.summary != nullptr;
     // leaf cost: ct * area in the collapse (transforms.cu:97), 1 * area in the LBVH (lbvh.cu:427)
     const float leaf_ct = a.flags ? a.ct : 1.0f;
-    // The CTA's leaf records and triangles are contiguous runs of 9 words
-    // each: read word by word across the CTA (coalesced) into the leaf rows,
-    // every load in flight before the first store.
+    // The CTA's triangles (or, without summaries, its leaf records) are
+    // contiguous runs of 9 words each: read word by word across the CTA
+    // (coalesced) into the leaf rows, every load in flight before the first
+    // store.  With the triangles at hand, a leaf's bounds are recomputed
+    // from its vertices below (exact min/max: the bits of its record).
     {
-        const uint32_t* nw = reinterpret_cast<const uint32_t*>(a.nodes + internal + j0);
-        const uint32_t* tw = reinterpret_cast<const uint32_t*>(a.tris + 9 * static_cast<size_t>(j0));
-        uint32_t bw[9], vw[9];
+        const uint32_t* src = with_summary ? reinterpret_cast<const uint32_t*>(a.tris + 9 * static_cast<size_t>(j0))
+                                           : reinterpret_cast<const uint32_t*>(a.nodes + internal + j0);
+        uint32_t vw[9];
 #pragma unroll
         for (int r = 0; r < 9; ++r) {
             const uint32_t w = t + r * kThreads;
-            bw[r] = w < 9 * m ? __ldcg(nw + w) : 0u;
-            vw[r] = with_summary && w < 9 * m ? __ldg(tw + w) : 0u;
+            vw[r] = w < 9 * m ? (with_summary ? __ldg(src + w) : __ldcg(src + w)) : 0u;
         }
 #pragma unroll
         for (int r = 0; r < 9; ++r) {
             const uint32_t w = t + r * kThreads;
             if (w >= 9 * m) continue;
             const uint32_t q = w / 9, k = w - 9 * q;
-            if (k < 6) sm.lslot[k * kRow + q] = bw[r];
             if (with_summary) sm.lslot[(6 + k) * kRow + q] = vw[r];
+            else if (k < 6) sm.lslot[k * kRow + q] = vw[r];
         }
     }
     const uint32_t leaf_parent = t < m ? a.parents[internal + j0 + t] : kNoParent;
@@ -289,6 +290,17 @@ __global__ void __launch_bounds__(kThreads, 4) fused_up_local_kernel(UpArgs a, u
     if (t == 0) sm.nfront = 0;
     __syncthreads();
     if (t < m) {
+        if (with_summary) {  // the triangle's box (lbvh::tri_box) from its vertex rows
+            f3 v[3];
+            leaf_vertices(sm, t, v);
+            const f3 lo = vmin3(vmin3(v[0], v[1]), v[2]), hi = vmax3(vmax3(v[0], v[1]), v[2]);
+            sm.lslot[0 * kRow + t] = __float_as_uint(lo.x);
+            sm.lslot[1 * kRow + t] = __float_as_uint(lo.y);
+            sm.lslot[2 * kRow + t] = __float_as_uint(lo.z);
+            sm.lslot[3 * kRow + t] = __float_as_uint(hi.x);
+            sm.lslot[4 * kRow + t] = __float_as_uint(hi.y);
+            sm.lslot[5 * kRow + t] = __float_as_uint(hi.z);
+        }
         Carry c;
         get_bounds(sm.lslot, t, c);
         __stcg(a.costs + internal + j0 + t, leaf_ct * box_area(c.lo, c.hi));
