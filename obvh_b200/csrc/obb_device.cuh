@@ -62,12 +62,11 @@ __device__ __forceinline__ Axes make_axes(f3 b0, f3 b1, f3 b2, float nz) {
     return Axes{make_float2(b0.x, b1.x), make_float2(b0.y, b1.y), make_float2(b0.z, b1.z), b2, make_float2(nz, nz)};
 }
 
-enum class From { kGlobal, kShared, kL2 };
+enum class From { kGlobal, kShared };
 
 template <From F>
 __device__ __forceinline__ float ld_tri(const float* t, int i) {
     if constexpr (F == From::kGlobal) return __ldg(t + i);
-    else if constexpr (F == From::kL2) return __ldcg(t + i);
     else return t[i];
 }
 
@@ -107,11 +106,6 @@ __device__ __forceinline__ void project_tri(const float* t, const Axes& ax, floa
 // project_tri for a triangle in shared memory
 __device__ __forceinline__ void project_tri_s(const float* t, const Axes& ax, float lo[3], float hi[3]) {
     project_tri_from<From::kShared>(t, ax, lo, hi);
-}
-
-// project_tri for triangles written earlier in the same kernel (through L2)
-__device__ __forceinline__ void project_tri_cg(const float* t, const Axes& ax, float lo[3], float hi[3]) {
-    project_tri_from<From::kL2>(t, ax, lo, hi);
 }
 
 // project_tri for triangles this CTA wrote (plain loads, as from shared memory)

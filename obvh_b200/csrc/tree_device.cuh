@@ -75,12 +75,6 @@ __device__ __forceinline__ f3 load_vertex(const kr_vec3* verts, uint32_t i) {
     return mk3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
 }
 
-// load_vertex for vertices written earlier in the same kernel (through L2).
-__device__ __forceinline__ f3 load_vertex_cg(const kr_vec3* verts, uint32_t i) {
-    const float* p = reinterpret_cast<const float*>(verts) + 3 * static_cast<size_t>(i);
-    return mk3(__ldcg(p), __ldcg(p + 1), __ldcg(p + 2));
-}
-
 // Where the data a load reads was written: before the kernel (the read-only
 // path), earlier in the kernel by other SMs (through L2), or earlier in the
 // kernel by this CTA (a plain load, cached in L1: an SM's own stores keep its
