@@ -400,11 +400,9 @@ __device__ void walk_chain(const ChainArgs& c, const uint32_t* counts, uint32_t 
 
 // The candidate of internal node a and its extents plan (nunits, keys, the
 // finalize list).
-__device__ __forceinline__ void candidate_node(uint32_t a, const uint4* summary, const kr_vec3* verts,
-                                               const uint32_t* counts, Cand* cand, uint32_t* nunits, uint32_t* keys,
-                                               const ChainArgs& chain) {
-    Summary s;
-    const Candidate c = summary_candidate<Src::kL2, Src::kReadOnly>(summary, verts, a, chain.nz, s);
+__device__ __forceinline__ void candidate_store(uint32_t a, const Summary& s, const Candidate& c,
+                                                const uint32_t* counts, Cand* cand, uint32_t* nunits, uint32_t* keys,
+                                                const ChainArgs& chain) {
     Cand out;
     out.ax[0] = c.b0.x; out.ax[1] = c.b0.y; out.ax[2] = c.b0.z;
     out.ax[3] = c.b1.x; out.ax[4] = c.b1.y; out.ax[5] = c.b1.z;
@@ -440,6 +438,14 @@ __device__ __forceinline__ void candidate_node(uint32_t a, const uint4* summary,
         base = g.shfl(base, 0);
         chain.final_list[base + g.thread_rank()] = a;
     }
+}
+
+__device__ __forceinline__ void candidate_node(uint32_t a, const uint4* summary, const kr_vec3* verts,
+                                               const uint32_t* counts, Cand* cand, uint32_t* nunits, uint32_t* keys,
+                                               const ChainArgs& chain) {
+    Summary s;
+    const Candidate c = summary_candidate<Src::kL2, Src::kReadOnly>(summary, verts, a, chain.nz, s);
+    candidate_store(a, s, c, counts, cand, nunits, keys, chain);
 }
 
 __global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* summary, const kr_vec3* verts,

@@ -484,6 +484,24 @@ __device__ inline Candidate node_candidate(const PointsK<K>& Q, f3 p0, f3 p1, co
     return c;
 }
 
+// The candidate of a node from its summary s and the 14 summary vertices P
+// (min, max per slab): the furthest slab pair (first on ties), then
+// node_candidate.
+__device__ __forceinline__ Candidate points_candidate(const Summary& s, const PointsK<14>& P) {
+    int at = 0;
+    float far = len2_3(sub3(P.get(1), P.get(0)));
+#pragma unroll
+    for (int k = 1; k < 7; ++k) {
+        const float d = len2_3(sub3(P.get(2 * k + 1), P.get(2 * k)));
+        if (d > far) { far = d; at = k; }
+    }
+    f3 p0 = P.get(0), p1 = P.get(1);
+#pragma unroll
+    for (int k = 1; k < 7; ++k)
+        if (at == k) { p0 = P.get(2 * k); p1 = P.get(2 * k + 1); }
+    return node_candidate<14>(P, p0, p1, s.lo, s.hi);
+}
+
 // The candidate of internal node a from its stored summary: the 14 extremal
 // vertices (min, max per slab), the furthest slab pair (first on ties), then
 // node_candidate.  SumSrc / VertSrc say where the summaries and the vertices
@@ -499,18 +517,7 @@ __device__ __forceinline__ Candidate summary_candidate(const uint4* summary, con
         P.set(2 * k, load_vertex_src<VertSrc>(verts, s.ilo[k]));
         P.set(2 * k + 1, load_vertex_src<VertSrc>(verts, s.ihi[k]));
     }
-    int at = 0;
-    float far = len2_3(sub3(P.get(1), P.get(0)));
-#pragma unroll
-    for (int k = 1; k < 7; ++k) {
-        const float d = len2_3(sub3(P.get(2 * k + 1), P.get(2 * k)));
-        if (d > far) { far = d; at = k; }
-    }
-    f3 p0 = P.get(0), p1 = P.get(1);
-#pragma unroll
-    for (int k = 1; k < 7; ++k)
-        if (at == k) { p0 = P.get(2 * k); p1 = P.get(2 * k + 1); }
-    return node_candidate<14>(P, p0, p1, s.lo, s.hi);
+    return points_candidate(s, P);
 }
 
 }  // namespace tree
