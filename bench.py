@@ -195,9 +195,10 @@ def profile_enable(on: bool):
     _native.check(_native.lib().obvh_profile_enable(1 if on else 0))
 
 
-def timed_steps(a, dist, step_fn, sampler, stream):
+def timed_steps(a, dist, step_fn, sampler, stream, profile=True):
     """Warm-up, then exactly a.steps steps between barriers; returns the max-over-ranks
-    device time (ms), the per-kernel profile of the timed region and the clocks."""
+    device time (ms), the per-kernel profile of the timed region (an event pair
+    around every launch; empty with profile=False) and the clocks."""
     import torch
     if not a.profile:
         sampler.start()
@@ -212,7 +213,7 @@ def timed_steps(a, dist, step_fn, sampler, stream):
     torch.cuda.synchronize()
     dist.barrier()
     torch.cuda.synchronize()
-    profile_enable(True)
+    profile_enable(profile)
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
     for j in range(a.steps):
@@ -354,15 +355,40 @@ def bench_tree_ours(a, dist, atrbvh=False):
                                      P["bounds"], P["obbs"], P["xfs"], P["collapsed"], P["prims"], W, S)
         _native.check(e)
 
+    def capture(m):
+        """The same build of mesh m as one CUDA graph (obvh_build_graph_create)."""
+        h = ctypes.c_void_p()
+        V, F = ctypes.c_void_p(m.verts.data_ptr()), ctypes.c_void_p(m.faces.data_ptr())
+        if atrbvh:
+            e = lib.obvh_build_atrbvh_graph_create(V, F, n, flags, a.treelet, 2, 1.2, 1.0, P["nodes"], P["parents"],
+                                                   P["counts"], P["costs"], P["bounds"], P["obbs"], P["xfs"],
+                                                   P["collapsed"], P["prims"], W, ctypes.byref(h))
+        else:
+            e = lib.obvh_build_graph_create(V, F, n, flags, 1.2, 1.0, P["nodes"], P["parents"], P["counts"],
+                                            P["costs"], P["bounds"], P["obbs"], P["xfs"], P["collapsed"], P["prims"],
+                                            W, ctypes.byref(h))
+        _native.check(e)
+        return h
+
+    wname = "atrbvh_obb_tree" if atrbvh else "lbvh_obb_tree"
     sampler = ClockSampler(dev.index, enabled=not a.profile)
-    total_ms, prof, clocks = timed_steps(a, dist, step, sampler, stream)
+    if a.profile:
+        total_ms, prof, clocks = timed_steps(a, dist, step, sampler, stream)
+        return {"profile": wname, "tris": n, "ms_per_step": total_ms / a.steps, "kernels": prof}
+    # the timed region: one graph replay per build, no per-launch events
+    graphs = [capture(m) for m in meshes]
+
+    def graph_step(j, g=None):
+        _native.check(lib.obvh_build_graph_launch(g or graphs[j & 1], S))
+
+    total_ms, _, clocks = timed_steps(a, dist, graph_step, sampler, stream, profile=False)
+    # the kernel table: as many builds again, launched one by one with an
+    # event pair around every launch (their own timed region)
+    kernel_ms, prof, _ = timed_steps(a, dist, step, ClockSampler(dev.index, enabled=False), stream)
     err, slots = ctypes.c_uint32(0), ctypes.c_uint32(0)
     _native.check(status_fn(W, n, S, ctypes.byref(err), ctypes.byref(slots)))
     if err.value != 0:
         raise RuntimeError(f"device error word {err.value}")
-    wname = "atrbvh_obb_tree" if atrbvh else "lbvh_obb_tree"
-    if a.profile:
-        return {"profile": wname, "tris": n, "ms_per_step": total_ms / a.steps, "kernels": prof}
 
     ms_step = total_ms / a.steps
     value = dist.world * nn * a.steps / (total_ms / 1e3) / 1e6
@@ -385,6 +411,7 @@ def bench_tree_ours(a, dist, atrbvh=False):
     pinned = [(torch.from_numpy(v).pin_memory(), torch.from_numpy(bvh.as_faces4(f).view(np.int32)).pin_memory())
               for v, f in host_meshes]
     stagings = [bvh.Mesh(host_meshes[0][0], host_meshes[0][1], device=dev) for _ in range(2)]
+    staging_graphs = [capture(m) for m in stagings]
     results = [torch.empty(16, dtype=f32).pin_memory() for _ in range(2)]
     e2e_steps = max(3, min(a.steps, 10))
 
@@ -393,7 +420,7 @@ def bench_tree_ours(a, dist, atrbvh=False):
         staging, result = stagings[0], results[0]
         staging.verts.copy_(pv, non_blocking=True)
         staging.faces.copy_(pf, non_blocking=True)
-        step(j, staging)
+        graph_step(j, staging_graphs[0])
         result[:15].copy_(out["obbs"][:15], non_blocking=True)
         result[15:].copy_(out["costs"][:1], non_blocking=True)
         stream.synchronize()
@@ -426,7 +453,7 @@ def bench_tree_ours(a, dist, atrbvh=False):
     def issue_build(j):
         b = j & 1
         stream.wait_event(h2d_done[b])
-        step(j, stagings[b])
+        graph_step(j, staging_graphs[b])
         build_done[b].record(stream)
         built[b] = True
         results[b][:15].copy_(out["obbs"][:15], non_blocking=True)
@@ -458,7 +485,7 @@ def bench_tree_ours(a, dist, atrbvh=False):
                   "morton_bits": 63, "treelet_size": a.treelet, "iterations": 2, "ci": 1.2, "ct": 1.0,
                   "l2": "two 26 MB knots alternated; each step writes ~0.6 GB after reading its input, no flush",
                   "parallelism": f"replicas{dist.world}"}
-        api = "obvh_build_atrbvh_async (ATRBVH + OBB tree + collapse), pinned host mesh"
+        api = "obvh_build_graph_launch of obvh_build_atrbvh_graph_create (ATRBVH + OBB tree + collapse), pinned host mesh"
     else:
         metric = "LBVH + OBB-tree + collapse build throughput (Mnodes/s)"
         data = "synthetic: thin random triangles (centroid U[0,1]^3, vertex radius log-U[0.002,0.02]), seeded"
@@ -466,12 +493,16 @@ def bench_tree_ours(a, dist, atrbvh=False):
                   "morton_bits": 30, "ci": 1.2, "ct": 1.0,
                   "l2": "two 104 MB meshes alternated between steps; each step writes ~1 GB",
                   "parallelism": f"replicas{dist.world}"}
-        api = "obvh_build_async (LBVH + OBB tree + collapse), pinned host mesh"
+        api = "obvh_build_graph_launch of obvh_build_graph_create (LBVH + OBB tree + collapse), pinned host mesh"
     line = {
         "metric": metric,
         "value": round(value, 3), "unit": "Mnodes/s", "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": round(ms_step, 5), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": data, "config": config,
+        "launch": "one CUDA graph replay per build (obvh_build_graph_launch); the kernels, their roofline and "
+                  "gpu_launches come from as many builds again launched one by one (obvh_build_*async) with an "
+                  "event pair around every launch",
+        "kernels_pass_ms_per_step": round(kernel_ms / a.steps, 5),
         "kernels": kern, "gpu_launches": launches, "roofline": roof,
         "e2e": {"value": round(dist.world * e2e_min, 3), "unit": "Mnodes/s",
                 "h2d_bytes_per_step": int(host_meshes[0][0].nbytes + n * 16), "d2h_bytes_per_step": 64,
@@ -485,6 +516,9 @@ def bench_tree_ours(a, dist, atrbvh=False):
     q.append(bvh.bvh_sah(out["collapsed"], out["parents"], out["obbs"]).cpu().tolist()[1])
     line["tree_quality"] = {"sah_aabb": round(q[0], 4), "sah_obb": round(q[1], 4), "sah_obb_collapsed": round(q[2], 4),
                             "ci": 1.2, "ct": 1.0, "api": "obvh_bvh_sah_async (kr_bvh_sah's cost, on the device)"}
+    torch.cuda.synchronize()
+    for g in graphs + staging_graphs:
+        _native.check(lib.obvh_build_graph_destroy(g))
     if dist.rank == 0 and dist.world == 1:
         line["cpu_baseline"] = cpu_atrbvh_baseline(a.treelet) if atrbvh else cpu_tree_baseline()
     return line

@@ -17,6 +17,7 @@
 #ifndef OBVH_ATRBVH_H
 #define OBVH_ATRBVH_H
 
+#include "obvh_build.h" /* obvh_build_graph */
 #include "obvh_types.h"
 
 #ifdef __cplusplus
@@ -53,6 +54,18 @@ OBVH_EXPORT kr_error obvh_build_atrbvh_async(const kr_vec3* d_vertices, const kr
  * the primitive slots the collapsed leaves use. */
 OBVH_EXPORT kr_error obvh_atrbvh_status(const void* d_workspace, kr_u32 face_count, void* stream,
                                         kr_u32* device_error, kr_u32* primitive_slots);
+
+/* obvh_build_atrbvh_async captured into a CUDA graph for fixed buffers, as
+ * obvh_build_graph_create does for the LBVH chain (same rules; replay and free
+ * it with obvh_build_graph_launch / obvh_build_graph_destroy). */
+OBVH_EXPORT kr_error obvh_build_atrbvh_graph_create(const kr_vec3* d_vertices, const kr_uvec4* d_faces,
+                                                    kr_u32 face_count, kr_u32 flags, kr_u32 treelet_size,
+                                                    kr_u32 iterations, kr_scalar ci, kr_scalar ct,
+                                                    kr_bvh_node* d_nodes, kr_u32* d_parents,
+                                                    kr_u32* d_primitive_counts, kr_scalar* d_costs,
+                                                    kr_aabb3* d_scene, kr_obb3* d_obbs, kr_mat4* d_transforms,
+                                                    kr_bvh_node* d_collapsed, kr_u32* d_primitives,
+                                                    void* d_workspace, obvh_build_graph* out);
 
 #ifdef __cplusplus
 }

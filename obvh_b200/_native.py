@@ -83,6 +83,10 @@ def _declare(lib: ctypes.CDLL) -> None:
         "obvh_build_workspace_init": (err, [vp, c.c_uint32, vp]),
         "obvh_build_async": (err, [vp, vp, c.c_uint32, c.c_uint32, c.c_float, c.c_float] + [vp] * 11),
         "obvh_build_status": (err, [vp, c.c_uint32, vp, c.POINTER(c.c_uint32), c.POINTER(c.c_uint32)]),
+        "obvh_build_graph_create": (err, [vp, vp, c.c_uint32, c.c_uint32, c.c_float, c.c_float] + [vp] * 10
+                                    + [c.POINTER(vp)]),
+        "obvh_build_graph_launch": (err, [vp, vp]),
+        "obvh_build_graph_destroy": (err, [vp]),
         "obvh_atrbvh_workspace_bytes": (c.c_uint64, [c.c_uint32]),
         "obvh_atrbvh_workspace_init": (err, [vp, c.c_uint32, vp]),
         "obvh_atrbvh_build_async": (err, [vp, vp, c.c_uint32, c.c_uint32, c.c_uint32, c.c_float, c.c_float]
@@ -90,6 +94,8 @@ def _declare(lib: ctypes.CDLL) -> None:
         "obvh_build_atrbvh_async": (err, [vp, vp, c.c_uint32, c.c_uint32, c.c_uint32, c.c_uint32, c.c_float,
                                           c.c_float] + [vp] * 11),
         "obvh_atrbvh_status": (err, [vp, c.c_uint32, vp, c.POINTER(c.c_uint32), c.POINTER(c.c_uint32)]),
+        "obvh_build_atrbvh_graph_create": (err, [vp, vp, c.c_uint32, c.c_uint32, c.c_uint32, c.c_uint32, c.c_float,
+                                                 c.c_float] + [vp] * 10 + [c.POINTER(vp)]),
         "obvh_dito_batch_create": (err, [vp, c.c_uint64, c.c_uint32, vp, c.POINTER(vp)]),
         "obvh_dito_batch_destroy": (err, [vp]),
         "obvh_dito_batch_get_tuning": (err, [vp, c.POINTER(DitoBatchTuning)]),

@@ -237,6 +237,37 @@ class ObvhBuilder:
                                                  ctypes.byref(slots)))
         return err.value, slots.value
 
+    def capture(self, mesh: Mesh, out, flags=BUILD_OBBS | BUILD_COLLAPSE, ci=1.2, ct=1.0):
+        """obvh_build_graph_create: the build of this mesh's buffers into `out`
+        as a CUDA graph (BuildGraph), replayed by its launch()."""
+        n = mesh.n_faces
+        ws = self._workspace(n, _stream(self.torch, None))
+        h = ctypes.c_void_p()
+        _native.check(self.lib.obvh_build_graph_create(
+            _ptr(mesh.verts), _ptr(mesh.faces), n, flags, ci, ct, _ptr(out["nodes"]), _ptr(out["parents"]),
+            _ptr(out["counts"]), _ptr(out["costs"]), _ptr(out["bounds"]), _ptr(out["obbs"]), _ptr(out["transforms"]),
+            _ptr(out["collapsed"]), _ptr(out["primitives"]), _ptr(ws), ctypes.byref(h)))
+        return BuildGraph(self, h)
+
+
+class BuildGraph:
+    """A captured obvh_build_async chain (obvh_build_graph_*); holds its
+    builder so that the workspace outlives the graph."""
+
+    def __init__(self, builder: ObvhBuilder, handle):
+        self.builder = builder
+        self.lib = builder.lib
+        self.handle = handle
+
+    def launch(self, stream=None):
+        _native.check(self.lib.obvh_build_graph_launch(self.handle, _stream(self.builder.torch, stream)))
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            self.lib.obvh_build_graph_destroy(h)
+            self.handle = None
+
 
 ATRBVH_TREELET_SIZE = 9  # OBVH_ATRBVH_TREELET_SIZE: the reference intersector's treelet size
 ATRBVH_ITERATIONS = 2
@@ -279,6 +310,18 @@ class AtrbvhBuilder(ObvhBuilder):
         _native.check(self.lib.obvh_atrbvh_status(_ptr(self.ws), n, _stream(self.torch, stream), ctypes.byref(err),
                                                   ctypes.byref(slots)))
         return err.value, slots.value
+
+    def capture(self, mesh: Mesh, out, flags=BUILD_OBBS | BUILD_COLLAPSE, ci=1.2, ct=1.0,
+                treelet_size=ATRBVH_TREELET_SIZE, iterations=ATRBVH_ITERATIONS):
+        """obvh_build_atrbvh_graph_create: this build as a CUDA graph (BuildGraph)."""
+        n = mesh.n_faces
+        ws = self._workspace(n, _stream(self.torch, None))
+        h = ctypes.c_void_p()
+        _native.check(self.lib.obvh_build_atrbvh_graph_create(
+            _ptr(mesh.verts), _ptr(mesh.faces), n, flags, treelet_size, iterations, ci, ct, _ptr(out["nodes"]),
+            _ptr(out["parents"]), _ptr(out["counts"]), _ptr(out["costs"]), _ptr(out["bounds"]), _ptr(out["obbs"]),
+            _ptr(out["transforms"]), _ptr(out["collapsed"]), _ptr(out["primitives"]), _ptr(ws), ctypes.byref(h)))
+        return BuildGraph(self, h)
 
 
 # ---- traversal packing (include/obvh_transforms.h) -------------------------

@@ -804,6 +804,24 @@ extern "C" kr_error obvh_build_atrbvh_async(const kr_vec3* d_vertices, const kr_
     return e ? fail(e) : kr_success;
 }
 
+extern "C" kr_error obvh_build_atrbvh_graph_create(const kr_vec3* d_vertices, const kr_uvec4* d_faces,
+                                                   kr_u32 face_count, kr_u32 flags, kr_u32 treelet_size,
+                                                   kr_u32 iterations, kr_scalar ci, kr_scalar ct,
+                                                   kr_bvh_node* d_nodes, kr_u32* d_parents,
+                                                   kr_u32* d_primitive_counts, kr_scalar* d_costs,
+                                                   kr_aabb3* d_scene, kr_obb3* d_obbs, kr_mat4* d_transforms,
+                                                   kr_bvh_node* d_collapsed, kr_u32* d_primitives,
+                                                   void* d_workspace, obvh_build_graph* out) {
+    const kr_error e = obvh::create_build_graph(
+        [&](cudaStream_t s) {
+            return obvh::atrbvh::enqueue_full(d_vertices, d_faces, face_count, flags, treelet_size, iterations, ci,
+                                              ct, d_nodes, d_parents, d_primitive_counts, d_costs, d_scene, d_obbs,
+                                              d_transforms, d_collapsed, d_primitives, d_workspace, s);
+        },
+        out);
+    return e ? fail(e) : kr_success;
+}
+
 extern "C" kr_error obvh_atrbvh_status(const void* d_workspace, kr_u32 face_count, void* stream, kr_u32* device_error,
                                        kr_u32* primitive_slots) {
     if (!d_workspace) return fail("obvh_atrbvh_status: null workspace");

@@ -865,30 +865,10 @@ extern "C" kr_error obvh_build_batch_capture(obvh_build_batch b, const kr_vec3* 
         cudaGraphDestroy(P.graph);
         P.graph = nullptr;
     }
-    cudaStream_t s = nullptr;
-    cudaError_t ce = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-    if (ce != cudaSuccess) return fail(cuda_error(ce));
-    kr_error e = nullptr;
-    ce = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-    if (ce == cudaSuccess) {
-        e = meshbatch::enqueue(P,
-                               buffers(d_vertices, d_faces, ci, ct, d_nodes, d_parents, d_primitive_counts, d_costs,
-                                       d_bounds, d_obbs, d_transforms, d_collapsed, d_primitives),
-                               s);
-        cudaGraph_t g = nullptr;
-        const cudaError_t ee = cudaStreamEndCapture(s, &g);
-        if (!e && ee != cudaSuccess) e = cuda_error(ee);
-        if (!e) {
-            const cudaError_t ie = cudaGraphInstantiate(&P.exec, g, 0);
-            if (ie != cudaSuccess) e = cuda_error(ie);
-            P.graph = g;
-        } else if (g) {
-            cudaGraphDestroy(g);
-        }
-    } else {
-        e = cuda_error(ce);
-    }
-    cudaStreamDestroy(s);
+    const meshbatch::Buffers bufs = buffers(d_vertices, d_faces, ci, ct, d_nodes, d_parents, d_primitive_counts,
+                                            d_costs, d_bounds, d_obbs, d_transforms, d_collapsed, d_primitives);
+    const kr_error e = capture_graph([&](cudaStream_t s) { return meshbatch::enqueue(P, bufs, s); }, &P.graph,
+                                     &P.exec);
     return e ? fail(e) : kr_success;
 }
 

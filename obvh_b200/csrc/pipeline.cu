@@ -740,6 +740,48 @@ extern "C" kr_error obvh_build_async(const kr_vec3* d_vertices, const kr_uvec4* 
     return e;
 }
 
+extern "C" kr_error obvh_build_graph_create(const kr_vec3* d_vertices, const kr_uvec4* d_faces, kr_u32 face_count,
+                                            kr_u32 flags, kr_scalar ci, kr_scalar ct, kr_bvh_node* d_nodes,
+                                            kr_u32* d_parents, kr_u32* d_primitive_counts, kr_scalar* d_costs,
+                                            kr_aabb3* d_bounds, kr_obb3* d_obbs, kr_mat4* d_transforms,
+                                            kr_bvh_node* d_collapsed, kr_u32* d_primitives, void* d_workspace,
+                                            obvh_build_graph* out) {
+    const kr_error e = create_build_graph(
+        [&](cudaStream_t s) {
+            return pipeline::enqueue(d_vertices, d_faces, face_count, flags, ci, ct, d_nodes, d_parents,
+                                     d_primitive_counts, d_costs, d_bounds, d_obbs, d_transforms, d_collapsed,
+                                     d_primitives, d_workspace, s);
+        },
+        out);
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error obvh_build_graph_launch(obvh_build_graph g, void* stream) {
+    kr_error e = g ? kr_success : "obvh_build_graph_launch: null graph";
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int dev = -1;
+    if (!e && cudaStreamGetDevice(s, &dev) != cudaSuccess) e = "obvh_build_graph_launch: unknown stream";
+    if (!e && dev != g->device) e = "obvh_build_graph_launch: the stream belongs to another device than the graph";
+    if (!e) {
+        ProfScope prof_scope_("build_graph", s);
+        const cudaError_t ce = cudaGraphLaunch(g->exec, s);
+        if (ce != cudaSuccess) e = cuda_error(ce);
+    }
+    if (e) set_last_error(e);
+    return e;
+}
+
+extern "C" kr_error obvh_build_graph_destroy(obvh_build_graph g) {
+    if (!g) return kr_success;
+    kr_error e = kr_success;
+    if (g->exec && cudaGraphExecDestroy(g->exec) != cudaSuccess) e = "obvh_build_graph_destroy: graph exec";
+    if (g->graph && cudaGraphDestroy(g->graph) != cudaSuccess) e = "obvh_build_graph_destroy: graph";
+    delete g;
+    if (e) set_last_error(e);
+    return e;
+}
+
 extern "C" kr_error obvh_build_status(const void* d_workspace, kr_u32 face_count, void* stream, kr_u32* device_error,
                                       kr_u32* primitive_slots) {
     if (!d_workspace) return "obvh_build_status: null workspace";

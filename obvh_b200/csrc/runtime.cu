@@ -86,6 +86,38 @@ kr_error join_from(ForkStreams& f, int i, cudaStream_t s) {
     return kr_success;
 }
 
+cudaStream_t capture_stream() {
+    thread_local std::unordered_map<int, cudaStream_t>* t_capture = nullptr;  // never freed, as the fork slots
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    if (!t_capture) t_capture = new std::unordered_map<int, cudaStream_t>();
+    auto it = t_capture->find(dev);
+    if (it != t_capture->end()) return it->second;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    t_capture->emplace(dev, s);
+    return s;
+}
+
+kr_error finish_capture(cudaStream_t s, kr_error enqueue_error, cudaGraph_t* graph, cudaGraphExec_t* exec) {
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s, &g);  // ends the capture even after a failed enqueue
+    kr_error e = enqueue_error ? enqueue_error : (ee != cudaSuccess ? cuda_error(ee) : nullptr);
+    cudaGraphExec_t x = nullptr;
+    if (!e) {
+        const cudaError_t ie = cudaGraphInstantiateWithFlags(&x, g, cudaGraphInstantiateFlagUseNodePriority);
+        if (ie != cudaSuccess) e = cuda_error(ie);
+    }
+    if (e) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();  // clears the (non-sticky) error a failed capture leaves behind
+        return e;
+    }
+    *graph = g;
+    *exec = x;
+    return kr_success;
+}
+
 const DeviceInfo& device_info() {
     int dev = 0;
     cudaGetDevice(&dev);

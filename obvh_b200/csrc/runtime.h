@@ -80,6 +80,53 @@ kr_error fork_to(ForkStreams& f, int i, cudaStream_t s);
 kr_error join_from(ForkStreams& f, int i, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
+// Graph capture of one enqueue: what `enqueue(s)` issues on a capture stream
+// of the current device (one per thread and device, created once, so that its
+// fork helpers are reused too) becomes an executable graph.  Its kernel nodes
+// keep the priorities of the streams they were captured from.  `graph` and
+// `exec` are written only on success.
+template <class Enqueue>
+kr_error capture_graph(Enqueue&& enqueue, cudaGraph_t* graph, cudaGraphExec_t* exec);
+cudaStream_t capture_stream();  // nullptr if it could not be created
+kr_error finish_capture(cudaStream_t s, kr_error enqueue_error, cudaGraph_t* graph, cudaGraphExec_t* exec);
+
+template <class Enqueue>
+kr_error capture_graph(Enqueue&& enqueue, cudaGraph_t* graph, cudaGraphExec_t* exec) {
+    cudaStream_t s = capture_stream();
+    if (!s) return "capture_graph: no capture stream";
+    OBVH_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    return finish_capture(s, enqueue(s), graph, exec);
+}
+}  // namespace obvh
+
+// The opaque handle of obvh_build_graph_create / obvh_build_atrbvh_graph_create:
+// one captured build chain and the device it was captured on.
+struct obvh_build_graph_s {
+    int device = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace obvh {
+
+// A build chain (`enqueue(s)`) captured into a new handle.
+template <class Enqueue>
+kr_error create_build_graph(Enqueue&& enqueue, obvh_build_graph_s** out) {
+    if (!out) return "build graph: null output";
+    obvh_build_graph_s* g = new obvh_build_graph_s();
+    kr_error e = kr_success;
+    const cudaError_t ce = cudaGetDevice(&g->device);
+    if (ce != cudaSuccess) e = cuda_error(ce);
+    if (!e) e = capture_graph(enqueue, &g->graph, &g->exec);
+    if (e) {
+        delete g;
+        return e;
+    }
+    *out = g;
+    return kr_success;
+}
+
+// ---------------------------------------------------------------------------
 // Per-kernel timing, off by default (obvh_profile_enable).  A ProfScope around
 // a launch records an event pair on the launching stream; the summary gives
 // launches and total device time per kernel name.

@@ -37,3 +37,21 @@ def test_struct_layouts_compile_against_headers(tmp_path):
 
 def test_workspace_size_is_reported():
     assert _native.lib().obvh_dito_workspace_bytes() > 256
+
+
+def test_build_graph_entry_points_check_their_handles():
+    """No CUDA call is made for a null handle: launch names the error,
+    destroy is a no-op, create wants somewhere to write the handle."""
+    lib = _native.lib()
+    assert b"null graph" in ctypes.string_at(lib.obvh_build_graph_launch(None, None))
+    assert lib.obvh_build_graph_destroy(None) is None
+    args = [None, None, 0, 0, 1.2, 1.0] + [None] * 10 + [None]
+    assert b"null output" in ctypes.string_at(lib.obvh_build_graph_create(*args))
+
+
+def test_build_headers_compile_as_c(tmp_path):
+    src = tmp_path / "b.c"
+    src.write_text('#include "obvh_build.h"\n#include "obvh_atrbvh.h"\nint main(void){obvh_build_graph g = 0;'
+                   'return g != 0;}\n')
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                    str(tmp_path / "b")], check=True)

@@ -169,3 +169,31 @@ def test_knot_full_size_properties(builder):
         while x != 0xFFFFFFFF:
             assert contained(tri, obbs[x]), (leaf, x)
             x = parents[x]
+
+
+def test_build_graph_equals_the_direct_build(builder):
+    """obvh_build_atrbvh_graph_create: the ATRBVH commit captured once and
+    replayed equals the direct commit bit for bit, also after the input
+    buffers were given a new mesh."""
+    import torch
+    n = 100_000
+    meshes = [workloads.triangle_soup(n, seed=90 + j) for j in range(2)]
+    direct = []
+    for v, f in meshes:
+        o, _ = _run(builder, v, f)
+        direct.append({k: t.clone() for k, t in o.items()})
+    dev = bvh.Mesh(*meshes[0])
+    out = builder.outputs(n)
+    g = builder.capture(dev, out)
+    for j in (0, 1):
+        if j:
+            v, f = meshes[1]
+            dev.verts.copy_(torch.from_numpy(v).to(dev.verts.device))
+            dev.faces.copy_(torch.from_numpy(bvh.as_faces4(f).view(np.int32)).to(dev.faces.device))
+            out["primitives"].zero_()  # slots past the collapsed leaves' are not written
+        g.launch()
+        torch.cuda.synchronize()
+        err, _ = builder.status(n)
+        assert err == 0
+        for k in direct[j]:
+            assert torch.equal(direct[j][k].view(torch.uint8), out[k].view(torch.uint8)), (j, k)

@@ -98,3 +98,46 @@ def test_fused_build_deep_and_tied_trees(builder, layout):
     v, f = deep_or_tied_mesh(layout)
     o, slots = _run(builder, v, f, 3)
     _check(o, slots, _expect(v, f), f.shape[0], 3)
+
+
+def test_build_graph_replays_equal_the_three_steps(builder):
+    """obvh_build_graph_create / _launch: the chain captured once per buffer
+    set; every replay rebuilds from what the input buffers hold then."""
+    import torch
+    n = 65_537
+    meshes = [workloads.triangle_soup(n, seed=70 + j) for j in range(3)]
+    dev = [bvh.Mesh(v, f) for v, f in meshes[:2]]
+    outs = [builder.outputs(n) for _ in range(2)]
+    graphs = [builder.capture(m, o) for m, o in zip(dev, outs)]
+    exps = [_expect(v, f) for v, f in meshes[:2]]
+    for rep in range(2):
+        for j in range(2):
+            graphs[j].launch()
+            torch.cuda.synchronize()
+            err, slots = builder.status(n)
+            assert err == 0
+            _check(outs[j], slots, exps[j], n, 3)
+    # new contents in mesh 0's buffers: the same graph builds them
+    v2, f2 = meshes[2]
+    dev[0].verts.copy_(torch.from_numpy(v2).to(dev[0].verts.device))
+    dev[0].faces.copy_(torch.from_numpy(bvh.as_faces4(f2).view(np.int32)).to(dev[0].faces.device))
+    graphs[0].launch()
+    torch.cuda.synchronize()
+    err, slots = builder.status(n)
+    assert err == 0
+    _check(outs[0], slots, _expect(v2, f2), n, 3)
+
+
+def test_build_graph_equals_the_direct_build_at_full_size(builder):
+    import torch
+    v, f = workloads.triangle_soup(2_000_000, seed=5)
+    mesh = bvh.Mesh(v, f)
+    direct = builder.build(mesh)
+    torch.cuda.synchronize()
+    out = builder.outputs(mesh.n_faces)
+    g = builder.capture(mesh, out)
+    g.launch()
+    torch.cuda.synchronize()
+    for k in direct:
+        assert torch.equal(direct[k].view(torch.uint8), out[k].view(torch.uint8)), k
+
