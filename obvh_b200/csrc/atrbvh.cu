@@ -55,7 +55,6 @@ constexpr int kTreeletThreads = 128;
 constexpr int kTreeletWarps = kTreeletThreads / 32;
 constexpr int kMinTau = 3;
 constexpr int kMaxTau = 20;
-constexpr int kMaxDist = (kMaxTau - 1) * kMaxTau / 2;
 
 // One node of the working tree (48 bytes).
 struct TNode {
@@ -239,12 +238,15 @@ __global__ void __launch_bounds__(kThreads) boxes_up_kernel(const kr_vec3* verts
 // ---------------------------------------------------------------------------
 // Treelet optimisation.
 
-// Per-treelet shared state (one per segment of a warp).
+// Per-treelet shared state (one per segment of W lanes; a treelet has at most
+// W leaves, so the arrays are sized by W: 208 bytes a segment at W = 8, which
+// lets 12 CTAs of 128 threads share an SM where 32-entry arrays allowed 5).
+template <int W>
 struct SegSmem {
-    int32_t internal[32];
-    int32_t leaves[32];
-    float areas[32];
-    float dist[kMaxDist];
+    int32_t internal[W];
+    int32_t leaves[W];
+    float areas[W];
+    float dist[W * (W - 1) / 2];
 };
 
 // A treelet of tau <= W leaves is processed by a segment of W lanes (W = 8,
@@ -345,7 +347,7 @@ __device__ __forceinline__ void shfl_box(const float* lo, const float* hi, int s
 // segment) on a malformed tree.
 template <int W>
 __device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, float ci, int32_t root, bool active,
-                                SegSmem& w) {
+                                SegSmem<W>& w) {
     const int sl = seg_lane<W>();
     const int32_t internal_count = n - 1;
     const int32_t node_count = 2 * n - 1;
@@ -503,10 +505,10 @@ __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, floa
                                                                   uint32_t* counters, int32_t n, int tau,
                                                                   int32_t gamma, float ci, float ct, uint32_t* err) {
     constexpr int S = 32 / W;  // segments (treelets in flight) per warp
-    __shared__ SegSmem smem[kTreeletWarps * S];
+    __shared__ SegSmem<W> smem[kTreeletWarps * S];
     const int lane = threadIdx.x & 31;
     const int seg = lane / W;
-    SegSmem& w = smem[(threadIdx.x >> 5) * S + seg];
+    SegSmem<W>& w = smem[(threadIdx.x >> 5) * S + seg];
     const int32_t i = static_cast<int32_t>(blockIdx.x * blockDim.x + threadIdx.x);
     const int32_t internal = n - 1;
     int32_t cur = -1;
@@ -525,6 +527,7 @@ __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, floa
         // (the arrival's release orders this lane's writes; the lanes that
         // rewrote a treelet fenced theirs before the warp synchronised)
         int32_t count = 0;
+        int32_t up = -1;
         if (cur >= 0) {
             // cur's children and area change only in cur's own treelet (or an
             // ancestor's), later: read them ahead of the arrival
@@ -534,6 +537,9 @@ __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, floa
                 L = __ldcg(&t[cur].left);
                 R = __ldcg(&t[cur].right);
                 area = __ldcg(&t[cur].area);
+                // cur's own parent link changes only in an ancestor's treelet
+                // (a treelet rewrites the links below its root)
+                up = __ldcg(&t[cur].parent);
             }
             if (cur >= internal) {
                 atomicOr(err, kErrCycle);
@@ -545,9 +551,12 @@ __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, floa
                     atomicOr(err, kErrCycle);
                     cur = -1;
                 } else {
-                    count = __ldcg(tris + L) + __ldcg(tris + R);
+                    // the four loads first, then the stores: one round of loads
+                    const int32_t tl = __ldcg(tris + L), tr = __ldcg(tris + R);
+                    const float sl_ = __ldcg(sah_arr + L), sr = __ldcg(sah_arr + R);
+                    count = tl + tr;
                     __stcg(tris + cur, count);
-                    __stcg(sah_arr + cur, ci * area + __ldcg(sah_arr + L) + __ldcg(sah_arr + R));
+                    __stcg(sah_arr + cur, ci * area + sl_ + sr);
                 }
             }
         }
@@ -565,7 +574,7 @@ __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, floa
             if (!process_treelet<W>(t, sah_arr, n, tau, ci, root, src >= 0, w) && (lane & (W - 1)) == 0)
                 atomicOr(err, kErrBadInput);
         }
-        if (cur >= 0) cur = __ldcg(&t[cur].parent);
+        if (cur >= 0) cur = up;
     }
 }
 
