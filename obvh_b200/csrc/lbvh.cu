@@ -105,14 +105,29 @@ __global__ void __launch_bounds__(kThreads) tri_bounds_kernel(const kr_vec3* ver
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // the last CTA folds the CTA records with all its threads (records t,
+    // t + kThreads, ...), then as above (min and max are exact in any order)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        acc[k] = kInf; acc[3 + k] = -kInf; acc[6 + k] = kInf; acc[9 + k] = -kInf;
+    }
+    for (uint32_t r = threadIdx.x; r < gridDim.x; r += kThreads) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            const float o = __ldcg(&recs[r].v[k]);
+            acc[k] = (k % 6) < 3 ? fminf(acc[k], o) : fmaxf(acc[k], o);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = warp_red(acc[k], (k % 6) < 3);
+    if (lane == 0)
+        for (int k = 0; k < 12; ++k) s[warp][k] = acc[k];
+    __syncthreads();
     if (threadIdx.x < 12) {
         const int k = threadIdx.x;
         const bool mn = (k % 6) < 3;
-        float v = mn ? kInf : -kInf;
-        for (uint32_t r = 0; r < gridDim.x; ++r) {
-            float o = __ldcg(&recs[r].v[k]);
-            v = mn ? fminf(v, o) : fmaxf(v, o);
-        }
+        float v = s[0][k];
+        for (int w = 1; w < kThreads / 32; ++w) v = mn ? fminf(v, s[w][k]) : fmaxf(v, s[w][k]);
         kr_aabb3* box = k < 6 ? scene_out : centroid_out;
         if (box) {
             float* dst = reinterpret_cast<float*>(box) + (k % 6);
@@ -224,7 +239,9 @@ Layout layout(uint32_t n) {
 }
 
 int bounds_grid(uint32_t n) {
-    int g = 2 * device_info().sm_count;
+    // 6 CTAs of 256 threads per SM (32 registers): enough loads in flight to
+    // stream the faces and vertices; the last CTA folds the records in parallel
+    int g = 6 * device_info().sm_count;
     const int need = static_cast<int>((n + kThreads - 1) / kThreads);
     if (need < g) g = need;
     if (g < 1) g = 1;

@@ -123,12 +123,13 @@ __device__ __forceinline__ void st_relaxed(uint32_t* a, uint32_t v) {
 }
 
 // Sort workspace: [0, 8 KB) digit counts then exclusive digit offsets per
-// pass, [8 KB, 8 KB + 64) tile counters and the error word, then the
-// per-pass tile status words.
+// pass, [8 KB, 8 KB + 256) tile counters, the error word and the counting
+// ticket, then the per-pass tile status words.
 struct SortTemp {
     uint32_t* digits;   // [kMaxPasses][kRadix]
     uint32_t* tiles;    // [kMaxPasses] tile counters, [kMaxPasses] error word
     uint32_t* err;
+    uint32_t* count_ticket;  // [kMaxPasses + 1]: CTAs done counting
     uint32_t* status;   // [passes][ntiles][kRadix]
 };
 constexpr size_t kSortHeader = kMaxPasses * kRadix * 4 + 256;
@@ -139,13 +140,16 @@ __host__ __device__ inline SortTemp sort_temp(void* temp) {
     t.digits = reinterpret_cast<uint32_t*>(c);
     t.tiles = reinterpret_cast<uint32_t*>(c + kMaxPasses * kRadix * 4);
     t.err = t.tiles + kMaxPasses;
+    t.count_ticket = t.tiles + kMaxPasses + 1;
     t.status = reinterpret_cast<uint32_t*>(c + kSortHeader);
     return t;
 }
 
+// Every pass's digit counts over all keys; the last CTA to finish (a ticket
+// in the zeroed header) turns them into exclusive digit offsets in place.
 template <typename K>
 __global__ void __launch_bounds__(kSortThreads) radix_digit_counts(const K* keys, uint64_t n, int begin_bit,
-                                                                   int passes, uint32_t* digits) {
+                                                                   int passes, uint32_t* digits, uint32_t* ticket) {
     __shared__ uint32_t h[kMaxPasses][kRadix];
     for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += kSortThreads) (&h[0][0])[i] = 0;
     __syncthreads();
@@ -157,13 +161,15 @@ __global__ void __launch_bounds__(kSortThreads) radix_digit_counts(const K* keys
     __syncthreads();
     for (int p = 0; p < passes; ++p)
         if (h[p][threadIdx.x]) atomicAdd(&digits[p * kRadix + threadIdx.x], h[p][threadIdx.x]);
-}
-
-// Global digit counts -> exclusive digit offsets, in place (one CTA).
-__global__ void __launch_bounds__(kSortThreads) radix_digit_offsets(uint32_t* digits, int passes) {
-    __shared__ uint32_t total;
+    __shared__ uint32_t last, total;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
     for (int p = 0; p < passes; ++p) {
-        const uint32_t c = digits[p * kRadix + threadIdx.x];
+        const uint32_t c = __ldcg(digits + p * kRadix + threadIdx.x);
         const uint32_t e = block_exclusive_sum(c, &total);
         __syncthreads();
         digits[p * kRadix + threadIdx.x] = e;
@@ -319,12 +325,7 @@ kr_error sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt, uin
         int grid = 2 * device_info().sm_count;
         const uint64_t need = div_up(n, kSortThreads);
         if (need < static_cast<uint64_t>(grid)) grid = static_cast<int>(need);
-        radix_digit_counts<K><<<grid, kSortThreads, 0, stream>>>(keys, n, begin_bit, passes, t.digits);
-    }
-    OBVH_TRY_CUDA(cudaGetLastError());
-    {
-        ProfScope prof_scope_("radix_digit_offsets", stream);
-        radix_digit_offsets<<<1, kSortThreads, 0, stream>>>(t.digits, passes);
+        radix_digit_counts<K><<<grid, kSortThreads, 0, stream>>>(keys, n, begin_bit, passes, t.digits, t.count_ticket);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     K* src_k = keys;
