@@ -229,27 +229,40 @@ __global__ void __launch_bounds__(kSortThreads) radix_onesweep(const K* keys_in,
         __syncwarp();
     }
     __syncthreads();
-    {
-        const int d = threadIdx.x;
-        uint32_t c = 0;  // this tile's count of digit d; warp bases exclusive over warps
+    const int d = threadIdx.x;
+    uint32_t c = 0;  // this tile's count of digit d; warp bases exclusive over warps
 #pragma unroll
-        for (int w = 0; w < kSortWarps; ++w) {
-            const uint32_t x = sm.wcount[w][d];
-            sm.wcount[w][d] = c;
-            c += x;
+    for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t x = sm.wcount[w][d];
+        sm.wcount[w][d] = c;
+        c += x;
+    }
+    sm.tstart[d] = block_exclusive_sum(c, &sm.total);
+    // publish this tile's count first, so that later tiles can use it while
+    // this one still orders its keys
+    uint32_t* mine = status + static_cast<uint64_t>(tile) * kRadix + d;
+    st_relaxed(mine, (tile == 0 ? kFlagPre : kFlagAgg) | c);
+    __syncthreads();
+    // the tile in digit order in shared memory (needs only the tile's own
+    // offsets); the keys, values and ranks leave the registers here
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+        const uint64_t idx = base + warp * (kRounds * 32) + r * 32 + lane;
+        if (idx < n) {
+            const uint32_t dk = static_cast<uint32_t>(k[r] >> shift) & (kRadix - 1);
+            const uint32_t p = sm.tstart[dk] + sm.wcount[warp][dk] + pos[r];
+            sm.keys[p] = k[r];
+            sm.vals[p] = v[r];
         }
-        sm.tstart[d] = block_exclusive_sum(c, &sm.total);
-        // decoupled look-back over the tiles before this one
-        uint32_t* mine = status + static_cast<uint64_t>(tile) * kRadix + d;
+    }
+    {
+        // decoupled look-back over the tiles before this one: kLook
+        // predecessors' words per step (independent loads), summed back to
+        // the first inclusive prefix; a word not yet published stops the
+        // step, and the walk resumes from it
         uint32_t excl = 0;
-        if (tile == 0) {
-            st_relaxed(mine, kFlagPre | c);
-        } else {
-            st_relaxed(mine, kFlagAgg | c);
-            // Eight predecessors' words per step (independent loads): sum
-            // their counts back to the first inclusive prefix; a word not yet
-            // published stops the step, and the walk resumes from it.
-            constexpr int kLook = 8;
+        if (tile != 0) {
+            constexpr int kLook = 16;
             int64_t j = static_cast<int64_t>(tile) - 1;
             const uint64_t t0 = global_ns();
             bool done = false;
@@ -280,17 +293,6 @@ __global__ void __launch_bounds__(kSortThreads) radix_onesweep(const K* keys_in,
             st_relaxed(mine, kFlagPre | (excl + c));
         }
         sm.gbase[d] = offsets[d] + excl;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < kRounds; ++r) {
-        const uint64_t idx = base + warp * (kRounds * 32) + r * 32 + lane;
-        if (idx < n) {
-            const uint32_t d = static_cast<uint32_t>(k[r] >> shift) & (kRadix - 1);
-            const uint32_t p = sm.tstart[d] + sm.wcount[warp][d] + pos[r];
-            sm.keys[p] = k[r];
-            sm.vals[p] = v[r];
-        }
     }
     __syncthreads();
     const uint32_t valid = static_cast<uint32_t>(n - base < static_cast<uint64_t>(kSortTile) ? n - base : kSortTile);
