@@ -269,7 +269,7 @@ def tree_bytes_per_launch(n):
     nn = 2 * n - 1
     return {
         "tri_bounds_kernel": 52 * n + 24 * n,          # face + 3 vertices in, triangle box out
-        "morton_kernel": 24 * n + 8 * n,               # box in, key + index out
+        "morton_count_kernel": 24 * n + 8 * n,         # box in, key + index out (digits counted on the way)
         "radix_digit_counts": 4 * n,                   # keys in (every pass's digits at once)
         "radix_onesweep": 16 * n,                      # key + value in and out (u32 keys)
         "leaves_kernel": 4 * n + 24 * n + 36 * n,      # order, box in; leaf node out

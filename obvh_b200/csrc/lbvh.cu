@@ -25,6 +25,7 @@
 #include "lbvh_host.h"
 #include "obvh_lbvh.h"
 #include "obvh_transforms.h"
+#include "sort_device.cuh"
 #include "runtime.h"
 #include "sort.h"
 #include "tree_device.cuh"
@@ -138,13 +139,27 @@ __global__ void __launch_bounds__(kThreads) tri_bounds_kernel(const kr_vec3* ver
     if (threadIdx.x == 0) ctl->ticket = 0;
 }
 
-// 30-bit Morton code of the triangle centroid (mortons_kernel); value = index.
-__global__ void __launch_bounds__(kThreads) morton_kernel(const float* tri_boxes, uint32_t n, const kr_aabb3* boxes,
-                                                          uint32_t* keys, uint32_t* vals) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    keys[i] = morton_code(tri_boxes + 6 * static_cast<size_t>(i), reinterpret_cast<const float*>(boxes + 1));
-    vals[i] = i;
+// 30-bit Morton code of the triangle centroid (mortons_kernel), with the
+// radix sort's digit counting (sortdev::count_key and finish_digit_counts):
+// keys[i] = code of triangle i, vals[i] = i, and the digit offsets of the
+// sort's 4 passes over the 30 bits.  Grid-stride, so that each CTA adds its
+// counts to the global ones once.
+constexpr int kMortonPasses = 4;
+__global__ void __launch_bounds__(kThreads) morton_count_kernel(const float* tri_boxes, uint32_t n,
+                                                                const kr_aabb3* boxes, uint32_t* keys,
+                                                                uint32_t* vals, uint32_t* digits, uint32_t* ticket) {
+    static_assert(kThreads == sortdev::kRadix, "one thread per digit in finish_digit_counts");
+    __shared__ uint32_t h[kMortonPasses][sortdev::kRadix];
+    for (int i = threadIdx.x; i < kMortonPasses * sortdev::kRadix; i += kThreads) (&h[0][0])[i] = 0;
+    __syncthreads();
+    const float* cb = reinterpret_cast<const float*>(boxes + 1);
+    for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+        const uint32_t k = morton_code(tri_boxes + 6 * static_cast<size_t>(i), cb);
+        keys[i] = k;
+        vals[i] = i;
+        sortdev::count_key(h, k, 0, kMortonPasses);
+    }
+    sortdev::finish_digit_counts(h, kMortonPasses, digits, ticket);
 }
 
 // Sorted leaf j -> node internal + j.
@@ -269,18 +284,24 @@ kr_error enqueue_codes(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, 
     const Layout L = layout(n);
     float* tri = reinterpret_cast<float*>(ws + L.tri);
     kr_aabb3* boxes = reinterpret_cast<kr_aabb3*>(ws + L.boxes);
-    const unsigned grid_n = (n + kThreads - 1) / kThreads;
+    // the sort's counts and status words are zeroed first; the codes kernel
+    // counts the digits as it writes the keys
+    OBVH_TRY(radix_sort_prepare(ws + L.sort, n, 0, 30, s));
     OBVH_TRY(enqueue_bounds(verts, faces, n, tri, ws, boxes, boxes + 1, true, s));
     {
-        ProfScope prof_scope_("morton_kernel", s);
-        morton_kernel<<<grid_n, kThreads, 0, s>>>(tri, n, boxes, reinterpret_cast<uint32_t*>(ws + L.keys0),
-                                                  reinterpret_cast<uint32_t*>(ws + L.vals0));
+        const sortdev::SortTemp st = sortdev::sort_temp(ws + L.sort);
+        const unsigned need = (n + kThreads - 1) / kThreads;
+        const unsigned cap = 4u * static_cast<unsigned>(device_info().sm_count);
+        ProfScope prof_scope_("morton_count_kernel", s);
+        morton_count_kernel<<<need < cap ? need : cap, kThreads, 0, s>>>(
+            tri, n, boxes, reinterpret_cast<uint32_t*>(ws + L.keys0), reinterpret_cast<uint32_t*>(ws + L.vals0),
+            st.digits, st.count_ticket);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     bool alt = false;
     OBVH_TRY(radix_sort_pairs(ws + L.keys0, ws + L.keys1, reinterpret_cast<uint32_t*>(ws + L.vals0),
                               reinterpret_cast<uint32_t*>(ws + L.vals1), n, 4, 0, 30, ws + L.sort, s, &alt,
-                              &reinterpret_cast<Ctl*>(ws + L.ctl)->error));
+                              &reinterpret_cast<Ctl*>(ws + L.ctl)->error, n >= 2));
     out->codes = reinterpret_cast<const uint32_t*>(ws + (alt ? L.keys1 : L.keys0));
     out->order = reinterpret_cast<const uint32_t*>(ws + (alt ? L.vals1 : L.vals0));
     out->tri_boxes = tri;

@@ -16,6 +16,7 @@
 
 #include "device_common.cuh"
 #include "runtime.h"
+#include "sort_device.cuh"
 
 namespace obvh {
 namespace {
@@ -26,33 +27,7 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
-__device__ __forceinline__ uint32_t block_exclusive_sum(uint32_t v, uint32_t* total) {
-    __shared__ uint32_t warp_sums[kScanThreads / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    if (lane == 31) warp_sums[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = lane < kScanThreads / 32 ? warp_sums[lane] : 0;
-        uint32_t wi = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += t;
-        }
-        if (lane < kScanThreads / 32) warp_sums[lane] = wi - w;
-        if (lane == kScanThreads / 32 - 1) *total = wi;
-    }
-    __syncthreads();
-    uint32_t r = warp_sums[warp] + incl - v;
-    __syncthreads();
-    return r;
-}
+using sortdev::block_exclusive_sum;
 
 __global__ void __launch_bounds__(kScanThreads) scan_tile_sums(const uint32_t* in, uint64_t n, uint32_t* sums) {
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanItems;
@@ -90,11 +65,15 @@ uint64_t div_up(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 
 // ---------------------------------------------------------------------------
 // Radix sort.
-constexpr int kSortThreads = 256;
+using sortdev::kMaxPasses;
+using sortdev::kRadix;
+using sortdev::kSortHeader;
+using sortdev::kSortThreads;
+using sortdev::SortTemp;
+using sortdev::sort_temp;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kRounds = 16;                       // keys per lane
 constexpr int kSortTile = kSortThreads * kRounds;  // 4096 keys per CTA
-constexpr int kRadix = 256;
 
 // ---------------------------------------------------------------------------
 // Stable LSD radix sort, one sweep per 8-bit digit (the single-pass scheme of
@@ -111,7 +90,6 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPre = 2u << 30;
 constexpr uint32_t kFlagMask = 3u << 30;
 constexpr uint32_t kCountMask = kFlagAgg - 1;
-constexpr int kMaxPasses = 8;
 
 __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* a) {
     uint32_t v;
@@ -122,31 +100,8 @@ __device__ __forceinline__ void st_relaxed(uint32_t* a, uint32_t v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(a), "r"(v) : "memory");
 }
 
-// Sort workspace: [0, 8 KB) digit counts then exclusive digit offsets per
-// pass, [8 KB, 8 KB + 256) tile counters, the error word and the counting
-// ticket, then the per-pass tile status words.
-struct SortTemp {
-    uint32_t* digits;   // [kMaxPasses][kRadix]
-    uint32_t* tiles;    // [kMaxPasses] tile counters, [kMaxPasses] error word
-    uint32_t* err;
-    uint32_t* count_ticket;  // [kMaxPasses + 1]: CTAs done counting
-    uint32_t* status;   // [passes][ntiles][kRadix]
-};
-constexpr size_t kSortHeader = kMaxPasses * kRadix * 4 + 256;
-
-__host__ __device__ inline SortTemp sort_temp(void* temp) {
-    SortTemp t;
-    char* c = static_cast<char*>(temp);
-    t.digits = reinterpret_cast<uint32_t*>(c);
-    t.tiles = reinterpret_cast<uint32_t*>(c + kMaxPasses * kRadix * 4);
-    t.err = t.tiles + kMaxPasses;
-    t.count_ticket = t.tiles + kMaxPasses + 1;
-    t.status = reinterpret_cast<uint32_t*>(c + kSortHeader);
-    return t;
-}
-
-// Every pass's digit counts over all keys; the last CTA to finish (a ticket
-// in the zeroed header) turns them into exclusive digit offsets in place.
+// Every pass's digit counts over all keys; the last CTA to finish turns them
+// into exclusive digit offsets (sortdev::finish_digit_counts).
 template <typename K>
 __global__ void __launch_bounds__(kSortThreads) radix_digit_counts(const K* keys, uint64_t n, int begin_bit,
                                                                    int passes, uint32_t* digits, uint32_t* ticket) {
@@ -154,27 +109,9 @@ __global__ void __launch_bounds__(kSortThreads) radix_digit_counts(const K* keys
     for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += kSortThreads) (&h[0][0])[i] = 0;
     __syncthreads();
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * kSortThreads;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * kSortThreads + threadIdx.x; i < n; i += stride) {
-        const K k = keys[i];
-        for (int p = 0; p < passes; ++p) atomicAdd(&h[p][static_cast<uint32_t>(k >> (begin_bit + 8 * p)) & (kRadix - 1)], 1u);
-    }
-    __syncthreads();
-    for (int p = 0; p < passes; ++p)
-        if (h[p][threadIdx.x]) atomicAdd(&digits[p * kRadix + threadIdx.x], h[p][threadIdx.x]);
-    __shared__ uint32_t last, total;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    for (int p = 0; p < passes; ++p) {
-        const uint32_t c = __ldcg(digits + p * kRadix + threadIdx.x);
-        const uint32_t e = block_exclusive_sum(c, &total);
-        __syncthreads();
-        digits[p * kRadix + threadIdx.x] = e;
-        __syncthreads();
-    }
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * kSortThreads + threadIdx.x; i < n; i += stride)
+        sortdev::count_key(h, keys[i], begin_bit, passes);
+    sortdev::finish_digit_counts(h, passes, digits, ticket);
 }
 
 template <typename K>
@@ -305,9 +242,15 @@ __global__ void __launch_bounds__(kSortThreads) radix_onesweep(const K* keys_in,
     }
 }
 
+size_t prepared_bytes(uint64_t n, int begin_bit, int end_bit) {
+    const uint32_t ntiles = static_cast<uint32_t>(div_up(n, kSortTile));
+    const int passes = (end_bit - begin_bit + 7) / 8;
+    return kSortHeader + static_cast<size_t>(passes) * ntiles * kRadix * 4;
+}
+
 template <typename K>
 kr_error sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt, uint64_t n, int begin_bit, int end_bit,
-                   void* temp, cudaStream_t stream, bool* in_alt, uint32_t* err) {
+                   void* temp, cudaStream_t stream, bool* in_alt, uint32_t* err, bool counted) {
     *in_alt = false;
     if (n <= 1 || end_bit <= begin_bit) return kr_success;
     const uint32_t ntiles = static_cast<uint32_t>(div_up(n, kSortTile));
@@ -320,16 +263,18 @@ kr_error sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt, uin
                                            static_cast<int>(sizeof(ScatterSmem<K>))));
         configured = true;
     }
-    // counts, tile counters, error word and this sort's status words start at zero
-    OBVH_TRY_CUDA(cudaMemsetAsync(temp, 0, kSortHeader + static_cast<size_t>(passes) * ntiles * kRadix * 4, stream));
-    {
+    // with counted, the key producer zeroed the header and the status words
+    // (radix_sort_prepare) and wrote the digit offsets
+    if (!counted) {
+        // counts, tile counters, error word and this sort's status words start at zero
+        OBVH_TRY_CUDA(cudaMemsetAsync(temp, 0, prepared_bytes(n, begin_bit, end_bit), stream));
         ProfScope prof_scope_("radix_digit_counts", stream);
         int grid = 2 * device_info().sm_count;
         const uint64_t need = div_up(n, kSortThreads);
         if (need < static_cast<uint64_t>(grid)) grid = static_cast<int>(need);
         radix_digit_counts<K><<<grid, kSortThreads, 0, stream>>>(keys, n, begin_bit, passes, t.digits, t.count_ticket);
+        OBVH_TRY_CUDA(cudaGetLastError());
     }
-    OBVH_TRY_CUDA(cudaGetLastError());
     K* src_k = keys;
     K* dst_k = keys_alt;
     uint32_t* src_v = vals;
@@ -400,15 +345,23 @@ size_t radix_sort_temp_bytes(uint64_t n) {
 uint32_t* radix_sort_error_word(void* temp) { return sort_temp(temp).err; }
 
 kr_error radix_sort_pairs(void* keys, void* keys_alt, uint32_t* vals, uint32_t* vals_alt, uint64_t n, int key_bytes,
-                          int begin_bit, int end_bit, void* temp, cudaStream_t stream, bool* in_alt, uint32_t* err) {
+                          int begin_bit, int end_bit, void* temp, cudaStream_t stream, bool* in_alt, uint32_t* err,
+                          bool counted) {
     if (n >= (1ull << 30)) return "radix_sort_pairs: at most 2^30 - 1 elements";
     if (key_bytes == 4)
         return sort_impl(static_cast<uint32_t*>(keys), static_cast<uint32_t*>(keys_alt), vals, vals_alt, n, begin_bit,
-                         end_bit, temp, stream, in_alt, err);
+                         end_bit, temp, stream, in_alt, err, counted);
     if (key_bytes == 8)
         return sort_impl(static_cast<uint64_t*>(keys), static_cast<uint64_t*>(keys_alt), vals, vals_alt, n, begin_bit,
-                         end_bit, temp, stream, in_alt, err);
+                         end_bit, temp, stream, in_alt, err, counted);
     return "radix_sort_pairs: key_bytes must be 4 or 8";
+}
+
+kr_error radix_sort_prepare(void* temp, uint64_t n, int begin_bit, int end_bit, cudaStream_t stream) {
+    if (n <= 1 || end_bit <= begin_bit) return kr_success;
+    if ((end_bit - begin_bit + 7) / 8 > kMaxPasses) return "radix_sort_prepare: at most 64 key bits";
+    OBVH_TRY_CUDA(cudaMemsetAsync(temp, 0, prepared_bytes(n, begin_bit, end_bit), stream));
+    return kr_success;
 }
 
 }  // namespace obvh

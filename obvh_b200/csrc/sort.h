@@ -26,9 +26,15 @@ size_t radix_sort_temp_bytes(uint64_t n);
 // ended in the *_alt buffers.
 // A bounded wait that times out sets kErrWaitTimeout in *err (a device word of
 // the caller's), or in the sort's own word inside `temp` when err is null.
+// With counted, the kernel that wrote the keys also counted their digits
+// (sort_device.cuh): radix_sort_prepare came before it, and only the passes
+// run here.
 kr_error radix_sort_pairs(void* keys, void* keys_alt, uint32_t* vals, uint32_t* vals_alt, uint64_t n, int key_bytes,
                           int begin_bit, int end_bit, void* temp, cudaStream_t stream, bool* in_alt,
-                          uint32_t* err = nullptr);
+                          uint32_t* err = nullptr, bool counted = false);
+// Zeroes the digit counts, the tickets and the status words of a sort of n
+// keys by bits [begin_bit, end_bit), for a key producer that counts digits.
+kr_error radix_sort_prepare(void* temp, uint64_t n, int begin_bit, int end_bit, cudaStream_t stream);
 uint32_t* radix_sort_error_word(void* temp);
 
 }  // namespace obvh
