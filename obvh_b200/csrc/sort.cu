@@ -125,8 +125,10 @@ struct ScatterSmem {
     uint32_t vals[kSortTile];
 };
 
+// 4 CTAs per SM for u32 keys (64 registers): every tile of 2M keys is
+// resident at once, so no tile waits for a slot; u64 keys keep 2.
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads) radix_onesweep(const K* keys_in, const uint32_t* vals_in, K* keys_out,
+__global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 2) radix_onesweep(const K* keys_in, const uint32_t* vals_in, K* keys_out,
                                                                uint32_t* vals_out, uint64_t n, int shift,
                                                                const uint32_t* offsets, uint32_t* status,
                                                                uint32_t* tile_counter, uint32_t* err) {
@@ -141,15 +143,15 @@ __global__ void __launch_bounds__(kSortThreads) radix_onesweep(const K* keys_in,
     const uint64_t base = static_cast<uint64_t>(tile) * kSortTile;
     const uint32_t lt = (1u << lane) - 1u;
     K k[kRounds];
-    uint32_t v[kRounds], pos[kRounds];
-    // every load in flight before the ranking (whose warp barriers would
-    // otherwise hold each round's load back until the round before is done)
+    uint32_t pos[kRounds];
+    // every key load in flight before the ranking (whose warp barriers would
+    // otherwise hold each round's load back until the round before is
+    // done); the values are read only when the tile is ordered, so that they
+    // hold no registers through the ranking
 #pragma unroll
     for (int r = 0; r < kRounds; ++r) {
         const uint64_t idx = base + warp * (kRounds * 32) + r * 32 + lane;
-        const bool ok = idx < n;
-        k[r] = ok ? keys_in[idx] : K(0);
-        v[r] = ok ? vals_in[idx] : 0u;
+        k[r] = idx < n ? keys_in[idx] : K(0);
     }
 #pragma unroll
     for (int r = 0; r < kRounds; ++r) {
@@ -189,7 +191,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_onesweep(const K* keys_in,
             const uint32_t dk = static_cast<uint32_t>(k[r] >> shift) & (kRadix - 1);
             const uint32_t p = sm.tstart[dk] + sm.wcount[warp][dk] + pos[r];
             sm.keys[p] = k[r];
-            sm.vals[p] = v[r];
+            sm.vals[p] = vals_in[idx];
         }
     }
     {
