@@ -448,11 +448,15 @@ __device__ __forceinline__ void candidate_node(uint32_t a, const uint4* summary,
     candidate_store(a, s, c, counts, cand, nunits, keys, chain);
 }
 
+// kList: the nodes of chain.list (FrameNodes::kAcross); else one thread per
+// node (kAll, kInside).  Two instantiations, so that each holds one inlined
+// copy of the search (fewer spills).
+template <bool kList>
 __global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* summary, const kr_vec3* verts,
                                                              const uint32_t* counts, uint32_t internal, Cand* cand,
                                                              uint32_t* nunits, uint32_t* keys, const uint32_t* err,
                                                              ChainArgs chain) {
-    if (chain.which == static_cast<uint32_t>(FrameNodes::kAcross)) {
+    if constexpr (kList) {
         // the listed nodes (written by the walk that completed them), a
         // grid-stride loop so that warps stay full
         const uint32_t total = min(*chain.list_count, internal);
@@ -469,22 +473,23 @@ __global__ void __launch_bounds__(kThreads, 2) candidate_kernel(const uint4* sum
             candidate_node(a, summary, verts, counts, cand, nunits, keys, chain);
         }
         return;
+    } else {
+        if (blockIdx.x < chain.walker_blocks) {
+            if (!*err) walk_chain(chain, counts, blockIdx.x * blockDim.x + threadIdx.x);
+            return;
+        }
+        const uint32_t a = (blockIdx.x - chain.walker_blocks) * blockDim.x + threadIdx.x;
+        if (a >= internal) return;
+        if (chain.which == static_cast<uint32_t>(FrameNodes::kInside)) {
+            const uint32_t f = __ldg(chain.first + a), cnt = __ldg(counts + a);
+            if ((f >> chain.block_shift) != ((f + cnt - 1) >> chain.block_shift)) return;
+        }
+        if (*err) {  // malformed tree: no summaries to read; nothing is scheduled after this
+            nunits[a] = 0;
+            return;
+        }
+        candidate_node(a, summary, verts, counts, cand, nunits, keys, chain);
     }
-    if (blockIdx.x < chain.walker_blocks) {
-        if (!*err) walk_chain(chain, counts, blockIdx.x * blockDim.x + threadIdx.x);
-        return;
-    }
-    const uint32_t a = (blockIdx.x - chain.walker_blocks) * blockDim.x + threadIdx.x;
-    if (a >= internal) return;
-    if (chain.which == static_cast<uint32_t>(FrameNodes::kInside)) {
-        const uint32_t f = __ldg(chain.first + a), cnt = __ldg(counts + a);
-        if ((f >> chain.block_shift) != ((f + cnt - 1) >> chain.block_shift)) return;
-    }
-    if (*err) {  // malformed tree: no summaries to read; nothing is scheduled after this
-        nunits[a] = 0;
-        return;
-    }
-    candidate_node(a, summary, verts, counts, cand, nunits, keys, chain);
 }
 
 // Nodes of at most kThreadMax leaves: one thread each, finalised here.
@@ -839,9 +844,12 @@ kr_error enqueue_candidates(const FrameBuffers& b, uint32_t internal, FrameNodes
                                                      : (internal + kThreads - 1) / kThreads;
     // the chain walks go first, so that they overlap the candidate search
     ProfScope prof_scope_("candidate_kernel", s);
-    candidate_kernel<<<gi + chain.walker_blocks, kThreads, 0, s>>>(b.summary, b.points, b.counts, internal,
-                                                                        static_cast<Cand*>(b.cand), b.nunits, b.keys,
-                                                                        b.err, chain);
+    if (which == FrameNodes::kAcross)
+        candidate_kernel<true><<<gi + chain.walker_blocks, kThreads, 0, s>>>(
+            b.summary, b.points, b.counts, internal, static_cast<Cand*>(b.cand), b.nunits, b.keys, b.err, chain);
+    else
+        candidate_kernel<false><<<gi + chain.walker_blocks, kThreads, 0, s>>>(
+            b.summary, b.points, b.counts, internal, static_cast<Cand*>(b.cand), b.nunits, b.keys, b.err, chain);
     OBVH_TRY_CUDA(cudaGetLastError());
     return kr_success;
 }
