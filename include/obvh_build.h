@@ -51,7 +51,8 @@ OBVH_EXPORT kr_error obvh_build_status(const void* d_workspace, kr_u32 face_coun
  * and the fork/join of its helper streams become one graph whose branches
  * keep their stream priorities.  Arguments are obvh_build_async's (every
  * pointer is baked into the graph: a replay reads whatever the input buffers
- * hold at that time and overwrites the same outputs).  Results equal
+ * hold at that time and overwrites the same outputs, so every buffer,
+ * workspace included, must stay allocated until the graph is destroyed).  Results equal
  * obvh_build_async's bit for bit.  The capture runs on the current device and
  * enqueues nothing; the workspace must have been initialised
  * (obvh_build_workspace_init).  Replays of one graph must not overlap one

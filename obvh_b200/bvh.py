@@ -247,17 +247,20 @@ class ObvhBuilder:
             _ptr(mesh.verts), _ptr(mesh.faces), n, flags, ci, ct, _ptr(out["nodes"]), _ptr(out["parents"]),
             _ptr(out["counts"]), _ptr(out["costs"]), _ptr(out["bounds"]), _ptr(out["obbs"]), _ptr(out["transforms"]),
             _ptr(out["collapsed"]), _ptr(out["primitives"]), _ptr(ws), ctypes.byref(h)))
-        return BuildGraph(self, h)
+        return BuildGraph(self, h, (ws, mesh, out))
 
 
 class BuildGraph:
-    """A captured obvh_build_async chain (obvh_build_graph_*); holds its
-    builder so that the workspace outlives the graph."""
+    """A captured obvh_build_async chain (obvh_build_graph_*).  It holds the
+    workspace, mesh and output tensors whose addresses the graph baked in, so
+    that none of them is freed while the graph exists (the builder may move
+    on to a larger workspace)."""
 
-    def __init__(self, builder: ObvhBuilder, handle):
+    def __init__(self, builder: ObvhBuilder, handle, buffers):
         self.builder = builder
         self.lib = builder.lib
         self.handle = handle
+        self.buffers = buffers
 
     def launch(self, stream=None):
         _native.check(self.lib.obvh_build_graph_launch(self.handle, _stream(self.builder.torch, stream)))
@@ -321,7 +324,7 @@ class AtrbvhBuilder(ObvhBuilder):
             _ptr(mesh.verts), _ptr(mesh.faces), n, flags, treelet_size, iterations, ci, ct, _ptr(out["nodes"]),
             _ptr(out["parents"]), _ptr(out["counts"]), _ptr(out["costs"]), _ptr(out["bounds"]), _ptr(out["obbs"]),
             _ptr(out["transforms"]), _ptr(out["collapsed"]), _ptr(out["primitives"]), _ptr(ws), ctypes.byref(h)))
-        return BuildGraph(self, h)
+        return BuildGraph(self, h, (ws, mesh, out))
 
 
 # ---- traversal packing (include/obvh_transforms.h) -------------------------

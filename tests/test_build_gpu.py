@@ -141,3 +141,23 @@ def test_build_graph_equals_the_direct_build_at_full_size(builder):
     for k in direct:
         assert torch.equal(direct[k].view(torch.uint8), out[k].view(torch.uint8)), k
 
+
+
+def test_build_graph_keeps_its_buffers_when_the_builder_grows():
+    """A graph captured on a small workspace still replays correctly after the
+    builder moved to a larger one (the graph holds the buffers it baked in)."""
+    import torch
+    b = bvh.ObvhBuilder()
+    n = 5_000
+    v, f = workloads.triangle_soup(n, seed=81)
+    mesh = bvh.Mesh(v, f)
+    out = b.outputs(n)
+    g = b.capture(mesh, out)
+    b.build(bvh.Mesh(*workloads.triangle_soup(3 * n, seed=82)))  # reallocates the builder's workspace
+    torch.cuda.synchronize()
+    g.launch()
+    torch.cuda.synchronize()
+    direct = bvh.ObvhBuilder().build(mesh)
+    torch.cuda.synchronize()
+    for k in ("nodes", "parents", "counts", "costs", "bounds", "obbs", "transforms", "collapsed", "primitives"):
+        assert torch.equal(direct[k].view(torch.uint8), out[k].view(torch.uint8)), k
