@@ -1648,8 +1648,13 @@ def bench_serve_ours(a, dist):
         return st, wall
 
     run(None)  # warm-up (plans, arena)
+    # saturated: three runs without per-launch events (the serial comparator
+    # has none either), the median reported; the kernel list comes from a
+    # fourth run with an event pair around every launch
+    sats = sorted((run(None)[0] for _ in range(3)), key=lambda st: st["span_s"])
+    sat = sats[1]
     profile_enable(True)
-    sat, sat_wall = run(None)
+    prof_st, _ = run(None)
     prof = profile_summary()
     profile_enable(False)
     served_rps = len(reqs) / sat["span_s"]
@@ -1679,7 +1684,9 @@ def bench_serve_ours(a, dist):
                    "points": pts, "build_nodes": nodes, "hbm_budget_bytes": budget, "build_lanes": 4,
                    "inputs": "device-resident", "l2": "GBs of inputs per run (> 126 MB L2)",
                    "parallelism": f"replicas{dist.world}"},
-        "served": {"p50_ms": round(sat["p50_ms"], 3), "p99_ms": round(sat["p99_ms"], 3),
+        "served": {"runs_rps": [round(len(reqs) / st["span_s"], 3) for st in sats], "reported": "median of 3",
+                   "profiled_run_rps": round(len(reqs) / prof_st["span_s"], 3),
+                   "p50_ms": round(sat["p50_ms"], 3), "p99_ms": round(sat["p99_ms"], 3),
                    "fit_batches": sat["fit_batches"], "peak_arena_bytes": sat["peak_bytes"],
                    "mpoints_per_s": round(pts / sat["span_s"] / 1e6, 2),
                    "mnodes_per_s": round(nodes / sat["span_s"] / 1e6, 2)},
@@ -1692,6 +1699,7 @@ def bench_serve_ours(a, dist):
         "poisson_sweep": sweep,
         "kernels": {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in prof.items()},
         "gpu_launches": sum(v[0] for v in prof.values()),
+        "gpu_launches_note": "counted in the profiled run; each timed run launches the same kernels",
         "roofline": None,
         "e2e": {"value": round(len(reqs) / e2e["span_s"], 3), "unit": "requests/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": 60 * n_fit, "api": "obvh_server_submit_fit / _build from pinned host memory",
