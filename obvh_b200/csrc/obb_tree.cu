@@ -25,7 +25,6 @@
 //                per 1,024 consecutive leaves stages their triangles in shared
 //                memory once and serves every node over them from there.
 //   finalize     the nodes of more than one unit or tile.
-#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -364,8 +363,7 @@ struct ChainArgs {
     uint32_t* chains;
     uint32_t* chain_counts;
     uint32_t* err;
-    uint32_t* final_list;     // tiles: the nodes finalize_list_kernel finishes
-    uint32_t* final_count;
+    uint32_t* arrivals;       // tiles: per node over several tiles, the tiles done with it
     float nz;                 // -0.0f (tree::mul2)
     uint32_t which;           // FrameNodes: all nodes, or those inside / across aligned leaf blocks
     uint32_t block_shift;     // the blocks hold 2^block_shift leaves
@@ -430,14 +428,7 @@ __device__ __forceinline__ void candidate_store(uint32_t a, const Summary& s, co
         k[0] = f2key(c.lo.x); k[1] = f2key(c.lo.y); k[2] = f2key(c.lo.z);
         k[3] = f2key(c.hi.x); k[4] = f2key(c.hi.y); k[5] = f2key(c.hi.z);
     }
-    if (chain.parents && units != 0) {  // listed for finalize_list_kernel, one atomic per warp
-        namespace cg = cooperative_groups;
-        const cg::coalesced_group g = cg::coalesced_threads();
-        uint32_t base = 0;
-        if (g.thread_rank() == 0) base = atomicAdd(chain.final_count, g.size());
-        base = g.shfl(base, 0);
-        chain.final_list[base + g.thread_rank()] = a;
-    }
+    if (chain.parents && units == 2) chain.arrivals[a] = 0u;  // counted up by extents_tile_kernel
 }
 
 __device__ __forceinline__ void candidate_node(uint32_t a, const uint4* summary, const kr_vec3* verts,
@@ -577,11 +568,27 @@ __global__ void __launch_bounds__(kThreads) extents_units_kernel(const Cand* can
 // the tile, combined in the keys with integer atomics.  Warps take items from
 // a shared counter; an item beyond the list's capacity is done by the thread
 // that found it.
+// A node over several tiles finishes in the last of them: each tile's part
+// folds its extents into the node's keys (atomics), fences them, and counts
+// itself in arrivals[a]; the part that completes the count reads the keys and
+// writes the box.
+__device__ __forceinline__ void part_done(const Cand* cand, const uint32_t* counts, const uint32_t* first,
+                                          const uint32_t* keys, uint32_t* arrivals, uint32_t a, kr_obb3* obbs,
+                                          kr_mat4* xfs) {
+    const uint32_t f = __ldg(first + a), cnt = __ldg(counts + a);
+    const uint32_t parts = ((f + cnt - 1) >> kTileShift) - (f >> kTileShift) + 1;
+    if (atomicAdd(arrivals + a, 1u) + 1u != parts) return;
+    __threadfence();
+    const uint32_t* k = keys + 6 * static_cast<size_t>(a);
+    finalize_node(load_cand(cand, a), mk3(key2f(__ldcg(k)), key2f(__ldcg(k + 1)), key2f(__ldcg(k + 2))),
+                  mk3(key2f(__ldcg(k + 3)), key2f(__ldcg(k + 4)), key2f(__ldcg(k + 5))), obbs + a, xfs + a);
+}
+
 __global__ void __launch_bounds__(kThreads) extents_tile_kernel(const Cand* cand, const uint32_t* counts,
                                                                 const uint32_t* first, const float* tris, uint32_t n,
                                                                 const uint32_t* chains, const uint32_t* chain_counts,
-                                                                uint32_t* keys, kr_obb3* obbs, kr_mat4* xfs,
-                                                                const uint32_t* err, float nz) {
+                                                                uint32_t* keys, uint32_t* arrivals, kr_obb3* obbs,
+                                                                kr_mat4* xfs, const uint32_t* err, float nz) {
     __shared__ __align__(16) float tri[kTile * 9];
     __shared__ uint32_t item_node[kTileItems];
     __shared__ uint16_t item_b[kTileItems], item_e[kTileItems];
@@ -618,15 +625,18 @@ __global__ void __launch_bounds__(kThreads) extents_tile_kernel(const Cand* cand
                                   mk3(c.ax[6], c.ax[7], c.ax[8]), nz);
         float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
         for (uint32_t i = b; i < e; ++i) project_tri_s(tri + 9 * i, ax, lo, hi);
-        for (int k = 0; k < 3; ++k) {
+        if (partial) {
             uint32_t* kk = keys + 6 * static_cast<size_t>(a);
-            if (partial) {
+            for (int k = 0; k < 3; ++k) {
                 atomicMin(kk + k, f2key(lo[k]));
                 atomicMax(kk + 3 + k, f2key(hi[k]));
-            } else {
-                __stcg(kk + k, f2key(fminf(c.olo[k], lo[k])));
-                __stcg(kk + 3 + k, f2key(fmaxf(c.ohi[k], hi[k])));
             }
+            __threadfence();
+            part_done(cand, counts, first, keys, arrivals, a, obbs, xfs);
+        } else {
+            finalize_node(c, mk3(fminf(c.olo[0], lo[0]), fminf(c.olo[1], lo[1]), fminf(c.olo[2], lo[2])),
+                          mk3(fmaxf(c.ohi[0], hi[0]), fmaxf(c.ohi[1], hi[1]), fmaxf(c.ohi[2], hi[2])), obbs + a,
+                          xfs + a);
         }
     };
     // nodes inside the tile: their indices lie in the tile too
@@ -677,31 +687,22 @@ __global__ void __launch_bounds__(kThreads) extents_tile_kernel(const Cand* cand
             lo[k] = warp_min(lo[k]);
             hi[k] = warp_max(hi[k]);
         }
-        if (lane < 6) {
-            uint32_t* kk = keys + 6 * static_cast<size_t>(a) + lane;
-            if (partial) {
+        if (partial) {
+            if (lane < 6) {
+                uint32_t* kk = keys + 6 * static_cast<size_t>(a) + lane;
                 if (lane < 3) atomicMin(kk, f2key(lo[lane])); else atomicMax(kk, f2key(hi[lane - 3]));
-            } else {
-                const float v = lane < 3 ? fminf(c.olo[lane], lo[lane]) : fmaxf(c.ohi[lane - 3], hi[lane - 3]);
-                __stcg(kk, f2key(v));
+                __threadfence();
             }
+            __syncwarp();
+            if (lane == 0) part_done(cand, counts, first, keys, arrivals, a, obbs, xfs);
+        } else if (lane == 0) {
+            // inside this tile: the box from the warp's extents (and the
+            // summary extremes the candidate holds), no keys
+            finalize_node(c, mk3(fminf(c.olo[0], lo[0]), fminf(c.olo[1], lo[1]), fminf(c.olo[2], lo[2])),
+                          mk3(fmaxf(c.ohi[0], hi[0]), fmaxf(c.ohi[1], hi[1]), fmaxf(c.ohi[2], hi[2])), obbs + a,
+                          xfs + a);
         }
-    }
-}
-
-// The listed nodes (those finished through the keys), one thread each.
-__global__ void __launch_bounds__(kThreads) finalize_list_kernel(const Cand* cand, const uint32_t* list,
-                                                                 const uint32_t* count, const uint32_t* keys,
-                                                                 uint32_t internal, kr_obb3* obbs, kr_mat4* xfs,
-                                                                 const uint32_t* err) {
-    if (*err) return;
-    const uint32_t total = min(*count, internal);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        const uint32_t a = list[i];
-        if (a >= internal) continue;
-        const uint32_t* k = keys + 6 * static_cast<size_t>(a);
-        finalize_node(load_cand(cand, a), mk3(key2f(k[0]), key2f(k[1]), key2f(k[2])),
-                      mk3(key2f(k[3]), key2f(k[4]), key2f(k[5])), obbs + a, xfs + a);
+        __syncwarp();
     }
 }
 
@@ -824,7 +825,7 @@ ChainArgs chain_args(const FrameBuffers& b, uint32_t internal, FrameNodes which,
     const bool walks = tiled && which != FrameNodes::kAcross;
     return ChainArgs{tiled ? b.parents : nullptr, b.first, n,
                      walks ? (2 * ntiles + kThreads - 1) / kThreads : 0u,
-                     b.chains, b.chain_counts, b.err, b.ustart, b.total_units, -0.0f,
+                     b.chains, b.chain_counts, b.err, b.ustart, -0.0f,
                      static_cast<uint32_t>(which), block_shift, b.across_list, b.across_count};
 }
 }  // namespace
@@ -870,15 +871,8 @@ kr_error enqueue_extents(const FrameBuffers& b, uint32_t internal, kr_obb3* obbs
         {
             ProfScope prof_scope_("extents_tile_kernel", s);
             extents_tile_kernel<<<ntiles, kThreads, 0, s>>>(cand, b.counts, b.first, b.tris, n, b.chains,
-                                                            b.chain_counts, b.keys, obbs, xfs, b.err, -0.0f);
-        }
-        OBVH_TRY_CUDA(cudaGetLastError());
-        {
-            // the list is a few percent of the nodes; its length is on the device
-            const unsigned cap = 2u * static_cast<unsigned>(device_info().sm_count);
-            ProfScope prof_scope_("finalize_list_kernel", s);
-            finalize_list_kernel<<<gi < cap ? gi : cap, kThreads, 0, s>>>(cand, b.ustart, b.total_units, b.keys,
-                                                                           internal, obbs, xfs, b.err);
+                                                            b.chain_counts, b.keys, b.ustart, obbs, xfs, b.err,
+                                                            -0.0f);
         }
         OBVH_TRY_CUDA(cudaGetLastError());
         return kr_success;
