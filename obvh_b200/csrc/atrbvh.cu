@@ -332,6 +332,13 @@ __device__ __forceinline__ int trm_col(int index) {
     return index - (y * (y - 1)) / 2;
 }
 
+// (row, col) of every index of the distance matrices of treelets of up to
+// kMaxTau leaves, row << 8 | col, tabulated once per CTA with the functions
+// above (a shared-memory load instead of a square root per lookup)
+constexpr int kTrmEntries = (kMaxTau - 1) * kMaxTau / 2;
+__device__ __forceinline__ int lut_row(const uint16_t* lut, int index) { return lut[index] >> 8; }
+__device__ __forceinline__ int lut_col(const uint16_t* lut, int index) { return lut[index] & 0xff; }
+
 template <int W>
 __device__ __forceinline__ void shfl_box(const float* lo, const float* hi, int src, float* olo, float* ohi) {
 #pragma unroll
@@ -347,7 +354,7 @@ __device__ __forceinline__ void shfl_box(const float* lo, const float* hi, int s
 // segment) on a malformed tree.
 template <int W>
 __device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, float ci, int32_t root, bool active,
-                                SegSmem<W>& w) {
+                                SegSmem<W>& w, const uint16_t* lut) {
     const int sl = seg_lane<W>();
     const int32_t internal_count = n - 1;
     const int32_t node_count = 2 * n - 1;
@@ -409,7 +416,7 @@ __device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, fl
     const int nd = (tau - 1) * tau / 2;
     for (int k0 = 0; k0 < nd; k0 += W) {  // every pair row > col
         const int k = k0 + sl;
-        const int r = k < nd ? trm_row(k) : 0, c = k < nd ? trm_col(k) : 0;
+        const int r = k < nd ? lut_row(lut, k) : 0, c = k < nd ? lut_col(lut, k) : 0;
         float rlo[3], rhi[3], clo[3], chi[3];
         shfl_box<W>(lo, hi, r, rlo, rhi);
         shfl_box<W>(lo, hi, c, clo, chi);
@@ -419,7 +426,7 @@ __device__ bool process_treelet(TNode* t, float* sah_arr, int32_t n, int tau, fl
 
     for (int last = tau - 1; last > 0; --last) {
         const int mi = min_distance_seg<W>(w.dist, last * (1 + last) / 2);
-        const int jr = trm_row(mi), jc = trm_col(mi);
+        const int jr = lut_row(lut, mi), jc = lut_col(lut, mi);
 
         // updateState (AgglomerativeTreelet.cu:92-147)
         const float s = __shfl_sync(0xffffffffu, sah, jr, W) + __shfl_sync(0xffffffffu, sah, jc, W);
@@ -506,6 +513,10 @@ __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, floa
                                                                   int32_t gamma, float ci, float ct, uint32_t* err) {
     constexpr int S = 32 / W;  // segments (treelets in flight) per warp
     __shared__ SegSmem<W> smem[kTreeletWarps * S];
+    __shared__ uint16_t lut[kTrmEntries];
+    for (int k = threadIdx.x; k < kTrmEntries; k += kTreeletThreads)
+        lut[k] = static_cast<uint16_t>((trm_row(k) << 8) | trm_col(k));
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int seg = lane / W;
     SegSmem<W>& w = smem[(threadIdx.x >> 5) * S + seg];
@@ -571,7 +582,7 @@ __global__ void __launch_bounds__(kTreeletThreads) treelet_kernel(TNode* t, floa
                 vote = vote ? (vote & (vote - 1)) : 0u;
             }
             const int32_t root = __shfl_sync(0xffffffffu, cur, src < 0 ? 0 : src);
-            if (!process_treelet<W>(t, sah_arr, n, tau, ci, root, src >= 0, w) && (lane & (W - 1)) == 0)
+            if (!process_treelet<W>(t, sah_arr, n, tau, ci, root, src >= 0, w, lut) && (lane & (W - 1)) == 0)
                 atomicOr(err, kErrBadInput);
         }
         if (cur >= 0) cur = up;
