@@ -76,7 +76,8 @@ __device__ __forceinline__ uint32_t* stage_at(uint32_t* stage, const void* dst, 
 __global__ void __launch_bounds__(kThreads) leaves_fused_kernel(const uint32_t* order,
                                                                 const kr_vec3* verts, const uint4* faces, uint32_t n,
                                                                 kr_bvh_node* nodes, kr_bvh_node* collapsed,
-                                                                float* tris, kr_obb3* obbs, kr_mat4* xfs) {
+                                                                float* tris, kr_obb3* obbs, kr_mat4* xfs,
+                                                                uint32_t* visits, uint8_t* cflags) {
     __shared__ __align__(16) uint32_t stage_a[kThreads * 15 + 4];  // node (9), triangle (9) or box (15) records
     __shared__ __align__(16) uint32_t stage_x[kThreads * 16 + 4];  // transforms
     const uint32_t j0 = blockIdx.x * blockDim.x;
@@ -84,6 +85,13 @@ __global__ void __launch_bounds__(kThreads) leaves_fused_kernel(const uint32_t* 
     const uint32_t count = min(static_cast<uint32_t>(blockDim.x), n - j0);
     const bool live = j < n;
     const uint32_t internal = n - 1;
+    // the bottom-up pass's arrival counters (internal entries) and collapse
+    // marks (2n - 1 bytes) start at zero; nothing reads them before it
+    if (j < internal) visits[j] = 0u;
+    if (cflags) {
+        if (2 * j < 2 * n - 1) cflags[2 * j] = 0;
+        if (2 * j + 1 < 2 * n - 1) cflags[2 * j + 1] = 0;
+    }
     uint32_t w[9];
     f3 v0 = mk3(0, 0, 0), v1 = v0, v2 = v0;
     if (live) {
@@ -618,12 +626,11 @@ kr_error enqueue(const kr_vec3* verts, const kr_uvec4* faces, uint32_t n, uint32
         ProfScope prof_scope_("leaves_fused_kernel", s);
         leaves_fused_kernel<<<gn, kThreads, 0, s>>>(c.order, verts, reinterpret_cast<const uint4*>(faces),
                                                     n, nodes, want_collapse ? collapsed : nullptr, tris,
-                                                    want_obbs ? obbs : nullptr, xfs);
+                                                    want_obbs ? obbs : nullptr, xfs, c.visits,
+                                                    want_collapse ? cflags : nullptr);
     }
     OBVH_TRY_CUDA(cudaGetLastError());
     OBVH_TRY(lbvh::enqueue_karras(c.codes, n, nodes, parents, first, counts, s));
-    if (internal > 0) OBVH_TRY_CUDA(cudaMemsetAsync(c.visits, 0, 4ull * internal, s));
-    if (want_collapse) OBVH_TRY_CUDA(cudaMemsetAsync(cflags, 0, nn, s));
     OBVH_TRY(allow_dynamic_smem(reinterpret_cast<const void*>(fused_up_local_kernel), kFusedSmemBytes));
     // Two helper streams.  aux[0] (the highest priority, so that its CTAs
     // are placed first) takes the latency-bound walk up the top of the tree
